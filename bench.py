@@ -1,0 +1,333 @@
+"""Benchmark: input edges sparsified per second on one B200 (or N replicas under torchrun).
+
+Workload (default): Erdos-Renyi G(n, p), n = 1,000,000, average degree 20 (m ~ 10M undirected edges),
+weights uniform [0.5, 2] rounded to FP32, eps = 0.5, k = ceil(24 ln n / eps^2) = 1327 JL columns of
++-1/sqrt(k) Philox signs, PCG relative tolerance 1e-8 -- a single graph through the FP64 path.
+A step is one full sparsification: device-resident input CSC -> device-resident L_H.
+
+  python bench.py [--gpus N --steps K --warmup W]          # our GPU path
+  python bench.py --impl reference [...]                    # the reference CPU path on the host cores
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (generator, kwargs, eps)
+    "er_n1M_deg20": ("er", dict(n=1_000_000, avg_degree=20.0, wlo=0.5, whi=2.0, seed=1), 0.5),
+    "grid2d_100": ("grid2d", dict(nx=100, ny=100), 0.5),
+    "er_n100k_deg20": ("er", dict(n=100_000, avg_degree=20.0, wlo=0.5, whi=2.0, seed=1), 0.5),
+}
+PCG_TOL = 1e-8
+
+
+def make_graph(S, name, rank=0):
+    kind, kw, eps = WORKLOADS[name]
+    kw = dict(kw)
+    if kind == "er":
+        kw["seed"] = kw["seed"] + rank
+        return S.gen_er(kw["n"], kw["avg_degree"], kw["wlo"], kw["whi"], kw["seed"]), eps
+    return S.gen_grid2d(kw["nx"], kw["ny"]), eps
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            try:
+                p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            except OSError:
+                return
+            while not self._stop.is_set():
+                line = p.stdout.readline()
+                if not line:
+                    break
+                self.samples.append([x.strip() for x in line.split(",")])
+            p.terminate()
+            try:
+                p.wait(timeout=5)
+            except Exception:
+                p.kill()
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        sm = []
+        mx = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[1]))
+                mx = float(s[2])
+                for nm, val in zip(names, s[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def spmm_bytes(n, nnz_lap, k):
+    # compulsory traffic of q = A p over k columns: row pointers, (index, value) per nonzero, read p, write q
+    return 8 * (n + 1) + nnz_lap * (4 + 8) + 2 * n * k * 8
+
+
+def precond_bytes(n, nnz_l, k):
+    # forward + backward triangular solves (each: pointers, L entries, read + write n x k) and D
+    return 2 * (8 * (n + 1) + nnz_l * (4 + 8) + 2 * n * k * 8) + 8 * n
+
+
+def cpu_baseline(eps, k_full, impl="port", budget_cols=16):
+    """The CPU path timed on a bounded sample: ER n=50K (avg degree 20) with the full pipeline on
+    `budget_cols` of the k_full RHS columns; per-column costs extrapolated to k_full."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import spec_spars_b200 as S
+    import pyoracle as ora
+    G = S.gen_er(50_000, 20.0, 0.5, 2.0, 11)
+    n = G.n
+    t0 = time.perf_counter()
+    v1, v2, w = ora.extract_edges(n, G.colptr, G.rowidx, G.values)
+    cp, ri, va = ora.laplacian(n, v1, v2, w)
+    t_graph = time.perf_counter() - t0
+    kc = budget_cols
+    scale = 1.0 / math.sqrt(k_full)
+    t0 = time.perf_counter()
+    Y = ora.sketch(n, v1, v2, w, kc, scale, 0)
+    t_sketch = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    if impl == "reference":
+        import refsolver
+        Z, info = refsolver.solve(n, cp, ri, va, Y, threads=os.cpu_count())
+        t_fact = info["factor_s"]
+        t_solve = time.perf_counter() - t0 - t_fact
+    else:
+        F = ora.Factor(n, cp, ri, va, 0, 4096)
+        t_fact = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        Z, it, rel, rc = ora.pcg(n, cp, ri, va, F, Y, PCG_TOL, 0.0, 400)
+        t_solve = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    d = ora.diff_norms(v1, v2, Z)
+    p = ora.probs(w, d, math.pow(eps, -2) * 4 * math.log(n), 1.0)
+    coins = ora.coins(0, len(w))
+    ora.sample_apply(n, v1, v2, w, p, coins, 0, (cp, ri, va))
+    t_rest = time.perf_counter() - t0
+    per_col = (t_sketch + t_solve + t_rest) / kc
+    total = t_graph + t_fact + per_col * k_full
+    cores = os.cpu_count() if impl == "reference" else 1
+    return {"value": len(w) / total, "unit": "edges/s", "cores": cores,
+            "kind": "reference" if impl == "reference" else "port",
+            "sample": f"ER n={n} avg deg 20 (m={len(w)}), full pipeline on {kc} of k={k_full} RHS columns, "
+                      f"per-column time extrapolated to k; measured {t_graph + t_fact + (t_sketch + t_solve + t_rest):.1f}s"}
+
+
+def run_reference(args):
+    """--impl reference: the reference CPU implementation of the path on this host's cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    _, kw, eps = WORKLOADS[args.workload]
+    n = kw.get("n", 10_000)
+    k = math.ceil(24 * math.log(n) / eps ** 2)
+    impl = "reference" if _ref_available() else "port"
+    vals = []
+    for _ in range(max(args.warmup, 0)):
+        pass  # the CPU path has no warm-up state worth timing; samples are independent
+    for _ in range(args.steps):
+        cb = cpu_baseline(eps, k, impl=impl, budget_cols=4)
+        vals.append(cb["value"])
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": "input edges sparsified/sec", "value": v, "unit": "edges/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "eps": eps, "k": k, "pcg_tol": PCG_TOL},
+            "cpu_baseline": {**cb, "value": v},
+            "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _ref_available():
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import refsolver
+        return refsolver.available()
+    except Exception:
+        return False
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="er_n1M_deg20", choices=list(WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import spec_spars_b200 as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    G, eps = make_graph(S, args.workload, rank)
+    prm = S.SparsifierParameters.baseline(eps, pcg_tol=PCG_TOL)
+    ctx = S.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    dev = torch.device("cuda", local)
+    cp = torch.from_numpy(G.colptr).to(dev)
+    ri = torch.from_numpy(G.rowidx).to(dev)
+    va = torch.from_numpy(G.values).to(dev)
+    torch.cuda.synchronize()
+
+    def step():
+        return ctx.sparsify_device(G.n, G.nnz, cp.data_ptr(), ri.data_ptr(), va.data_ptr(), prm)
+
+    for _ in range(args.warmup):
+        _, st = step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    k0 = ctx.kernels_launched
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t_start.record(stream)
+    stats = []
+    for _ in range(args.steps):
+        _, st = step()
+        stats.append(st)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks.stop()
+    launches = ctx.kernels_launched - k0
+    ms = t_start.elapsed_time(t_end) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    m = stats[-1]["m_in"]
+    value = m * world / (ms / 1000.0)
+
+    # end to end through the public API with host buffers (H2D of the input, D2H of L_H, every step)
+    e2e = None
+    if args.e2e_steps > 0:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        h2d = G.colptr.nbytes + G.rowidx.nbytes + G.values.nbytes
+        d2h = 0
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            H, st2 = ctx.sparsify(G, prm)
+            d2h = H.colptr.nbytes + H.rowidx.nbytes + H.values.nbytes
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1) / args.e2e_steps
+        if world > 1:
+            t = torch.tensor([ems], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": m * world / (ems / 1000.0), "unit": "edges/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": ems}
+
+    st = stats[-1]
+    n, k = st["n"], st["k"]
+    peak, src = peaks()
+    sp_ms = sum(s["ms_spmm"] for s in stats) / max(1, sum(s["n_spmm"] for s in stats))
+    pc_ms = sum(s["ms_precond"] for s in stats) / max(1, sum(s["n_precond"] for s in stats))
+    sp_tot = sum(s["ms_spmm"] for s in stats)
+    pc_tot = sum(s["ms_precond"] for s in stats)
+    if pc_tot >= sp_tot:
+        kern, byts, kms = "precond (fwd+bwd level-set triangular solves, all k columns)", \
+            precond_bytes(n, st["nnz_factor"], k), pc_ms
+    else:
+        kern, byts, kms = "spmm (Laplacian x n-by-k block)", spmm_bytes(n, st["nnz_laplacian"], k), sp_ms
+    achieved = byts / (kms / 1000.0) / 1e9 if kms > 0 else None
+    roof = {"kernel": kern, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if achieved else None, "traffic": None, "peak_source": src,
+            "algorithmic_bytes_per_launch": byts, "avg_launch_ms": kms,
+            "spmm_avg_ms": sp_ms, "precond_avg_ms": pc_ms,
+            "spmm_GBps": spmm_bytes(n, st["nnz_laplacian"], k) / (sp_ms / 1000.0) / 1e9 if sp_ms > 0 else None,
+            "precond_GBps": precond_bytes(n, st["nnz_factor"], k) / (pc_ms / 1000.0) / 1e9 if pc_ms > 0 else None}
+    line = {"metric": "input edges sparsified/sec", "value": value, "unit": "edges/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "n": n, "m": m, "eps": eps, "k": k, "pcg_tol": PCG_TOL,
+                       "l2": "inputs and n-by-k working set larger than L2; no flush",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "gpu_launches": launches,
+            "stages_ms": {x: st[x] for x in ("ms_assembly", "ms_sketch", "ms_factor", "ms_solve", "ms_leverage",
+                                             "ms_sample", "ms_total")},
+            "kept_fraction": st["m_out"] / st["m_in"], "pcg_iters_max": st["pcg_max_iters_used"],
+            "pcg_iters_mean": st["pcg_mean_iters"], "pcg_max_relres": st["pcg_max_relres"],
+            "factor_nnz": st["nnz_factor"], "factor_levels": st["factor_levels"],
+            "roofline": roof, "clocks": clocks.summary(), "e2e": e2e}
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(eps, k)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

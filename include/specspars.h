@@ -1,0 +1,235 @@
+/*
+ * specspars.h -- C ABI of the B200-native spec_spars sparsification path.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, returns an
+ * int status (SSP_OK == 0) and never throws across the boundary.  The message
+ * of the last failure on the calling thread is available from
+ * ssp_last_error().
+ *
+ * Reference interfaces replaced (tenchd/spec_spars):
+ *   ssp_run_solve_lap   <- ffi::run_solve_lap          src/lib.rs:103, include/example.h:18,
+ *                                                      src/example.cc:668-703
+ *   ssp_solve_lap       <- same, with explicit options/report and host or device buffers
+ *   ssp_sparsify        <- Sparsifier::sparsify         src/sparsifier.rs:722-770, driven like
+ *                          InputStream::run_stream      src/stream.rs:40-64
+ *   ssp_sparsify_mtx    <- sparsify_dataset             src/lib.rs:145-166 (read .mtx, sparsify, write .mtx)
+ *   ssp_params_default  <- SparsifierParameters::new_default  src/sparsifier.rs:182-209
+ *   ssp_params_new      <- SparsifierParameters::new          src/sparsifier.rs:163-179
+ *   ssp_params_cli      <- the knobs sparsify_dataset hard-codes, src/lib.rs:149-156
+ *   ssp_read_mtx / ssp_write_mtx <- utils::read_mtx / write_mtx  src/utils.rs:149-154,189-191
+ *   stage entry points (ssp_stage_*) expose each kernel of the path for parity testing:
+ *     edges+Laplacian <- Triplet::insert/to_csc, form_laplacian  src/sparsifier.rs:48-87,693-709
+ *     sketch          <- jl_sketch_colwise_flat                  src/sparsifier.rs:490-539
+ *     factor          <- factorization_driver                    src/example.cc:332-471
+ *     diff norms      <- compute_diff_norms                      src/sparsifier.rs:565-583
+ *     probabilities   <- compute_probs                           src/sparsifier.rs:542-562
+ *     sample/apply    <- sample_and_reweight + apply_reweightings src/sparsifier.rs:625-691
+ */
+#ifndef SPECSPARS_H
+#define SPECSPARS_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define SSP_OK 0
+#define SSP_ERR_INVALID (-1)       /* malformed input / bad argument */
+#define SSP_ERR_CUDA (-2)          /* CUDA runtime failure */
+#define SSP_ERR_NOMEM (-3)         /* device or host allocation failed */
+#define SSP_ERR_NOT_CONVERGED (-4) /* PCG relative residual >= 0.01 (reference throws, example.cc:566) */
+#define SSP_ERR_CAPACITY (-5)      /* internal pool capacity exceeded */
+#define SSP_ERR_IO (-6)            /* file I/O or .mtx parse error */
+#define SSP_ERR_NO_DEVICE (-7)     /* no CUDA device visible */
+
+#define SSP_MEM_HOST 0
+#define SSP_MEM_DEVICE 1
+
+/* JL dimension rule */
+#define SSP_JL_DIM_REF 0  /* k = ceil(log2(n) * jl_factor)   (sparsifier.rs:272) */
+#define SSP_JL_DIM_24 1   /* k = ceil(24 ln(n) / eps^2)                           */
+/* sketch entry scale */
+#define SSP_JL_SCALE_FIXED 0      /* entries +-jl_scaling_factor (lib.rs:151)   */
+#define SSP_JL_SCALE_INV_SQRT_K 1 /* entries +-1/sqrt(k)                        */
+/* reweighting of kept edges */
+#define SSP_REWEIGHT_INV_SQRT_P 0 /* w / sqrt(p)  (sparsifier.rs:657)           */
+#define SSP_REWEIGHT_INV_P 1      /* w / p        (stream_sparsify.jl:135)      */
+
+typedef struct ssp_context ssp_context;
+
+/* Sparse matrix in compressed-sparse-column form (for the symmetric matrices
+ * of this path CSC == CSR).  Row indices strictly increasing within a column. */
+typedef struct {
+    int64_t n;               /* square: n x n */
+    int64_t nnz;
+    const int64_t* colptr;   /* [n+1] */
+    const int32_t* rowidx;   /* [nnz] */
+    const double* values;    /* [nnz] */
+    int32_t mem;             /* SSP_MEM_HOST or SSP_MEM_DEVICE */
+} ssp_csc;
+
+/* Library-allocated CSC result; release with ssp_csc_free(). */
+typedef struct {
+    int64_t n;
+    int64_t nnz;
+    int64_t* colptr;
+    int32_t* rowidx;
+    double* values;
+    int32_t mem;             /* where the arrays live */
+    int32_t owned_by_context;/* device results may live in the context until its next call */
+} ssp_csc_out;
+
+/* SparsifierParameters (sparsifier.rs:146-159) plus the options this build adds. */
+typedef struct {
+    double epsilon;
+    int32_t beta_constant;
+    int32_t row_constant;
+    int32_t verbose;
+    double jl_factor;
+    double jl_scaling_factor;
+    uint64_t sketch_seed;
+    uint64_t sampling_seed;
+    int32_t bench;
+    int32_t sketch_uniform;
+    int32_t streaming;       /* accepted, not acted on: the reference's CLI path sets it false (lib.rs:155) */
+    const char* output_file; /* "" or NULL: do not write */
+    /* additions */
+    int32_t jl_dim_rule;     /* SSP_JL_DIM_* */
+    int32_t jl_scale_rule;   /* SSP_JL_SCALE_* */
+    int32_t prob_variance_correction; /* 1: divide probabilities by k*s^2 instead of k */
+    int32_t reweight;        /* SSP_REWEIGHT_* */
+    double pcg_tol;          /* relative residual stop */
+    double pcg_abs_tol;      /* absolute residual stop (reference: sqrt(2e-7), custom_cg.hpp:159,213) */
+    int32_t pcg_max_iters;   /* reference: 400 (custom_cg.hpp:153) */
+    uint64_t factor_seed;    /* elimination order + fill sampling */
+    int64_t dense_threshold; /* live-vertex count that switches elimination to the dense tail */
+} ssp_params;
+
+typedef struct {
+    int64_t n;
+    int64_t m_in;            /* edges before (sparsifier.rs:686) */
+    int64_t m_out;           /* edges after  (sparsifier.rs:688) */
+    int32_t k;               /* JL columns */
+    double beta;
+    int64_t nnz_factor;
+    int32_t factor_levels;
+    int32_t pcg_max_iters_used;
+    double pcg_mean_iters;
+    double pcg_max_relres;
+    /* per-stage milliseconds (Benchmarker phases, utils.rs:126-143) */
+    double ms_assembly, ms_sketch, ms_factor, ms_solve, ms_leverage, ms_sample, ms_total;
+    int64_t kernels_launched;
+    /* device time of the PCG's Laplacian products and preconditioner applications (CUDA events) */
+    double ms_spmm;
+    int64_t n_spmm;
+    double ms_precond;
+    int64_t n_precond;
+    int64_t nnz_laplacian;
+} ssp_stats;
+
+typedef struct {
+    double tol;
+    double abs_tol;
+    int32_t max_iters;
+    uint64_t factor_seed;
+    int64_t dense_threshold;
+    int32_t verbose;
+} ssp_solve_opts;
+
+typedef struct {
+    int32_t k;
+    int32_t max_iters_used;
+    double mean_iters;
+    double max_relres;
+    int32_t not_converged;
+    int64_t nnz_factor;
+    int32_t factor_levels;
+    double ms_factor;
+    double ms_solve;
+} ssp_solve_report;
+
+/* ---- errors ---- */
+const char* ssp_last_error(void);
+
+/* ---- context: one device, one stream, grow-only workspace ---- */
+int ssp_context_create(int32_t device, ssp_context** ctx);
+int ssp_context_destroy(ssp_context* ctx);
+/* stream: a cudaStream_t (NULL = the context's own stream) */
+int ssp_context_set_stream(ssp_context* ctx, void* stream);
+int64_t ssp_context_kernels_launched(const ssp_context* ctx);
+int64_t ssp_context_workspace_bytes(const ssp_context* ctx);
+
+/* ---- parameters ---- */
+void ssp_params_default(ssp_params* p);
+void ssp_params_new(ssp_params* p, double epsilon, int32_t beta_constant, int32_t row_constant, int32_t verbose,
+                    double jl_factor, double jl_scaling_factor, uint64_t sketch_seed, uint64_t sampling_seed,
+                    int32_t bench, int32_t sketch_uniform, const char* output_file, int32_t streaming);
+void ssp_params_cli(ssp_params* p, double epsilon, int32_t verbose, uint64_t sketch_seed, uint64_t sampling_seed,
+                    int32_t bench, const char* output_file);
+/* derived values (sparsifier.rs:264,272) */
+int32_t ssp_params_jl_dim(const ssp_params* p, int64_t n);
+double ssp_params_beta(const ssp_params* p, int64_t n);
+double ssp_params_jl_scale(const ssp_params* p, int32_t k);
+
+/* ---- drop-in for ffi::run_solve_lap (src/lib.rs:103) ----
+ * shared_jl_cols: row-major num_nodes x k (FlattenedVec effective layout), k = num_cols.
+ * col_ptrs/row_indices/values: the Laplacian in CSC (int32, as the bridge passes it).
+ * solution_out: row-major num_nodes x k, caller-allocated.
+ * Stopping rule of the reference: ||r||^2 <= 2e-7 or 400 iterations; returns
+ * SSP_ERR_NOT_CONVERGED where the reference throws (relative residual >= 0.01).
+ * solver_output_filename is accepted and ignored, as in the reference. */
+int ssp_run_solve_lap(const double* shared_jl_cols, size_t num_rows, size_t num_cols, const int32_t* col_ptrs,
+                      size_t col_ptrs_len, const int32_t* row_indices, const double* values, size_t nnz,
+                      const char* solver_output_filename, int32_t num_nodes, int32_t verbose,
+                      double* solution_out);
+
+/* ---- Laplacian solve with explicit options; Y and Z row-major n x k, host or device ---- */
+void ssp_solve_opts_default(ssp_solve_opts* o);
+int ssp_solve_lap(ssp_context* ctx, const ssp_csc* lap, const double* Y, int32_t k, double* Z, int32_t mem,
+                  const ssp_solve_opts* opts, ssp_solve_report* rep);
+
+/* ---- sparsify one graph (input: symmetric matrix whose upper triangle holds the edges) ---- */
+int ssp_sparsify(ssp_context* ctx, const ssp_csc* graph, const ssp_params* params, int32_t out_mem,
+                 ssp_csc_out* out, ssp_stats* stats);
+int ssp_csc_free(ssp_csc_out* out);
+
+/* ---- .mtx path (sparsify_dataset) ---- */
+int ssp_sparsify_mtx(const char* input_file, const char* output_file, const ssp_params* params, ssp_stats* stats);
+int ssp_read_mtx(const char* path, ssp_csc_out* out);             /* host CSC, duplicates summed */
+int ssp_write_mtx(const char* path, const ssp_csc* m);            /* coordinate real general */
+
+/* ---- synthetic graphs (seeded, identical on every host) as symmetric host CSC ---- */
+int ssp_gen_grid2d(int64_t nx, int64_t ny, double w, ssp_csc_out* out);
+int ssp_gen_grid3d(int64_t nx, int64_t ny, int64_t nz, double wlog10_lo, double wlog10_hi, uint64_t seed,
+                   ssp_csc_out* out);
+int ssp_gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, ssp_csc_out* out);
+
+/* ---- stage entry points (device-resident, for parity tests) ---- */
+/* edges of the input (v1 < v2, weights, CSC order) and L_G, copied to caller-allocated host buffers;
+ * call once with v1 == NULL to obtain m and nnz(L_G). */
+int ssp_stage_graph(ssp_context* ctx, const ssp_csc* graph, int64_t* m, int64_t* lap_nnz, int32_t* v1, int32_t* v2,
+                    double* w, int64_t* lap_colptr, int32_t* lap_rowidx, double* lap_values);
+int ssp_stage_sketch(ssp_context* ctx, int64_t n, int64_t m, const int32_t* v1, const int32_t* v2,
+                     const double* w, int32_t mem, int32_t k, double scale, uint64_t seed, int32_t uniform,
+                     double* Y);
+/* factor of a Laplacian: column CSC of L (vertex ids, strictly lower, unit diagonal implicit), D, levels.
+ * Output arrays are caller-allocated host buffers; call once with rows==NULL to get nnz. */
+int ssp_stage_factor(ssp_context* ctx, const ssp_csc* lap, uint64_t seed, int64_t dense_threshold, int64_t* nnz,
+                     int64_t* colptr, int32_t* rows, double* vals, double* D, int32_t* level, int32_t* num_levels);
+/* M^{-1} applied to the k columns of R (host, row-major n x k) with the factor of `lap` */
+int ssp_stage_precond(ssp_context* ctx, const ssp_csc* lap, uint64_t seed, int64_t dense_threshold,
+                      const double* R, int32_t k, double* Zout);
+int ssp_stage_diff_norms(ssp_context* ctx, int64_t n, int64_t m, const int32_t* v1, const int32_t* v2,
+                         const double* Z, int32_t k, int32_t mem, double* d);
+int ssp_stage_probs(ssp_context* ctx, int64_t m, const double* w, const double* d, double beta, double denom,
+                    int32_t mem, double* p);
+int ssp_stage_coins(ssp_context* ctx, int64_t m, uint64_t seed, int32_t mem, double* coins);
+int ssp_stage_sample_apply(ssp_context* ctx, const ssp_csc* graph, const double* p, const double* coins,
+                           int32_t reweight, int32_t mem, uint8_t* keep, ssp_csc_out* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,554 @@
+"""ctypes bindings of include/specspars.h and the reference-shaped Python API on top of them."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libspecspars.so")
+HEADER = os.path.join(HERE, "..", "include", "specspars.h")
+
+SSP_OK = 0
+SSP_MEM_HOST, SSP_MEM_DEVICE = 0, 1
+SSP_JL_DIM_REF, SSP_JL_DIM_24 = 0, 1
+SSP_JL_SCALE_FIXED, SSP_JL_SCALE_INV_SQRT_K = 0, 1
+SSP_REWEIGHT_INV_SQRT_P, SSP_REWEIGHT_INV_P = 0, 1
+
+ERROR_NAMES = {-1: "SSP_ERR_INVALID", -2: "SSP_ERR_CUDA", -3: "SSP_ERR_NOMEM", -4: "SSP_ERR_NOT_CONVERGED",
+               -5: "SSP_ERR_CAPACITY", -6: "SSP_ERR_IO", -7: "SSP_ERR_NO_DEVICE"}
+
+
+def _header_symbols():
+    try:
+        txt = open(HEADER).read()
+    except OSError:
+        return []
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\**\s+(ssp_[a-z_0-9]+)\s*\(", txt, re.M)))
+
+
+HEADER_SYMBOLS = _header_symbols()
+
+
+class SspError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _Csc(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("nnz", ctypes.c_int64), ("colptr", ctypes.c_void_p),
+                ("rowidx", ctypes.c_void_p), ("values", ctypes.c_void_p), ("mem", ctypes.c_int32)]
+
+
+class _CscOut(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("nnz", ctypes.c_int64), ("colptr", ctypes.c_void_p),
+                ("rowidx", ctypes.c_void_p), ("values", ctypes.c_void_p), ("mem", ctypes.c_int32),
+                ("owned_by_context", ctypes.c_int32)]
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("epsilon", ctypes.c_double), ("beta_constant", ctypes.c_int32), ("row_constant", ctypes.c_int32),
+                ("verbose", ctypes.c_int32), ("jl_factor", ctypes.c_double), ("jl_scaling_factor", ctypes.c_double),
+                ("sketch_seed", ctypes.c_uint64), ("sampling_seed", ctypes.c_uint64), ("bench", ctypes.c_int32),
+                ("sketch_uniform", ctypes.c_int32), ("streaming", ctypes.c_int32), ("output_file", ctypes.c_char_p),
+                ("jl_dim_rule", ctypes.c_int32), ("jl_scale_rule", ctypes.c_int32),
+                ("prob_variance_correction", ctypes.c_int32), ("reweight", ctypes.c_int32),
+                ("pcg_tol", ctypes.c_double), ("pcg_abs_tol", ctypes.c_double), ("pcg_max_iters", ctypes.c_int32),
+                ("factor_seed", ctypes.c_uint64), ("dense_threshold", ctypes.c_int64)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("m_in", ctypes.c_int64), ("m_out", ctypes.c_int64), ("k", ctypes.c_int32),
+                ("beta", ctypes.c_double), ("nnz_factor", ctypes.c_int64), ("factor_levels", ctypes.c_int32),
+                ("pcg_max_iters_used", ctypes.c_int32), ("pcg_mean_iters", ctypes.c_double),
+                ("pcg_max_relres", ctypes.c_double), ("ms_assembly", ctypes.c_double),
+                ("ms_sketch", ctypes.c_double), ("ms_factor", ctypes.c_double), ("ms_solve", ctypes.c_double),
+                ("ms_leverage", ctypes.c_double), ("ms_sample", ctypes.c_double), ("ms_total", ctypes.c_double),
+                ("kernels_launched", ctypes.c_int64), ("ms_spmm", ctypes.c_double), ("n_spmm", ctypes.c_int64),
+                ("ms_precond", ctypes.c_double), ("n_precond", ctypes.c_int64), ("nnz_laplacian", ctypes.c_int64)]
+
+
+class _SolveOpts(ctypes.Structure):
+    _fields_ = [("tol", ctypes.c_double), ("abs_tol", ctypes.c_double), ("max_iters", ctypes.c_int32),
+                ("factor_seed", ctypes.c_uint64), ("dense_threshold", ctypes.c_int64), ("verbose", ctypes.c_int32)]
+
+
+class _SolveReport(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_int32), ("max_iters_used", ctypes.c_int32), ("mean_iters", ctypes.c_double),
+                ("max_relres", ctypes.c_double), ("not_converged", ctypes.c_int32),
+                ("nnz_factor", ctypes.c_int64), ("factor_levels", ctypes.c_int32), ("ms_factor", ctypes.c_double),
+                ("ms_solve", ctypes.c_double)]
+
+
+_LIB = None
+P = ctypes.c_void_p
+I32, I64, U64, DBL = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double
+
+
+def lib():
+    """Load libspecspars.so from the package directory.  Missing library is an error, not a fallback."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise SspError(-1, f"{LIB_PATH} is not built; run `python -m spec_spars_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        sig = {
+            "ssp_last_error": ([], ctypes.c_char_p),
+            "ssp_context_create": ([I32, ctypes.POINTER(P)], ctypes.c_int),
+            "ssp_context_destroy": ([P], ctypes.c_int),
+            "ssp_context_set_stream": ([P, P], ctypes.c_int),
+            "ssp_context_kernels_launched": ([P], I64),
+            "ssp_context_workspace_bytes": ([P], I64),
+            "ssp_params_default": ([ctypes.POINTER(_Params)], None),
+            "ssp_params_new": ([ctypes.POINTER(_Params), DBL, I32, I32, I32, DBL, DBL, U64, U64, I32, I32,
+                                ctypes.c_char_p, I32], None),
+            "ssp_params_cli": ([ctypes.POINTER(_Params), DBL, I32, U64, U64, I32, ctypes.c_char_p], None),
+            "ssp_params_jl_dim": ([ctypes.POINTER(_Params), I64], I32),
+            "ssp_params_beta": ([ctypes.POINTER(_Params), I64], DBL),
+            "ssp_params_jl_scale": ([ctypes.POINTER(_Params), I32], DBL),
+            "ssp_run_solve_lap": ([P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_size_t, P, P, ctypes.c_size_t,
+                                   ctypes.c_char_p, I32, I32, P], ctypes.c_int),
+            "ssp_solve_opts_default": ([ctypes.POINTER(_SolveOpts)], None),
+            "ssp_solve_lap": ([P, ctypes.POINTER(_Csc), P, I32, P, I32, ctypes.POINTER(_SolveOpts),
+                               ctypes.POINTER(_SolveReport)], ctypes.c_int),
+            "ssp_sparsify": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(_Params), I32, ctypes.POINTER(_CscOut),
+                              ctypes.POINTER(_Stats)], ctypes.c_int),
+            "ssp_csc_free": ([ctypes.POINTER(_CscOut)], ctypes.c_int),
+            "ssp_sparsify_mtx": ([ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_Params),
+                                  ctypes.POINTER(_Stats)], ctypes.c_int),
+            "ssp_read_mtx": ([ctypes.c_char_p, ctypes.POINTER(_CscOut)], ctypes.c_int),
+            "ssp_write_mtx": ([ctypes.c_char_p, ctypes.POINTER(_Csc)], ctypes.c_int),
+            "ssp_gen_grid2d": ([I64, I64, DBL, ctypes.POINTER(_CscOut)], ctypes.c_int),
+            "ssp_gen_grid3d": ([I64, I64, I64, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
+            "ssp_gen_er": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
+            "ssp_stage_graph": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(I64), ctypes.POINTER(I64), P, P, P, P, P, P],
+                                ctypes.c_int),
+            "ssp_stage_sketch": ([P, I64, I64, P, P, P, I32, I32, DBL, U64, I32, P], ctypes.c_int),
+            "ssp_stage_factor": ([P, ctypes.POINTER(_Csc), U64, I64, ctypes.POINTER(I64), P, P, P, P, P,
+                                  ctypes.POINTER(I32)], ctypes.c_int),
+            "ssp_stage_precond": ([P, ctypes.POINTER(_Csc), U64, I64, P, I32, P], ctypes.c_int),
+            "ssp_stage_diff_norms": ([P, I64, I64, P, P, P, I32, I32, P], ctypes.c_int),
+            "ssp_stage_probs": ([P, I64, P, P, DBL, DBL, I32, P], ctypes.c_int),
+            "ssp_stage_coins": ([P, I64, U64, I32, P], ctypes.c_int),
+            "ssp_stage_sample_apply": ([P, ctypes.POINTER(_Csc), P, P, I32, I32, P, ctypes.POINTER(_CscOut)],
+                                       ctypes.c_int),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _LIB = L
+    return _LIB
+
+
+def _check(rc):
+    if rc != SSP_OK:
+        msg = lib().ssp_last_error()
+        raise SspError(rc, msg.decode() if msg else "")
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "data_ptr"):  # torch tensor
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+# ---------------------------------------------------------------- CSC container
+class CSC:
+    """Host CSC matrix (colptr int64, rowidx int32, values float64)."""
+
+    def __init__(self, n, colptr, rowidx, values):
+        self.n = int(n)
+        self.colptr = np.ascontiguousarray(colptr, np.int64)
+        self.rowidx = np.ascontiguousarray(rowidx, np.int32)
+        self.values = np.ascontiguousarray(values, np.float64)
+
+    @property
+    def nnz(self):
+        return int(self.colptr[-1])
+
+    def _struct(self):
+        return _Csc(self.n, self.nnz, _ptr(self.colptr), _ptr(self.rowidx), _ptr(self.values), SSP_MEM_HOST)
+
+    @classmethod
+    def _from_out(cls, out):
+        n, nnz = out.n, out.nnz
+        cp = np.ctypeslib.as_array((ctypes.c_int64 * (n + 1)).from_address(out.colptr)).copy()
+        if nnz:
+            ri = np.ctypeslib.as_array((ctypes.c_int32 * nnz).from_address(out.rowidx)).copy()
+            va = np.ctypeslib.as_array((ctypes.c_double * nnz).from_address(out.values)).copy()
+        else:
+            ri = np.zeros(0, np.int32)
+            va = np.zeros(0, np.float64)
+        return cls(n, cp, ri, va)
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csc_matrix((self.values, self.rowidx, self.colptr), shape=(self.n, self.n))
+
+    @classmethod
+    def from_scipy(cls, m):
+        import scipy.sparse as sp
+        m = sp.csc_matrix(m)
+        m.sort_indices()
+        m.sum_duplicates()
+        return cls(m.shape[0], m.indptr, m.indices, m.data)
+
+    def num_edges(self):
+        """(nnz - stored diagonal) / 2 (Sparsifier::num_edges, sparsifier.rs:346-353)."""
+        cols = np.repeat(np.arange(self.n), np.diff(self.colptr))
+        diag = int(np.count_nonzero(cols == self.rowidx))
+        return (self.nnz - diag) // 2
+
+
+def _take_out(out):
+    try:
+        return CSC._from_out(out)
+    finally:
+        lib().ssp_csc_free(ctypes.byref(out))
+
+
+def read_mtx(path):
+    out = _CscOut()
+    _check(lib().ssp_read_mtx(path.encode(), ctypes.byref(out)))
+    return _take_out(out)
+
+
+def write_mtx(path, m):
+    s = m._struct()
+    _check(lib().ssp_write_mtx(path.encode(), ctypes.byref(s)))
+
+
+def gen_grid2d(nx, ny, w=1.0):
+    out = _CscOut()
+    _check(lib().ssp_gen_grid2d(nx, ny, w, ctypes.byref(out)))
+    return _take_out(out)
+
+
+def gen_grid3d(nx, ny, nz, wlog10_lo=-3.0, wlog10_hi=3.0, seed=2):
+    out = _CscOut()
+    _check(lib().ssp_gen_grid3d(nx, ny, nz, wlog10_lo, wlog10_hi, seed, ctypes.byref(out)))
+    return _take_out(out)
+
+
+def gen_er(n, avg_degree, wlo=0.5, whi=2.0, seed=1):
+    out = _CscOut()
+    _check(lib().ssp_gen_er(n, avg_degree, wlo, whi, seed, ctypes.byref(out)))
+    return _take_out(out)
+
+
+# ---------------------------------------------------------------- parameters
+class SparsifierParameters:
+    """SparsifierParameters (sparsifier.rs:146-210) plus this build's options."""
+
+    _FIELDS = [f for f, _ in _Params._fields_]
+
+    def __init__(self, s=None):
+        object.__setattr__(self, "_s", s if s is not None else _Params())
+        object.__setattr__(self, "_out", b"")
+
+    @classmethod
+    def new(cls, epsilon, beta_constant, row_constant, verbose, jl_factor, jl_scaling_factor, sketch_seed,
+            sampling_seed, bench, sketch_uniform, output_file, streaming):
+        p = cls()
+        out = (output_file or "").encode()
+        object.__setattr__(p, "_out", out)
+        lib().ssp_params_new(ctypes.byref(p._s), epsilon, beta_constant, row_constant, int(verbose), jl_factor,
+                             jl_scaling_factor, sketch_seed, sampling_seed, int(bench), int(sketch_uniform), out,
+                             int(streaming))
+        return p
+
+    @classmethod
+    def new_default(cls, bench=False):
+        p = cls()
+        lib().ssp_params_default(ctypes.byref(p._s))
+        p._s.bench = int(bench)
+        return p
+
+    @classmethod
+    def cli(cls, epsilon=0.5, verbose=False, sketch_seed=0, sampling_seed=0, bench=False, output_file=""):
+        """The knobs sparsify_dataset hard-codes (lib.rs:149-156)."""
+        p = cls()
+        out = (output_file or "").encode()
+        object.__setattr__(p, "_out", out)
+        lib().ssp_params_cli(ctypes.byref(p._s), epsilon, int(verbose), sketch_seed, sampling_seed, int(bench), out)
+        return p
+
+    @classmethod
+    def baseline(cls, epsilon=0.5, pcg_tol=1e-8, sketch_seed=0, sampling_seed=0):
+        """k = ceil(24 ln n / eps^2) columns of +-1/sqrt(k) signs, variance-corrected probabilities."""
+        p = cls.cli(epsilon=epsilon, sketch_seed=sketch_seed, sampling_seed=sampling_seed)
+        p.jl_dim_rule = SSP_JL_DIM_24
+        p.jl_scale_rule = SSP_JL_SCALE_INV_SQRT_K
+        p.prob_variance_correction = 1
+        p.pcg_tol = pcg_tol
+        p.pcg_abs_tol = 0.0
+        return p
+
+    def __getattr__(self, k):
+        if k in SparsifierParameters._FIELDS:
+            v = getattr(self._s, k)
+            return v.decode() if isinstance(v, bytes) else v
+        raise AttributeError(k)
+
+    def __setattr__(self, k, v):
+        if k == "output_file":
+            b = (v or "").encode()
+            object.__setattr__(self, "_out", b)
+            self._s.output_file = b
+        elif k in SparsifierParameters._FIELDS:
+            setattr(self._s, k, v)
+        else:
+            raise AttributeError(k)
+
+    def jl_dim(self, n):
+        return lib().ssp_params_jl_dim(ctypes.byref(self._s), n)
+
+    def beta(self, n):
+        return lib().ssp_params_beta(ctypes.byref(self._s), n)
+
+    def jl_scale(self, k):
+        return lib().ssp_params_jl_scale(ctypes.byref(self._s), k)
+
+
+def _stats_dict(st):
+    return {f: getattr(st, f) for f, _ in _Stats._fields_}
+
+
+class SparsificationStats:
+    """SparsificationStats (sparsifier.rs:213-237)."""
+
+    def __init__(self, d):
+        self.__dict__.update(d)
+        self.original_num_edges = d["m_in"]
+        self.final_num_edges = d["m_out"]
+
+    def sparsification_rate(self):
+        return self.final_num_edges / self.original_num_edges if self.original_num_edges else 0.0
+
+
+# ---------------------------------------------------------------- context
+class Context:
+    def __init__(self, device=0):
+        h = P()
+        _check(lib().ssp_context_create(device, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ssp_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_ptr):
+        _check(lib().ssp_context_set_stream(self._h, stream_ptr))
+
+    @property
+    def kernels_launched(self):
+        return lib().ssp_context_kernels_launched(self._h)
+
+    @property
+    def workspace_bytes(self):
+        return lib().ssp_context_workspace_bytes(self._h)
+
+    def sparsify(self, graph, params):
+        """Host CSC in, host CSC L_H out."""
+        g = graph._struct()
+        out = _CscOut()
+        st = _Stats()
+        _check(lib().ssp_sparsify(self._h, ctypes.byref(g), ctypes.byref(params._s), SSP_MEM_HOST,
+                                  ctypes.byref(out), ctypes.byref(st)))
+        return _take_out(out), _stats_dict(st)
+
+    def sparsify_device(self, n, nnz, colptr_ptr, rowidx_ptr, values_ptr, params):
+        """Device CSC in (raw pointers), device CSC out (context-owned until the next call)."""
+        g = _Csc(n, nnz, colptr_ptr, rowidx_ptr, values_ptr, SSP_MEM_DEVICE)
+        out = _CscOut()
+        st = _Stats()
+        _check(lib().ssp_sparsify(self._h, ctypes.byref(g), ctypes.byref(params._s), SSP_MEM_DEVICE,
+                                  ctypes.byref(out), ctypes.byref(st)))
+        return (out.nnz, out.colptr, out.rowidx, out.values), _stats_dict(st)
+
+    def solve_lap(self, lap, Y, tol=0.0, abs_tol=np.sqrt(2e-7), max_iters=400, factor_seed=0,
+                  dense_threshold=4096, raise_on_failure=True):
+        Y = np.ascontiguousarray(Y, np.float64)
+        n, k = Y.shape
+        Z = np.zeros_like(Y)
+        o = _SolveOpts(tol, abs_tol, max_iters, factor_seed, dense_threshold, 0)
+        rep = _SolveReport()
+        s = lap._struct()
+        rc = lib().ssp_solve_lap(self._h, ctypes.byref(s), _ptr(Y), k, _ptr(Z), SSP_MEM_HOST, ctypes.byref(o),
+                                 ctypes.byref(rep))
+        if rc != SSP_OK and (raise_on_failure or rc != -4):
+            _check(rc)
+        return Z, {f: getattr(rep, f) for f, _ in _SolveReport._fields_}
+
+
+_DEFAULT_CTX = None
+
+
+def _ctx():
+    global _DEFAULT_CTX
+    if _DEFAULT_CTX is None:
+        _DEFAULT_CTX = Context(0)
+    return _DEFAULT_CTX
+
+
+def solve_lap(lap, Y, **kw):
+    return _ctx().solve_lap(lap, Y, **kw)
+
+
+def run_solve_lap(shared_jl_cols, col_ptrs, row_indices, values, solver_output_filename, num_nodes, verbose):
+    """Drop-in for ffi::run_solve_lap (lib.rs:103): FlattenedVec-like (vec, num_rows, num_cols) in,
+    row-major solution out.  Raises SspError where the reference throws."""
+    vec, num_rows, num_cols = shared_jl_cols
+    vec = np.ascontiguousarray(vec, np.float64)
+    cp = np.ascontiguousarray(col_ptrs, np.int32)
+    ri = np.ascontiguousarray(row_indices, np.int32)
+    va = np.ascontiguousarray(values, np.float64)
+    sol = np.zeros(num_rows * num_cols, np.float64)
+    _check(lib().ssp_run_solve_lap(_ptr(vec), num_rows, num_cols, _ptr(cp), len(cp), _ptr(ri), _ptr(va), len(va),
+                                   (solver_output_filename or "").encode(), num_nodes, int(verbose), _ptr(sol)))
+    return sol, num_rows, num_cols
+
+
+class Sparsifier:
+    """Holds the current Laplacian of a graph; sparsify() runs the GPU path (sparsifier.rs:722-770)."""
+
+    def __init__(self, graph, parameters, ctx=None):
+        self.graph = graph
+        self.params = parameters
+        self.ctx = ctx or _ctx()
+        self.current_laplacian = None
+        self.stats = None
+
+    def sparsify(self):
+        self.current_laplacian, st = self.ctx.sparsify(self.graph, self.params)
+        self.stats = SparsificationStats(st)
+        return self.stats
+
+    def num_edges(self):
+        return self.current_laplacian.num_edges() if self.current_laplacian is not None else None
+
+
+class InputStream:
+    """Reads a .mtx file (InputStream::new, stream.rs:18-37)."""
+
+    def __init__(self, filename, dataset_name=""):
+        self.input_matrix = read_mtx(filename)
+        self.num_nodes = self.input_matrix.n
+        self.dataset_name = dataset_name
+
+    def run_stream(self, parameters, test=False, writeout=False):
+        sp = Sparsifier(self.input_matrix, parameters)
+        stats = sp.sparsify()
+        if writeout and not test and parameters.output_file:
+            write_mtx(parameters.output_file, sp.current_laplacian)
+        return sp, stats
+
+
+def sparsify_dataset(input_filename, dataset_name, output_filename, epsilon, verbose, sketch_seed, sampling_seed,
+                     benchmark):
+    """sparsify_dataset (lib.rs:145-166)."""
+    p = SparsifierParameters.cli(epsilon, verbose, sketch_seed, sampling_seed, benchmark, output_filename)
+    st = _Stats()
+    _check(lib().ssp_sparsify_mtx(input_filename.encode(), (output_filename or "").encode(), ctypes.byref(p._s),
+                                  ctypes.byref(st)))
+    return SparsificationStats(_stats_dict(st))
+
+
+# ---------------------------------------------------------------- stage entry points (parity tests)
+def stage_graph(ctx, graph):
+    """Edges (v1, v2, w) and L_G as built on the device."""
+    m, lnnz = I64(), I64()
+    g = graph._struct()
+    _check(lib().ssp_stage_graph(ctx._h, ctypes.byref(g), ctypes.byref(m), ctypes.byref(lnnz), None, None, None,
+                                 None, None, None))
+    mm, nn = m.value, lnnz.value
+    v1 = np.zeros(max(mm, 1), np.int32); v2 = np.zeros(max(mm, 1), np.int32); w = np.zeros(max(mm, 1), np.float64)
+    cp = np.zeros(graph.n + 1, np.int64); ri = np.zeros(max(nn, 1), np.int32); va = np.zeros(max(nn, 1), np.float64)
+    _check(lib().ssp_stage_graph(ctx._h, ctypes.byref(g), ctypes.byref(m), ctypes.byref(lnnz), _ptr(v1), _ptr(v2),
+                                 _ptr(w), _ptr(cp), _ptr(ri), _ptr(va)))
+    return (v1[:mm], v2[:mm], w[:mm]), CSC(graph.n, cp, ri[:nn], va[:nn])
+
+
+def stage_sketch(ctx, n, v1, v2, w, k, scale, seed, uniform=False):
+    v1 = np.ascontiguousarray(v1, np.int32); v2 = np.ascontiguousarray(v2, np.int32)
+    w = np.ascontiguousarray(w, np.float64)
+    Y = np.zeros((n, k), np.float64)
+    _check(lib().ssp_stage_sketch(ctx._h, n, len(v1), _ptr(v1), _ptr(v2), _ptr(w), SSP_MEM_HOST, k, scale, seed,
+                                  int(uniform), _ptr(Y)))
+    return Y
+
+
+def stage_factor(ctx, lap, seed, dense_threshold=4096):
+    s = lap._struct()
+    nnz = I64()
+    nl = I32()
+    _check(lib().ssp_stage_factor(ctx._h, ctypes.byref(s), seed, dense_threshold, ctypes.byref(nnz), None, None,
+                                  None, None, None, ctypes.byref(nl)))
+    n = lap.n
+    cp = np.zeros(n + 1, np.int64); rows = np.zeros(max(nnz.value, 1), np.int32)
+    vals = np.zeros(max(nnz.value, 1), np.float64); D = np.zeros(n, np.float64); lvl = np.zeros(n, np.int32)
+    _check(lib().ssp_stage_factor(ctx._h, ctypes.byref(s), seed, dense_threshold, ctypes.byref(nnz), _ptr(cp),
+                                  _ptr(rows), _ptr(vals), _ptr(D), _ptr(lvl), ctypes.byref(nl)))
+    return {"colptr": cp, "rows": rows[:nnz.value], "vals": vals[:nnz.value], "D": D, "level": lvl,
+            "num_levels": nl.value}
+
+
+def stage_precond(ctx, lap, seed, R, dense_threshold=4096):
+    R = np.ascontiguousarray(R, np.float64)
+    if R.ndim == 1:
+        R = R[:, None]
+    Z = np.zeros_like(R)
+    s = lap._struct()
+    _check(lib().ssp_stage_precond(ctx._h, ctypes.byref(s), seed, dense_threshold, _ptr(R), R.shape[1], _ptr(Z)))
+    return Z
+
+
+def stage_diff_norms(ctx, v1, v2, Z):
+    Z = np.ascontiguousarray(Z, np.float64)
+    v1 = np.ascontiguousarray(v1, np.int32); v2 = np.ascontiguousarray(v2, np.int32)
+    d = np.zeros(len(v1), np.float64)
+    _check(lib().ssp_stage_diff_norms(ctx._h, Z.shape[0], len(v1), _ptr(v1), _ptr(v2), _ptr(Z), Z.shape[1],
+                                      SSP_MEM_HOST, _ptr(d)))
+    return d
+
+
+def stage_probs(ctx, w, d, beta, denom):
+    w = np.ascontiguousarray(w, np.float64); d = np.ascontiguousarray(d, np.float64)
+    p = np.zeros_like(w)
+    _check(lib().ssp_stage_probs(ctx._h, len(w), _ptr(w), _ptr(d), beta, denom, SSP_MEM_HOST, _ptr(p)))
+    return p
+
+
+def stage_coins(ctx, m, seed):
+    c = np.zeros(m, np.float64)
+    _check(lib().ssp_stage_coins(ctx._h, m, seed, SSP_MEM_HOST, _ptr(c)))
+    return c
+
+
+def stage_sample_apply(ctx, graph, p, coins, reweight):
+    p = np.ascontiguousarray(p, np.float64); coins = np.ascontiguousarray(coins, np.float64)
+    keep = np.zeros(max(len(p), 1), np.uint8)
+    out = _CscOut()
+    g = graph._struct()
+    _check(lib().ssp_stage_sample_apply(ctx._h, ctypes.byref(g), _ptr(p), _ptr(coins), int(reweight), SSP_MEM_HOST,
+                                        _ptr(keep), ctypes.byref(out)))
+    return _take_out(out), keep[:len(p)].astype(bool)

@@ -1,0 +1,782 @@
+// ssp_api.cu -- extern "C" entry points (include/specspars.h).
+//
+// Sparsifier flow (Sparsifier::sparsify, sparsifier.rs:722-770): edges and L_G from the input
+// matrix (a2/a3/a5) -> JL sketch (a4) -> approximate Cholesky (a7) -> PCG on all k columns (a8,
+// the ffi::run_solve_lap call of get_probs, sparsifier.rs:593) -> diff norms (a9) -> probabilities
+// (a10) -> coins, reweighting and L_H (a11/a12).  Every stage runs on the device; there is no CPU
+// fallback.  C++ exceptions never cross this boundary: each entry point returns a status code and
+// records a message for ssp_last_error().
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ssp_host.h"
+#include "ssp_internal.cuh"
+
+struct ssp_context {
+    ssp::Context ctx;
+};
+
+namespace ssp {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+void precond_apply_device(Context& C, const DevFactor& F, const double* R, double* Z, int64_t ld);
+
+template <class Fn>
+static int guarded(Fn&& fn) {
+    try {
+        fn();
+        return SSP_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return SSP_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return SSP_ERR_INVALID;
+    }
+}
+
+static void init_context(Context& C, int device) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        throw Error(SSP_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    SSP_REQUIRE(device >= 0 && device < count, SSP_ERR_INVALID, "device index out of range");
+    C.device = device;
+    SSP_CUDA(cudaSetDevice(device));
+    SSP_CUDA(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
+    C.own_stream = true;
+    SSP_CUDA(cudaMallocHost(&C.h_pinned, 64 * sizeof(int64_t)));
+}
+
+static void destroy_context(Context& C) {
+    cudaSetDevice(C.device);
+    if (C.stream) cudaStreamSynchronize(C.stream);
+    C.ws.release();
+    if (C.h_pinned) cudaFreeHost(C.h_pinned);
+    if (C.own_stream && C.stream) cudaStreamDestroy(C.stream);
+    C.h_pinned = nullptr;
+    C.stream = nullptr;
+}
+
+// process-wide default context for the reference-shaped entry points that carry none
+static std::mutex g_default_mu;
+static ssp_context* g_default = nullptr;
+static Context& default_context() {
+    if (!g_default) {
+        auto* c = new ssp_context();
+        try {
+            init_context(c->ctx, 0);
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        g_default = c;
+    }
+    cudaSetDevice(g_default->ctx.device);
+    return g_default->ctx;
+}
+
+// device copy of a CSC (or pass-through when already on the device)
+struct DevCsc {
+    int64_t n = 0, nnz = 0;
+    const int64_t* colptr = nullptr;
+    const int32_t* rowidx = nullptr;
+    const double* val = nullptr;
+};
+static DevCsc to_device(Context& C, const ssp_csc* m, const char* tag) {
+    SSP_REQUIRE(m && m->n > 0 && m->nnz >= 0 && m->colptr && (m->nnz == 0 || (m->rowidx && m->values)),
+                SSP_ERR_INVALID, "invalid CSC descriptor");
+    SSP_REQUIRE(m->n < (int64_t)INT32_MAX, SSP_ERR_INVALID, "n must be < 2^31");
+    DevCsc d;
+    d.n = m->n;
+    d.nnz = m->nnz;
+    if (m->mem == SSP_MEM_DEVICE) {
+        d.colptr = m->colptr;
+        d.rowidx = m->rowidx;
+        d.val = m->values;
+        return d;
+    }
+    SSP_REQUIRE(m->colptr[0] == 0 && m->colptr[m->n] == m->nnz, SSP_ERR_INVALID,
+                "CSC colptr must start at 0 and end at nnz");
+    std::string t(tag);
+    int64_t* cp = C.ws.get_t<int64_t>(t + "_cp", m->n + 1);
+    int32_t* ri = C.ws.get_t<int32_t>(t + "_ri", m->nnz + 1);
+    double* va = C.ws.get_t<double>(t + "_va", m->nnz + 1);
+    SSP_CUDA(cudaMemcpyAsync(cp, m->colptr, sizeof(int64_t) * (m->n + 1), cudaMemcpyHostToDevice, C.stream));
+    if (m->nnz) {
+        SSP_CUDA(cudaMemcpyAsync(ri, m->rowidx, sizeof(int32_t) * m->nnz, cudaMemcpyHostToDevice, C.stream));
+        SSP_CUDA(cudaMemcpyAsync(va, m->values, sizeof(double) * m->nnz, cudaMemcpyHostToDevice, C.stream));
+    }
+    d.colptr = cp;
+    d.rowidx = ri;
+    d.val = va;
+    return d;
+}
+
+// ---------------------------------------------------------------- parameters
+static int32_t jl_dim(const ssp_params* p, int64_t n) {
+    double k;
+    if (p->jl_dim_rule == SSP_JL_DIM_24) k = std::ceil(24.0 * std::log((double)n) / (p->epsilon * p->epsilon));
+    else k = std::ceil(std::log2((double)n) * p->jl_factor);
+    if (k < 1) k = 1;
+    return (int32_t)k;
+}
+static double jl_scale(const ssp_params* p, int32_t k) {
+    return p->jl_scale_rule == SSP_JL_SCALE_INV_SQRT_K ? 1.0 / std::sqrt((double)k) : p->jl_scaling_factor;
+}
+static double beta_of(const ssp_params* p, int64_t n) {
+    return std::pow(p->epsilon, -2.0) * (double)p->beta_constant * std::log((double)n);
+}
+
+// events for per-stage timing
+struct StageTimer {
+    Context& C;
+    std::vector<cudaEvent_t> ev;
+    explicit StageTimer(Context& c) : C(c) {}
+    void mark() {
+        cudaEvent_t e;
+        SSP_CUDA(cudaEventCreate(&e));
+        SSP_CUDA(cudaEventRecord(e, C.stream));
+        ev.push_back(e);
+    }
+    double ms(size_t a, size_t b) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ev[a], ev[b]);
+        return t;
+    }
+    ~StageTimer() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+};
+
+__global__ void k_count_diag(int64_t n, const int64_t* ptr, const int32_t* idx, int64_t* out) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        for (int64_t p = ptr[v]; p < ptr[v + 1]; p++)
+            if (idx[p] == v) atomicAdd((unsigned long long*)out, 1ull);
+}
+
+static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* prm, int32_t out_mem, ssp_csc_out* out,
+                          ssp_stats* st) {
+    SSP_REQUIRE(prm, SSP_ERR_INVALID, "params is NULL");
+    SSP_REQUIRE(prm->epsilon > 0 && std::isfinite(prm->epsilon), SSP_ERR_INVALID, "epsilon must be positive");
+    SSP_CUDA(cudaSetDevice(C.device));
+    StageTimer T(C);
+    T.mark();  // 0
+    DevCsc g = to_device(C, graph, "in");
+    DevGraph G;
+    build_graph_from_csc(C, g.n, g.colptr, g.rowidx, g.val, g.nnz, G);
+    T.mark();  // 1
+    const int64_t n = G.n;
+    const int32_t k = jl_dim(prm, n);
+    const double scale = jl_scale(prm, k);
+    const int64_t ld = ((int64_t)k + 7) / 8 * 8;
+    double* Y = C.ws.get_t<double>("sp_Y", (size_t)n * ld);
+    sketch_device(C, G, k, scale, prm->sketch_seed, prm->sketch_uniform, Y, ld);
+    T.mark();  // 2
+    DevFactor F;
+    FactorOptions fo;
+    fo.seed = prm->factor_seed;
+    fo.dense_threshold = prm->dense_threshold;
+    factor_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, fo, F, "f");
+    T.mark();  // 3
+    PcgOptions po;
+    po.tol = prm->pcg_tol;
+    po.abs_tol = prm->pcg_abs_tol;
+    po.max_iters = prm->pcg_max_iters;
+    po.verbose = prm->verbose;
+    PcgReport rep;
+    pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, k, ld, Y, po, rep);  // Z overwrites Y
+    T.mark();  // 4
+    double* d = C.ws.get_t<double>("sp_d", G.m + 1);
+    double* p = C.ws.get_t<double>("sp_p", G.m + 1);
+    double* coins = C.ws.get_t<double>("sp_coins", G.m + 1);
+    diff_norms_device(C, G.m, G.v1, G.v2, Y, k, ld, d);
+    const double beta = beta_of(prm, n);
+    const double denom = prm->prob_variance_correction ? (double)k * scale * scale : (double)k;
+    probs_device(C, G.m, G.w, d, beta, denom, p);
+    T.mark();  // 5
+    coins_device(C, G.m, prm->sampling_seed, coins);
+    int64_t *lh_ptr;
+    int32_t* lh_idx;
+    double* lh_val;
+    const int64_t nnz = sample_apply_device(C, G, p, coins, prm->reweight, &lh_ptr, &lh_idx, &lh_val, nullptr);
+    int64_t* nd = C.ws.get_t<int64_t>("sp_ndiag", 1);
+    SSP_CUDA(cudaMemsetAsync(nd, 0, sizeof(int64_t), C.stream));
+    k_count_diag<<<grid_for(n, 256), 256, 0, C.stream>>>(n, lh_ptr, lh_idx, nd);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+    T.mark();  // 6
+    const int64_t ndiag = read_i64(C, nd);
+    int64_t lg_diag = 0;
+    {
+        SSP_CUDA(cudaMemsetAsync(nd, 0, sizeof(int64_t), C.stream));
+        k_count_diag<<<grid_for(n, 256), 256, 0, C.stream>>>(n, G.lap_ptr, G.lap_idx, nd);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched++;
+        lg_diag = read_i64(C, nd);
+    }
+    if (out) {
+        memset(out, 0, sizeof(*out));
+        out->n = n;
+        out->nnz = nnz;
+        if (out_mem == SSP_MEM_DEVICE) {
+            out->colptr = lh_ptr;
+            out->rowidx = lh_idx;
+            out->values = lh_val;
+            out->mem = SSP_MEM_DEVICE;
+            out->owned_by_context = 1;
+        } else {
+            out->colptr = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+            out->rowidx = (int32_t*)malloc(sizeof(int32_t) * (nnz + 1));
+            out->values = (double*)malloc(sizeof(double) * (nnz + 1));
+            if (!out->colptr || !out->rowidx || !out->values) {
+                free(out->colptr); free(out->rowidx); free(out->values);
+                memset(out, 0, sizeof(*out));
+                throw Error(SSP_ERR_NOMEM, "host allocation of the output failed");
+            }
+            SSP_CUDA(cudaMemcpyAsync(out->colptr, lh_ptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(out->rowidx, lh_idx, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(out->values, lh_val, sizeof(double) * nnz, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaStreamSynchronize(C.stream));
+            out->mem = SSP_MEM_HOST;
+        }
+    }
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    if (st) {
+        memset(st, 0, sizeof(*st));
+        st->n = n;
+        st->m_in = (G.lap_nnz - lg_diag) / 2;
+        st->m_out = (nnz - ndiag) / 2;
+        st->k = k;
+        st->beta = beta;
+        st->nnz_factor = F.nnz;
+        st->factor_levels = F.num_levels;
+        st->pcg_max_iters_used = rep.max_iters_used;
+        st->pcg_mean_iters = rep.mean_iters;
+        st->pcg_max_relres = rep.max_relres;
+        st->ms_assembly = T.ms(0, 1);
+        st->ms_sketch = T.ms(1, 2);
+        st->ms_factor = T.ms(2, 3);
+        st->ms_solve = T.ms(3, 4);
+        st->ms_leverage = T.ms(4, 5);
+        st->ms_sample = T.ms(5, 6);
+        st->ms_total = T.ms(0, 6);
+        st->kernels_launched = C.kernels_launched;
+        st->ms_spmm = rep.ms_spmm;
+        st->n_spmm = rep.n_spmm;
+        st->ms_precond = rep.ms_precond;
+        st->n_precond = rep.n_precond;
+        st->nnz_laplacian = G.lap_nnz;
+    }
+    if (prm->verbose) {
+        fprintf(stderr, "[ssp] n=%lld m=%lld k=%d nnz(L)=%lld levels=%d pcg iters max %d mean %.1f relres %.3g\n",
+                (long long)n, (long long)G.m, k, (long long)F.nnz, F.num_levels, rep.max_iters_used, rep.mean_iters,
+                rep.max_relres);
+    }
+    if (prm->output_file && prm->output_file[0]) {
+        std::vector<int64_t> cp(n + 1);
+        std::vector<int32_t> ri(nnz);
+        std::vector<double> va(nnz);
+        SSP_CUDA(cudaMemcpy(cp.data(), lh_ptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost));
+        SSP_CUDA(cudaMemcpy(ri.data(), lh_idx, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost));
+        SSP_CUDA(cudaMemcpy(va.data(), lh_val, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
+        std::string err;
+        if (write_mtx(prm->output_file, n, cp.data(), ri.data(), va.data(), err) != 0) throw Error(SSP_ERR_IO, err);
+    }
+}
+
+static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t k, double* Z, int32_t mem,
+                       const ssp_solve_opts* o, ssp_solve_report* rep, int32_t* iters, double* relres) {
+    SSP_REQUIRE(lap && Y && Z && k > 0, SSP_ERR_INVALID, "solve: bad arguments");
+    ssp_solve_opts od;
+    ssp_solve_opts_default(&od);
+    if (!o) o = &od;
+    SSP_CUDA(cudaSetDevice(C.device));
+    StageTimer T(C);
+    T.mark();
+    DevCsc L = to_device(C, lap, "lap");
+    const int64_t n = L.n;
+    const double* dY = Y;
+    double* dZ = Z;
+    if (mem == SSP_MEM_HOST) {
+        double* y = C.ws.get_t<double>("sl_Y", (size_t)n * k);
+        SSP_CUDA(cudaMemcpyAsync(y, Y, sizeof(double) * n * k, cudaMemcpyHostToDevice, C.stream));
+        dY = y;
+        dZ = C.ws.get_t<double>("sl_Z", (size_t)n * k);
+    }
+    DevFactor F;
+    FactorOptions fo;
+    fo.seed = o->factor_seed;
+    fo.dense_threshold = o->dense_threshold;
+    factor_device(C, n, L.colptr, L.rowidx, L.val, fo, F, "f");
+    T.mark();
+    PcgOptions po;
+    po.tol = o->tol;
+    po.abs_tol = o->abs_tol;
+    po.max_iters = o->max_iters;
+    po.verbose = o->verbose;
+    PcgReport pr;
+    pcg_device(C, n, L.colptr, L.rowidx, L.val, F, dY, k, k, dZ, po, pr, iters, relres);
+    T.mark();
+    if (mem == SSP_MEM_HOST)
+        SSP_CUDA(cudaMemcpyAsync(Z, dZ, sizeof(double) * n * k, cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    if (rep) {
+        rep->k = k;
+        rep->max_iters_used = pr.max_iters_used;
+        rep->mean_iters = pr.mean_iters;
+        rep->max_relres = pr.max_relres;
+        rep->not_converged = pr.not_converged;
+        rep->nnz_factor = F.nnz;
+        rep->factor_levels = F.num_levels;
+        rep->ms_factor = T.ms(0, 1);
+        rep->ms_solve = T.ms(1, 2);
+    }
+    if (pr.not_converged > 0)
+        throw Error(SSP_ERR_NOT_CONVERGED, "solver did not converge: " + std::to_string(pr.not_converged) +
+                                               " column(s) with relative residual >= 0.01 (max " +
+                                               std::to_string(pr.max_relres) + ")");
+}
+
+template <class T>
+static const T* stage_in(Context& C, const T* p, int64_t cnt, int32_t mem, const char* tag) {
+    if (mem == SSP_MEM_DEVICE || cnt == 0) return p;
+    T* d = C.ws.get_t<T>(tag, cnt);
+    SSP_CUDA(cudaMemcpyAsync(d, p, sizeof(T) * cnt, cudaMemcpyHostToDevice, C.stream));
+    return d;
+}
+
+}  // namespace ssp
+
+using namespace ssp;
+
+extern "C" {
+
+const char* ssp_last_error(void) { return g_last_error.c_str(); }
+
+int ssp_context_create(int32_t device, ssp_context** out) {
+    return guarded([&] {
+        SSP_REQUIRE(out, SSP_ERR_INVALID, "ctx out pointer is NULL");
+        auto* c = new ssp_context();
+        try {
+            init_context(c->ctx, device);
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+int ssp_context_destroy(ssp_context* c) {
+    return guarded([&] {
+        if (!c) return;
+        destroy_context(c->ctx);
+        delete c;
+    });
+}
+
+int ssp_context_set_stream(ssp_context* c, void* stream) {
+    return guarded([&] {
+        SSP_REQUIRE(c, SSP_ERR_INVALID, "ctx is NULL");
+        SSP_CUDA(cudaStreamSynchronize(c->ctx.stream));
+        if (c->ctx.own_stream && c->ctx.stream && stream) {
+            cudaStreamDestroy(c->ctx.stream);
+            c->ctx.own_stream = false;
+        }
+        if (stream) {
+            c->ctx.stream = (cudaStream_t)stream;
+        } else if (!c->ctx.own_stream) {
+            SSP_CUDA(cudaStreamCreateWithFlags(&c->ctx.stream, cudaStreamNonBlocking));
+            c->ctx.own_stream = true;
+        }
+    });
+}
+
+int64_t ssp_context_kernels_launched(const ssp_context* c) { return c ? c->ctx.kernels_launched : 0; }
+int64_t ssp_context_workspace_bytes(const ssp_context* c) { return c ? (int64_t)c->ctx.ws.total_bytes() : 0; }
+
+void ssp_params_new(ssp_params* p, double epsilon, int32_t beta_constant, int32_t row_constant, int32_t verbose,
+                    double jl_factor, double jl_scaling_factor, uint64_t sketch_seed, uint64_t sampling_seed,
+                    int32_t bench, int32_t sketch_uniform, const char* output_file, int32_t streaming) {
+    memset(p, 0, sizeof(*p));
+    p->epsilon = epsilon;
+    p->beta_constant = beta_constant;
+    p->row_constant = row_constant;
+    p->verbose = verbose;
+    p->jl_factor = jl_factor;
+    p->jl_scaling_factor = jl_scaling_factor;
+    p->sketch_seed = sketch_seed;
+    p->sampling_seed = sampling_seed;
+    p->bench = bench;
+    p->sketch_uniform = sketch_uniform;
+    p->output_file = output_file;
+    p->streaming = streaming;
+    p->jl_dim_rule = SSP_JL_DIM_REF;
+    p->jl_scale_rule = SSP_JL_SCALE_FIXED;
+    p->prob_variance_correction = 0;
+    p->reweight = SSP_REWEIGHT_INV_SQRT_P;
+    p->pcg_tol = 0.0;
+    p->pcg_abs_tol = std::sqrt(2e-7);
+    p->pcg_max_iters = 400;
+    p->factor_seed = 0;
+    p->dense_threshold = 4096;
+}
+
+void ssp_params_default(ssp_params* p) {
+    ssp_params_new(p, 0.5, 4, 2, 0, 1.5, std::sqrt(3.0), 1, 1, 0, 1, "", 0);
+}
+
+void ssp_params_cli(ssp_params* p, double epsilon, int32_t verbose, uint64_t sketch_seed, uint64_t sampling_seed,
+                    int32_t bench, const char* output_file) {
+    ssp_params_new(p, epsilon, 4, 2, verbose, 4.0, std::sqrt(3.0), sketch_seed, sampling_seed, bench, 0, output_file,
+                   0);
+}
+
+int32_t ssp_params_jl_dim(const ssp_params* p, int64_t n) { return jl_dim(p, n); }
+double ssp_params_beta(const ssp_params* p, int64_t n) { return beta_of(p, n); }
+double ssp_params_jl_scale(const ssp_params* p, int32_t k) { return jl_scale(p, k); }
+
+void ssp_solve_opts_default(ssp_solve_opts* o) {
+    o->tol = 0.0;
+    o->abs_tol = std::sqrt(2e-7);
+    o->max_iters = 400;
+    o->factor_seed = 0;
+    o->dense_threshold = 4096;
+    o->verbose = 0;
+}
+
+int ssp_run_solve_lap(const double* shared_jl_cols, size_t num_rows, size_t num_cols, const int32_t* col_ptrs,
+                      size_t col_ptrs_len, const int32_t* row_indices, const double* values, size_t nnz,
+                      const char* solver_output_filename, int32_t num_nodes, int32_t verbose,
+                      double* solution_out) {
+    (void)solver_output_filename;
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(g_default_mu);
+        SSP_REQUIRE(num_nodes > 0 && (size_t)num_nodes == num_rows && col_ptrs_len == (size_t)num_nodes + 1,
+                    SSP_ERR_INVALID, "run_solve_lap: inconsistent dimensions");
+        SSP_REQUIRE((size_t)col_ptrs[num_nodes] == nnz, SSP_ERR_INVALID, "run_solve_lap: col_ptrs[n] != nnz");
+        Context& C = default_context();
+        std::vector<int64_t> cp(num_nodes + 1);
+        for (int32_t i = 0; i <= num_nodes; i++) cp[i] = col_ptrs[i];
+        ssp_csc L{num_nodes, (int64_t)nnz, cp.data(), row_indices, values, SSP_MEM_HOST};
+        ssp_solve_opts o;
+        ssp_solve_opts_default(&o);
+        o.verbose = verbose;
+        solve_impl(C, &L, shared_jl_cols, (int32_t)num_cols, solution_out, SSP_MEM_HOST, &o, nullptr, nullptr,
+                   nullptr);
+    });
+}
+
+int ssp_solve_lap(ssp_context* c, const ssp_csc* lap, const double* Y, int32_t k, double* Z, int32_t mem,
+                  const ssp_solve_opts* opts, ssp_solve_report* rep) {
+    return guarded([&] {
+        SSP_REQUIRE(c, SSP_ERR_INVALID, "ctx is NULL");
+        solve_impl(c->ctx, lap, Y, k, Z, mem, opts, rep, nullptr, nullptr);
+    });
+}
+
+int ssp_sparsify(ssp_context* c, const ssp_csc* graph, const ssp_params* params, int32_t out_mem, ssp_csc_out* out,
+                 ssp_stats* stats) {
+    return guarded([&] {
+        SSP_REQUIRE(c, SSP_ERR_INVALID, "ctx is NULL");
+        sparsify_impl(c->ctx, graph, params, out_mem, out, stats);
+    });
+}
+
+int ssp_csc_free(ssp_csc_out* out) {
+    if (!out) return SSP_OK;
+    if (out->mem == SSP_MEM_HOST) {
+        free(out->colptr);
+        free(out->rowidx);
+        free(out->values);
+    } else if (!out->owned_by_context) {
+        cudaFree(out->colptr);
+        cudaFree(out->rowidx);
+        cudaFree(out->values);
+    }
+    memset(out, 0, sizeof(*out));
+    return SSP_OK;
+}
+
+static void host_out(const HostCsc& h, ssp_csc_out* out) {
+    memset(out, 0, sizeof(*out));
+    out->n = h.n;
+    out->nnz = h.colptr.empty() ? 0 : h.colptr[h.n];
+    out->colptr = (int64_t*)malloc(sizeof(int64_t) * (h.n + 1));
+    out->rowidx = (int32_t*)malloc(sizeof(int32_t) * (out->nnz + 1));
+    out->values = (double*)malloc(sizeof(double) * (out->nnz + 1));
+    if (!out->colptr || !out->rowidx || !out->values) throw std::bad_alloc();
+    memcpy(out->colptr, h.colptr.data(), sizeof(int64_t) * (h.n + 1));
+    if (out->nnz) {
+        memcpy(out->rowidx, h.rowidx.data(), sizeof(int32_t) * out->nnz);
+        memcpy(out->values, h.val.data(), sizeof(double) * out->nnz);
+    }
+    out->mem = SSP_MEM_HOST;
+}
+
+int ssp_read_mtx(const char* path, ssp_csc_out* out) {
+    return guarded([&] {
+        SSP_REQUIRE(path && out, SSP_ERR_INVALID, "bad arguments");
+        HostCsc h;
+        std::string err;
+        if (read_mtx(path, h, err) != 0) throw Error(SSP_ERR_IO, err);
+        host_out(h, out);
+    });
+}
+
+int ssp_write_mtx(const char* path, const ssp_csc* m) {
+    return guarded([&] {
+        SSP_REQUIRE(path && m && m->mem == SSP_MEM_HOST, SSP_ERR_INVALID, "write_mtx needs a host CSC");
+        std::string err;
+        if (write_mtx(path, m->n, m->colptr, m->rowidx, m->values, err) != 0) throw Error(SSP_ERR_IO, err);
+    });
+}
+
+int ssp_sparsify_mtx(const char* input_file, const char* output_file, const ssp_params* params, ssp_stats* stats) {
+    return guarded([&] {
+        SSP_REQUIRE(input_file && params, SSP_ERR_INVALID, "bad arguments");
+        HostCsc h;
+        std::string err;
+        if (read_mtx(input_file, h, err) != 0) throw Error(SSP_ERR_IO, err);
+        // InputStream::new zeroes the stored diagonal (stream.rs:23-28): the edge extraction only
+        // reads row < col, so the diagonal never reaches the sparsifier.
+        ssp_params p = *params;
+        p.output_file = output_file;
+        std::lock_guard<std::mutex> lk(g_default_mu);
+        Context& C = default_context();
+        ssp_csc g{h.n, h.colptr[h.n], h.colptr.data(), h.rowidx.data(), h.val.data(), SSP_MEM_HOST};
+        sparsify_impl(C, &g, &p, SSP_MEM_HOST, nullptr, stats);
+    });
+}
+
+int ssp_gen_grid2d(int64_t nx, int64_t ny, double w, ssp_csc_out* out) {
+    return guarded([&] {
+        SSP_REQUIRE(nx > 0 && ny > 0 && out, SSP_ERR_INVALID, "bad arguments");
+        HostCsc h;
+        gen_grid2d(nx, ny, w, h);
+        host_out(h, out);
+    });
+}
+int ssp_gen_grid3d(int64_t nx, int64_t ny, int64_t nz, double lo, double hi, uint64_t seed, ssp_csc_out* out) {
+    return guarded([&] {
+        SSP_REQUIRE(nx > 0 && ny > 0 && nz > 0 && out, SSP_ERR_INVALID, "bad arguments");
+        HostCsc h;
+        gen_grid3d(nx, ny, nz, lo, hi, seed, h);
+        host_out(h, out);
+    });
+}
+int ssp_gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, ssp_csc_out* out) {
+    return guarded([&] {
+        SSP_REQUIRE(n > 1 && avg_degree > 0 && out, SSP_ERR_INVALID, "bad arguments");
+        HostCsc h;
+        gen_er(n, avg_degree, wlo, whi, seed, h);
+        host_out(h, out);
+    });
+}
+
+// ---------------------------------------------------------------- stage entry points
+int ssp_stage_graph(ssp_context* c, const ssp_csc* graph, int64_t* m, int64_t* lap_nnz, int32_t* v1, int32_t* v2,
+                    double* w, int64_t* lap_colptr, int32_t* lap_rowidx, double* lap_values) {
+    return guarded([&] {
+        SSP_REQUIRE(c && graph && m && lap_nnz, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        DevCsc g = to_device(C, graph, "in");
+        DevGraph G;
+        build_graph_from_csc(C, g.n, g.colptr, g.rowidx, g.val, g.nnz, G);
+        *m = G.m;
+        *lap_nnz = G.lap_nnz;
+        if (v1) {
+            if (G.m) {
+                SSP_CUDA(cudaMemcpyAsync(v1, G.v1, sizeof(int32_t) * G.m, cudaMemcpyDeviceToHost, C.stream));
+                SSP_CUDA(cudaMemcpyAsync(v2, G.v2, sizeof(int32_t) * G.m, cudaMemcpyDeviceToHost, C.stream));
+                SSP_CUDA(cudaMemcpyAsync(w, G.w, sizeof(double) * G.m, cudaMemcpyDeviceToHost, C.stream));
+            }
+            SSP_CUDA(cudaMemcpyAsync(lap_colptr, G.lap_ptr, sizeof(int64_t) * (G.n + 1), cudaMemcpyDeviceToHost,
+                                     C.stream));
+            if (G.lap_nnz) {
+                SSP_CUDA(cudaMemcpyAsync(lap_rowidx, G.lap_idx, sizeof(int32_t) * G.lap_nnz, cudaMemcpyDeviceToHost,
+                                         C.stream));
+                SSP_CUDA(cudaMemcpyAsync(lap_values, G.lap_val, sizeof(double) * G.lap_nnz, cudaMemcpyDeviceToHost,
+                                         C.stream));
+            }
+        }
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int ssp_stage_sketch(ssp_context* c, int64_t n, int64_t m, const int32_t* v1, const int32_t* v2, const double* w,
+                     int32_t mem, int32_t k, double scale, uint64_t seed, int32_t uniform, double* Y) {
+    return guarded([&] {
+        SSP_REQUIRE(c && n > 0 && m >= 0 && k > 0 && Y, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        DevGraph G;
+        G.n = n;
+        G.m = m;
+        if (mem == SSP_MEM_HOST) {
+            G.v1 = C.ws.get_t<int32_t>("g_v1", m + 1);
+            G.v2 = C.ws.get_t<int32_t>("g_v2", m + 1);
+            G.w = C.ws.get_t<double>("g_w", m + 1);
+            SSP_CUDA(cudaMemcpyAsync(G.v1, v1, sizeof(int32_t) * m, cudaMemcpyHostToDevice, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(G.v2, v2, sizeof(int32_t) * m, cudaMemcpyHostToDevice, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(G.w, w, sizeof(double) * m, cudaMemcpyHostToDevice, C.stream));
+        } else {
+            G.v1 = (int32_t*)v1;
+            G.v2 = (int32_t*)v2;
+            G.w = (double*)w;
+        }
+        build_graph_from_edges(C, G);
+        double* dY = Y;
+        if (mem == SSP_MEM_HOST) dY = C.ws.get_t<double>("st_Y", (size_t)n * k);
+        sketch_device(C, G, k, scale, seed, uniform, dY, k);
+        if (mem == SSP_MEM_HOST)
+            SSP_CUDA(cudaMemcpyAsync(Y, dY, sizeof(double) * n * k, cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int ssp_stage_factor(ssp_context* c, const ssp_csc* lap, uint64_t seed, int64_t dense_threshold, int64_t* nnz,
+                     int64_t* colptr, int32_t* rows, double* vals, double* D, int32_t* level, int32_t* num_levels) {
+    return guarded([&] {
+        SSP_REQUIRE(c && lap && nnz, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        DevCsc L = to_device(C, lap, "lap");
+        DevFactor F;
+        FactorOptions fo;
+        fo.seed = seed;
+        fo.dense_threshold = dense_threshold;
+        factor_device(C, L.n, L.colptr, L.rowidx, L.val, fo, F, "f");
+        *nnz = F.nnz;
+        if (num_levels) *num_levels = F.num_levels;
+        if (rows) {
+            SSP_CUDA(cudaMemcpyAsync(colptr, F.col_ptr, sizeof(int64_t) * (L.n + 1), cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(rows, F.col_idx, sizeof(int32_t) * F.nnz, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(vals, F.col_val, sizeof(double) * F.nnz, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(D, F.D, sizeof(double) * L.n, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(level, F.level, sizeof(int32_t) * L.n, cudaMemcpyDeviceToHost, C.stream));
+        }
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int ssp_stage_precond(ssp_context* c, const ssp_csc* lap, uint64_t seed, int64_t dense_threshold, const double* R,
+                      int32_t k, double* Zout) {
+    return guarded([&] {
+        SSP_REQUIRE(c && lap && R && Zout && k > 0, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        DevCsc L = to_device(C, lap, "lap");
+        DevFactor F;
+        FactorOptions fo;
+        fo.seed = seed;
+        fo.dense_threshold = dense_threshold;
+        factor_device(C, L.n, L.colptr, L.rowidx, L.val, fo, F, "f");
+        const int64_t ld = ((int64_t)k + 7) / 8 * 8;
+        double* dR = C.ws.get_t<double>("pc_R", (size_t)L.n * ld);
+        double* dZ = C.ws.get_t<double>("pc_Z", (size_t)L.n * ld);
+        SSP_CUDA(cudaMemsetAsync(dR, 0, sizeof(double) * L.n * ld, C.stream));
+        SSP_CUDA(cudaMemcpy2DAsync(dR, sizeof(double) * ld, R, sizeof(double) * k, sizeof(double) * k, L.n,
+                                   cudaMemcpyHostToDevice, C.stream));
+        precond_apply_device(C, F, dR, dZ, ld);
+        SSP_CUDA(cudaMemcpy2DAsync(Zout, sizeof(double) * k, dZ, sizeof(double) * ld, sizeof(double) * k, L.n,
+                                   cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int ssp_stage_diff_norms(ssp_context* c, int64_t n, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z,
+                         int32_t k, int32_t mem, double* d) {
+    return guarded([&] {
+        SSP_REQUIRE(c && k > 0 && d, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        const int32_t* dv1 = stage_in(C, v1, m, mem, "dn_v1");
+        const int32_t* dv2 = stage_in(C, v2, m, mem, "dn_v2");
+        const double* dZ = stage_in(C, Z, n * (int64_t)k, mem, "dn_Z");
+        double* dd = mem == SSP_MEM_DEVICE ? d : C.ws.get_t<double>("dn_d", m + 1);
+        diff_norms_device(C, m, dv1, dv2, dZ, k, k, dd);
+        if (mem == SSP_MEM_HOST && m)
+            SSP_CUDA(cudaMemcpyAsync(d, dd, sizeof(double) * m, cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int ssp_stage_probs(ssp_context* c, int64_t m, const double* w, const double* d, double beta, double denom,
+                    int32_t mem, double* p) {
+    return guarded([&] {
+        SSP_REQUIRE(c && p, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        const double* dw = stage_in(C, w, m, mem, "pr_w");
+        const double* dd = stage_in(C, d, m, mem, "pr_d");
+        double* dp = mem == SSP_MEM_DEVICE ? p : C.ws.get_t<double>("pr_p", m + 1);
+        probs_device(C, m, dw, dd, beta, denom, dp);
+        if (mem == SSP_MEM_HOST && m)
+            SSP_CUDA(cudaMemcpyAsync(p, dp, sizeof(double) * m, cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int ssp_stage_coins(ssp_context* c, int64_t m, uint64_t seed, int32_t mem, double* coins) {
+    return guarded([&] {
+        SSP_REQUIRE(c && coins, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        double* dc = mem == SSP_MEM_DEVICE ? coins : C.ws.get_t<double>("co_c", m + 1);
+        coins_device(C, m, seed, dc);
+        if (mem == SSP_MEM_HOST && m)
+            SSP_CUDA(cudaMemcpyAsync(coins, dc, sizeof(double) * m, cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int ssp_stage_sample_apply(ssp_context* c, const ssp_csc* graph, const double* p, const double* coins,
+                           int32_t reweight, int32_t mem, uint8_t* keep, ssp_csc_out* out) {
+    return guarded([&] {
+        SSP_REQUIRE(c && graph && p && coins && out, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        DevCsc g = to_device(C, graph, "in");
+        DevGraph G;
+        build_graph_from_csc(C, g.n, g.colptr, g.rowidx, g.val, g.nnz, G);
+        const double* dp = stage_in(C, p, G.m, mem, "sa_p");
+        const double* dc = stage_in(C, coins, G.m, mem, "sa_c");
+        uint8_t* dkeep = C.ws.get_t<uint8_t>("sa_keep", G.m + 1);
+        int64_t* lp;
+        int32_t* li;
+        double* lv;
+        int64_t nnz = sample_apply_device(C, G, dp, dc, reweight, &lp, &li, &lv, dkeep);
+        memset(out, 0, sizeof(*out));
+        out->n = G.n;
+        out->nnz = nnz;
+        out->mem = SSP_MEM_HOST;
+        out->colptr = (int64_t*)malloc(sizeof(int64_t) * (G.n + 1));
+        out->rowidx = (int32_t*)malloc(sizeof(int32_t) * (nnz + 1));
+        out->values = (double*)malloc(sizeof(double) * (nnz + 1));
+        SSP_CUDA(cudaMemcpyAsync(out->colptr, lp, sizeof(int64_t) * (G.n + 1), cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaMemcpyAsync(out->rowidx, li, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaMemcpyAsync(out->values, lv, sizeof(double) * nnz, cudaMemcpyDeviceToHost, C.stream));
+        if (keep && G.m)
+            SSP_CUDA(cudaMemcpyAsync(keep, dkeep, G.m, mem == SSP_MEM_HOST ? cudaMemcpyDeviceToHost
+                                                                            : cudaMemcpyDeviceToDevice,
+                                     C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,261 @@
+// ssp_host.cpp -- host-side I/O and synthetic graphs.
+//
+// read_mtx / write_mtx restate utils::read_mtx / write_mtx (utils.rs:149-154,189-191): Matrix
+// Market coordinate files, symmetric storage expanded, duplicates summed, CSC with sorted rows.
+// Pattern files (which the reference cannot read, utils.rs:172-186) load with weight 1.
+//
+// Generators produce the symmetric adjacency of the synthetic graphs used by the benchmark
+// configurations, seeded through Philox so every host builds the same graph.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ssp_host.h"
+
+namespace ssp {
+
+static inline uint64_t mulhi(uint64_t a, uint64_t b) { return (uint64_t)(((unsigned __int128)a * b) >> 64); }
+static void philox_host(uint64_t c0, uint64_t c1, uint64_t c2, uint64_t c3, uint64_t k0, uint64_t k1,
+                        uint64_t out[4]) {
+    for (int r = 0; r < 10; r++) {
+        if (r > 0) {
+            k0 += 0x9E3779B97F4A7C15ULL;
+            k1 += 0xBB67AE8584CAA73BULL;
+        }
+        const uint64_t M0 = 0xD2E7470EE14C6C93ULL, M1 = 0xCA5A826395121157ULL;
+        uint64_t lo0 = M0 * c0, hi0 = mulhi(M0, c0), lo1 = M1 * c2, hi1 = mulhi(M1, c2);
+        uint64_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+static constexpr uint64_t STREAM_GEN = 0x47454e31ULL;
+static inline double gen_u53(uint64_t seed, uint64_t a, uint64_t b) {
+    uint64_t o[4];
+    philox_host(a, b, 0, 0, seed, STREAM_GEN, o);
+    return (double)(o[0] >> 11) * 0x1.0p-53;
+}
+
+void HostCsc::from_upper_edges(int64_t n_, const std::vector<int32_t>& a, const std::vector<int32_t>& b,
+                               const std::vector<double>& w) {
+    // edges (a < b) sorted by (b, a): CSC-upper order.  Emit both triangles.
+    n = n_;
+    const int64_t m = (int64_t)a.size();
+    std::vector<int64_t> cnt(n + 1, 0);
+    for (int64_t e = 0; e < m; e++) {
+        cnt[a[e] + 1]++;
+        cnt[b[e] + 1]++;
+    }
+    colptr.assign(n + 1, 0);
+    for (int64_t v = 0; v < n; v++) colptr[v + 1] = colptr[v] + cnt[v + 1];
+    rowidx.assign(colptr[n], 0);
+    val.assign(colptr[n], 0.0);
+    std::vector<int64_t> cur(colptr.begin(), colptr.end() - 1);
+    // column c: rows < c are edges (r, c) with b == c in order of r; rows > c are edges (c, v) in order of v.
+    // Edges sorted by (b, a) visit every column's lower-row entries before any later column, and a
+    // vertex's upper entries (c, v) arrive in increasing v.
+    for (int64_t e = 0; e < m; e++) {
+        int32_t r = a[e], c = b[e];
+        rowidx[cur[c]] = r;
+        val[cur[c]++] = w[e];
+        rowidx[cur[r]] = c;
+        val[cur[r]++] = w[e];
+    }
+}
+
+// ---------------------------------------------------------------- generators
+void gen_grid2d(int64_t nx, int64_t ny, double w, HostCsc& out) {
+    const int64_t n = nx * ny;
+    std::vector<int32_t> a, b;
+    std::vector<double> ww;
+    // CSC-upper order: for each column c (ascending), rows r < c ascending: r = c - nx, c - 1
+    for (int64_t c = 0; c < n; c++) {
+        int64_t x = c % nx, y = c / nx;
+        if (y > 0) { a.push_back((int32_t)(c - nx)); b.push_back((int32_t)c); ww.push_back(w); }
+        if (x > 0) { a.push_back((int32_t)(c - 1)); b.push_back((int32_t)c); ww.push_back(w); }
+    }
+    out.from_upper_edges(n, a, b, ww);
+}
+
+// 7-point grid, weight 10^U(lo,hi) per edge, drawn from Philox(seed, smaller endpoint, direction)
+void gen_grid3d(int64_t nx, int64_t ny, int64_t nz, double lo, double hi, uint64_t seed, HostCsc& out) {
+    const int64_t n = nx * ny * nz, nxy = nx * ny;
+    std::vector<int32_t> a, b;
+    std::vector<double> ww;
+    a.reserve(3 * n); b.reserve(3 * n); ww.reserve(3 * n);
+    for (int64_t c = 0; c < n; c++) {
+        int64_t x = c % nx, y = (c / nx) % ny, z = c / nxy;
+        int64_t rows[3];
+        int dirs[3];
+        int cnt = 0;
+        if (z > 0) { rows[cnt] = c - nxy; dirs[cnt++] = 2; }
+        if (y > 0) { rows[cnt] = c - nx; dirs[cnt++] = 1; }
+        if (x > 0) { rows[cnt] = c - 1; dirs[cnt++] = 0; }
+        for (int i = 0; i < cnt; i++) {
+            double u = gen_u53(seed, (uint64_t)rows[i], (uint64_t)dirs[i]);
+            double wv = std::pow(10.0, lo + (hi - lo) * u);
+            a.push_back((int32_t)rows[i]);
+            b.push_back((int32_t)c);
+            ww.push_back(wv);
+        }
+    }
+    out.from_upper_edges(n, a, b, ww);
+}
+
+// Erdos-Renyi G(n, p), p = avg_degree/(n-1), by geometric skipping over the pairs (w < v) in
+// order of v then w (Batagelj & Brandes 2005); weights U[wlo, whi] rounded to float.
+void gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, HostCsc& out) {
+    const double p = std::min(1.0, avg_degree / (double)(n - 1));
+    std::vector<int32_t> a, b;
+    std::vector<double> ww;
+    const int64_t expect = (int64_t)(p * (double)n * (double)(n - 1) / 2.0 * 1.05) + 16;
+    a.reserve(expect); b.reserve(expect); ww.reserve(expect);
+    const double lp = std::log1p(-p);
+    int64_t v = 1, w = -1;
+    uint64_t draw = 0;
+    while (v < n) {
+        double u = gen_u53(seed, draw++, 0);
+        int64_t skip = (p >= 1.0) ? 0 : (int64_t)std::floor(std::log1p(-u) / lp);
+        w += 1 + skip;
+        while (w >= v && v < n) {
+            w -= v;
+            v++;
+        }
+        if (v < n) {
+            double uw = gen_u53(seed, draw++, 1);
+            float wf = (float)(wlo + (whi - wlo) * uw);
+            a.push_back((int32_t)w);
+            b.push_back((int32_t)v);
+            ww.push_back((double)wf);
+        }
+    }
+    out.from_upper_edges(n, a, b, ww);
+}
+
+// ---------------------------------------------------------------- Matrix Market
+static bool lower_eq(const std::string& a, const char* b) {
+    if (a.size() != strlen(b)) return false;
+    for (size_t i = 0; i < a.size(); i++)
+        if (tolower(a[i]) != b[i]) return false;
+    return true;
+}
+
+int read_mtx(const char* path, HostCsc& out, std::string& err) {
+    FILE* f = fopen(path, "r");
+    if (!f) {
+        err = std::string("cannot open ") + path;
+        return -1;
+    }
+    char line[4096];
+    if (!fgets(line, sizeof line, f)) {
+        fclose(f);
+        err = "empty file";
+        return -1;
+    }
+    char banner[64], object[64], format[64], field[64], sym[64];
+    if (sscanf(line, "%63s %63s %63s %63s %63s", banner, object, format, field, sym) != 5 ||
+        !lower_eq(banner, "%%matrixmarket") || !lower_eq(object, "matrix") || !lower_eq(format, "coordinate")) {
+        fclose(f);
+        err = "not a MatrixMarket coordinate matrix";
+        return -1;
+    }
+    bool pattern = lower_eq(field, "pattern");
+    if (!pattern && !lower_eq(field, "real") && !lower_eq(field, "integer") && !lower_eq(field, "double")) {
+        fclose(f);
+        err = std::string("unsupported field ") + field;
+        return -1;
+    }
+    bool symmetric = lower_eq(sym, "symmetric");
+    if (!symmetric && !lower_eq(sym, "general")) {
+        fclose(f);
+        err = std::string("unsupported symmetry ") + sym;
+        return -1;
+    }
+    long long nr = 0, nc = 0, nnz = 0;
+    while (fgets(line, sizeof line, f)) {
+        if (line[0] == '%') continue;
+        if (sscanf(line, "%lld %lld %lld", &nr, &nc, &nnz) == 3) break;
+        fclose(f);
+        err = "bad size line";
+        return -1;
+    }
+    if (nr <= 0 || nr != nc || nnz < 0) {
+        fclose(f);
+        err = "matrix must be square";
+        return -1;
+    }
+    std::vector<int64_t> I, J;
+    std::vector<double> V;
+    I.reserve(symmetric ? 2 * nnz : nnz);
+    J.reserve(symmetric ? 2 * nnz : nnz);
+    V.reserve(symmetric ? 2 * nnz : nnz);
+    for (long long t = 0; t < nnz; t++) {
+        long long i, j;
+        double x = 1.0;
+        int got;
+        if (pattern) got = fscanf(f, "%lld %lld", &i, &j) == 2;
+        else got = fscanf(f, "%lld %lld %lf", &i, &j, &x) == 3;
+        if (!got || i < 1 || j < 1 || i > nr || j > nc) {
+            fclose(f);
+            err = "bad entry " + std::to_string(t);
+            return -1;
+        }
+        I.push_back(i - 1);
+        J.push_back(j - 1);
+        V.push_back(x);
+        if (symmetric && i != j) {
+            I.push_back(j - 1);
+            J.push_back(i - 1);
+            V.push_back(x);
+        }
+    }
+    fclose(f);
+    // CSC: sort by (col, row), sum duplicates
+    const int64_t n = nr;
+    std::vector<int64_t> order(I.size());
+    for (size_t t = 0; t < order.size(); t++) order[t] = (int64_t)t;
+    std::sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+        return J[x] != J[y] ? J[x] < J[y] : (I[x] != I[y] ? I[x] < I[y] : x < y);
+    });
+    out.n = n;
+    out.colptr.assign(n + 1, 0);
+    out.rowidx.clear();
+    out.val.clear();
+    for (size_t t = 0; t < order.size(); t++) {
+        int64_t o = order[t];
+        if (!out.rowidx.empty() && t > 0 && J[order[t - 1]] == J[o] && I[order[t - 1]] == I[o]) {
+            out.val.back() += V[o];
+            continue;
+        }
+        out.rowidx.push_back((int32_t)I[o]);
+        out.val.push_back(V[o]);
+        out.colptr[J[o] + 1]++;
+    }
+    for (int64_t c = 0; c < n; c++) out.colptr[c + 1] += out.colptr[c];
+    return 0;
+}
+
+int write_mtx(const char* path, int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,
+              std::string& err) {
+    FILE* f = fopen(path, "w");
+    if (!f) {
+        err = std::string("cannot open ") + path + " for writing";
+        return -1;
+    }
+    fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n");
+    fprintf(f, "%lld %lld %lld\n", (long long)n, (long long)n, (long long)colptr[n]);
+    for (int64_t c = 0; c < n; c++)
+        for (int64_t p = colptr[c]; p < colptr[c + 1]; p++)
+            fprintf(f, "%d %lld %.17g\n", rowidx[p] + 1, (long long)(c + 1), val[p]);
+    if (fclose(f) != 0) {
+        err = "write failed";
+        return -1;
+    }
+    return 0;
+}
+
+}  // namespace ssp

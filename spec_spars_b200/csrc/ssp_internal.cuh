@@ -1,0 +1,274 @@
+// ssp_internal.cuh -- shared device/host helpers of the spec_spars B200 library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include "../../include/specspars.h"
+
+namespace ssp {
+
+// ---------------------------------------------------------------- errors
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+void set_last_error(const std::string& msg);
+
+#define SSP_CUDA(call)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            throw ::ssp::Error(SSP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+#define SSP_CHECK_LAUNCH() SSP_CUDA(cudaGetLastError())
+#define SSP_REQUIRE(cond, code, msg)                       \
+    do {                                                   \
+        if (!(cond)) throw ::ssp::Error((code), (msg));    \
+    } while (0)
+
+// ---------------------------------------------------------------- RNG
+// Philox4x64-10 (Salmon et al., SC'11).  Stream ids go into the second key word.
+constexpr uint64_t STREAM_SIGN = 0x5349474eULL;
+constexpr uint64_t STREAM_UNIF = 0x554e4946ULL;
+constexpr uint64_t STREAM_FACTOR = 0x46414354ULL;
+constexpr uint64_t STREAM_PRIO = 0x5052494fULL;
+constexpr uint64_t STREAM_COIN = 0x434f494eULL;
+
+struct u64x4 { uint64_t x, y, z, w; };
+
+__host__ __device__ __forceinline__ uint64_t mulhi64(uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+    return __umul64hi(a, b);
+#else
+    return (uint64_t)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+__host__ __device__ __forceinline__ u64x4 philox(uint64_t c0, uint64_t c1, uint64_t c2, uint64_t c3,
+                                                 uint64_t k0, uint64_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        if (r > 0) {
+            k0 += 0x9E3779B97F4A7C15ULL;
+            k1 += 0xBB67AE8584CAA73BULL;
+        }
+        const uint64_t M0 = 0xD2E7470EE14C6C93ULL, M1 = 0xCA5A826395121157ULL;
+        uint64_t lo0 = M0 * c0, hi0 = mulhi64(M0, c0);
+        uint64_t lo1 = M1 * c2, hi1 = mulhi64(M1, c2);
+        uint64_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    }
+    return {c0, c1, c2, c3};
+}
+__host__ __device__ __forceinline__ uint64_t pick(const u64x4& r, int i) {
+    return i == 0 ? r.x : i == 1 ? r.y : i == 2 ? r.z : r.w;
+}
+__host__ __device__ __forceinline__ double u53(uint64_t x) { return (double)(x >> 11) * 0x1.0p-53; }
+
+__host__ __device__ __forceinline__ uint64_t vertex_priority(uint64_t seed, int64_t v) {
+    return philox((uint64_t)v, 0, 0, 0, seed, STREAM_PRIO).x;
+}
+__host__ __device__ __forceinline__ double factor_uniform(uint64_t seed, int64_t v, int64_t slot) {
+    u64x4 r = philox((uint64_t)v, (uint64_t)(slot >> 2), 0, 0, seed, STREAM_FACTOR);
+    return u53(pick(r, (int)(slot & 3)));
+}
+__host__ __device__ __forceinline__ double edge_coin(uint64_t seed, int64_t e) {
+    u64x4 r = philox((uint64_t)(e >> 2), 0, 0, 0, seed, STREAM_COIN);
+    return u53(pick(r, (int)(e & 3)));
+}
+
+// ---------------------------------------------------------------- device memory
+// Grow-only named buffers owned by a context, so repeated calls on one
+// context do not pay cudaMalloc/cudaFree inside the hot loop.
+class Workspace {
+public:
+    ~Workspace() { release(); }
+    void* get(const std::string& name, size_t bytes) {
+        bytes = bytes ? bytes : 16;
+        auto it = bufs_.find(name);
+        if (it != bufs_.end() && it->second.bytes >= bytes) return it->second.ptr;
+        if (it != bufs_.end()) {
+            cudaFree(it->second.ptr);
+            bufs_.erase(it);
+        }
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(SSP_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes for '" + name +
+                                           "' failed: " + cudaGetErrorString(e));
+        }
+        bufs_[name] = {p, bytes};
+        return p;
+    }
+    template <class T>
+    T* get_t(const std::string& name, size_t count) { return (T*)get(name, count * sizeof(T)); }
+    // enlarge `name` to `bytes`, preserving its first `keep` bytes
+    void* grow(const std::string& name, size_t keep, size_t bytes, cudaStream_t stream) {
+        auto it = bufs_.find(name);
+        if (it != bufs_.end() && it->second.bytes >= bytes) return it->second.ptr;
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(SSP_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes for '" + name +
+                                           "' failed: " + cudaGetErrorString(e));
+        }
+        if (it != bufs_.end()) {
+            if (keep) {
+                e = cudaMemcpyAsync(p, it->second.ptr, keep, cudaMemcpyDeviceToDevice, stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+                if (e != cudaSuccess) {
+                    cudaFree(p);
+                    throw Error(SSP_ERR_CUDA, std::string("workspace grow copy: ") + cudaGetErrorString(e));
+                }
+            }
+            cudaFree(it->second.ptr);
+            bufs_.erase(it);
+        }
+        bufs_[name] = {p, bytes};
+        return p;
+    }
+    void release() {
+        for (auto& kv : bufs_) cudaFree(kv.second.ptr);
+        bufs_.clear();
+    }
+    size_t total_bytes() const {
+        size_t s = 0;
+        for (auto& kv : bufs_) s += kv.second.bytes;
+        return s;
+    }
+private:
+    struct Buf { void* ptr; size_t bytes; };
+    std::map<std::string, Buf> bufs_;
+};
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Workspace ws;
+    int64_t* h_pinned = nullptr;  // small pinned scratch for scalar readbacks
+    int verbose = 0;
+    int64_t kernels_launched = 0;  // count of library kernel launches (for bench accounting)
+};
+
+// ---------------------------------------------------------------- small device helpers
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+template <class T>
+inline T ceil_div(T a, T b) { return (a + b - 1) / b; }
+
+inline int grid_for(int64_t items, int per_block, int max_blocks = 148 * 32) {
+    int64_t g = (items + per_block - 1) / per_block;
+    if (g < 1) g = 1;
+    if (g > max_blocks) g = max_blocks;
+    return (int)g;
+}
+
+// Device-wide exclusive scan of int64 counts (three-phase, deterministic).
+// out may alias in.  Returns total via *d_total (device) if non-null.
+void exclusive_scan_i64(Context& C, const int64_t* in, int64_t* out, int64_t n, int64_t* d_total);
+void exclusive_scan_i32_to_i64(Context& C, const int32_t* in, int64_t* out, int64_t n, int64_t* d_total);
+
+// read a device scalar synchronously (on the context stream)
+int64_t read_i64(Context& C, const int64_t* d_ptr);
+void read_i64s(Context& C, const int64_t* d_ptr, int64_t* host, int cnt);
+
+// Segmented sort of int32 keys in place (ascending).  Segments [start[i], start[i]+len[i]).
+void segsort_i32(Context& C, int32_t* keys, const int64_t* seg_start, const int32_t* seg_len, int64_t nseg,
+                 int32_t max_len);
+// Segmented sort of (int32 key, double payload) pairs by key (keys unique within a segment).
+void segsort_pairs_i32_f64(Context& C, int32_t* keys, double* vals, const int64_t* seg_start,
+                           const int32_t* seg_len, int64_t nseg, int32_t max_len);
+
+// ---------------------------------------------------------------- stage entry points (internal C++)
+struct DevGraph {
+    int64_t n = 0, m = 0;
+    int32_t *v1 = nullptr, *v2 = nullptr;  // edges in reference order
+    double* w = nullptr;
+    int64_t* adj_ptr = nullptr;            // [n+1] symmetric adjacency, neighbour-sorted
+    int32_t* adj_nbr = nullptr;            // [2m]
+    int32_t* adj_eid = nullptr;            // [2m]
+    int32_t max_deg = 0;
+    // Laplacian L_G (CSC == CSR)
+    int64_t lap_nnz = 0;
+    int64_t* lap_ptr = nullptr;
+    int32_t* lap_idx = nullptr;
+    double* lap_val = nullptr;
+};
+
+// a2+a5: build edges, adjacency and L_G from an input CSC already on the device.
+void build_graph_from_csc(Context& C, int64_t n, const int64_t* colptr, const int32_t* rowidx,
+                          const double* val, int64_t nnz, DevGraph& G);
+// adjacency + Laplacian for a given device edge list (v1<v2, CSC order)
+void build_graph_from_edges(Context& C, DevGraph& G);
+
+// a4: Y (n x ldy row-major, columns [0,k)) = B^T Q
+void sketch_device(Context& C, const DevGraph& G, int32_t k, double scale, uint64_t seed, int uniform,
+                   double* Y, int64_t ldy);
+
+// a7: factor
+struct DevFactor {
+    int64_t n = 0;
+    int64_t nnz = 0;
+    // column form (backward solve): vertex-indexed CSC
+    int64_t* col_ptr = nullptr;
+    int32_t* col_idx = nullptr;
+    double* col_val = nullptr;
+    // row form (forward solve): vertex-indexed CSR, columns sorted
+    int64_t* row_ptr = nullptr;
+    int32_t* row_idx = nullptr;
+    double* row_val = nullptr;
+    double* D = nullptr;
+    int32_t* level = nullptr;       // [n]
+    int32_t* level_ptr_d = nullptr; // [num_levels+1] (device)
+    int32_t* level_rows = nullptr;  // [n] vertices grouped by level
+    std::vector<int32_t> level_ptr; // host copy
+    int32_t num_levels = 0;
+    int32_t dense_levels = 0;       // trailing single-vertex levels from the dense phase
+    int32_t max_level_rows = 0;
+};
+struct FactorOptions {
+    uint64_t seed = 0;
+    int64_t dense_threshold = 4096;
+};
+// Input: Laplacian CSC on device (rows > col used, |value| as weight).
+void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,
+                   const FactorOptions& opt, DevFactor& F, const std::string& tag = "f");
+
+// a8: PCG on all k columns.  Y, Z: n x ld row-major device arrays.
+struct PcgOptions {
+    double tol = 1e-8;
+    double abs_tol = 0.0;
+    int32_t max_iters = 400;
+    int verbose = 0;
+};
+struct PcgReport {
+    int32_t max_iters_used = 0;
+    double mean_iters = 0;
+    double max_relres = 0;
+    int32_t not_converged = 0;
+    double ms_spmm = 0;
+    int64_t n_spmm = 0;
+    double ms_precond = 0;
+    int64_t n_precond = 0;
+};
+void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx, const double* lap_val,
+                const DevFactor& F, const double* Y, int32_t k, int64_t ld, double* Z, const PcgOptions& opt,
+                PcgReport& rep, int32_t* h_iters = nullptr, double* h_relres = nullptr);
+
+// a9-a12
+void diff_norms_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z, int32_t k,
+                       int64_t ldz, double* d);
+void probs_device(Context& C, int64_t m, const double* w, const double* d, double beta, double denom, double* p);
+void coins_device(Context& C, int64_t m, uint64_t seed, double* coins);
+// returns nnz(L_H); writes L_H CSC into workspace buffers returned through pointers
+int64_t sample_apply_device(Context& C, const DevGraph& G, const double* p, const double* coins, int reweight,
+                            int64_t** lh_ptr, int32_t** lh_idx, double** lh_val, uint8_t* keep_out);
+
+}  // namespace ssp

@@ -1,0 +1,172 @@
+// ssp_sample.cu -- a9..a12: leverage estimates, probabilities, coins, reweighting and L_H.
+//
+// d_e = ||Z[v1] - Z[v2]||            compute_diff_norms   (sparsifier.rs:565-583)
+// p_e = min(beta w d^2 / denom, 1)   compute_probs        (sparsifier.rs:542-562)
+// keep iff coin_e < p_e              sample_and_reweight  (sparsifier.rs:635-680)
+// L_H = L_G + dL, exact zeros drop   apply_reweightings   (sparsifier.rs:682-691)
+//
+// The diff-norm reduction order is fixed (lane l sums columns l, l+32, ... with fma, then an xor
+// butterfly) and mirrored by the CPU oracle, so given the same Z the norms are bit-identical.
+#include "ssp_internal.cuh"
+
+namespace ssp {
+
+__global__ void __launch_bounds__(256) k_diff_norms(int64_t m, const int32_t* __restrict__ v1,
+                                                    const int32_t* __restrict__ v2, const double* __restrict__ Z,
+                                                    int32_t k, int64_t ldz, double* __restrict__ d) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < m; e += nw) {
+        const double* za = Z + (int64_t)v1[e] * ldz;
+        const double* zb = Z + (int64_t)v2[e] * ldz;
+        double s = 0.0;
+        for (int32_t j = lane; j < k; j += 32) {
+            const double x = __dsub_rn(za[j], zb[j]);
+            s = __fma_rn(x, x, s);
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+        if (lane == 0) d[e] = sqrt(s);
+    }
+}
+
+__global__ void k_probs(int64_t m, const double* __restrict__ w, const double* __restrict__ d, double beta,
+                        double denom, double* __restrict__ p) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
+        const double d2 = __dmul_rn(d[e], d[e]);
+        const double x = __ddiv_rn(__dmul_rn(__dmul_rn(beta, w[e]), d2), denom);
+        p[e] = (x < 1.0) ? x : 1.0;
+        if (x != x) p[e] = 1.0;
+    }
+}
+
+__global__ void k_coins(int64_t m, uint64_t seed, double* __restrict__ coins) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x)
+        coins[e] = edge_coin(seed, e);
+}
+
+// per edge: keep flag and the off-diagonal change X*-1 (Triplet::insert semantics)
+__global__ void k_edge_changes(int64_t m, const double* __restrict__ w, const double* __restrict__ p,
+                               const double* __restrict__ coins, int reweight, double* __restrict__ X,
+                               uint8_t* __restrict__ keep) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
+        const bool kept = coins[e] < p[e];
+        double x;
+        if (kept) {
+            const double t = reweight ? __ddiv_rn(w[e], p[e]) : __ddiv_rn(w[e], sqrt(p[e]));
+            const double change = __dsub_rn(w[e], t);
+            x = __dmul_rn(change, -1.0);
+        } else {
+            x = __dmul_rn(w[e], -1.0);
+        }
+        X[e] = x;
+        if (keep) keep[e] = kept ? 1 : 0;
+    }
+}
+
+// thread per vertex: diagonal change summed in edge order; then the L_H column, dropping exact zeros
+__global__ void k_lh_count(int64_t n, const int64_t* __restrict__ adj_ptr, const int32_t* __restrict__ adj_nbr,
+                           const int32_t* __restrict__ adj_eid, const double* __restrict__ X,
+                           const int64_t* __restrict__ lg_ptr, const int32_t* __restrict__ lg_idx,
+                           const double* __restrict__ lg_val, double* __restrict__ dchange,
+                           int32_t* __restrict__ cnt) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        double dc = 0.0;
+        for (int64_t p = adj_ptr[v]; p < adj_ptr[v + 1]; p++) dc = __dadd_rn(dc, X[adj_eid[p]]);
+        dchange[v] = dc;
+        int32_t c = 0;
+        int64_t a = adj_ptr[v];
+        for (int64_t t = lg_ptr[v]; t < lg_ptr[v + 1]; t++) {
+            double x;
+            if (lg_idx[t] == v) {
+                x = __dadd_rn(lg_val[t], dc);
+            } else {
+                x = __dadd_rn(lg_val[t], __dmul_rn(X[adj_eid[a]], -1.0));
+                a++;
+            }
+            c += (x != 0.0) ? 1 : 0;
+        }
+        cnt[v] = c;
+    }
+}
+
+__global__ void k_lh_fill(int64_t n, const int64_t* __restrict__ adj_ptr, const int32_t* __restrict__ adj_eid,
+                          const double* __restrict__ X, const int64_t* __restrict__ lg_ptr,
+                          const int32_t* __restrict__ lg_idx, const double* __restrict__ lg_val,
+                          const double* __restrict__ dchange, const int64_t* __restrict__ lh_ptr,
+                          int32_t* __restrict__ lh_idx, double* __restrict__ lh_val) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        int64_t a = adj_ptr[v];
+        int64_t q = lh_ptr[v];
+        const double dc = dchange[v];
+        for (int64_t t = lg_ptr[v]; t < lg_ptr[v + 1]; t++) {
+            double x;
+            if (lg_idx[t] == v) {
+                x = __dadd_rn(lg_val[t], dc);
+            } else {
+                x = __dadd_rn(lg_val[t], __dmul_rn(X[adj_eid[a]], -1.0));
+                a++;
+            }
+            if (x != 0.0) {
+                lh_idx[q] = lg_idx[t];
+                lh_val[q++] = x;
+            }
+        }
+    }
+}
+
+void diff_norms_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z, int32_t k,
+                       int64_t ldz, double* d) {
+    if (m == 0) return;
+    k_diff_norms<<<grid_for(m * 32, 256, 148 * 16), 256, 0, C.stream>>>(m, v1, v2, Z, k, ldz, d);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+}
+
+void probs_device(Context& C, int64_t m, const double* w, const double* d, double beta, double denom, double* p) {
+    if (m == 0) return;
+    k_probs<<<grid_for(m, 256), 256, 0, C.stream>>>(m, w, d, beta, denom, p);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+}
+
+void coins_device(Context& C, int64_t m, uint64_t seed, double* coins) {
+    if (m == 0) return;
+    k_coins<<<grid_for(m, 256), 256, 0, C.stream>>>(m, seed, coins);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+}
+
+int64_t sample_apply_device(Context& C, const DevGraph& G, const double* p, const double* coins, int reweight,
+                            int64_t** lh_ptr_out, int32_t** lh_idx_out, double** lh_val_out, uint8_t* keep) {
+    const int64_t n = G.n, m = G.m;
+    Workspace& W = C.ws;
+    double* X = W.get_t<double>("s_X", m + 1);
+    double* dchange = W.get_t<double>("s_dchange", n + 1);
+    int32_t* cnt = W.get_t<int32_t>("s_cnt", n + 1);
+    int64_t* lh_ptr = W.get_t<int64_t>("s_lh_ptr", n + 1);
+    int64_t* d_tot = W.get_t<int64_t>("s_tot", 1);
+    if (m > 0) {
+        k_edge_changes<<<grid_for(m, 256), 256, 0, C.stream>>>(m, G.w, p, coins, reweight, X, keep);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched++;
+    }
+    k_lh_count<<<grid_for(n, 128), 128, 0, C.stream>>>(n, G.adj_ptr, G.adj_nbr, G.adj_eid, X, G.lap_ptr, G.lap_idx,
+                                                       G.lap_val, dchange, cnt);
+    SSP_CHECK_LAUNCH();
+    SSP_CUDA(cudaMemsetAsync(cnt + n, 0, sizeof(int32_t), C.stream));
+    exclusive_scan_i32_to_i64(C, cnt, lh_ptr, n + 1, d_tot);
+    int64_t nnz = read_i64(C, d_tot);
+    int32_t* lh_idx = W.get_t<int32_t>("s_lh_idx", nnz + 1);
+    double* lh_val = W.get_t<double>("s_lh_val", nnz + 1);
+    k_lh_fill<<<grid_for(n, 128), 128, 0, C.stream>>>(n, G.adj_ptr, G.adj_eid, X, G.lap_ptr, G.lap_idx, G.lap_val,
+                                                      dchange, lh_ptr, lh_idx, lh_val);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched += 2;
+    *lh_ptr_out = lh_ptr;
+    *lh_idx_out = lh_idx;
+    *lh_val_out = lh_val;
+    return nnz;
+}
+
+}  // namespace ssp

@@ -1,0 +1,253 @@
+// ssp_util.cu -- deterministic device-wide scans and segmented sorts used by the
+// graph assembly and factorization stages.
+#include "ssp_internal.cuh"
+#include "ssp_sort.cuh"
+
+namespace ssp {
+
+// ---------------------------------------------------------------- scan
+// Three-phase exclusive scan over int64 with 4096-element tiles.
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+template <class TIn>
+__global__ void k_tile_sums(const TIn* in, int64_t n, int64_t* sums) {
+    __shared__ int64_t warp_sums[32];
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+    int64_t s = 0;
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        int64_t idx = base + (int64_t)i * SCAN_THREADS + threadIdx.x;
+        if (idx < n) s += (int64_t)in[idx];
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int64_t t = warp_sums[threadIdx.x];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (threadIdx.x == 0) sums[blockIdx.x] = t;
+    }
+}
+
+// Scans one tile in shared memory; adds `offsets[blockIdx.x]` (if non-null).
+template <class TIn>
+__global__ void k_tile_scan(const TIn* in, int64_t* out, int64_t n, const int64_t* offsets, int64_t* total) {
+    __shared__ int64_t warp_tot[32];
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    int64_t v[SCAN_ITEMS];
+    int64_t run = 0;
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        int64_t idx = base + i;
+        int64_t x = (idx < n) ? (int64_t)in[idx] : 0;
+        v[i] = run;
+        run += x;
+    }
+    // exclusive scan of `run` over the block
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int64_t incl = run;
+    for (int o = 1; o < 32; o <<= 1) {
+        int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int64_t t = warp_tot[lane];
+        int64_t ti = t;
+        for (int o = 1; o < 32; o <<= 1) {
+            int64_t u = __shfl_up_sync(0xffffffffu, ti, o);
+            if (lane >= o) ti += u;
+        }
+        warp_tot[lane] = ti - t;  // exclusive
+        if (lane == 31 && total && offsets == nullptr && gridDim.x == 1) *total = ti;
+    }
+    __syncthreads();
+    int64_t off = warp_tot[wid] + (incl - run) + (offsets ? offsets[blockIdx.x] : 0);
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        int64_t idx = base + i;
+        if (idx < n) out[idx] = off + v[i];
+    }
+    if (total && offsets != nullptr && blockIdx.x == gridDim.x - 1 && threadIdx.x == SCAN_THREADS - 1) {
+        *total = off + run;
+    }
+}
+
+template <class TIn>
+static void scan_impl(Context& C, const TIn* in, int64_t* out, int64_t n, int64_t* d_total) {
+    if (n <= 0) {
+        if (d_total) SSP_CUDA(cudaMemsetAsync(d_total, 0, sizeof(int64_t), C.stream));
+        return;
+    }
+    int64_t tiles = ceil_div<int64_t>(n, SCAN_TILE);
+    if (tiles == 1) {
+        k_tile_scan<TIn><<<1, SCAN_THREADS, 0, C.stream>>>(in, out, n, nullptr, d_total);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched++;
+        return;
+    }
+    // tile sums are staged in a per-depth buffer: (in may alias out)
+    static thread_local int depth = 0;
+    std::string tag = "scan_sums_" + std::to_string(depth);
+    int64_t* sums = C.ws.get_t<int64_t>(tag, tiles + 1);
+    k_tile_sums<TIn><<<(unsigned)tiles, SCAN_THREADS, 0, C.stream>>>(in, n, sums);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+    depth++;
+    try {
+        scan_impl<int64_t>(C, sums, sums, tiles, nullptr);
+    } catch (...) {
+        depth--;
+        throw;
+    }
+    depth--;
+    k_tile_scan<TIn><<<(unsigned)tiles, SCAN_THREADS, 0, C.stream>>>(in, out, n, sums, d_total);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+}
+
+void exclusive_scan_i64(Context& C, const int64_t* in, int64_t* out, int64_t n, int64_t* d_total) {
+    scan_impl<int64_t>(C, in, out, n, d_total);
+}
+void exclusive_scan_i32_to_i64(Context& C, const int32_t* in, int64_t* out, int64_t n, int64_t* d_total) {
+    scan_impl<int32_t>(C, in, out, n, d_total);
+}
+
+int64_t read_i64(Context& C, const int64_t* d_ptr) {
+    SSP_CUDA(cudaMemcpyAsync(C.h_pinned, d_ptr, sizeof(int64_t), cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    return C.h_pinned[0];
+}
+void read_i64s(Context& C, const int64_t* d_ptr, int64_t* host, int cnt) {
+    SSP_CUDA(cudaMemcpyAsync(C.h_pinned, d_ptr, sizeof(int64_t) * cnt, cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    for (int i = 0; i < cnt; i++) host[i] = C.h_pinned[i];
+}
+
+// ---------------------------------------------------------------- segmented sort
+struct KeyLessI32 {
+    __device__ bool operator()(const int32_t& a, const int32_t& b) const { return a < b; }
+};
+
+// segments of length <= 32: one warp each, in registers
+template <bool PAIRS>
+__global__ void k_segsort_warp(int32_t* keys, double* vals, const int64_t* seg_start, const int32_t* seg_len,
+                               int64_t nseg) {
+    int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (w >= nseg) return;
+    int32_t len = seg_len[w];
+    if (len <= 1 || len > 32) return;
+    int64_t s = seg_start[w];
+    int32_t k = lane < len ? keys[s + lane] : INT32_MAX;
+    double v = (PAIRS && lane < len) ? vals[s + lane] : 0.0;
+    warp_bitonic_kv(k, v, lane, KeyLessI32());
+    if (lane < len) {
+        keys[s + lane] = k;
+        if (PAIRS) vals[s + lane] = v;
+    }
+}
+
+// segments longer than 32: one block each, bitonic over `cap` padded slots in shared memory
+// (or in a global scratch slice when cap exceeds the shared budget).
+template <bool PAIRS>
+__global__ void k_segsort_block(int32_t* keys, double* vals, const int64_t* seg_start, const int32_t* seg_len,
+                                const int32_t* list, int64_t nlist, int32_t cap, int32_t* gkeys, double* gvals) {
+    extern __shared__ unsigned char smem[];
+    for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
+        int64_t sg = list[li];
+        int32_t len = seg_len[sg];
+        int64_t s = seg_start[sg];
+        int P = 64;
+        while (P < len) P <<= 1;
+        int32_t* sk;
+        double* sv;
+        if (gkeys) {
+            sk = gkeys + (int64_t)blockIdx.x * cap;
+            sv = gvals + (int64_t)blockIdx.x * cap;
+        } else {
+            sv = (double*)smem;
+            sk = (int32_t*)(smem + sizeof(double) * (size_t)(PAIRS ? cap : 0));
+        }
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            sk[i] = i < len ? keys[s + i] : INT32_MAX;
+            if (PAIRS) sv[i] = i < len ? vals[s + i] : 0.0;
+        }
+        __syncthreads();
+        block_bitonic_kv<PAIRS>(sk, sv, P, KeyLessI32());
+        for (int i = threadIdx.x; i < len; i += blockDim.x) {
+            keys[s + i] = sk[i];
+            if (PAIRS) vals[s + i] = sv[i];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_seg_classify(const int32_t* seg_len, int64_t nseg, int32_t lim_smem, int32_t* list_mid,
+                               int64_t* cnt_mid, int32_t* list_big, int64_t* cnt_big) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nseg; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t len = seg_len[i];
+        if (len <= 32) continue;
+        if (len <= lim_smem) list_mid[atomicAdd((unsigned long long*)cnt_mid, 1ull)] = (int32_t)i;
+        else list_big[atomicAdd((unsigned long long*)cnt_big, 1ull)] = (int32_t)i;
+    }
+}
+
+template <bool PAIRS>
+static void segsort_impl(Context& C, int32_t* keys, double* vals, const int64_t* seg_start, const int32_t* seg_len,
+                         int64_t nseg, int32_t max_len) {
+    if (nseg <= 0 || max_len <= 1) return;
+    {
+        int threads = 256;
+        int64_t blocks = ceil_div<int64_t>(nseg * 32, threads);
+        k_segsort_warp<PAIRS><<<(unsigned)blocks, threads, 0, C.stream>>>(keys, vals, seg_start, seg_len, nseg);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched++;
+    }
+    if (max_len <= 32) return;
+    const int32_t lim_smem = PAIRS ? 8192 : 16384;
+    int32_t* list_mid = C.ws.get_t<int32_t>("segsort_mid", nseg);
+    int32_t* list_big = C.ws.get_t<int32_t>("segsort_big", nseg);
+    int64_t* cnts = C.ws.get_t<int64_t>("segsort_cnt", 2);
+    SSP_CUDA(cudaMemsetAsync(cnts, 0, 2 * sizeof(int64_t), C.stream));
+    k_seg_classify<<<grid_for(nseg, 256), 256, 0, C.stream>>>(seg_len, nseg, lim_smem, list_mid, cnts, list_big,
+                                                               cnts + 1);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+    int64_t hc[2];
+    read_i64s(C, cnts, hc, 2);
+    if (hc[0] > 0) {
+        int32_t cap = 64;
+        while (cap < std::min(max_len, lim_smem)) cap <<= 1;
+        size_t smem = (size_t)cap * (sizeof(int32_t) + (PAIRS ? sizeof(double) : 0));
+        SSP_CUDA(cudaFuncSetAttribute(k_segsort_block<PAIRS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        int blocks = (int)std::min<int64_t>(hc[0], 148 * 4);
+        k_segsort_block<PAIRS><<<blocks, 512, smem, C.stream>>>(keys, vals, seg_start, seg_len, list_mid, hc[0],
+                                                                cap, nullptr, nullptr);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched++;
+    }
+    if (hc[1] > 0) {
+        int32_t cap = 64;
+        while (cap < max_len) cap <<= 1;
+        int blocks = (int)std::min<int64_t>(hc[1], 64);
+        int32_t* gk = C.ws.get_t<int32_t>("segsort_gk", (size_t)cap * blocks);
+        double* gv = PAIRS ? C.ws.get_t<double>("segsort_gv", (size_t)cap * blocks) : nullptr;
+        k_segsort_block<PAIRS><<<blocks, 1024, 0, C.stream>>>(keys, vals, seg_start, seg_len, list_big, hc[1], cap,
+                                                              gk, gv);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched++;
+    }
+}
+
+void segsort_i32(Context& C, int32_t* keys, const int64_t* seg_start, const int32_t* seg_len, int64_t nseg,
+                 int32_t max_len) {
+    segsort_impl<false>(C, keys, nullptr, seg_start, seg_len, nseg, max_len);
+}
+void segsort_pairs_i32_f64(Context& C, int32_t* keys, double* vals, const int64_t* seg_start,
+                           const int32_t* seg_len, int64_t nseg, int32_t max_len) {
+    segsort_impl<true>(C, keys, vals, seg_start, seg_len, nseg, max_len);
+}
+
+}  // namespace ssp

@@ -1,0 +1,272 @@
+"""GPU parity: every stage of the CUDA path against the CPU oracle, through the C ABI.
+
+Bit-exact: edges, L_G, sketch, factor (L, D, levels), diff norms given Z, probabilities, coins, keep set and
+L_H given p and coins.  Tolerance: M^{-1} application (1e-12 relative) and PCG solutions (1e-7 relative on
+edge differences at tol 1e-10; the residual itself must meet the requested tolerance).
+"""
+import math
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.csgraph as csg
+
+from conftest import rand_graph
+
+pytestmark = pytest.mark.gpu
+
+
+def _csc(ssp, A):
+    return ssp.CSC.from_scipy(A)
+
+
+GRAPHS = {
+    "rand300": lambda ssp: _csc(ssp, rand_graph(300, 1500, 1)),
+    "rand2k_disconnected": lambda ssp: _csc(ssp, rand_graph(2000, 2200, 2)),
+    "grid40": lambda ssp: ssp.gen_grid2d(40, 40),
+    "grid3d": lambda ssp: ssp.gen_grid3d(10, 9, 8, -3, 3, 2),
+    "er5k": lambda ssp: ssp.gen_er(5000, 20.0, 0.5, 2.0, 1),
+}
+
+
+def _oracle_graph(ora, G):
+    v1, v2, w = ora.extract_edges(G.n, G.colptr, G.rowidx, G.values)
+    lg = ora.laplacian(G.n, v1, v2, w)
+    return (v1, v2, w), lg
+
+
+@pytest.mark.parametrize("name", list(GRAPHS))
+def test_graph_assembly_bit_exact(ssp, ora, ctx, name):
+    G = GRAPHS[name](ssp)
+    (v1, v2, w), L = ssp.stage_graph(ctx, G)
+    (o1, o2, ow), (cp, ri, va) = _oracle_graph(ora, G)
+    assert np.array_equal(v1, o1) and np.array_equal(v2, o2) and np.array_equal(w, ow)
+    assert np.array_equal(L.colptr, cp) and np.array_equal(L.rowidx, ri) and np.array_equal(L.values, va)
+
+
+@pytest.mark.parametrize("k", [1, 7, 256, 300, 885])
+@pytest.mark.parametrize("uniform", [False, True])
+def test_sketch_bit_exact(ssp, ora, ctx, k, uniform):
+    G = GRAPHS["rand300"](ssp)
+    (v1, v2, w), _ = _oracle_graph(ora, G)
+    scale = 1.0 / math.sqrt(k) if not uniform else math.sqrt(3.0)
+    Y = ssp.stage_sketch(ctx, G.n, v1, v2, w, k, scale, 17, uniform)
+    Yo = ora.sketch(G.n, v1, v2, w, k, scale, 17, uniform)
+    assert np.array_equal(Y, Yo)
+
+
+def _canon_cols(colptr, rows, vals, n):
+    return [sorted(zip(rows[colptr[v]:colptr[v + 1]].tolist(), vals[colptr[v]:colptr[v + 1]].tolist()))
+            for v in range(n)]
+
+
+@pytest.mark.parametrize("name", ["rand300", "rand2k_disconnected", "grid40", "grid3d", "er5k"])
+@pytest.mark.parametrize("dense", [0, 64, 4096])
+def test_factor_bit_exact(ssp, ora, ctx, name, dense):
+    G = GRAPHS[name](ssp)
+    (v1, v2, w), (cp, ri, va) = _oracle_graph(ora, G)
+    lap = ssp.CSC(G.n, cp, ri, va)
+    seed = 5
+    f = ssp.stage_factor(ctx, lap, seed, dense)
+    o = ora.Factor(G.n, cp, ri, va, seed, dense)
+    assert f["num_levels"] == o.num_levels
+    assert np.array_equal(f["level"], o.level)
+    assert np.array_equal(f["D"], o.D)
+    assert _canon_cols(f["colptr"], f["rows"], f["vals"], G.n) == _canon_cols(o.colstart, o.rows, o.vals, G.n)
+
+
+def test_factor_deterministic(ssp, ora, ctx):
+    G = GRAPHS["er5k"](ssp)
+    (_, _, _), (cp, ri, va) = _oracle_graph(ora, G)
+    lap = ssp.CSC(G.n, cp, ri, va)
+    a = ssp.stage_factor(ctx, lap, 9, 256)
+    b = ssp.stage_factor(ctx, lap, 9, 256)
+    for key in ("colptr", "D", "level"):
+        assert np.array_equal(a[key], b[key])
+
+
+@pytest.mark.parametrize("dense", [0, 128])
+def test_precond_matches_oracle(ssp, ora, ctx, dense):
+    G = GRAPHS["grid3d"](ssp)
+    (_, _, _), (cp, ri, va) = _oracle_graph(ora, G)
+    lap = ssp.CSC(G.n, cp, ri, va)
+    rng = np.random.default_rng(0)
+    R = rng.standard_normal((G.n, 19))
+    Z = ssp.stage_precond(ctx, lap, 3, R, dense)
+    o = ora.Factor(G.n, cp, ri, va, 3, dense)
+    Zo = np.column_stack([o.precond(R[:, j].copy()) for j in range(R.shape[1])])
+    assert np.abs(Z - Zo).max() <= 1e-12 * np.abs(Zo).max()
+
+
+@pytest.mark.parametrize("name", ["rand300", "grid40", "er5k"])
+def test_pcg_matches_oracle(ssp, ora, ctx, name):
+    G = GRAPHS[name](ssp)
+    (v1, v2, w), (cp, ri, va) = _oracle_graph(ora, G)
+    lap = ssp.CSC(G.n, cp, ri, va)
+    k = 13
+    Y = ora.sketch(G.n, v1, v2, w, k, 1 / math.sqrt(k), 3)
+    Z, rep = ctx.solve_lap(lap, Y, tol=1e-10, abs_tol=0.0, max_iters=400, factor_seed=4, dense_threshold=256)
+    F = ora.Factor(G.n, cp, ri, va, 4, 256)
+    Zo, it, rel, rc = ora.pcg(G.n, cp, ri, va, F, Y, 1e-10, 0.0, 400)
+    assert rc == 0 and rep["not_converged"] == 0 and rep["max_relres"] < 1e-8
+    dz, do = Z[v1] - Z[v2], Zo[v1] - Zo[v2]
+    assert np.abs(dz - do).max() <= 1e-7 * np.abs(do).max()
+    assert abs(rep["max_iters_used"] - it.max()) <= 2
+
+
+def test_run_solve_lap_dropin(ssp, ora, ctx):
+    """ffi::run_solve_lap semantics (lib.rs:103, example.cc:668-703): FlattenedVec row-major n x k in and
+    out, ||r||^2 <= 2e-7 stop, success iff relative residual < 0.01."""
+    G = GRAPHS["grid40"](ssp)
+    (v1, v2, w), (cp, ri, va) = _oracle_graph(ora, G)
+    k = 24
+    Y = ora.sketch(G.n, v1, v2, w, k, math.sqrt(3.0), 0)
+    sol, nr, nc = ssp.run_solve_lap((Y.ravel(), G.n, k), cp.astype(np.int32), ri, va, "", G.n, False)
+    assert (nr, nc) == (G.n, k)
+    Z = sol.reshape(G.n, k)
+    Lg = sp.csc_matrix((va, ri, cp), shape=(G.n, G.n))
+    b = Y - Y.mean(0)
+    res = np.linalg.norm(b - Lg @ Z, axis=0)
+    assert (res <= math.sqrt(2e-7) * 1.0000001).all()
+    assert (res / np.linalg.norm(b, axis=0) < 0.01).all()
+
+
+def test_run_solve_lap_not_converged_is_an_error(ssp, ora):
+    G = GRAPHS["grid3d"](ssp)
+    (v1, v2, w), (cp, ri, va) = _oracle_graph(ora, G)
+    lap = ssp.CSC(G.n, cp, ri, va)
+    ctx2 = ssp.Context(0)
+    Y = ora.sketch(G.n, v1, v2, w, 4, 1.0, 0)
+    with pytest.raises(ssp.SspError) as e:
+        ctx2.solve_lap(lap, Y, tol=1e-12, abs_tol=0.0, max_iters=1)
+    assert e.value.code == -4
+    ctx2.close()
+
+
+def test_leverage_stages_bit_exact(ssp, ora, ctx):
+    G = GRAPHS["er5k"](ssp)
+    (v1, v2, w), _ = _oracle_graph(ora, G)
+    rng = np.random.default_rng(3)
+    Z = rng.standard_normal((G.n, 77))
+    d = ssp.stage_diff_norms(ctx, v1, v2, Z)
+    assert np.array_equal(d, ora.diff_norms(v1, v2, Z))
+    p = ssp.stage_probs(ctx, w, d, 123.4, 77.0)
+    assert np.array_equal(p, ora.probs(w, d, 123.4, 77.0))
+    c = ssp.stage_coins(ctx, len(w), 99)
+    assert np.array_equal(c, ora.coins(99, len(w)))
+
+
+@pytest.mark.parametrize("reweight", [0, 1])
+def test_sample_apply_bit_exact(ssp, ora, ctx, reweight):
+    G = GRAPHS["grid3d"](ssp)
+    (v1, v2, w), lg = _oracle_graph(ora, G)
+    rng = np.random.default_rng(reweight)
+    p = rng.uniform(0, 1, len(w))
+    p[::7] = 1.0
+    p[::11] = 0.0
+    coins = ora.coins(5, len(w))
+    H, keep = ssp.stage_sample_apply(ctx, G, p, coins, reweight)
+    (hcp, hri, hva), okeep = ora.sample_apply(G.n, v1, v2, w, p, coins, reweight, lg)
+    assert np.array_equal(keep, okeep)
+    assert np.array_equal(H.colptr, hcp) and np.array_equal(H.rowidx, hri) and np.array_equal(H.values, hva)
+
+
+def _oracle_pipeline(ora, ssp, G, params):
+    (v1, v2, w), (cp, ri, va) = _oracle_graph(ora, G)
+    n = G.n
+    k = params.jl_dim(n)
+    s = params.jl_scale(k)
+    Y = ora.sketch(n, v1, v2, w, k, s, params.sketch_seed, params.sketch_uniform)
+    F = ora.Factor(n, cp, ri, va, params.factor_seed, params.dense_threshold)
+    Z, it, rel, rc = ora.pcg(n, cp, ri, va, F, Y, params.pcg_tol, params.pcg_abs_tol, params.pcg_max_iters)
+    d = ora.diff_norms(v1, v2, Z)
+    denom = k * s * s if params.prob_variance_correction else float(k)
+    p = ora.probs(w, d, params.beta(n), denom)
+    coins = ora.coins(params.sampling_seed, len(w))
+    (hcp, hri, hva), keep = ora.sample_apply(n, v1, v2, w, p, coins, params.reweight, (cp, ri, va))
+    return dict(k=k, Z=Z, d=d, p=p, keep=keep, H=(hcp, hri, hva), iters=it, v=(v1, v2, w), lg=(cp, ri, va))
+
+
+def test_sparsify_config_grid2d_100(ssp, ora, ctx):
+    """Configuration C1: 2-D 4-neighbour grid 100x100, unit weights, eps 0.5, k = ceil(24 ln n / eps^2) = 885
+    columns of +-1/sqrt(k) Philox signs (seed 0), PCG tol 1e-8."""
+    G = ssp.gen_grid2d(100, 100)
+    prm = ssp.SparsifierParameters.baseline(0.5, pcg_tol=1e-8)
+    H, st = ctx.sparsify(G, prm)
+    assert st["k"] == 885 and st["m_in"] == 19_800
+    o = _oracle_pipeline(ora, ssp, G, prm)
+    # leverage estimates agree to the solver tolerance; p equals wherever it is clipped at 1
+    assert st["pcg_max_relres"] < 1e-7
+    sp_run = ssp.Sparsifier(G, prm, ctx)
+    sp_run.sparsify()
+    Hm = sp_run.current_laplacian.to_scipy()
+    Ho = sp.csc_matrix((o["H"][2], o["H"][1], o["H"][0]), shape=(G.n, G.n))
+    assert (Hm != 0).nnz == (Ho != 0).nnz
+    assert abs(Hm - Ho).max() <= 1e-12 * abs(Ho).max()
+    assert st["m_out"] == int(o["keep"].sum())
+
+
+def test_spectral_check_dense_graph(ssp, ora, ctx):
+    """A graph that actually gets sparsified: K_300 with eps = 0.7 and unbiased w/p reweighting.
+    Every probe x^T L_H x / x^T L_G x and every eigenvalue of L_G^+ L_H must lie within 1 +- eps."""
+    n = 300
+    A = sp.csc_matrix(np.triu(np.ones((n, n)), 1))
+    A = (A + A.T).tocsc()
+    A.sort_indices()
+    G = ssp.CSC.from_scipy(A)
+    eps = 0.7
+    prm = ssp.SparsifierParameters.baseline(eps, pcg_tol=1e-10)
+    prm.reweight = ssp.SSP_REWEIGHT_INV_P
+    H, st = ctx.sparsify(G, prm)
+    assert st["m_out"] < 0.6 * st["m_in"]
+    Lg = sp.diags(np.asarray(A.sum(0)).ravel()) - A
+    Lh = H.to_scipy()
+    rng = np.random.default_rng(0)
+    for _ in range(100):
+        x = rng.uniform(-1, 1, n)
+        x -= x.mean()
+        r = (x @ (Lh @ x)) / (x @ (Lg @ x))
+        assert 1 - eps <= r <= 1 + eps
+    Lgd, Lhd = Lg.toarray(), Lh.toarray()
+    ev = np.linalg.eigvals(np.linalg.pinv(Lgd) @ Lhd).real
+    ev = np.sort(ev)[1:]  # drop the shared nullspace
+    assert ev.min() >= 1 - eps and ev.max() <= 1 + eps
+
+
+def test_sparsify_deterministic(ssp, ctx):
+    G = ssp.gen_er(20_000, 20.0, 0.5, 2.0, 7)
+    prm = ssp.SparsifierParameters.baseline(0.5, pcg_tol=1e-6)
+    H1, s1 = ctx.sparsify(G, prm)
+    H2, s2 = ctx.sparsify(G, prm)
+    assert np.array_equal(H1.colptr, H2.colptr) and np.array_equal(H1.values, H2.values)
+    assert s1["pcg_mean_iters"] == s2["pcg_mean_iters"]
+
+
+def test_invalid_inputs_rejected(ssp, ctx):
+    A = rand_graph(100, 300, 4)
+    bad = A.copy()
+    bad.data = -bad.data
+    with pytest.raises(ssp.SspError) as e:
+        ctx.sparsify(ssp.CSC.from_scipy(bad), ssp.SparsifierParameters.cli(0.5))
+    assert e.value.code == -1
+    G = ssp.CSC.from_scipy(A)
+    ri = G.rowidx.copy()
+    s0, s1 = G.colptr[3], G.colptr[4]
+    ri[s0], ri[s0 + 1] = ri[s0 + 1], ri[s0]
+    with pytest.raises(ssp.SspError):
+        ctx.sparsify(ssp.CSC(G.n, G.colptr, ri, G.values), ssp.SparsifierParameters.cli(0.5))
+    # the context stays usable after a rejected call
+    H, st = ctx.sparsify(G, ssp.SparsifierParameters.cli(0.5))
+    assert st["m_in"] == G.nnz // 2
+
+
+def test_sparsify_dataset_mtx(ssp, tmp_path):
+    G = ssp.gen_grid2d(30, 30)
+    src, dst = str(tmp_path / "in.mtx"), str(tmp_path / "out.mtx")
+    ssp.write_mtx(src, G)
+    st = ssp.sparsify_dataset(src, "grid", dst, 0.5, False, 0, 0, True)
+    H = ssp.read_mtx(dst)
+    assert st.original_num_edges == 2 * 30 * 29
+    assert H.num_edges() == st.final_num_edges
+    Lh = H.to_scipy()
+    assert np.abs(np.asarray(Lh.sum(axis=0))).max() < 1e-9
