@@ -105,6 +105,9 @@ typedef struct {
     int32_t pcg_max_iters;   /* reference: 400 (custom_cg.hpp:153) */
     uint64_t factor_seed;    /* elimination order + fill sampling */
     int64_t dense_threshold; /* live-vertex count that switches elimination to the dense tail */
+    int64_t factor_max_degree; /* stop eliminating once the Schur complement's average degree exceeds
+                                  this; the rest is preconditioned by its diagonal (0 = eliminate all) */
+    int32_t jl_dim_override;   /* > 0: use exactly this many JL columns instead of jl_dim_rule */
 } ssp_params;
 
 typedef struct {
@@ -136,6 +139,7 @@ typedef struct {
     uint64_t factor_seed;
     int64_t dense_threshold;
     int32_t verbose;
+    int64_t factor_max_degree;
 } ssp_solve_opts;
 
 typedef struct {
@@ -216,11 +220,12 @@ int ssp_stage_sketch(ssp_context* ctx, int64_t n, int64_t m, const int32_t* v1, 
                      double* Y);
 /* factor of a Laplacian: column CSC of L (vertex ids, strictly lower, unit diagonal implicit), D, levels.
  * Output arrays are caller-allocated host buffers; call once with rows==NULL to get nnz. */
-int ssp_stage_factor(ssp_context* ctx, const ssp_csc* lap, uint64_t seed, int64_t dense_threshold, int64_t* nnz,
-                     int64_t* colptr, int32_t* rows, double* vals, double* D, int32_t* level, int32_t* num_levels);
+int ssp_stage_factor(ssp_context* ctx, const ssp_csc* lap, uint64_t seed, int64_t dense_threshold,
+                     int64_t max_degree, int64_t* nnz, int64_t* colptr, int32_t* rows, double* vals, double* D,
+                     int32_t* level, int32_t* num_levels);
 /* M^{-1} applied to the k columns of R (host, row-major n x k) with the factor of `lap` */
 int ssp_stage_precond(ssp_context* ctx, const ssp_csc* lap, uint64_t seed, int64_t dense_threshold,
-                      const double* R, int32_t k, double* Zout);
+                      int64_t max_degree, const double* R, int32_t k, double* Zout);
 int ssp_stage_diff_norms(ssp_context* ctx, int64_t n, int64_t m, const int32_t* v1, const int32_t* v2,
                          const double* Z, int32_t k, int32_t mem, double* d);
 int ssp_stage_probs(ssp_context* ctx, int64_t m, const double* w, const double* d, double beta, double denom,

@@ -56,7 +56,7 @@ def lib():
         L.ora_sketch.argtypes = [ctypes.c_int64, ctypes.c_int64, i32p, i32p, f64p, ctypes.c_int32,
                                  ctypes.c_double, ctypes.c_uint64, ctypes.c_int, f64p]
         L.ora_factor.argtypes = [ctypes.c_int64, i64p, i32p, f64p, ctypes.c_uint64, ctypes.c_int64,
-                                 ctypes.POINTER(_Factor)]
+                                 ctypes.c_int64, ctypes.POINTER(_Factor)]
         L.ora_factor.restype = ctypes.c_int
         L.ora_factor_free.argtypes = [ctypes.POINTER(_Factor)]
         L.ora_factor_export.argtypes = [ctypes.POINTER(_Factor), i64p, i32p, f64p, f64p, i32p, i32p]
@@ -133,12 +133,12 @@ def sketch(n, v1, v2, w, k, scale, seed, uniform=False):
 class Factor:
     """L (strictly lower, columns = vertex ids), D, levels and elimination order."""
 
-    def __init__(self, n, colptr, rowidx, val, seed, dense_threshold=0):
+    def __init__(self, n, colptr, rowidx, val, seed, dense_threshold=0, max_degree=0):
         self._f = _Factor()
         colptr = np.ascontiguousarray(colptr, np.int64)
         rowidx = np.ascontiguousarray(rowidx, np.int32)
         val = np.ascontiguousarray(val, np.float64)
-        rc = lib().ora_factor(n, colptr, rowidx, val, seed, dense_threshold, ctypes.byref(self._f))
+        rc = lib().ora_factor(n, colptr, rowidx, val, seed, dense_threshold, max_degree, ctypes.byref(self._f))
         if rc != 0:
             raise RuntimeError("oracle factorization failed")
         nnz = self._f.nnz

@@ -214,10 +214,12 @@ void ora_sketch(int64_t n, int64_t m, const int32_t* v1, const int32_t* v2, cons
  *    sequential carry between chunks (the CUDA warp scan).
  *  - u = Philox(seed, column, slot) instead of mt19937(random_device()).
  *  - dense tail: once at most `dense_threshold` vertices are live at a level
- *    boundary, the live Schur complement is merged into a dense matrix W and the
+ *    boundary and the next frontier holds at most 8 vertices (the Schur complement
+ *    has become dense), the live Schur complement is merged into a dense matrix W and the
  *    remaining vertices are eliminated one per level in key order, with fill added
  *    to W in elimination order.
  */
+#define ORA_DENSE_FRONTIER_MAX 8
 typedef struct { int32_t u; double w; } ent_t;
 
 typedef struct { ent_t* e; int64_t n, cap; } bag_t;
@@ -332,7 +334,7 @@ static int cmp_i32(const void* x, const void* y) {
 }
 
 int ora_factor(int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,
-               uint64_t seed, int64_t dense_threshold, ora_factor_t* out) {
+               uint64_t seed, int64_t dense_threshold, int64_t max_degree, ora_factor_t* out) {
     memset(out, 0, sizeof(*out));
     out->n = n;
     bag_t* bag = calloc((size_t)n + 1, sizeof(bag_t));
@@ -346,6 +348,8 @@ int ora_factor(int64_t n, const int64_t* colptr, const int32_t* rowidx, const do
                 bag_push(&bag[r], (int32_t)c, w);
             }
         }
+    int64_t live_entries = 0;
+    for (int64_t v = 0; v < n; v++) live_entries += bag[v].n;
     uint64_t* prio = malloc(sizeof(uint64_t) * (size_t)(n + 1));
     for (int64_t v = 0; v < n; v++) prio[v] = ora_priority(seed, v);
     g_prio = prio;
@@ -364,8 +368,12 @@ int ora_factor(int64_t n, const int64_t* colptr, const int32_t* rowidx, const do
     for (int64_t v = 0; v < n; v++) if (count[v] == 0) frontier[nfr++] = (int32_t)v;
     fill_t* fills = NULL; int64_t nf = 0, fcap = 0;
     int32_t lvl = 0;
+    int truncated = 0;
     while (nfr > 0) {
-        if (dense_threshold > 0 && (n - neliminated) <= dense_threshold) break;
+        /* truncation: the live Schur complement is too dense to be worth eliminating */
+        if (max_degree > 0 && live_entries > max_degree * (n - neliminated)) { truncated = 1; break; }
+        /* dense tail once few vertices remain and the frontier has collapsed */
+        if (dense_threshold > 0 && (n - neliminated) <= dense_threshold && nfr <= ORA_DENSE_FRONTIER_MAX) break;
         qsort(frontier, (size_t)nfr, sizeof(int32_t), cmp_i32);
         nf = 0;
         for (int64_t f = 0; f < nfr; f++) {
@@ -378,9 +386,11 @@ int ora_factor(int64_t n, const int64_t* colptr, const int32_t* rowidx, const do
             int64_t mc = merge_entries(E, cnt);
             eliminate_merged(seed, v, E, mc, &cols[v], &fills, &nf, &fcap);
             free(E);
+            live_entries -= 2 * cnt;
             out->level[v] = lvl;
             out->order[neliminated++] = v;
         }
+        live_entries += 2 * nf;
         for (int64_t f = 0; f < nfr; f++) dead[frontier[f]] = 1;
         /* fill: both directions into the bags; the endpoint with the larger key counts it */
         nnext = 0;
@@ -410,7 +420,28 @@ int ora_factor(int64_t n, const int64_t* colptr, const int32_t* rowidx, const do
         lvl++;
     }
     out->dense_start = (int32_t)neliminated;
-    if (neliminated < n) {
+    if (truncated) {
+        /* remaining vertices: one final level, no L entries, D = sum of the merged live weights (row order) */
+        int32_t* rem = malloc(sizeof(int32_t) * (size_t)(n - neliminated + 1));
+        int64_t t = 0;
+        for (int64_t v = 0; v < n; v++) if (!dead[v]) rem[t++] = (int32_t)v;
+        for (int64_t i = 0; i < t; i++) {
+            int32_t v = rem[i];
+            int64_t cnt = 0;
+            ent_t* E = malloc(sizeof(ent_t) * (size_t)(bag[v].n + 1));
+            for (int64_t q = 0; q < bag[v].n; q++)
+                if (!dead[bag[v].e[q].u]) E[cnt++] = bag[v].e[q];
+            int64_t mc = merge_entries(E, cnt);
+            double d = 0.0;
+            for (int64_t q = 0; q < mc; q++) d = d + E[q].w;
+            free(E);
+            cols[v].cnt = 0; cols[v].rows = NULL; cols[v].vals = NULL; cols[v].D = d;
+            out->level[v] = lvl;
+            out->order[neliminated++] = v;
+        }
+        free(rem);
+        lvl++;
+    } else if (neliminated < n) {
         /* dense tail */
         int64_t T = n - neliminated;
         int32_t* rem = malloc(sizeof(int32_t) * (size_t)T);

@@ -68,9 +68,12 @@ typedef struct {
 
 /* Lower-triangle input: CSC of L_G (full), only entries with row > col are used, |value| is the weight
  * (pre_process.hpp:734-812).  dense_threshold: switch to the dense sequential phase once at most this
- * many vertices are live at a level boundary (0 = never). */
+ * many vertices are live at a level boundary and the frontier holds at most 8 vertices (0 = never). */
+/* max_degree: at a level boundary, once the live entries exceed max_degree times the live vertices
+ * (average Schur-complement degree), stop: every remaining vertex goes into one final level with no L
+ * entries and D = the sum of its merged live weights in row order (0 = eliminate everything). */
 int ora_factor(int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,
-               uint64_t seed, int64_t dense_threshold, ora_factor_t* out);
+               uint64_t seed, int64_t dense_threshold, int64_t max_degree, ora_factor_t* out);
 void ora_factor_free(ora_factor_t* f);
 /* accessors for ctypes */
 int64_t ora_factor_nnz(const ora_factor_t* f);

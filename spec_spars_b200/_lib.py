@@ -55,7 +55,8 @@ class _Params(ctypes.Structure):
                 ("jl_dim_rule", ctypes.c_int32), ("jl_scale_rule", ctypes.c_int32),
                 ("prob_variance_correction", ctypes.c_int32), ("reweight", ctypes.c_int32),
                 ("pcg_tol", ctypes.c_double), ("pcg_abs_tol", ctypes.c_double), ("pcg_max_iters", ctypes.c_int32),
-                ("factor_seed", ctypes.c_uint64), ("dense_threshold", ctypes.c_int64)]
+                ("factor_seed", ctypes.c_uint64), ("dense_threshold", ctypes.c_int64),
+                ("factor_max_degree", ctypes.c_int64), ("jl_dim_override", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -71,7 +72,8 @@ class _Stats(ctypes.Structure):
 
 class _SolveOpts(ctypes.Structure):
     _fields_ = [("tol", ctypes.c_double), ("abs_tol", ctypes.c_double), ("max_iters", ctypes.c_int32),
-                ("factor_seed", ctypes.c_uint64), ("dense_threshold", ctypes.c_int64), ("verbose", ctypes.c_int32)]
+                ("factor_seed", ctypes.c_uint64), ("dense_threshold", ctypes.c_int64), ("verbose", ctypes.c_int32),
+                ("factor_max_degree", ctypes.c_int64)]
 
 
 class _SolveReport(ctypes.Structure):
@@ -125,9 +127,9 @@ def lib():
             "ssp_stage_graph": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(I64), ctypes.POINTER(I64), P, P, P, P, P, P],
                                 ctypes.c_int),
             "ssp_stage_sketch": ([P, I64, I64, P, P, P, I32, I32, DBL, U64, I32, P], ctypes.c_int),
-            "ssp_stage_factor": ([P, ctypes.POINTER(_Csc), U64, I64, ctypes.POINTER(I64), P, P, P, P, P,
+            "ssp_stage_factor": ([P, ctypes.POINTER(_Csc), U64, I64, I64, ctypes.POINTER(I64), P, P, P, P, P,
                                   ctypes.POINTER(I32)], ctypes.c_int),
-            "ssp_stage_precond": ([P, ctypes.POINTER(_Csc), U64, I64, P, I32, P], ctypes.c_int),
+            "ssp_stage_precond": ([P, ctypes.POINTER(_Csc), U64, I64, I64, P, I32, P], ctypes.c_int),
             "ssp_stage_diff_norms": ([P, I64, I64, P, P, P, I32, I32, P], ctypes.c_int),
             "ssp_stage_probs": ([P, I64, P, P, DBL, DBL, I32, P], ctypes.c_int),
             "ssp_stage_coins": ([P, I64, U64, I32, P], ctypes.c_int),
@@ -386,11 +388,11 @@ class Context:
         return (out.nnz, out.colptr, out.rowidx, out.values), _stats_dict(st)
 
     def solve_lap(self, lap, Y, tol=0.0, abs_tol=np.sqrt(2e-7), max_iters=400, factor_seed=0,
-                  dense_threshold=4096, raise_on_failure=True):
+                  dense_threshold=4096, max_degree=64, raise_on_failure=True):
         Y = np.ascontiguousarray(Y, np.float64)
         n, k = Y.shape
         Z = np.zeros_like(Y)
-        o = _SolveOpts(tol, abs_tol, max_iters, factor_seed, dense_threshold, 0)
+        o = _SolveOpts(tol, abs_tol, max_iters, factor_seed, dense_threshold, 0, max_degree)
         rep = _SolveReport()
         s = lap._struct()
         rc = lib().ssp_solve_lap(self._h, ctypes.byref(s), _ptr(Y), k, _ptr(Z), SSP_MEM_HOST, ctypes.byref(o),
@@ -497,28 +499,29 @@ def stage_sketch(ctx, n, v1, v2, w, k, scale, seed, uniform=False):
     return Y
 
 
-def stage_factor(ctx, lap, seed, dense_threshold=4096):
+def stage_factor(ctx, lap, seed, dense_threshold=4096, max_degree=0):
     s = lap._struct()
     nnz = I64()
     nl = I32()
-    _check(lib().ssp_stage_factor(ctx._h, ctypes.byref(s), seed, dense_threshold, ctypes.byref(nnz), None, None,
-                                  None, None, None, ctypes.byref(nl)))
+    _check(lib().ssp_stage_factor(ctx._h, ctypes.byref(s), seed, dense_threshold, max_degree, ctypes.byref(nnz),
+                                  None, None, None, None, None, ctypes.byref(nl)))
     n = lap.n
     cp = np.zeros(n + 1, np.int64); rows = np.zeros(max(nnz.value, 1), np.int32)
     vals = np.zeros(max(nnz.value, 1), np.float64); D = np.zeros(n, np.float64); lvl = np.zeros(n, np.int32)
-    _check(lib().ssp_stage_factor(ctx._h, ctypes.byref(s), seed, dense_threshold, ctypes.byref(nnz), _ptr(cp),
-                                  _ptr(rows), _ptr(vals), _ptr(D), _ptr(lvl), ctypes.byref(nl)))
+    _check(lib().ssp_stage_factor(ctx._h, ctypes.byref(s), seed, dense_threshold, max_degree, ctypes.byref(nnz),
+                                  _ptr(cp), _ptr(rows), _ptr(vals), _ptr(D), _ptr(lvl), ctypes.byref(nl)))
     return {"colptr": cp, "rows": rows[:nnz.value], "vals": vals[:nnz.value], "D": D, "level": lvl,
             "num_levels": nl.value}
 
 
-def stage_precond(ctx, lap, seed, R, dense_threshold=4096):
+def stage_precond(ctx, lap, seed, R, dense_threshold=4096, max_degree=0):
     R = np.ascontiguousarray(R, np.float64)
     if R.ndim == 1:
         R = R[:, None]
     Z = np.zeros_like(R)
     s = lap._struct()
-    _check(lib().ssp_stage_precond(ctx._h, ctypes.byref(s), seed, dense_threshold, _ptr(R), R.shape[1], _ptr(Z)))
+    _check(lib().ssp_stage_precond(ctx._h, ctypes.byref(s), seed, dense_threshold, max_degree, _ptr(R), R.shape[1],
+                                   _ptr(Z)))
     return Z
 
 

@@ -26,8 +26,6 @@ namespace ssp {
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
-void precond_apply_device(Context& C, const DevFactor& F, const double* R, double* Z, int64_t ld);
-
 template <class Fn>
 static int guarded(Fn&& fn) {
     try {
@@ -127,6 +125,7 @@ static DevCsc to_device(Context& C, const ssp_csc* m, const char* tag) {
 
 // ---------------------------------------------------------------- parameters
 static int32_t jl_dim(const ssp_params* p, int64_t n) {
+    if (p->jl_dim_override > 0) return p->jl_dim_override;
     double k;
     if (p->jl_dim_rule == SSP_JL_DIM_24) k = std::ceil(24.0 * std::log((double)n) / (p->epsilon * p->epsilon));
     else k = std::ceil(std::log2((double)n) * p->jl_factor);
@@ -183,12 +182,13 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     const double scale = jl_scale(prm, k);
     const int64_t ld = ((int64_t)k + 7) / 8 * 8;
     double* Y = C.ws.get_t<double>("sp_Y", (size_t)n * ld);
-    sketch_device(C, G, k, scale, prm->sketch_seed, prm->sketch_uniform, Y, ld);
+    sketch_device(C, G, k, scale, prm->sketch_seed, prm->sketch_uniform, Y, ld, 1);
     T.mark();  // 2
     DevFactor F;
     FactorOptions fo;
     fo.seed = prm->factor_seed;
     fo.dense_threshold = prm->dense_threshold;
+    fo.max_degree = prm->factor_max_degree;
     factor_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, fo, F, "f");
     T.mark();  // 3
     PcgOptions po;
@@ -197,12 +197,13 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     po.max_iters = prm->pcg_max_iters;
     po.verbose = prm->verbose;
     PcgReport rep;
-    pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, k, ld, Y, po, rep);  // Z overwrites Y
+    const double* Zt = nullptr;
+    pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, k, &Zt, po, rep);
     T.mark();  // 4
     double* d = C.ws.get_t<double>("sp_d", G.m + 1);
     double* p = C.ws.get_t<double>("sp_p", G.m + 1);
     double* coins = C.ws.get_t<double>("sp_coins", G.m + 1);
-    diff_norms_device(C, G.m, G.v1, G.v2, Y, k, ld, d);
+    diff_norms_device(C, G.m, G.v1, G.v2, Zt, k, ld, d, n);
     const double beta = beta_of(prm, n);
     const double denom = prm->prob_variance_correction ? (double)k * scale * scale : (double)k;
     probs_device(C, G.m, G.w, d, beta, denom, p);
@@ -281,9 +282,15 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
         st->nnz_laplacian = G.lap_nnz;
     }
     if (prm->verbose) {
-        fprintf(stderr, "[ssp] n=%lld m=%lld k=%d nnz(L)=%lld levels=%d pcg iters max %d mean %.1f relres %.3g\n",
-                (long long)n, (long long)G.m, k, (long long)F.nnz, F.num_levels, rep.max_iters_used, rep.mean_iters,
-                rep.max_relres);
+        fprintf(stderr, "[ssp] n=%lld m=%lld k=%d nnz(L)=%lld levels=%d (sparse %zu, dense %d, compactions %d) "
+                        "pcg iters max %d mean %.1f relres %.3g\n",
+                (long long)n, (long long)G.m, k, (long long)F.nnz, F.num_levels, F.frontier_sizes.size(),
+                F.dense_levels, (long long)F.truncated_rows, F.compactions, rep.max_iters_used, rep.mean_iters, rep.max_relres);
+        fprintf(stderr, "[ssp] frontier sizes:");
+        for (size_t i = 0; i < F.frontier_sizes.size(); i++)
+            if (i < 24 || i % 50 == 0 || i + 5 > F.frontier_sizes.size())
+                fprintf(stderr, " %zu:%lld", i, (long long)F.frontier_sizes[i]);
+        fprintf(stderr, "\n");
     }
     if (prm->output_file && prm->output_file[0]) {
         std::vector<int64_t> cp(n + 1);
@@ -308,18 +315,20 @@ static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t 
     T.mark();
     DevCsc L = to_device(C, lap, "lap");
     const int64_t n = L.n;
+    const int64_t ld = ((int64_t)k + 7) / 8 * 8;
     const double* dY = Y;
-    double* dZ = Z;
     if (mem == SSP_MEM_HOST) {
-        double* y = C.ws.get_t<double>("sl_Y", (size_t)n * k);
+        double* y = C.ws.get_t<double>("sl_Yrm", (size_t)n * k);
         SSP_CUDA(cudaMemcpyAsync(y, Y, sizeof(double) * n * k, cudaMemcpyHostToDevice, C.stream));
         dY = y;
-        dZ = C.ws.get_t<double>("sl_Z", (size_t)n * k);
     }
+    double* Yt = C.ws.get_t<double>("sl_Yt", (size_t)n * ld);
+    rowmajor_to_tiles(C, n, k, k, dY, Yt);
     DevFactor F;
     FactorOptions fo;
     fo.seed = o->factor_seed;
     fo.dense_threshold = o->dense_threshold;
+    fo.max_degree = o->factor_max_degree;
     factor_device(C, n, L.colptr, L.rowidx, L.val, fo, F, "f");
     T.mark();
     PcgOptions po;
@@ -328,10 +337,16 @@ static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t 
     po.max_iters = o->max_iters;
     po.verbose = o->verbose;
     PcgReport pr;
-    pcg_device(C, n, L.colptr, L.rowidx, L.val, F, dY, k, k, dZ, po, pr, iters, relres);
+    const double* Xt = nullptr;
+    pcg_device(C, n, L.colptr, L.rowidx, L.val, F, Yt, k, &Xt, po, pr, iters, relres);
     T.mark();
-    if (mem == SSP_MEM_HOST)
-        SSP_CUDA(cudaMemcpyAsync(Z, dZ, sizeof(double) * n * k, cudaMemcpyDeviceToHost, C.stream));
+    if (mem == SSP_MEM_HOST) {
+        double* z = C.ws.get_t<double>("sl_Zrm", (size_t)n * k);
+        tiles_to_rowmajor(C, n, k, Xt, z, k);
+        SSP_CUDA(cudaMemcpyAsync(Z, z, sizeof(double) * n * k, cudaMemcpyDeviceToHost, C.stream));
+    } else {
+        tiles_to_rowmajor(C, n, k, Xt, Z, k);
+    }
     SSP_CUDA(cudaStreamSynchronize(C.stream));
     if (rep) {
         rep->k = k;
@@ -433,6 +448,7 @@ void ssp_params_new(ssp_params* p, double epsilon, int32_t beta_constant, int32_
     p->pcg_max_iters = 400;
     p->factor_seed = 0;
     p->dense_threshold = 4096;
+    p->factor_max_degree = 64;
 }
 
 void ssp_params_default(ssp_params* p) {
@@ -456,6 +472,7 @@ void ssp_solve_opts_default(ssp_solve_opts* o) {
     o->factor_seed = 0;
     o->dense_threshold = 4096;
     o->verbose = 0;
+    o->factor_max_degree = 64;
 }
 
 int ssp_run_solve_lap(const double* shared_jl_cols, size_t num_rows, size_t num_cols, const int32_t* col_ptrs,
@@ -642,15 +659,16 @@ int ssp_stage_sketch(ssp_context* c, int64_t n, int64_t m, const int32_t* v1, co
         build_graph_from_edges(C, G);
         double* dY = Y;
         if (mem == SSP_MEM_HOST) dY = C.ws.get_t<double>("st_Y", (size_t)n * k);
-        sketch_device(C, G, k, scale, seed, uniform, dY, k);
+        sketch_device(C, G, k, scale, seed, uniform, dY, k, 0);
         if (mem == SSP_MEM_HOST)
             SSP_CUDA(cudaMemcpyAsync(Y, dY, sizeof(double) * n * k, cudaMemcpyDeviceToHost, C.stream));
         SSP_CUDA(cudaStreamSynchronize(C.stream));
     });
 }
 
-int ssp_stage_factor(ssp_context* c, const ssp_csc* lap, uint64_t seed, int64_t dense_threshold, int64_t* nnz,
-                     int64_t* colptr, int32_t* rows, double* vals, double* D, int32_t* level, int32_t* num_levels) {
+int ssp_stage_factor(ssp_context* c, const ssp_csc* lap, uint64_t seed, int64_t dense_threshold,
+                     int64_t max_degree, int64_t* nnz, int64_t* colptr, int32_t* rows, double* vals, double* D,
+                     int32_t* level, int32_t* num_levels) {
     return guarded([&] {
         SSP_REQUIRE(c && lap && nnz, SSP_ERR_INVALID, "bad arguments");
         Context& C = c->ctx;
@@ -660,6 +678,7 @@ int ssp_stage_factor(ssp_context* c, const ssp_csc* lap, uint64_t seed, int64_t 
         FactorOptions fo;
         fo.seed = seed;
         fo.dense_threshold = dense_threshold;
+        fo.max_degree = max_degree;
         factor_device(C, L.n, L.colptr, L.rowidx, L.val, fo, F, "f");
         *nnz = F.nnz;
         if (num_levels) *num_levels = F.num_levels;
@@ -674,8 +693,8 @@ int ssp_stage_factor(ssp_context* c, const ssp_csc* lap, uint64_t seed, int64_t 
     });
 }
 
-int ssp_stage_precond(ssp_context* c, const ssp_csc* lap, uint64_t seed, int64_t dense_threshold, const double* R,
-                      int32_t k, double* Zout) {
+int ssp_stage_precond(ssp_context* c, const ssp_csc* lap, uint64_t seed, int64_t dense_threshold,
+                      int64_t max_degree, const double* R, int32_t k, double* Zout) {
     return guarded([&] {
         SSP_REQUIRE(c && lap && R && Zout && k > 0, SSP_ERR_INVALID, "bad arguments");
         Context& C = c->ctx;
@@ -685,16 +704,17 @@ int ssp_stage_precond(ssp_context* c, const ssp_csc* lap, uint64_t seed, int64_t
         FactorOptions fo;
         fo.seed = seed;
         fo.dense_threshold = dense_threshold;
+        fo.max_degree = max_degree;
         factor_device(C, L.n, L.colptr, L.rowidx, L.val, fo, F, "f");
         const int64_t ld = ((int64_t)k + 7) / 8 * 8;
         double* dR = C.ws.get_t<double>("pc_R", (size_t)L.n * ld);
         double* dZ = C.ws.get_t<double>("pc_Z", (size_t)L.n * ld);
-        SSP_CUDA(cudaMemsetAsync(dR, 0, sizeof(double) * L.n * ld, C.stream));
-        SSP_CUDA(cudaMemcpy2DAsync(dR, sizeof(double) * ld, R, sizeof(double) * k, sizeof(double) * k, L.n,
-                                   cudaMemcpyHostToDevice, C.stream));
+        double* dRr = C.ws.get_t<double>("pc_Rrm", (size_t)L.n * k);
+        SSP_CUDA(cudaMemcpyAsync(dRr, R, sizeof(double) * L.n * k, cudaMemcpyHostToDevice, C.stream));
+        rowmajor_to_tiles(C, L.n, k, k, dRr, dR);
         precond_apply_device(C, F, dR, dZ, ld);
-        SSP_CUDA(cudaMemcpy2DAsync(Zout, sizeof(double) * k, dZ, sizeof(double) * ld, sizeof(double) * k, L.n,
-                                   cudaMemcpyDeviceToHost, C.stream));
+        tiles_to_rowmajor(C, L.n, k, dZ, dRr, k);
+        SSP_CUDA(cudaMemcpyAsync(Zout, dRr, sizeof(double) * L.n * k, cudaMemcpyDeviceToHost, C.stream));
         SSP_CUDA(cudaStreamSynchronize(C.stream));
     });
 }

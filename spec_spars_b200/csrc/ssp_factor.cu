@@ -12,7 +12,8 @@
 // natural order.  Every ready vertex of a level is eliminated in parallel; they are pairwise
 // non-adjacent, so the factor equals sequential elimination in key order.  Once at most
 // `dense_threshold` vertices are live at a level boundary, the live Schur complement is merged into
-// a dense matrix and eliminated one vertex per level by a single block.
+// a dense matrix and eliminated one vertex per level by a single block.  (The switch also waits for the
+// frontier to collapse to at most 8 vertices, so sparse Schur complements stay in the sparse phase.)
 //
 // Every random draw is Philox(seed, column, slot); merges sort by (row, weight) and sum runs
 // left to right; prefix sums are 32-wide Kogge-Stone chunks with a sequential carry.  Compiled
@@ -22,10 +23,11 @@
 
 namespace ssp {
 
-enum { C_NEXT = 0, C_LCUR, C_FCUR, C_ERR, C_NB, C_NG, C_MAXLIVE, C_POOL, C_OWNERS, C_REM, C_NCTR };
+enum { C_NEXT = 0, C_LCUR, C_FCUR, C_ERR, C_NB, C_NG, C_MAXLIVE, C_POOL, C_OWNERS, C_REM, C_NFILL, C_NCTR };
 enum { FERR_POOL = 1, FERR_OVERFLOW = 2 };
 
-constexpr int BLOCK_TIER_MAX = 4096;  // live entries handled in shared memory
+constexpr int BLOCK_TIER_MAX = 4096;    // live entries handled in shared memory
+constexpr int DENSE_FRONTIER_MAX = 8;   // dense tail once the frontier has collapsed to this size
 
 struct FDev {
     int64_t n;
@@ -271,6 +273,7 @@ __global__ void __launch_bounds__(128) k_elim_warp(FDev F, const int32_t* fronti
             F.D[v] = S;
             F.Lcnt[v] = cnt;
             F.fcnt[fi] = cnt > 0 ? cnt - 1 : 0;
+            if (cnt > 1) atomicAdd((unsigned long long*)&F.ctr[C_NFILL], (unsigned long long)(cnt - 1));
         }
         __syncwarp();
     }
@@ -409,7 +412,10 @@ __device__ void block_finish_column(const FDev& F, int32_t v, int64_t fidx, int3
     if (threadIdx.x == 0) {
         F.D[v] = S;
         F.Lcnt[v] = cnt;
-        if (fidx >= 0) F.fcnt[fidx] = cnt - 1;
+        if (fidx >= 0) {
+            F.fcnt[fidx] = cnt - 1;
+            if (cnt > 1) atomicAdd((unsigned long long*)&F.ctr[C_NFILL], (unsigned long long)(cnt - 1));
+        }
     }
     __syncthreads();
 }
@@ -570,6 +576,7 @@ __global__ void k_level_begin(int64_t* ctr) {
     ctr[C_REM] = ctr[C_NEXT];
     ctr[C_NEXT] = 0;
     ctr[C_OWNERS] = 0;
+    ctr[C_NFILL] = 0;
 }
 __global__ void k_level_prep(int64_t* ctr) {
     // the upcoming frontier's counts become the live-count kernel's domain
@@ -733,6 +740,54 @@ __global__ void __launch_bounds__(1024) k_dense_elim(FDev F, const int32_t* rem,
     }
 }
 
+// ---------------------------------------------------------------- truncation
+// block per remaining vertex: no L entries, D = merged live weights summed in row order
+__global__ void k_trunc_diag(FDev F, const int32_t* rem, int32_t T, int32_t lvl, int32_t cap, int32_t* g_u,
+                             double* g_w, int use_global) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int32_t s_warp[33];
+    __shared__ int32_t s_cnt;
+    __shared__ int32_t s_live;
+    for (int32_t i = blockIdx.x; i < T; i += gridDim.x) {
+        const int32_t v = rem[i];
+        if (threadIdx.x == 0) s_live = 0;
+        __syncthreads();
+        const int64_t s = F.bag_start[v];
+        const int32_t len = F.bag_len[v];
+        int32_t c = 0;
+        for (int32_t q = threadIdx.x; q < len; q += blockDim.x) c += (F.level[F.pool_u[s + q]] < 0) ? 1 : 0;
+        atomicAdd(&s_live, c);
+        __syncthreads();
+        const int32_t L = s_live;
+        int32_t *su, *mu;
+        double *sw, *mw;
+        if (use_global) {
+            int64_t base = (int64_t)blockIdx.x * cap;
+            su = g_u + 2 * base;
+            mu = su + cap;
+            sw = g_w + 4 * base;
+            mw = sw + cap;
+        } else {
+            sw = (double*)smem;
+            mw = sw + cap;
+            su = (int32_t*)(mw + cap);
+            mu = su + cap;
+        }
+        const int32_t cnt = block_gather_merge(F, v, L, cap, su, sw, mu, mw, s_warp, &s_cnt);
+        if (threadIdx.x == 0) {
+            double d = 0.0;
+            for (int32_t q = 0; q < cnt; q++) d = d + mw[q];
+            F.D[v] = d;
+            F.Lcnt[v] = 0;
+            F.Lstart[v] = 0;
+        }
+        __syncthreads();
+    }
+}
+__global__ void k_set_level(const int32_t* rem, int32_t T, int32_t lvl, int32_t* level) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) level[rem[i]] = lvl;
+}
+
 // ---------------------------------------------------------------- post-processing
 __global__ void k_copy_cols(int64_t n, const int64_t* Lstart, const int32_t* Lcnt, const int32_t* Lrow,
                             const double* Lval, const int64_t* col_ptr, int32_t* col_idx, double* col_val) {
@@ -783,6 +838,79 @@ __global__ void k_i64_to_i32(int64_t n, const int64_t* a, int32_t* b) {
         b[i] = (int32_t)a[i];
 }
 
+// ---------------------------------------------------------------- bag pool compaction
+// warp per vertex: live bags get 2*live + 8 slots in a fresh pool; eliminated vertices get none
+__global__ void k_compact_caps(FDev F, int32_t* newcap) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < F.n; v += nw) {
+        int32_t live = 0;
+        if (F.level[v] < 0) {
+            const int64_t s = F.bag_start[v];
+            const int32_t len = F.bag_len[v];
+            for (int32_t q = lane; q < len; q += 32) live += (F.level[F.pool_u[s + q]] < 0) ? 1 : 0;
+            for (int o = 16; o > 0; o >>= 1) live += __shfl_xor_sync(0xffffffffu, live, o);
+        }
+        if (lane == 0) newcap[v] = F.level[v] < 0 ? 2 * live + 8 : 0;
+    }
+}
+
+__global__ void k_compact_copy(FDev F, const int64_t* newstart, const int32_t* newcap, int32_t* nu, double* nw_) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < F.n; v += nw) {
+        if (F.level[v] >= 0) continue;
+        const int64_t s = F.bag_start[v], d = newstart[v];
+        const int32_t len = F.bag_len[v];
+        int32_t out = 0;
+        for (int32_t q0 = 0; q0 < len; q0 += 32) {
+            int32_t q = q0 + lane;
+            bool lv = false;
+            int32_t uu = 0;
+            double ww = 0;
+            if (q < len) {
+                uu = F.pool_u[s + q];
+                ww = F.pool_w[s + q];
+                lv = F.level[uu] < 0;
+            }
+            unsigned m = __ballot_sync(0xffffffffu, lv);
+            if (lv) {
+                int32_t p = out + __popc(m & ((1u << lane) - 1u));
+                nu[d + p] = uu;
+                nw_[d + p] = ww;
+            }
+            out += __popc(m);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            F.bag_start[v] = d;
+            F.bag_len[v] = out;
+            F.bag_cap[v] = newcap[v];
+        }
+    }
+}
+
+// storage-order copies of the row and column forms
+__global__ void k_perm_count(int64_t n, const int32_t* perm, const int64_t* ptr, int32_t* cnt) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = perm[i];
+        cnt[i] = (int32_t)(ptr[v + 1] - ptr[v]);
+    }
+}
+__global__ void k_perm_copy(int64_t n, const int32_t* perm, const int64_t* ptr, const int32_t* idx, const double* val,
+                            const int64_t* pptr, int32_t* pidx, double* pval) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const int32_t v = perm[i];
+        const int64_t s = ptr[v], d = pptr[i], c = ptr[v + 1] - s;
+        for (int64_t q = lane; q < c; q += 32) {
+            pidx[d + q] = idx[s + q];
+            pval[d + q] = val[s + q];
+        }
+    }
+}
+
 // ---------------------------------------------------------------- host driver
 // grow a device buffer, keeping its first `keep` bytes
 static void* grow_keep(Context& C, const std::string& name, void* old, size_t keep, size_t bytes) {
@@ -827,10 +955,14 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
     exclusive_scan_i32_to_i64(C, F.bag_cap, F.bag_start, n + 1, d_tot);
     const int64_t pool_init = read_i64(C, d_tot);
     // room for relocations: the live entry count never grows, so 3x the initial layout plus slack
-    int64_t pool_cap = pool_init * 3 + 4 * n + 1024;
+    int64_t pool_cap = pool_init * 4 + 20 * n + 4096;
     F.pool_u = W.get_t<int32_t>(nm("pool_u"), pool_cap);
     F.pool_w = W.get_t<double>(nm("pool_w"), pool_cap);
     F.pool_cap = pool_cap;
+    int pool_gen = 0;
+    out.frontier_sizes.clear();
+    out.compactions = 0;
+    out.truncated_rows = 0;
     k_bag_fill<<<grid_for(n, T256), T256, 0, C.stream>>>(n, colptr, rowidx, val, F);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
@@ -871,6 +1003,15 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
     int64_t h[C_NCTR];
     int64_t eliminated = 0;
     int32_t lvl = 0;
+    int64_t live_entries = 0;  // live entries of the current Schur complement (both directions)
+    {
+        SSP_CUDA(cudaMemsetAsync(deg + n, 0, sizeof(int32_t), C.stream));
+        int64_t* tmp = W.get_t<int64_t>(nm("degscan"), n + 1);
+        exclusive_scan_i32_to_i64(C, deg, tmp, n + 1, d_tot);
+        live_entries = read_i64(C, d_tot);
+    }
+    int64_t prev_fcur = -1;
+    bool truncated = false;
     int64_t Lused_prev = 0;
     const size_t blk_smem = (size_t)BLOCK_TIER_MAX * (3 * sizeof(double) + 2 * sizeof(int32_t));
     SSP_CUDA(cudaFuncSetAttribute(k_elim_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem));
@@ -878,11 +1019,42 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
         read_i64s(C, F.ctr, h, C_NCTR);
         if (h[C_ERR] & FERR_POOL) throw Error(SSP_ERR_CAPACITY, "factor: bag pool exhausted");
         if (h[C_ERR] & FERR_OVERFLOW) throw Error(SSP_ERR_CAPACITY, "factor: bag overflow");
+        if (prev_fcur >= 0) live_entries += 2 * h[C_NFILL] - 2 * prev_fcur;
         const int64_t nf = h[C_NEXT];
         if (nf == 0) break;
+        if (opt.max_degree > 0 && live_entries > opt.max_degree * (n - eliminated)) {
+            truncated = true;
+            break;
+        }
         if (eliminated + nf > n || lvl > n)
             throw Error(SSP_ERR_CAPACITY, "factor: frontier accounting inconsistent (eliminated > n)");
-        if (opt.dense_threshold > 0 && n - eliminated <= opt.dense_threshold) break;
+        if (opt.dense_threshold > 0 && n - eliminated <= opt.dense_threshold && nf <= DENSE_FRONTIER_MAX) break;
+        out.frontier_sizes.push_back(nf);
+        // relocations of this level allocate at most 2*(live entries + incoming fill) + 16 per owner
+        {
+            const int64_t reserve = 2 * (pool_init + 2 * h[C_FCUR]) + 16 * (n - eliminated) + 1024;
+            if (h[C_POOL] + reserve > pool_cap) {
+                int32_t* newcap = W.get_t<int32_t>(nm("newcap"), n + 1);
+                int64_t* newstart = W.get_t<int64_t>(nm("newstart"), n + 1);
+                k_compact_caps<<<grid_for(n * 32, T256, 148 * 64), T256, 0, C.stream>>>(F, newcap);
+                SSP_CUDA(cudaMemsetAsync(newcap + n, 0, sizeof(int32_t), C.stream));
+                exclusive_scan_i32_to_i64(C, newcap, newstart, n + 1, d_tot);
+                const int64_t used = read_i64(C, d_tot);
+                const int64_t ncap = std::max<int64_t>(pool_cap, used + reserve + used / 2);
+                const std::string other = (pool_gen & 1) ? "" : "_b";
+                int32_t* nu = W.get_t<int32_t>(nm("pool_u") + other, ncap);
+                double* nwp = W.get_t<double>(nm("pool_w") + other, ncap);
+                k_compact_copy<<<grid_for(n * 32, T256, 148 * 64), T256, 0, C.stream>>>(F, newstart, newcap, nu, nwp);
+                SSP_CHECK_LAUNCH();
+                C.kernels_launched += 2;
+                F.pool_u = nu;
+                F.pool_w = nwp;
+                F.pool_cap = pool_cap = ncap;
+                SSP_CUDA(cudaMemcpyAsync(F.ctr + C_POOL, d_tot, sizeof(int64_t), cudaMemcpyDeviceToDevice, C.stream));
+                pool_gen++;
+                out.compactions++;
+            }
+        }
         // capacities for this level's reservations
         if (h[C_LCUR] > Lcap) {
             int64_t ncap = std::max<int64_t>(h[C_LCUR] + h[C_LCUR] / 2, Lcap * 2);
@@ -897,6 +1069,7 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
             F.fill_w = W.get_t<double>(nm("fill_w"), Fcap);
         }
         Lused_prev = h[C_LCUR];
+        prev_fcur = h[C_FCUR];
         std::swap(frontier, next);
         k_level_begin<<<1, 1, 0, C.stream>>>(F.ctr);  // REM <- NEXT (frontier size), NEXT <- 0
         k_elim_warp<<<grid_for(nf * 32, 128, 148 * 64), 128, 0, C.stream>>>(F, frontier, live_cnt);
@@ -933,7 +1106,41 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
         live_count(next);
     }
     const int32_t sparse_levels = lvl;
-    const int64_t T = n - eliminated;
+    const int64_t T = truncated ? 0 : n - eliminated;
+    if (truncated) {
+        const int64_t R = n - eliminated;
+        int32_t* rem = W.get_t<int32_t>(nm("rem"), R + 1);
+        SSP_CUDA(cudaMemsetAsync(F.ctr + C_REM, 0, sizeof(int64_t), C.stream));
+        k_collect_live<<<grid_for(n, T256), T256, 0, C.stream>>>(n, F.level, rem, F.ctr + C_REM);
+        int32_t maxlen = 0;
+        {
+            std::vector<int32_t> lens(n);
+            SSP_CUDA(cudaMemcpyAsync(lens.data(), F.bag_len, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaStreamSynchronize(C.stream));
+            for (auto x : lens) maxlen = std::max(maxlen, x);
+        }
+        int32_t cap = 64;
+        while (cap < maxlen) cap <<= 1;
+        if (cap <= BLOCK_TIER_MAX) {
+            size_t smem = (size_t)cap * (2 * sizeof(double) + 2 * sizeof(int32_t));
+            SSP_CUDA(cudaFuncSetAttribute(k_trunc_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_trunc_diag<<<(int)std::min<int64_t>(R, 148 * 8), 256, smem, C.stream>>>(F, rem, (int32_t)R, lvl, cap,
+                                                                                      nullptr, nullptr, 0);
+        } else {
+            int blocks = 32;
+            int32_t* gu = W.get_t<int32_t>(nm("gscr_u"), (size_t)2 * cap * blocks);
+            double* gw = W.get_t<double>(nm("gscr_w"), (size_t)4 * cap * blocks);
+            k_trunc_diag<<<blocks, 1024, 0, C.stream>>>(F, rem, (int32_t)R, lvl, cap, gu, gw, 1);
+        }
+        k_set_level<<<grid_for(R, T256), T256, 0, C.stream>>>(rem, (int32_t)R, lvl, F.level);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched += 3;
+        int64_t hh[C_NCTR];
+        read_i64s(C, F.ctr, hh, C_NCTR);
+        if (hh[C_ERR]) throw Error(SSP_ERR_CAPACITY, "factor: truncation overflow");
+        out.truncated_rows = R;
+        lvl++;
+    }
     int64_t Lused = Lused_prev;
     // note: Lused_prev covers reservations up to the last processed level
     if (T > 0) {
@@ -993,7 +1200,7 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
         if (hh[C_ERR]) throw Error(SSP_ERR_CAPACITY, "factor: dense tail overflow");
     }
     out.n = n;
-    out.num_levels = sparse_levels + (int32_t)T;
+    out.num_levels = lvl + (int32_t)T;
     out.dense_levels = (int32_t)T;
     // compact columns
     out.col_ptr = W.get_t<int64_t>(nm("col_ptr"), n + 1);
@@ -1056,6 +1263,43 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
     out.max_level_rows = 0;
     for (int32_t l = 0; l <= NL; l++) out.level_ptr[l] = (int32_t)lp[l];
     for (int32_t l = 0; l < NL; l++) out.max_level_rows = std::max(out.max_level_rows, (int32_t)(lp[l + 1] - lp[l]));
+    // storage-order row and column forms + per-level chunk lists
+    {
+        int32_t* cnt = W.get_t<int32_t>(nm("permcnt"), n + 1);
+        auto build = [&](const int64_t* ptr, const int32_t* idx, const double* val, const char* tagp,
+                         int64_t** pptr, int32_t** pidx, double** pval, int32_t** chunks,
+                         std::vector<int32_t>& chunk_lvl) {
+            *pptr = W.get_t<int64_t>(nm(tagp) + "_ptr", n + 1);
+            k_perm_count<<<grid_for(n, T256), T256, 0, C.stream>>>(n, out.level_rows, ptr, cnt);
+            SSP_CUDA(cudaMemsetAsync(cnt + n, 0, sizeof(int32_t), C.stream));
+            exclusive_scan_i32_to_i64(C, cnt, *pptr, n + 1, nullptr);
+            *pidx = W.get_t<int32_t>(nm(tagp) + "_idx", out.nnz + 1);
+            *pval = W.get_t<double>(nm(tagp) + "_val", out.nnz + 1);
+            k_perm_copy<<<grid_for(n * 32, T256, 148 * 64), T256, 0, C.stream>>>(n, out.level_rows, ptr, idx, val,
+                                                                                *pptr, *pidx, *pval);
+            SSP_CHECK_LAUNCH();
+            C.kernels_launched += 2;
+            std::vector<int64_t> hp(n + 1);
+            SSP_CUDA(cudaMemcpyAsync(hp.data(), *pptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaStreamSynchronize(C.stream));
+            std::vector<int32_t> starts;
+            chunk_lvl.assign(NL + 1, 0);
+            for (int32_t l = 0; l < NL; l++) {
+                chunk_lvl[l] = (int32_t)starts.size();
+                make_chunks(hp, (int32_t)lp[l], (int32_t)lp[l + 1], starts);
+            }
+            chunk_lvl[NL] = (int32_t)starts.size();
+            starts.push_back((int32_t)n);
+            *chunks = W.get_t<int32_t>(nm(tagp) + "_chunks", starts.size());
+            SSP_CUDA(cudaMemcpyAsync(*chunks, starts.data(), sizeof(int32_t) * starts.size(), cudaMemcpyHostToDevice,
+                                     C.stream));
+            SSP_CUDA(cudaStreamSynchronize(C.stream));
+        };
+        build(out.row_ptr, out.row_idx, out.row_val, "prow", &out.prow_ptr, &out.prow_idx, &out.prow_val,
+              &out.fchunk, out.fchunk_lvl);
+        build(out.col_ptr, out.col_idx, out.col_val, "pcol", &out.pcol_ptr, &out.pcol_idx, &out.pcol_val,
+              &out.bchunk, out.bchunk_lvl);
+    }
 }
 
 }  // namespace ssp

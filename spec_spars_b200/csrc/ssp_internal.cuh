@@ -179,6 +179,12 @@ void exclusive_scan_i32_to_i64(Context& C, const int32_t* in, int64_t* out, int6
 int64_t read_i64(Context& C, const int64_t* d_ptr);
 void read_i64s(Context& C, const int64_t* d_ptr, int64_t* host, int cnt);
 
+// Row-aligned chunks of a CSR row range: each holds at most CHUNK_CAP entries and CHUNK_ROWS rows
+// (a longer row is a chunk of its own).  Appends chunk starts for rows [r0, r1).
+constexpr int CHUNK_CAP = 1024;
+constexpr int CHUNK_ROWS = 128;
+void make_chunks(const std::vector<int64_t>& ptr, int32_t r0, int32_t r1, std::vector<int32_t>& starts);
+
 // Segmented sort of int32 keys in place (ascending).  Segments [start[i], start[i]+len[i]).
 void segsort_i32(Context& C, int32_t* keys, const int64_t* seg_start, const int32_t* seg_len, int64_t nseg,
                  int32_t max_len);
@@ -208,9 +214,9 @@ void build_graph_from_csc(Context& C, int64_t n, const int64_t* colptr, const in
 // adjacency + Laplacian for a given device edge list (v1<v2, CSC order)
 void build_graph_from_edges(Context& C, DevGraph& G);
 
-// a4: Y (n x ldy row-major, columns [0,k)) = B^T Q
+// a4: Y = B^T Q, columns [0,k): row-major with leading dimension ldy, or tile-major (8-column slabs)
 void sketch_device(Context& C, const DevGraph& G, int32_t k, double scale, uint64_t seed, int uniform,
-                   double* Y, int64_t ldy);
+                   double* Y, int64_t ldy, int tile_major);
 
 // a7: factor
 struct DevFactor {
@@ -227,21 +233,38 @@ struct DevFactor {
     double* D = nullptr;
     int32_t* level = nullptr;       // [n]
     int32_t* level_ptr_d = nullptr; // [num_levels+1] (device)
-    int32_t* level_rows = nullptr;  // [n] vertices grouped by level
+    int32_t* level_rows = nullptr;  // [n] vertices grouped by level ("storage order")
     std::vector<int32_t> level_ptr; // host copy
+    // L rows (forward solve) and columns (backward solve) re-laid in storage order, so that the rows of
+    // a level are contiguous; chunk lists split each level into row-aligned pieces of bounded size
+    int64_t* prow_ptr = nullptr;
+    int32_t* prow_idx = nullptr;
+    double* prow_val = nullptr;
+    int64_t* pcol_ptr = nullptr;
+    int32_t* pcol_idx = nullptr;
+    double* pcol_val = nullptr;
+    int32_t* fchunk = nullptr;           // device chunk starts (storage rows) for the forward solve
+    int32_t* bchunk = nullptr;           // ... for the backward solve
+    std::vector<int32_t> fchunk_lvl;     // [num_levels+1] chunk index range per level
+    std::vector<int32_t> bchunk_lvl;
     int32_t num_levels = 0;
     int32_t dense_levels = 0;       // trailing single-vertex levels from the dense phase
     int32_t max_level_rows = 0;
+    std::vector<int64_t> frontier_sizes;  // rows of each sparse level
+    int32_t compactions = 0;
+    int64_t truncated_rows = 0;           // vertices left to the diagonal final level
 };
 struct FactorOptions {
     uint64_t seed = 0;
     int64_t dense_threshold = 4096;
+    int64_t max_degree = 0;  // stop once the live Schur complement's average degree exceeds this (0: never)
 };
 // Input: Laplacian CSC on device (rows > col used, |value| as weight).
 void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,
                    const FactorOptions& opt, DevFactor& F, const std::string& tag = "f");
 
-// a8: PCG on all k columns.  Y, Z: n x ld row-major device arrays.
+// a8: PCG on all k columns.  Y: tile-major n x round8(k) device block; the solution is left in the
+// workspace (tile-major) and returned through *x_out.
 struct PcgOptions {
     double tol = 1e-8;
     double abs_tol = 0.0;
@@ -259,12 +282,16 @@ struct PcgReport {
     int64_t n_precond = 0;
 };
 void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx, const double* lap_val,
-                const DevFactor& F, const double* Y, int32_t k, int64_t ld, double* Z, const PcgOptions& opt,
+                const DevFactor& F, const double* Y, int32_t k, const double** x_out, const PcgOptions& opt,
                 PcgReport& rep, int32_t* h_iters = nullptr, double* h_relres = nullptr);
+void rowmajor_to_tiles(Context& C, int64_t n, int32_t k, int64_t ldr, const double* src, double* dst);
+void tiles_to_rowmajor(Context& C, int64_t n, int32_t k, const double* src, double* dst, int64_t ldr);
+void precond_apply_device(Context& C, const DevFactor& F, const double* R, double* Z, int64_t ld);
 
 // a9-a12
+// Z row-major (leading dimension ldz) or, when n_tile_major > 0, tile-major with that many rows
 void diff_norms_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z, int32_t k,
-                       int64_t ldz, double* d);
+                       int64_t ldz, double* d, int64_t n_tile_major = 0);
 void probs_device(Context& C, int64_t m, const double* w, const double* d, double beta, double denom, double* p);
 void coins_device(Context& C, int64_t m, uint64_t seed, double* coins);
 // returns nnz(L_H); writes L_H CSC into workspace buffers returned through pointers

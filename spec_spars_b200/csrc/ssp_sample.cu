@@ -11,17 +11,19 @@
 
 namespace ssp {
 
+template <bool TM>
 __global__ void __launch_bounds__(256) k_diff_norms(int64_t m, const int32_t* __restrict__ v1,
                                                     const int32_t* __restrict__ v2, const double* __restrict__ Z,
-                                                    int32_t k, int64_t ldz, double* __restrict__ d) {
+                                                    int32_t k, int64_t ldz, int64_t n, double* __restrict__ d) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < m; e += nw) {
-        const double* za = Z + (int64_t)v1[e] * ldz;
-        const double* zb = Z + (int64_t)v2[e] * ldz;
+        const int64_t a = v1[e], b = v2[e];
         double s = 0.0;
         for (int32_t j = lane; j < k; j += 32) {
-            const double x = __dsub_rn(za[j], zb[j]);
+            const int64_t oa = TM ? ((int64_t)(j >> 3) * n + a) * 8 + (j & 7) : a * ldz + j;
+            const int64_t ob = TM ? ((int64_t)(j >> 3) * n + b) * 8 + (j & 7) : b * ldz + j;
+            const double x = __dsub_rn(Z[oa], Z[ob]);
             s = __fma_rn(x, x, s);
         }
 #pragma unroll
@@ -116,9 +118,12 @@ __global__ void k_lh_fill(int64_t n, const int64_t* __restrict__ adj_ptr, const 
 }
 
 void diff_norms_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z, int32_t k,
-                       int64_t ldz, double* d) {
+                       int64_t ldz, double* d, int64_t n_tile_major) {
     if (m == 0) return;
-    k_diff_norms<<<grid_for(m * 32, 256, 148 * 16), 256, 0, C.stream>>>(m, v1, v2, Z, k, ldz, d);
+    if (n_tile_major > 0)
+        k_diff_norms<true><<<grid_for(m * 32, 256, 148 * 16), 256, 0, C.stream>>>(m, v1, v2, Z, k, ldz, n_tile_major, d);
+    else
+        k_diff_norms<false><<<grid_for(m * 32, 256, 148 * 16), 256, 0, C.stream>>>(m, v1, v2, Z, k, ldz, 0, d);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
 }

@@ -9,7 +9,8 @@
 // One warp per (vertex, 256-column tile).  Lane l owns columns tile*256 + l + 32 t (t < 8), so
 // every store instruction writes 32 consecutive doubles.  The 256 sign bits of one edge come from
 // one Philox4x64 call; up to 32 edges are hashed at once (one per lane) and their words are
-// broadcast with shuffles.
+// broadcast with shuffles.  The output is row-major (leading dimension ldy) or tile-major (the
+// PCG layout: 8-column slabs of n x 8).
 #include "ssp_internal.cuh"
 
 namespace ssp {
@@ -18,7 +19,7 @@ __global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, const int64_t* _
                                                      const int32_t* __restrict__ adj_eid,
                                                      const int32_t* __restrict__ v2, const double* __restrict__ w,
                                                      int32_t k, int32_t ntiles, double scale, uint64_t seed,
-                                                     double* __restrict__ Y, int64_t ldy) {
+                                                     double* __restrict__ Y, int64_t ldy, int tm) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t item = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < n * ntiles; item += nw) {
@@ -55,11 +56,10 @@ __global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, const int64_t* _
                 }
             }
         }
-        double* yrow = Y + v * ldy + (int64_t)tile * 256;
 #pragma unroll
         for (int t = 0; t < 8; t++) {
-            int32_t col = tile * 256 + lane + 32 * t;
-            if (col < k) yrow[lane + 32 * t] = acc[t];
+            const int64_t col = (int64_t)tile * 256 + lane + 32 * t;
+            if (col < k) Y[tm ? ((col >> 3) * n + v) * 8 + (col & 7) : v * ldy + col] = acc[t];
         }
     }
 }
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, const int64_t* _
                                                      const int32_t* __restrict__ adj_eid,
                                                      const int32_t* __restrict__ v2, const double* __restrict__ w,
                                                      int32_t k, int32_t ntiles, double scale, uint64_t seed,
-                                                     double* __restrict__ Y, int64_t ldy) {
+                                                     double* __restrict__ Y, int64_t ldy, int tm) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t item = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < n * ntiles; item += nw) {
@@ -101,28 +101,27 @@ __global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, const int64_t* _
                 acc[t] = __dadd_rn(acc[t], __dmul_rn(hs, b));
             }
         }
-        double* yrow = Y + v * ldy + (int64_t)tile * 256;
 #pragma unroll
         for (int t = 0; t < 8; t++) {
-            int32_t col = tile * 256 + lane + 32 * t;
-            if (col < k) yrow[lane + 32 * t] = acc[t];
+            const int64_t col = (int64_t)tile * 256 + lane + 32 * t;
+            if (col < k) Y[tm ? ((col >> 3) * n + v) * 8 + (col & 7) : v * ldy + col] = acc[t];
         }
     }
 }
 
 void sketch_device(Context& C, const DevGraph& G, int32_t k, double scale, uint64_t seed, int uniform, double* Y,
-                   int64_t ldy) {
-    SSP_REQUIRE(k > 0 && ldy >= k, SSP_ERR_INVALID, "sketch: need 0 < k <= ld");
+                   int64_t ldy, int tile_major) {
+    SSP_REQUIRE(k > 0 && (tile_major || ldy >= k), SSP_ERR_INVALID, "sketch: need 0 < k <= ld");
     const int32_t ntiles = (k + 255) / 256;
     const int64_t items = G.n * ntiles;
     const int threads = 256;
     const int blocks = grid_for(items * 32, threads, 148 * 16);
     if (uniform)
         k_sketch_unif<<<blocks, threads, 0, C.stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, k, ntiles, scale, seed,
-                                                        Y, ldy);
+                                                        Y, ldy, tile_major);
     else
         k_sketch_sign<<<blocks, threads, 0, C.stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, k, ntiles, scale, seed,
-                                                        Y, ldy);
+                                                        Y, ldy, tile_major);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
 }

@@ -113,6 +113,16 @@ void exclusive_scan_i32_to_i64(Context& C, const int32_t* in, int64_t* out, int6
     scan_impl<int32_t>(C, in, out, n, d_total);
 }
 
+void make_chunks(const std::vector<int64_t>& ptr, int32_t r0, int32_t r1, std::vector<int32_t>& starts) {
+    int32_t r = r0;
+    while (r < r1) {
+        starts.push_back(r);
+        int32_t e = r + 1;
+        while (e < r1 && e - r < CHUNK_ROWS && ptr[e + 1] - ptr[r] <= CHUNK_CAP) e++;
+        r = e;
+    }
+}
+
 int64_t read_i64(Context& C, const int64_t* d_ptr) {
     SSP_CUDA(cudaMemcpyAsync(C.h_pinned, d_ptr, sizeof(int64_t), cudaMemcpyDeviceToHost, C.stream));
     SSP_CUDA(cudaStreamSynchronize(C.stream));

@@ -61,14 +61,14 @@ def _canon_cols(colptr, rows, vals, n):
 
 
 @pytest.mark.parametrize("name", ["rand300", "rand2k_disconnected", "grid40", "grid3d", "er5k"])
-@pytest.mark.parametrize("dense", [0, 64, 4096])
-def test_factor_bit_exact(ssp, ora, ctx, name, dense):
+@pytest.mark.parametrize("dense,maxdeg", [(0, 0), (64, 0), (4096, 0), (4096, 12), (0, 30)])
+def test_factor_bit_exact(ssp, ora, ctx, name, dense, maxdeg):
     G = GRAPHS[name](ssp)
     (v1, v2, w), (cp, ri, va) = _oracle_graph(ora, G)
     lap = ssp.CSC(G.n, cp, ri, va)
     seed = 5
-    f = ssp.stage_factor(ctx, lap, seed, dense)
-    o = ora.Factor(G.n, cp, ri, va, seed, dense)
+    f = ssp.stage_factor(ctx, lap, seed, dense, maxdeg)
+    o = ora.Factor(G.n, cp, ri, va, seed, dense, maxdeg)
     assert f["num_levels"] == o.num_levels
     assert np.array_equal(f["level"], o.level)
     assert np.array_equal(f["D"], o.D)
@@ -79,21 +79,21 @@ def test_factor_deterministic(ssp, ora, ctx):
     G = GRAPHS["er5k"](ssp)
     (_, _, _), (cp, ri, va) = _oracle_graph(ora, G)
     lap = ssp.CSC(G.n, cp, ri, va)
-    a = ssp.stage_factor(ctx, lap, 9, 256)
-    b = ssp.stage_factor(ctx, lap, 9, 256)
+    a = ssp.stage_factor(ctx, lap, 9, 256, 40)
+    b = ssp.stage_factor(ctx, lap, 9, 256, 40)
     for key in ("colptr", "D", "level"):
         assert np.array_equal(a[key], b[key])
 
 
-@pytest.mark.parametrize("dense", [0, 128])
-def test_precond_matches_oracle(ssp, ora, ctx, dense):
+@pytest.mark.parametrize("dense,maxdeg", [(0, 0), (128, 0), (4096, 8)])
+def test_precond_matches_oracle(ssp, ora, ctx, dense, maxdeg):
     G = GRAPHS["grid3d"](ssp)
     (_, _, _), (cp, ri, va) = _oracle_graph(ora, G)
     lap = ssp.CSC(G.n, cp, ri, va)
     rng = np.random.default_rng(0)
     R = rng.standard_normal((G.n, 19))
-    Z = ssp.stage_precond(ctx, lap, 3, R, dense)
-    o = ora.Factor(G.n, cp, ri, va, 3, dense)
+    Z = ssp.stage_precond(ctx, lap, 3, R, dense, maxdeg)
+    o = ora.Factor(G.n, cp, ri, va, 3, dense, maxdeg)
     Zo = np.column_stack([o.precond(R[:, j].copy()) for j in range(R.shape[1])])
     assert np.abs(Z - Zo).max() <= 1e-12 * np.abs(Zo).max()
 
@@ -105,8 +105,9 @@ def test_pcg_matches_oracle(ssp, ora, ctx, name):
     lap = ssp.CSC(G.n, cp, ri, va)
     k = 13
     Y = ora.sketch(G.n, v1, v2, w, k, 1 / math.sqrt(k), 3)
-    Z, rep = ctx.solve_lap(lap, Y, tol=1e-10, abs_tol=0.0, max_iters=400, factor_seed=4, dense_threshold=256)
-    F = ora.Factor(G.n, cp, ri, va, 4, 256)
+    Z, rep = ctx.solve_lap(lap, Y, tol=1e-10, abs_tol=0.0, max_iters=400, factor_seed=4, dense_threshold=256,
+                           max_degree=16)
+    F = ora.Factor(G.n, cp, ri, va, 4, 256, 16)
     Zo, it, rel, rc = ora.pcg(G.n, cp, ri, va, F, Y, 1e-10, 0.0, 400)
     assert rc == 0 and rep["not_converged"] == 0 and rep["max_relres"] < 1e-8
     dz, do = Z[v1] - Z[v2], Zo[v1] - Zo[v2]
@@ -177,7 +178,7 @@ def _oracle_pipeline(ora, ssp, G, params):
     k = params.jl_dim(n)
     s = params.jl_scale(k)
     Y = ora.sketch(n, v1, v2, w, k, s, params.sketch_seed, params.sketch_uniform)
-    F = ora.Factor(n, cp, ri, va, params.factor_seed, params.dense_threshold)
+    F = ora.Factor(n, cp, ri, va, params.factor_seed, params.dense_threshold, params.factor_max_degree)
     Z, it, rel, rc = ora.pcg(n, cp, ri, va, F, Y, params.pcg_tol, params.pcg_abs_tol, params.pcg_max_iters)
     d = ora.diff_norms(v1, v2, Z)
     denom = k * s * s if params.prob_variance_correction else float(k)

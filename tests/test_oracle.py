@@ -277,6 +277,31 @@ def test_factor_unbiased(ora, dense):
     assert errs[1] < errs[0] and errs[1] < 0.02
 
 
+@pytest.mark.parametrize("maxdeg", [16, 24])
+def test_factor_truncation(ora, maxdeg):
+    """Truncated elimination: every vertex left once the Schur complement's average degree exceeds
+    maxdeg sits in one final level with no L entries and D = its merged live weight sum; the
+    preconditioner stays SPD and PCG still converges to the same solution."""
+    A = rand_graph(400, 2400, 21)
+    n = A.shape[0]
+    v1, v2, w = ora.extract_edges(n, A.indptr, A.indices, A.data)
+    cp, ri, va = ora.laplacian(n, v1, v2, w)
+    F = ora.Factor(n, cp, ri, va, 3, 0, maxdeg)
+    last = F.level == F.level.max()
+    assert 0 < last.sum() < n
+    assert np.all(np.diff(F.colstart)[last] == 0) and np.all(F.D[last] > 0)
+    Ffull = ora.Factor(n, cp, ri, va, 3, 0, 0)
+    # eliminated vertices are identical to the untruncated run (same order, same columns)
+    elim = ~last
+    assert np.array_equal(F.D[elim], Ffull.D[elim])
+    Y = ora.sketch(n, v1, v2, w, 6, 1 / math.sqrt(6), 1)
+    Z, it, rel, rc = ora.pcg(n, cp, ri, va, F, Y, 1e-10, 0.0, 400)
+    Zf, itf, relf, rcf = ora.pcg(n, cp, ri, va, Ffull, Y, 1e-10, 0.0, 400)
+    assert rc == 0 and rel.max() < 1e-9
+    dz, df = Z[v1] - Z[v2], Zf[v1] - Zf[v2]
+    assert np.abs(dz - df).max() <= 1e-7 * np.abs(df).max()
+
+
 def test_precond_is_spd_on_range(ora):
     A = rand_graph(80, 300, 8)
     n = A.shape[0]
