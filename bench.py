@@ -140,7 +140,7 @@ def cpu_baseline(eps, k_full, impl="port", budget_cols=16):
         t_fact = info["factor_s"]
         t_solve = time.perf_counter() - t0 - t_fact
     else:
-        F = ora.Factor(n, cp, ri, va, 0, 4096)
+        F = ora.Factor(n, cp, ri, va, 0, 4096, 64)
         t_fact = time.perf_counter() - t0
         t0 = time.perf_counter()
         Z, it, rel, rc = ora.pcg(n, cp, ri, va, F, Y, PCG_TOL, 0.0, 400)

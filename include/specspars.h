@@ -106,7 +106,8 @@ typedef struct {
     uint64_t factor_seed;    /* elimination order + fill sampling */
     int64_t dense_threshold; /* live-vertex count that switches elimination to the dense tail */
     int64_t factor_max_degree; /* stop eliminating once the Schur complement's average degree exceeds
-                                  this; the rest is preconditioned by its diagonal (0 = eliminate all) */
+                                  this; the rest is preconditioned by its diagonal (0 = eliminate all,
+                                  -1 = choose by the autotuner) */
     int32_t jl_dim_override;   /* > 0: use exactly this many JL columns instead of jl_dim_rule */
 } ssp_params;
 
@@ -130,6 +131,8 @@ typedef struct {
     double ms_precond;
     int64_t n_precond;
     int64_t nnz_laplacian;
+    int64_t factor_max_degree_used; /* truncation actually used (autotuner's choice when requested) */
+    double ms_autotune;             /* device time spent choosing it (included in ms_factor) */
 } ssp_stats;
 
 typedef struct {
@@ -152,6 +155,7 @@ typedef struct {
     int32_t factor_levels;
     double ms_factor;
     double ms_solve;
+    int64_t factor_max_degree_used;
 } ssp_solve_report;
 
 /* ---- errors ---- */

@@ -67,7 +67,8 @@ class _Stats(ctypes.Structure):
                 ("ms_sketch", ctypes.c_double), ("ms_factor", ctypes.c_double), ("ms_solve", ctypes.c_double),
                 ("ms_leverage", ctypes.c_double), ("ms_sample", ctypes.c_double), ("ms_total", ctypes.c_double),
                 ("kernels_launched", ctypes.c_int64), ("ms_spmm", ctypes.c_double), ("n_spmm", ctypes.c_int64),
-                ("ms_precond", ctypes.c_double), ("n_precond", ctypes.c_int64), ("nnz_laplacian", ctypes.c_int64)]
+                ("ms_precond", ctypes.c_double), ("n_precond", ctypes.c_int64), ("nnz_laplacian", ctypes.c_int64),
+                ("factor_max_degree_used", ctypes.c_int64), ("ms_autotune", ctypes.c_double)]
 
 
 class _SolveOpts(ctypes.Structure):
@@ -80,7 +81,7 @@ class _SolveReport(ctypes.Structure):
     _fields_ = [("k", ctypes.c_int32), ("max_iters_used", ctypes.c_int32), ("mean_iters", ctypes.c_double),
                 ("max_relres", ctypes.c_double), ("not_converged", ctypes.c_int32),
                 ("nnz_factor", ctypes.c_int64), ("factor_levels", ctypes.c_int32), ("ms_factor", ctypes.c_double),
-                ("ms_solve", ctypes.c_double)]
+                ("ms_solve", ctypes.c_double), ("factor_max_degree_used", ctypes.c_int64)]
 
 
 _LIB = None
@@ -388,7 +389,7 @@ class Context:
         return (out.nnz, out.colptr, out.rowidx, out.values), _stats_dict(st)
 
     def solve_lap(self, lap, Y, tol=0.0, abs_tol=np.sqrt(2e-7), max_iters=400, factor_seed=0,
-                  dense_threshold=4096, max_degree=64, raise_on_failure=True):
+                  dense_threshold=4096, max_degree=-1, raise_on_failure=True):
         Y = np.ascontiguousarray(Y, np.float64)
         n, k = Y.shape
         Z = np.zeros_like(Y)

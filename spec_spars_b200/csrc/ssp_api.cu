@@ -180,7 +180,7 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     const int64_t n = G.n;
     const int32_t k = jl_dim(prm, n);
     const double scale = jl_scale(prm, k);
-    const int64_t ld = ((int64_t)k + 7) / 8 * 8;
+    const int64_t ld = tile_ld(k);
     double* Y = C.ws.get_t<double>("sp_Y", (size_t)n * ld);
     sketch_device(C, G, k, scale, prm->sketch_seed, prm->sketch_uniform, Y, ld, 1);
     T.mark();  // 2
@@ -189,13 +189,18 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     fo.seed = prm->factor_seed;
     fo.dense_threshold = prm->dense_threshold;
     fo.max_degree = prm->factor_max_degree;
-    factor_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, fo, F, "f");
-    T.mark();  // 3
     PcgOptions po;
     po.tol = prm->pcg_tol;
     po.abs_tol = prm->pcg_abs_tol;
     po.max_iters = prm->pcg_max_iters;
     po.verbose = prm->verbose;
+    double ms_tune = 0.0;
+    int64_t deg_used = fo.max_degree;
+    if (fo.max_degree < 0)
+        deg_used = autotune_factor(C, n, G.lap_ptr, G.lap_idx, G.lap_val, 2 * G.m, Y, k, fo, po, F, &ms_tune);
+    else
+        factor_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, fo, F, "f");
+    T.mark();  // 3
     PcgReport rep;
     const double* Zt = nullptr;
     pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, k, &Zt, po, rep);
@@ -280,9 +285,11 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
         st->ms_precond = rep.ms_precond;
         st->n_precond = rep.n_precond;
         st->nnz_laplacian = G.lap_nnz;
+        st->factor_max_degree_used = deg_used;
+        st->ms_autotune = ms_tune;
     }
     if (prm->verbose) {
-        fprintf(stderr, "[ssp] n=%lld m=%lld k=%d nnz(L)=%lld levels=%d (sparse %zu, dense %d, compactions %d) "
+        fprintf(stderr, "[ssp] n=%lld m=%lld k=%d nnz(L)=%lld levels=%d (sparse %zu, dense %d, truncated %lld, compactions %d) "
                         "pcg iters max %d mean %.1f relres %.3g\n",
                 (long long)n, (long long)G.m, k, (long long)F.nnz, F.num_levels, F.frontier_sizes.size(),
                 F.dense_levels, (long long)F.truncated_rows, F.compactions, rep.max_iters_used, rep.mean_iters, rep.max_relres);
@@ -315,7 +322,7 @@ static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t 
     T.mark();
     DevCsc L = to_device(C, lap, "lap");
     const int64_t n = L.n;
-    const int64_t ld = ((int64_t)k + 7) / 8 * 8;
+    const int64_t ld = tile_ld(k);
     const double* dY = Y;
     if (mem == SSP_MEM_HOST) {
         double* y = C.ws.get_t<double>("sl_Yrm", (size_t)n * k);
@@ -329,13 +336,20 @@ static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t 
     fo.seed = o->factor_seed;
     fo.dense_threshold = o->dense_threshold;
     fo.max_degree = o->factor_max_degree;
-    factor_device(C, n, L.colptr, L.rowidx, L.val, fo, F, "f");
-    T.mark();
     PcgOptions po;
     po.tol = o->tol;
     po.abs_tol = o->abs_tol;
     po.max_iters = o->max_iters;
     po.verbose = o->verbose;
+    int64_t deg_used = fo.max_degree;
+    if (fo.max_degree < 0) {
+        const int64_t offdiag = L.nnz - n;  // every vertex of a connected Laplacian stores its diagonal
+        deg_used = autotune_factor(C, n, L.colptr, L.rowidx, L.val, offdiag > 0 ? offdiag : L.nnz, Yt, k, fo, po, F,
+                                   nullptr);
+    } else {
+        factor_device(C, n, L.colptr, L.rowidx, L.val, fo, F, "f");
+    }
+    T.mark();
     PcgReport pr;
     const double* Xt = nullptr;
     pcg_device(C, n, L.colptr, L.rowidx, L.val, F, Yt, k, &Xt, po, pr, iters, relres);
@@ -358,6 +372,7 @@ static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t 
         rep->factor_levels = F.num_levels;
         rep->ms_factor = T.ms(0, 1);
         rep->ms_solve = T.ms(1, 2);
+        rep->factor_max_degree_used = deg_used;
     }
     if (pr.not_converged > 0)
         throw Error(SSP_ERR_NOT_CONVERGED, "solver did not converge: " + std::to_string(pr.not_converged) +
@@ -448,7 +463,8 @@ void ssp_params_new(ssp_params* p, double epsilon, int32_t beta_constant, int32_
     p->pcg_max_iters = 400;
     p->factor_seed = 0;
     p->dense_threshold = 4096;
-    p->factor_max_degree = 64;
+    p->factor_max_degree = -1;
+    p->jl_dim_override = 0;
 }
 
 void ssp_params_default(ssp_params* p) {
@@ -472,7 +488,7 @@ void ssp_solve_opts_default(ssp_solve_opts* o) {
     o->factor_seed = 0;
     o->dense_threshold = 4096;
     o->verbose = 0;
-    o->factor_max_degree = 64;
+    o->factor_max_degree = -1;
 }
 
 int ssp_run_solve_lap(const double* shared_jl_cols, size_t num_rows, size_t num_cols, const int32_t* col_ptrs,
@@ -706,7 +722,7 @@ int ssp_stage_precond(ssp_context* c, const ssp_csc* lap, uint64_t seed, int64_t
         fo.dense_threshold = dense_threshold;
         fo.max_degree = max_degree;
         factor_device(C, L.n, L.colptr, L.rowidx, L.val, fo, F, "f");
-        const int64_t ld = ((int64_t)k + 7) / 8 * 8;
+        const int64_t ld = tile_ld(k);
         double* dR = C.ws.get_t<double>("pc_R", (size_t)L.n * ld);
         double* dZ = C.ws.get_t<double>("pc_Z", (size_t)L.n * ld);
         double* dRr = C.ws.get_t<double>("pc_Rrm", (size_t)L.n * k);

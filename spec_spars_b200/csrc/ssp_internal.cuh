@@ -157,6 +157,19 @@ struct Context {
     int64_t kernels_launched = 0;  // count of library kernel launches (for bench accounting)
 };
 
+// ---------------------------------------------------------------- n x k block layout
+// Tile-major: k columns are split into tiles of SSP_TILE columns; each tile is a contiguous n x SSP_TILE
+// slab, element (r, c) at ((c / SSP_TILE) * n + r) * SSP_TILE + c % SSP_TILE.  Kernels that gather
+// rows work on one tile at a time so the slab stays in L2.
+#ifndef SSP_TILE_SHIFT
+#define SSP_TILE_SHIFT 3
+#endif
+constexpr int SSP_TILE = 1 << SSP_TILE_SHIFT;
+__host__ __device__ __forceinline__ int64_t tile_off(int64_t n, int64_t r, int64_t c) {
+    return ((c >> SSP_TILE_SHIFT) * n + r) * SSP_TILE + (c & (SSP_TILE - 1));
+}
+__host__ __device__ __forceinline__ int64_t tile_ld(int64_t k) { return (k + SSP_TILE - 1) / SSP_TILE * SSP_TILE; }
+
 // ---------------------------------------------------------------- small device helpers
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
@@ -181,8 +194,8 @@ void read_i64s(Context& C, const int64_t* d_ptr, int64_t* host, int cnt);
 
 // Row-aligned chunks of a CSR row range: each holds at most CHUNK_CAP entries and CHUNK_ROWS rows
 // (a longer row is a chunk of its own).  Appends chunk starts for rows [r0, r1).
-constexpr int CHUNK_CAP = 1024;
-constexpr int CHUNK_ROWS = 128;
+constexpr int CHUNK_CAP = 256;
+constexpr int CHUNK_ROWS = 32;
 void make_chunks(const std::vector<int64_t>& ptr, int32_t r0, int32_t r1, std::vector<int32_t>& starts);
 
 // Segmented sort of int32 keys in place (ascending).  Segments [start[i], start[i]+len[i]).
@@ -270,6 +283,7 @@ struct PcgOptions {
     double abs_tol = 0.0;
     int32_t max_iters = 400;
     int verbose = 0;
+    std::vector<double>* history = nullptr;  // per iteration: max over columns of ||r|| / ||b||
 };
 struct PcgReport {
     int32_t max_iters_used = 0;
@@ -280,7 +294,15 @@ struct PcgReport {
     int64_t n_spmm = 0;
     double ms_precond = 0;
     int64_t n_precond = 0;
+    double ms_loop = 0;      // device time of the iteration loop
+    int32_t iters_run = 0;   // iterations of the loop (all columns)
 };
+// Picks the elimination truncation (FactorOptions::max_degree) for this Laplacian and right-hand sides
+// by factoring a few candidates and timing a short PCG probe on the first column tile of Y.  Leaves
+// the chosen factor in F and returns the chosen max_degree.
+int64_t autotune_factor(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx,
+                        const double* lap_val, int64_t lap_offdiag_nnz, const double* Ytiles, int32_t k,
+                        const FactorOptions& base, const PcgOptions& popt, DevFactor& F, double* ms_tuning);
 void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx, const double* lap_val,
                 const DevFactor& F, const double* Y, int32_t k, const double** x_out, const PcgOptions& opt,
                 PcgReport& rep, int32_t* h_iters = nullptr, double* h_relres = nullptr);

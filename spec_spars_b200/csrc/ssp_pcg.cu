@@ -6,22 +6,20 @@
 // ||r|| <= max(abs_tol, tol ||b||) (the reference's own rule is ||r||^2 <= 2e-7, :159,213), at most
 // max_iters iterations (:153), and success iff ||b - A x|| / ||b|| < 0.01 (:251-258).
 //
-// Layout ("tile-major"): an n x k block is stored as k/8 slabs of n x 8 doubles; element (r, c) lives
-// at ((c / 8) * n + r) * 8 + c % 8.  Every kernel works on one 8-column tile at a time across all
-// rows, so the rows it gathers (one slab, n * 64 bytes) stay resident in L2 while the sparse matrix
-// streams.  Column reductions are two-stage with a fixed order (deterministic run to run).
+// Layout ("tile-major", tile_off): an n x k block is stored as slabs of n x SSP_TILE doubles.  Every
+// kernel works on one tile at a time across all rows, so the rows it gathers (one slab) stay resident
+// in L2 while the sparse matrix streams.  Column reductions are two-stage with a fixed order
+// (deterministic run to run).
 #include "ssp_internal.cuh"
 
 namespace ssp {
 
-constexpr int TILE = 8;           // columns per tile (64 bytes of FP64 per row)
+constexpr int TILE = SSP_TILE;    // columns per tile
 constexpr int SLOTS = 32 / TILE;  // nonzeros processed in parallel per warp
 constexpr int ROWS_PER_BLOCK = 8; // warps per 256-thread block, one row each
-constexpr int RED_THREADS = 256;  // column reductions: 32 row lanes x 8 columns
+constexpr int RED_THREADS = 256;  // column reductions: (256 / TILE) row lanes x TILE columns
 
-__host__ __device__ __forceinline__ int64_t tm_off(int64_t n, int64_t r, int64_t c) {
-    return ((c >> 3) * n + r) * TILE + (c & 7);
-}
+__host__ __device__ __forceinline__ int64_t tm_off(int64_t n, int64_t r, int64_t c) { return tile_off(n, r, c); }
 
 // ---------------------------------------------------------------- layout conversion
 __global__ void k_rm_to_tm(int64_t n, int32_t k, int64_t ldr, const double* __restrict__ src, double* __restrict__ dst,
@@ -63,7 +61,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_colred_partial(int64_t n, const
                                                                 int64_t ld, double* __restrict__ part) {
     __shared__ double s[RED_THREADS];
     const int64_t t = blockIdx.y;
-    const int c = threadIdx.x & 7, rl = threadIdx.x >> 3;
+    const int c = threadIdx.x % TILE, rl = threadIdx.x / TILE;
     const int64_t r0 = (int64_t)blockIdx.x * rows_per_blk, r1 = min(n, r0 + rows_per_blk);
     const double* at = a + t * n * TILE;
     const double* bt = b ? b + t * n * TILE : nullptr;
@@ -133,7 +131,7 @@ __global__ void k_center(int64_t n, int32_t k, const double* __restrict__ Y, con
     const int64_t t = blockIdx.y;
     const int64_t cnt = n * TILE;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t c = t * TILE + (i & 7);
+        const int64_t c = t * TILE + (i % TILE);
         const int64_t o = t * cnt + i;
         const double mu = c < k ? colsum[c] / (double)n : 0.0;
         if (i < TILE && blockIdx.x == 0) mean[c] = mu;
@@ -149,7 +147,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_axpy_xr_rr(int64_t n, const dou
                                                             int64_t rows_per_blk, int64_t ld, double* __restrict__ part) {
     __shared__ double s[RED_THREADS];
     const int64_t t = blockIdx.y;
-    const int c = threadIdx.x & 7, rl = threadIdx.x >> 3;
+    const int c = threadIdx.x % TILE, rl = threadIdx.x / TILE;
     const int64_t r0 = (int64_t)blockIdx.x * rows_per_blk, r1 = min(n, r0 + rows_per_blk);
     const double a = alpha[t * TILE + c];
     const int64_t base = t * n * TILE;
@@ -179,7 +177,7 @@ __global__ void k_update_p(int64_t n, const double* __restrict__ beta, const dou
     const int64_t cnt = n * TILE;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t o = t * cnt + i;
-        p[o] = z[o] + beta[t * TILE + (i & 7)] * p[o];
+        p[o] = z[o] + beta[t * TILE + (i % TILE)] * p[o];
     }
 }
 
@@ -238,7 +236,7 @@ __global__ void k_cols_beta(int64_t ld, ColState S) {
 }
 
 // ---------------------------------------------------------------- SpMM and triangular solves
-// Warp per row; lane = slot * 8 + column.  xt points at the tile's slab (row stride 8 doubles).
+// Warp per row; lane = slot * TILE + column.  xt points at the tile's slab (row stride TILE doubles).
 // Two independent gathers per lane per step keep more loads in flight.
 __device__ __forceinline__ double warp_row_gather(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                                                   const double* __restrict__ val, int64_t row, const double* xt,
@@ -330,12 +328,31 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(int64_t n, const int32_t* __re
 
 
 // ---------------------------------------------------------------- chunked gather (SpMM-shaped work)
-// A chunk is a run of consecutive stored rows with at most CHUNK_CAP entries (or one longer row).  The
-// block stages the chunk's (index, value) pairs in shared memory with coalesced loads, then each
-// (row, column) thread sums its row with independent gathers from the tile slab, so many loads are
-// in flight per thread.  Modes: SpMM (+ p.q partials), forward solve, backward solve.
+// A chunk is a run of consecutive stored rows with at most CHUNK_CAP entries and CHUNK_ROWS rows (or
+// one longer row).  Each warp owns whole chunks: it stages the chunk's (index, value) pairs in its own
+// shared-memory slice with coalesced streaming loads (the matrix is read once per tile and should not
+// evict the gathered slab from L2), then every (row, column) lane pair sums its row with independent
+// gathers from the tile slab.  Warps never wait for each other.  Modes: SpMM (+ p.q partials),
+// forward solve, backward solve.
 enum { M_SPMM = 0, M_FWD = 1, M_BWD = 2 };
 constexpr int CH_THREADS = 256;
+constexpr int CH_WARPS = CH_THREADS / 32;
+
+template <int MODE>
+__device__ __forceinline__ void chunk_epilogue(double* out, const double* aux, const double* xt, int64_t toff,
+                                               int64_t v, int col, double acc, double& dot) {
+    const int64_t o = toff + v * TILE + col;
+    if (MODE == M_SPMM) {
+        out[o] = acc;
+        dot += acc * xt[v * TILE + col];
+    } else if (MODE == M_FWD) {
+        out[o] = aux[o] - acc;
+    } else {
+        const double d = aux[v];
+        const double yu = out[o];
+        out[o] = (d != 0.0 ? yu / d : yu) - acc;
+    }
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks,
@@ -345,83 +362,60 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
                                                         const int32_t* __restrict__ rowmap, const double* xsrc,
                                                         double* out, const double* __restrict__ aux, int64_t ld,
                                                         double* __restrict__ part) {
-    __shared__ int32_t s_idx[CHUNK_CAP];
-    __shared__ double s_val[CHUNK_CAP];
-    __shared__ int32_t s_ptr[CHUNK_ROWS + 1];
+    __shared__ int32_t s_idx[CH_WARPS][CHUNK_CAP];
+    __shared__ double s_val[CH_WARPS][CHUNK_CAP];
+    __shared__ int32_t s_ptr[CH_WARPS][CHUNK_ROWS + 1];
     __shared__ double s_red[CH_THREADS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t t = blockIdx.y;
     const int64_t toff = t * n * TILE;
     const double* xt = xsrc + toff;
-    double dot = 0.0;  // SpMM: per-thread partial of p.q for column (tid & 7)
-    for (int32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    int32_t* si = s_idx[w];
+    double* sv = s_val[w];
+    int32_t* sp = s_ptr[w];
+    double dot = 0.0;  // SpMM: per-lane partial of p.q for column (lane % TILE)
+    for (int32_t c = blockIdx.x * CH_WARPS + w; c < nchunks; c += gridDim.x * CH_WARPS) {
         const int32_t r0 = cstart[c], r1 = cstart[c + 1];
         const int64_t e0 = ptr[r0], e1 = ptr[r1];
         const int64_t ne = e1 - e0;
         if (ne <= CHUNK_CAP) {
-            for (int64_t i = threadIdx.x; i < ne; i += CH_THREADS) {
-                s_idx[i] = idx[e0 + i];
-                s_val[i] = val[e0 + i];
+            for (int64_t i = lane; i < ne; i += 32) {
+                si[i] = __ldcs(idx + e0 + i);
+                sv[i] = __ldcs(val + e0 + i);
             }
-            for (int32_t i = threadIdx.x; i <= r1 - r0; i += CH_THREADS) s_ptr[i] = (int32_t)(ptr[r0 + i] - e0);
-            __syncthreads();
+            for (int32_t i = lane; i <= r1 - r0; i += 32) sp[i] = (int32_t)(ptr[r0 + i] - e0);
+            __syncwarp();
             const int32_t pairs = (r1 - r0) * TILE;
-            for (int32_t pr = threadIdx.x; pr < pairs; pr += CH_THREADS) {
-                const int32_t rr = pr >> 3, col = pr & 7;
-                const int32_t q0 = s_ptr[rr], q1 = s_ptr[rr + 1];
+            for (int32_t pr = lane; pr < pairs; pr += 32) {
+                const int32_t rr = pr / TILE, col = pr % TILE;
+                const int32_t q0 = sp[rr], q1 = sp[rr + 1];
                 double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
                 int32_t q = q0;
                 for (; q + 3 < q1; q += 4) {
-                    a0 += s_val[q] * xt[(int64_t)s_idx[q] * TILE + col];
-                    a1 += s_val[q + 1] * xt[(int64_t)s_idx[q + 1] * TILE + col];
-                    a2 += s_val[q + 2] * xt[(int64_t)s_idx[q + 2] * TILE + col];
-                    a3 += s_val[q + 3] * xt[(int64_t)s_idx[q + 3] * TILE + col];
+                    a0 += sv[q] * xt[(int64_t)si[q] * TILE + col];
+                    a1 += sv[q + 1] * xt[(int64_t)si[q + 1] * TILE + col];
+                    a2 += sv[q + 2] * xt[(int64_t)si[q + 2] * TILE + col];
+                    a3 += sv[q + 3] * xt[(int64_t)si[q + 3] * TILE + col];
                 }
-                for (; q < q1; q++) a0 += s_val[q] * xt[(int64_t)s_idx[q] * TILE + col];
-                const double acc = (a0 + a1) + (a2 + a3);
+                for (; q < q1; q++) a0 += sv[q] * xt[(int64_t)si[q] * TILE + col];
                 const int64_t row = r0 + rr;
-                const int64_t v = rowmap ? rowmap[row] : row;
-                const int64_t o = toff + v * TILE + col;
-                if (MODE == M_SPMM) {
-                    out[o] = acc;
-                    dot += acc * xt[v * TILE + col];
-                } else if (MODE == M_FWD) {
-                    out[o] = aux[toff + v * TILE + col] - acc;
-                } else {
-                    const double d = aux[v];
-                    const double yu = out[o];
-                    out[o] = (d != 0.0 ? yu / d : yu) - acc;
-                }
+                chunk_epilogue<MODE>(out, aux, xt, toff, rowmap ? rowmap[row] : row, col, (a0 + a1) + (a2 + a3), dot);
             }
-            __syncthreads();
+            __syncwarp();
         } else {
-            // one long row: 32 entry lanes x 8 columns, then a reduction over the entry lanes
-            const int el = threadIdx.x >> 3, col = threadIdx.x & 7;
+            // one long row: (32 / TILE) entry slots x TILE columns per step, then a reduction over the slots
+            const int slot = lane / TILE, col = lane % TILE;
             double a0 = 0.0, a1 = 0.0;
-            int64_t q = e0 + el;
-            for (; q + 32 < e1; q += 64) {
-                a0 += val[q] * xt[(int64_t)idx[q] * TILE + col];
-                a1 += val[q + 32] * xt[(int64_t)idx[q + 32] * TILE + col];
+            int64_t q = e0 + slot;
+            for (; q + SLOTS < e1; q += 2 * SLOTS) {
+                a0 += __ldcs(val + q) * xt[(int64_t)__ldcs(idx + q) * TILE + col];
+                a1 += __ldcs(val + q + SLOTS) * xt[(int64_t)__ldcs(idx + q + SLOTS) * TILE + col];
             }
-            if (q < e1) a0 += val[q] * xt[(int64_t)idx[q] * TILE + col];
-            s_red[threadIdx.x] = a0 + a1;
-            __syncthreads();
-            if (threadIdx.x < TILE) {
-                double acc = 0.0;
-                for (int i = 0; i < CH_THREADS / TILE; i++) acc += s_red[i * TILE + threadIdx.x];
-                const int64_t v = rowmap ? rowmap[r0] : r0;
-                const int64_t o = toff + v * TILE + threadIdx.x;
-                if (MODE == M_SPMM) {
-                    out[o] = acc;
-                    dot += acc * xt[v * TILE + threadIdx.x];
-                } else if (MODE == M_FWD) {
-                    out[o] = aux[o] - acc;
-                } else {
-                    const double d = aux[v];
-                    const double yu = out[o];
-                    out[o] = (d != 0.0 ? yu / d : yu) - acc;
-                }
-            }
-            __syncthreads();
+            if (q < e1) a0 += __ldcs(val + q) * xt[(int64_t)__ldcs(idx + q) * TILE + col];
+            double acc = a0 + a1;
+#pragma unroll
+            for (int o = TILE; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane < TILE) chunk_epilogue<MODE>(out, aux, xt, toff, rowmap ? rowmap[r0] : r0, col, acc, dot);
         }
     }
     if (MODE == M_SPMM && part) {
@@ -437,7 +431,9 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
 
 // blocks per tile: about one wave of resident blocks, so the gathered slab of the tile being worked
 // on is the only one live in L2
-static int chunk_blocks(int32_t nchunks) { return std::max(1, std::min(nchunks, 148 * 6)); }
+static int chunk_blocks(int32_t nchunks) {
+    return std::max(1, std::min((nchunks + CH_WARPS - 1) / CH_WARPS, 148 * 6));
+}
 
 // Runs of thin levels: the k columns are independent, so one block per 8-column tile can walk a run
 // of consecutive levels on its own, with only a block barrier between levels (its own writes are the
@@ -669,7 +665,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
     Precond P;
     int64_t pc_launches = 0;
     int32_t it = 0;
-    EventPairs ev_spmm, ev_pc;
+    EventPairs ev_spmm, ev_pc, ev_loop;
     if (active > 0) {
         build_precond_graph(C, F, n, r, z, ld, P, pc_launches);
         ev_pc.begin(C.stream);
@@ -678,6 +674,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         C.kernels_launched += pc_launches;
         R.run<OP_DOT>(r, z, S.rz);
         SSP_CUDA(cudaMemcpyAsync(p, z, sizeof(double) * total, cudaMemcpyDeviceToDevice, C.stream));
+        ev_loop.begin(C.stream);
         while (it < opt.max_iters) {
             ev_spmm.begin(C.stream);
             k_chunked<M_SPMM><<<sgrid, CH_THREADS, 0, C.stream>>>(n, d_achunks, anch, lap_ptr, lap_idx, lap_val,
@@ -696,6 +693,16 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
             SSP_CHECK_LAUNCH();
             C.kernels_launched++;
             active = read_i64(C, nact);
+            if (opt.history) {
+                std::vector<double> hrr(k), hbb(k);
+                SSP_CUDA(cudaMemcpyAsync(hrr.data(), S.rr, sizeof(double) * k, cudaMemcpyDeviceToHost, C.stream));
+                SSP_CUDA(cudaMemcpyAsync(hbb.data(), S.bnorm2, sizeof(double) * k, cudaMemcpyDeviceToHost, C.stream));
+                SSP_CUDA(cudaStreamSynchronize(C.stream));
+                double mx = 0.0;
+                for (int32_t j = 0; j < k; j++)
+                    if (hbb[j] > 0) mx = std::max(mx, std::sqrt(hrr[j] / hbb[j]));
+                opt.history->push_back(mx);
+            }
             if (opt.verbose && (it % 10 == 0 || active == 0))
                 fprintf(stderr, "[ssp] pcg iter %d: %lld columns active\n", it, (long long)active);
             if (active == 0) break;
@@ -709,6 +716,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
             SSP_CHECK_LAUNCH();
             C.kernels_launched += 2;
         }
+        ev_loop.end(C.stream);
     }
     // true relative residual ||(Y - mean) - A x|| / ||Y - mean||
     k_chunked<M_SPMM><<<sgrid, CH_THREADS, 0, C.stream>>>(n, d_achunks, anch, lap_ptr, lap_idx, lap_val, nullptr, x,
@@ -738,6 +746,8 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
     rep.n_spmm = (int64_t)ev_spmm.used;
     rep.ms_precond = ev_pc.total_ms();
     rep.n_precond = (int64_t)ev_pc.used;
+    rep.ms_loop = ev_loop.total_ms();
+    rep.iters_run = it;
     if (x_out) *x_out = x;
 }
 

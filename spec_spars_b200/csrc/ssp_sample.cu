@@ -21,8 +21,8 @@ __global__ void __launch_bounds__(256) k_diff_norms(int64_t m, const int32_t* __
         const int64_t a = v1[e], b = v2[e];
         double s = 0.0;
         for (int32_t j = lane; j < k; j += 32) {
-            const int64_t oa = TM ? ((int64_t)(j >> 3) * n + a) * 8 + (j & 7) : a * ldz + j;
-            const int64_t ob = TM ? ((int64_t)(j >> 3) * n + b) * 8 + (j & 7) : b * ldz + j;
+            const int64_t oa = TM ? tile_off(n, a, j) : a * ldz + j;
+            const int64_t ob = TM ? tile_off(n, b, j) : b * ldz + j;
             const double x = __dsub_rn(Z[oa], Z[ob]);
             s = __fma_rn(x, x, s);
         }

@@ -10,7 +10,7 @@
 // every store instruction writes 32 consecutive doubles.  The 256 sign bits of one edge come from
 // one Philox4x64 call; up to 32 edges are hashed at once (one per lane) and their words are
 // broadcast with shuffles.  The output is row-major (leading dimension ldy) or tile-major (the
-// PCG layout: 8-column slabs of n x 8).
+// PCG layout, see tile_off).
 #include "ssp_internal.cuh"
 
 namespace ssp {
@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, const int64_t* _
 #pragma unroll
         for (int t = 0; t < 8; t++) {
             const int64_t col = (int64_t)tile * 256 + lane + 32 * t;
-            if (col < k) Y[tm ? ((col >> 3) * n + v) * 8 + (col & 7) : v * ldy + col] = acc[t];
+            if (col < k) Y[tm ? tile_off(n, v, col) : v * ldy + col] = acc[t];
         }
     }
 }
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, const int64_t* _
 #pragma unroll
         for (int t = 0; t < 8; t++) {
             const int64_t col = (int64_t)tile * 256 + lane + 32 * t;
-            if (col < k) Y[tm ? ((col >> 3) * n + v) * 8 + (col & 7) : v * ldy + col] = acc[t];
+            if (col < k) Y[tm ? tile_off(n, v, col) : v * ldy + col] = acc[t];
         }
     }
 }

@@ -172,13 +172,13 @@ def test_sample_apply_bit_exact(ssp, ora, ctx, reweight):
     assert np.array_equal(H.colptr, hcp) and np.array_equal(H.rowidx, hri) and np.array_equal(H.values, hva)
 
 
-def _oracle_pipeline(ora, ssp, G, params):
+def _oracle_pipeline(ora, ssp, G, params, max_degree):
     (v1, v2, w), (cp, ri, va) = _oracle_graph(ora, G)
     n = G.n
     k = params.jl_dim(n)
     s = params.jl_scale(k)
     Y = ora.sketch(n, v1, v2, w, k, s, params.sketch_seed, params.sketch_uniform)
-    F = ora.Factor(n, cp, ri, va, params.factor_seed, params.dense_threshold, params.factor_max_degree)
+    F = ora.Factor(n, cp, ri, va, params.factor_seed, params.dense_threshold, max_degree)
     Z, it, rel, rc = ora.pcg(n, cp, ri, va, F, Y, params.pcg_tol, params.pcg_abs_tol, params.pcg_max_iters)
     d = ora.diff_norms(v1, v2, Z)
     denom = k * s * s if params.prob_variance_correction else float(k)
@@ -195,7 +195,7 @@ def test_sparsify_config_grid2d_100(ssp, ora, ctx):
     prm = ssp.SparsifierParameters.baseline(0.5, pcg_tol=1e-8)
     H, st = ctx.sparsify(G, prm)
     assert st["k"] == 885 and st["m_in"] == 19_800
-    o = _oracle_pipeline(ora, ssp, G, prm)
+    o = _oracle_pipeline(ora, ssp, G, prm, st["factor_max_degree_used"])
     # leverage estimates agree to the solver tolerance; p equals wherever it is clipped at 1
     assert st["pcg_max_relres"] < 1e-7
     sp_run = ssp.Sparsifier(G, prm, ctx)
