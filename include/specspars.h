@@ -238,6 +238,23 @@ int ssp_stage_coins(ssp_context* ctx, int64_t m, uint64_t seed, int32_t mem, dou
 int ssp_stage_sample_apply(ssp_context* ctx, const ssp_csc* graph, const double* p, const double* coins,
                            int32_t reweight, int32_t mem, uint8_t* keep, ssp_csc_out* out);
 
+/* ---- allocation-free leverage stage (no counterpart in the reference) ----
+ * p[e] = min(((beta*w[e]) * d_e^2) / denom, 1) with d_e = ||Z[v1[e],:] - Z[v2[e],:]||_2, the same values as
+ * ssp_stage_diff_norms followed by ssp_stage_probs.  For callers that must not allocate device memory after
+ * start-up -- a host whose HBM is owned by its own pool under a fixed budget, or one that cannot take the
+ * device-wide synchronisation a cudaFree implies: it needs no ssp_context and calls no cudaMalloc/cudaFree.
+ * All pointers are device pointers on the current device; Z is row-major n x k; the work is enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and the call returns without synchronising.
+ * d lives in a static device array of SSP_STATIC_SCRATCH_EDGES doubles: m above that returns
+ * SSP_ERR_CAPACITY before anything is launched; nothing in it must start at zero.  The array is shared by
+ * all calls on a device, so overlapping calls (two streams or threads in flight at once) race: serialise
+ * them.  The first call with each device current looks the array up with cudaGetSymbolAddress; make that
+ * first call before any stream capture.  An edge with an endpoint outside [0, n) gets p = 1 (d = NaN). */
+#define SSP_STATIC_SCRATCH_EDGES (1 << 20)
+int ssp_stage_leverage_probs_static(void* stream, int64_t n, int64_t m, const int32_t* v1, const int32_t* v2,
+                                    const double* Z, int32_t k, const double* w, double beta, double denom,
+                                    double* p);
+
 #ifdef __cplusplus
 }
 #endif

@@ -136,6 +136,7 @@ def lib():
             "ssp_stage_coins": ([P, I64, U64, I32, P], ctypes.c_int),
             "ssp_stage_sample_apply": ([P, ctypes.POINTER(_Csc), P, P, I32, I32, P, ctypes.POINTER(_CscOut)],
                                        ctypes.c_int),
+            "ssp_stage_leverage_probs_static": ([P, I64, I64, P, P, P, I32, P, DBL, DBL, P], ctypes.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)

@@ -16,9 +16,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
           "--expt-relaxed-constexpr", "-Xptxas", "-O3"]
 # Translation units whose results must be bit-identical to the CPU oracle: no FMA contraction.
-EXACT = {"ssp_graph.cu", "ssp_sketch.cu", "ssp_factor.cu", "ssp_sample.cu"}
+EXACT = {"ssp_graph.cu", "ssp_sketch.cu", "ssp_factor.cu", "ssp_sample.cu", "ssp_noalloc.cu"}
 SOURCES = ["ssp_util.cu", "ssp_graph.cu", "ssp_sketch.cu", "ssp_factor.cu", "ssp_pcg.cu", "ssp_sample.cu",
-           "ssp_autotune.cu", "ssp_api.cu", "ssp_host.cpp"]
+           "ssp_autotune.cu", "ssp_noalloc.cu", "ssp_api.cu", "ssp_host.cpp"]
 HEADERS = ["ssp_internal.cuh", "ssp_sort.cuh", "ssp_host.h"]
 
 

@@ -1,0 +1,122 @@
+// ssp_noalloc.cu -- the leverage-probability stage without any allocation.
+//
+// ssp_stage_leverage_probs_static computes, for every edge e = (v1_e, v2_e),
+//     d_e = || Z[v1_e, :] - Z[v2_e, :] ||_2          (the per-edge effective-resistance estimate)
+//     p_e = min(((beta * w_e) * d_e^2) / denom, 1)    (the sampling probability)
+// with the same arithmetic, in the same order, as ssp_stage_diff_norms followed by ssp_stage_probs.
+// The intermediate d lives in a file-scope device array instead of the context workspace, so the call
+// needs no ssp_context and performs no cudaMalloc/cudaFree: it is meant for hosts whose device memory is
+// owned by their own pool with a fixed budget, or that cannot accept the device-wide synchronisation a
+// cudaFree implies, after start-up.
+//
+// Scratch contract:
+//   * capacity SSP_STATIC_SCRATCH_EDGES doubles (8 MiB); larger m is rejected with SSP_ERR_CAPACITY
+//     before anything is launched;
+//   * nothing in the scratch has to start at zero: entries [0, m) are written before they are read;
+//   * the scratch is shared by every call on a device, so two calls in flight at the same time on one
+//     device (different streams or host threads) race -- callers serialise them (one stream, or events);
+//   * the scratch address is looked up with cudaGetSymbolAddress on the first call made with each device
+//     current; that first call should come before any stream capture.
+#include <atomic>
+#include <cstdio>
+
+#include "ssp_internal.cuh"
+
+namespace {
+
+static __device__ __align__(256) double g_ssp_static_scratch[SSP_STATIC_SCRATCH_EDGES];
+
+constexpr int kMaxDevices = 64;
+std::atomic<double*> g_scratch_addr[kMaxDevices];
+
+// d_e into the scratch: one warp per edge, lanes stride the k columns of row-major Z (leading dimension
+// k), a lane-local fused multiply-add chain, then a fixed xor-butterfly -- the order of k_diff_norms.
+// An edge with an endpoint outside [0, n) is not read and gets d_e = NaN.
+__global__ void __launch_bounds__(256) k_norms_static(int64_t n, int64_t m, const int32_t* __restrict__ v1,
+                                                      const int32_t* __restrict__ v2, const double* __restrict__ Z,
+                                                      int32_t k, double* __restrict__ d) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < m; e += nw) {
+        const int64_t a = v1[e], b = v2[e];
+        if (a < 0 || a >= n || b < 0 || b >= n) {
+            if (lane == 0) d[e] = __longlong_as_double(0x7ff8000000000000LL);
+            continue;
+        }
+        double s = 0.0;
+        for (int32_t j = lane; j < k; j += 32) {
+            const double x = __dsub_rn(Z[a * k + j], Z[b * k + j]);
+            s = __fma_rn(x, x, s);
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+        if (lane == 0) d[e] = sqrt(s);
+    }
+}
+
+// p_e from the scratch d_e, as k_probs: a NaN ratio maps to probability 1.
+__global__ void k_probs_static(int64_t m, const double* __restrict__ w, const double* __restrict__ d, double beta,
+                               double denom, double* __restrict__ p) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
+        const double d2 = __dmul_rn(d[e], d[e]);
+        const double x = __ddiv_rn(__dmul_rn(__dmul_rn(beta, w[e]), d2), denom);
+        p[e] = (x < 1.0) ? x : 1.0;
+        if (x != x) p[e] = 1.0;
+    }
+}
+
+int fail(int code, const char* msg) {
+    ssp::set_last_error(msg);
+    return code;
+}
+
+}  // namespace
+
+extern "C" int ssp_stage_leverage_probs_static(void* stream, int64_t n, int64_t m, const int32_t* v1,
+                                               const int32_t* v2, const double* Z, int32_t k, const double* w,
+                                               double beta, double denom, double* p) {
+    char msg[192];
+    if (m < 0 || n < 0 || k <= 0)
+        return fail(SSP_ERR_INVALID, "ssp_stage_leverage_probs_static: need n >= 0, m >= 0, k > 0");
+    if (m > (int64_t)SSP_STATIC_SCRATCH_EDGES) {
+        snprintf(msg, sizeof msg,
+                 "ssp_stage_leverage_probs_static: m = %lld edges exceeds the static scratch capacity of %lld edges",
+                 (long long)m, (long long)SSP_STATIC_SCRATCH_EDGES);
+        return fail(SSP_ERR_CAPACITY, msg);
+    }
+    if (m == 0) return SSP_OK;
+    if (!v1 || !v2 || !Z || !w || !p)
+        return fail(SSP_ERR_INVALID, "ssp_stage_leverage_probs_static: null device pointer");
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        snprintf(msg, sizeof msg, "ssp_stage_leverage_probs_static: cudaGetDevice: %s",
+                 e != cudaSuccess ? cudaGetErrorString(e) : "device index out of range");
+        return fail(e == cudaErrorNoDevice ? SSP_ERR_NO_DEVICE : SSP_ERR_CUDA, msg);
+    }
+    double* d = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!d) {
+        void* addr = nullptr;
+        e = cudaGetSymbolAddress(&addr, g_ssp_static_scratch);
+        if (e != cudaSuccess || !addr) {
+            snprintf(msg, sizeof msg, "ssp_stage_leverage_probs_static: cudaGetSymbolAddress: %s",
+                     cudaGetErrorString(e));
+            return fail(SSP_ERR_CUDA, msg);
+        }
+        d = static_cast<double*>(addr);
+        g_scratch_addr[dev].store(d, std::memory_order_release);
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t warp_blocks = (m * 32 + 255) / 256;
+    const int g1 = (int)(warp_blocks < 148 * 16 ? warp_blocks : 148 * 16);
+    k_norms_static<<<g1, 256, 0, s>>>(n, m, v1, v2, Z, k, d);
+    const int64_t blocks = (m + 255) / 256;
+    const int g2 = (int)(blocks < 148 * 32 ? blocks : 148 * 32);
+    k_probs_static<<<g2, 256, 0, s>>>(m, w, d, beta, denom, p);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        snprintf(msg, sizeof msg, "ssp_stage_leverage_probs_static: launch: %s", cudaGetErrorString(e));
+        return fail(SSP_ERR_CUDA, msg);
+    }
+    return SSP_OK;
+}
