@@ -1,0 +1,209 @@
+// mkl_rci_shim.cc -- the handful of Intel MKL routines the reference's PCG driver calls
+// (include/custom_cg.hpp:95-274), written from MKL's public API documentation so that the reference solver
+// can be compiled and run without MKL.  Test infrastructure only: used to build oracle/_ref/ref_solve.
+//
+// dcg_* follow the documented reverse-communication protocol of MKL's CG solver:
+//   tmp is n x 4 column-major: tmp[0:n] = the vector to multiply by A (the search direction),
+//   tmp[n:2n] = A * tmp[0:n], tmp[2n:3n] = the residual r, tmp[3n:4n] = the preconditioned residual.
+//   RCI_request 1: caller computes tmp[n:2n] = A tmp[0:n]; 2: caller's stopping test (dpar[4] = ||r||^2);
+//   3: caller applies the preconditioner tmp[2n:3n] -> tmp[3n:4n]; 0: converged (built-in test);
+//   -1: iteration limit ipar[4] reached (when ipar[7] != 0).
+//   ipar[3] counts iterations; dpar[0] relative tolerance, dpar[1] absolute tolerance, dpar[2] ||r0||^2,
+//   dpar[3] = dpar[0] * dpar[2] + dpar[1], dpar[4] current ||r||^2, dpar[5] previous ||r||^2,
+//   dpar[6] alpha, dpar[7] beta.  The iteration is textbook preconditioned CG from x0.
+// MKL's own summation orders are not reproduced, so iterates agree with MKL's to rounding only.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "mkl.h"
+
+struct sparse_matrix {
+    MKL_INT rows, cols;
+    const MKL_INT* rs;
+    const MKL_INT* re;
+    const MKL_INT* ci;
+    const double* v;
+};
+
+namespace {
+// private solver state kept in ipar[] slots the documentation reserves for internal use
+constexpr int kState = 100;
+enum { S_START = 0, S_AFTER_AX0 = 1, S_AFTER_PREC = 2, S_AFTER_AP = 3, S_AFTER_USER = 4 };
+
+// vector kernels run on all OpenMP threads, as MKL's threaded layer does
+double dot(MKL_INT n, const double* a, const double* b) {
+    double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+    for (MKL_INT i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+}
+}  // namespace
+
+void dcg_init(const MKL_INT* n, const double*, const double*, MKL_INT* rci, MKL_INT* ipar, double* dpar,
+              double*) {
+    for (int i = 0; i < 128; ++i) ipar[i] = 0, dpar[i] = 0.0;
+    ipar[0] = *n;
+    ipar[1] = 6;
+    ipar[4] = *n < 150 ? *n : 150;
+    ipar[7] = 1;
+    ipar[9] = 1;
+    dpar[0] = 1e-6;
+    ipar[kState] = S_START;
+    *rci = 0;
+}
+
+void dcg_check(const MKL_INT* n, const double*, const double*, MKL_INT* rci, MKL_INT* ipar, double*, double*) {
+    *rci = (ipar[0] == *n && *n > 0) ? 0 : -1100;
+    ipar[kState] = S_START;
+}
+
+void dcg(const MKL_INT* np, double* x, const double* b, MKL_INT* rci, MKL_INT* ipar, double* dpar, double* tmp) {
+    const MKL_INT n = *np;
+    double* p = tmp;
+    double* q = tmp + n;
+    double* r = tmp + 2 * n;
+    double* z = tmp + 3 * n;
+    for (;;) {
+        switch (ipar[kState]) {
+            case S_START:
+                std::memcpy(p, x, sizeof(double) * n);
+                ipar[3] = 0;
+                ipar[kState] = S_AFTER_AX0;
+                *rci = 1;
+                return;
+            case S_AFTER_AX0:
+#pragma omp parallel for schedule(static)
+                for (MKL_INT i = 0; i < n; ++i) r[i] = b[i] - q[i];
+                dpar[2] = dot(n, r, r);
+                dpar[4] = dpar[2];
+                dpar[3] = dpar[0] * dpar[2] + dpar[1];
+                ipar[kState] = S_AFTER_USER;
+                continue;
+            case S_AFTER_USER:
+                if (ipar[7] && ipar[3] >= ipar[4]) {
+                    *rci = -1;
+                    return;
+                }
+                if (ipar[10]) {
+                    ipar[kState] = S_AFTER_PREC;
+                    *rci = 3;
+                    return;
+                }
+                std::memcpy(z, r, sizeof(double) * n);
+                ipar[kState] = S_AFTER_PREC;
+                continue;
+            case S_AFTER_PREC: {
+                const double rho = dot(n, r, z);
+                if (ipar[3] == 0) {
+                    std::memcpy(p, z, sizeof(double) * n);
+                } else {
+                    const double beta = rho / dpar[8];
+                    dpar[7] = beta;
+#pragma omp parallel for schedule(static)
+                    for (MKL_INT i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+                }
+                dpar[8] = rho;
+                ipar[kState] = S_AFTER_AP;
+                *rci = 1;
+                return;
+            }
+            case S_AFTER_AP: {
+                const double alpha = dpar[8] / dot(n, p, q);
+                dpar[6] = alpha;
+#pragma omp parallel for schedule(static)
+                for (MKL_INT i = 0; i < n; ++i) {
+                    x[i] += alpha * p[i];
+                    r[i] -= alpha * q[i];
+                }
+                ipar[3] += 1;
+                dpar[5] = dpar[4];
+                dpar[4] = dot(n, r, r);
+                ipar[kState] = S_AFTER_USER;
+                if (ipar[8] && dpar[4] <= dpar[3]) {
+                    *rci = 0;
+                    return;
+                }
+                if (ipar[9]) {
+                    *rci = 2;
+                    return;
+                }
+                continue;
+            }
+            default:
+                *rci = -10000;
+                return;
+        }
+    }
+}
+
+sparse_status_t mkl_sparse_d_create_csr(sparse_matrix_t* A, sparse_index_base_t indexing, MKL_INT rows,
+                                        MKL_INT cols, MKL_INT* rows_start, MKL_INT* rows_end, MKL_INT* col_indx,
+                                        double* values) {
+    if (!A || indexing != SPARSE_INDEX_BASE_ZERO) return SPARSE_STATUS_INVALID_VALUE;
+    *A = new sparse_matrix{rows, cols, rows_start, rows_end, col_indx, values};
+    return SPARSE_STATUS_SUCCESS;
+}
+
+sparse_status_t mkl_sparse_destroy(sparse_matrix_t A) {
+    delete A;
+    return SPARSE_STATUS_SUCCESS;
+}
+
+// y = alpha * op(A) x + beta * y.  The reference calls it with a fully stored symmetric matrix
+// (SPARSE_FILL_MODE_FULL), which is a plain CSR product.
+sparse_status_t mkl_sparse_d_mv(sparse_operation_t op, double alpha, const sparse_matrix_t A,
+                                struct matrix_descr descr, const double* x, double beta, double* y) {
+    if (op != SPARSE_OPERATION_NON_TRANSPOSE || descr.mode != SPARSE_FILL_MODE_FULL)
+        return SPARSE_STATUS_INVALID_VALUE;
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (MKL_INT i = 0; i < A->rows; ++i) {
+        double s = 0.0;
+        for (MKL_INT t = A->rs[i]; t < A->re[i]; ++t) s += A->v[t] * x[A->ci[t]];
+        y[i] = alpha * s + (beta == 0.0 ? 0.0 : beta * y[i]);
+    }
+    return SPARSE_STATUS_SUCCESS;
+}
+
+// Triangular solve with the upper triangle (diagonal included) of the CSR matrix A:
+// NON_TRANSPOSE solves U y = alpha x (backward), TRANSPOSE solves U^T y = alpha x (forward, row-oriented
+// scatter).  Entries below the diagonal are ignored, as SPARSE_FILL_MODE_UPPER specifies.
+sparse_status_t mkl_sparse_d_trsv(sparse_operation_t op, double alpha, const sparse_matrix_t A,
+                                  struct matrix_descr descr, const double* x, double* y) {
+    if (descr.type != SPARSE_MATRIX_TYPE_TRIANGULAR || descr.mode != SPARSE_FILL_MODE_UPPER)
+        return SPARSE_STATUS_INVALID_VALUE;
+    const MKL_INT n = A->rows;
+    const bool unit = descr.diag == SPARSE_DIAG_UNIT;
+    auto diag = [&](MKL_INT i) {
+        if (unit) return 1.0;
+        for (MKL_INT t = A->rs[i]; t < A->re[i]; ++t)
+            if (A->ci[t] == i) return A->v[t];
+        return 0.0;
+    };
+    if (op == SPARSE_OPERATION_NON_TRANSPOSE) {
+        for (MKL_INT i = n - 1; i >= 0; --i) {
+            double s = alpha * x[i];
+            for (MKL_INT t = A->rs[i]; t < A->re[i]; ++t)
+                if (A->ci[t] > i) s -= A->v[t] * y[A->ci[t]];
+            y[i] = s / diag(i);
+        }
+    } else {
+        std::vector<double> acc(x, x + n);
+        for (MKL_INT i = 0; i < n; ++i) acc[i] *= alpha;
+        for (MKL_INT i = 0; i < n; ++i) {
+            const double yi = acc[i] / diag(i);
+            y[i] = yi;
+            for (MKL_INT t = A->rs[i]; t < A->re[i]; ++t)
+                if (A->ci[t] > i) acc[A->ci[t]] -= A->v[t] * yi;
+        }
+    }
+    return SPARSE_STATUS_SUCCESS;
+}
+
+double cblas_dnrm2(const MKL_INT n, const double* x, const MKL_INT incx) {
+    double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+    for (MKL_INT i = 0; i < n; ++i) s += x[(size_t)i * incx] * x[(size_t)i * incx];
+    return std::sqrt(s);
+}
+

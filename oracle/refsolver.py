@@ -1,0 +1,63 @@
+"""Runs the reference's own CPU Laplacian solver (src/example.cc factorization_driver + include/custom_cg.hpp,
+built into oracle/_ref/ref_solve by oracle/ref/Makefile) as a subprocess.
+
+Test infrastructure only: tests/ and bench.py's reference/CPU legs use it to check the oracle and to time
+the reference's CPU path.  It is a separate process because the reference asserts and throws on failure.
+"""
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BIN = os.path.join(HERE, "_ref", "ref_solve")
+
+
+def available():
+    return os.path.exists(BIN) and os.access(BIN, os.X_OK)
+
+
+def build(ref_root="/root/reference"):
+    """Compile ref_solve from the reference sources when they are present (never on a machine without them)."""
+    if not os.path.exists(os.path.join(ref_root, "src", "example.cc")):
+        return available()
+    r = subprocess.run(["make", "-s", f"REF={ref_root}"], cwd=os.path.join(HERE, "ref"), capture_output=True,
+                       text=True)
+    if r.returncode != 0:
+        raise RuntimeError("building the reference solver failed:\n" + r.stdout + r.stderr)
+    return available()
+
+
+def solve(n, colptr, rowidx, values, rhs, threads=1, verbose=False, timeout=600):
+    """Solve L x_j = b_j for the columns of rhs (n x k) with the reference solver.
+
+    Returns (status, seconds, X): status 0 = every column converged (relative residual < 0.01,
+    custom_cg.hpp:256), 1 = the driver returned false, 2 = it threw (example.cc:566); seconds covers the
+    solver's set-up (elimination tree), factorization and all solves.
+    """
+    rhs = np.asarray(rhs, np.float64)
+    if rhs.ndim == 1:
+        rhs = rhs[:, None]
+    k = rhs.shape[1]
+    colptr = np.ascontiguousarray(colptr, np.int32)
+    rowidx = np.ascontiguousarray(rowidx, np.int32)
+    values = np.ascontiguousarray(values, np.float64)
+    with tempfile.TemporaryDirectory() as d:
+        fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(b"SSPR" + struct.pack("<4iq", n, k, threads, int(verbose), len(values)))
+            f.write(colptr.tobytes())
+            f.write(rowidx.tobytes())
+            f.write(values.tobytes())
+            f.write(np.ascontiguousarray(rhs.T).tobytes())
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        r = subprocess.run([BIN, fin, fout], capture_output=True, text=True, timeout=timeout, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_solve exited {r.returncode}: {r.stderr[-2000:]}")
+        raw = open(fout, "rb").read()
+    status, secs = struct.unpack_from("<id", raw, 0)
+    off = 12
+    X = np.frombuffer(raw, np.float64, count=k * n, offset=off).reshape(k, n).T.copy()
+    return status, secs, X
