@@ -26,6 +26,7 @@ WORKLOADS = {
     "er_n1M_deg20": ("er", dict(n=1_000_000, avg_degree=20.0, wlo=0.5, whi=2.0, seed=1), 0.5),
     "grid2d_100": ("grid2d", dict(nx=100, ny=100), 0.5),
     "er_n100k_deg20": ("er", dict(n=100_000, avg_degree=20.0, wlo=0.5, whi=2.0, seed=1), 0.5),
+    "er_n250k_deg20": ("er", dict(n=250_000, avg_degree=20.0, wlo=0.5, whi=2.0, seed=1), 0.5),
 }
 PCG_TOL = 1e-8
 
@@ -103,6 +104,11 @@ def peaks():
         return float(j["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+# DRAM bytes per (Laplacian nonzero, 8-column tile) of one FP64 SpMM launch, from the ncu capture of
+# ER n=250K, k=256 (profiles/k_chunked_spmm_er_n250k_k256.md: 3.86 GB / (5.25M nonzeros x 32 tiles))
+SPMM_TRAFFIC_PER_NNZ_TILE = 3.86e9 / (5.25e6 * 32)
 
 
 def spmm_bytes(n, nnz_lap, k):
@@ -217,6 +223,8 @@ def main():
     ap.add_argument("--workload", default="er_n1M_deg20", choices=list(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--jl-cols", type=int, default=0,
+                    help="use this many JL columns instead of ceil(24 ln n / eps^2) (smaller profiling cases)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -236,6 +244,8 @@ def main():
 
     G, eps = make_graph(S, args.workload, rank)
     prm = S.SparsifierParameters.baseline(eps, pcg_tol=PCG_TOL)
+    if args.jl_cols > 0:
+        prm.jl_dim_override = args.jl_cols
     ctx = S.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
@@ -315,8 +325,12 @@ def main():
     else:
         kern, byts, kms = "spmm (Laplacian x n-by-k block)", spmm_bytes(n, st["nnz_laplacian"], k), sp_ms
     achieved = byts / (kms / 1000.0) / 1e9 if kms > 0 else None
+    traffic = None
+    if kern.startswith("spmm"):
+        # scaled from the small-case capture by the units one launch processes
+        traffic = SPMM_TRAFFIC_PER_NNZ_TILE * st["nnz_laplacian"] * math.ceil(k / 8)
     roof = {"kernel": kern, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak if achieved else None, "traffic": None, "peak_source": src,
+            "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_source": src,
             "algorithmic_bytes_per_launch": byts, "avg_launch_ms": kms,
             "spmm_avg_ms": sp_ms, "precond_avg_ms": pc_ms,
             "spmm_GBps": spmm_bytes(n, st["nnz_laplacian"], k) / (sp_ms / 1000.0) / 1e9 if sp_ms > 0 else None,
