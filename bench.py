@@ -111,14 +111,15 @@ def peaks():
 SPMM_TRAFFIC_PER_NNZ_TILE = 3.86e9 / (5.25e6 * 32)
 
 
-def spmm_bytes(n, nnz_lap, k):
-    # compulsory traffic of q = A p over k columns: row pointers, (index, value) per nonzero, read p, write q
-    return 8 * (n + 1) + nnz_lap * (4 + 8) + 2 * n * k * 8
+def spmm_bytes(n, nnz_lap, k, s=8):
+    # compulsory traffic of q = A p over k columns: row pointers, (index, value) per nonzero, read p, write q;
+    # s = bytes per value (8 FP64, 4 for the FP32 inner solves of the mixed mode)
+    return 8 * (n + 1) + nnz_lap * (4 + s) + 2 * n * k * s
 
 
-def precond_bytes(n, nnz_l, k):
+def precond_bytes(n, nnz_l, k, s=8):
     # forward + backward triangular solves (each: pointers, L entries, read + write n x k) and D
-    return 2 * (8 * (n + 1) + nnz_l * (4 + 8) + 2 * n * k * 8) + 8 * n
+    return 2 * (8 * (n + 1) + nnz_l * (4 + s) + 2 * n * k * s) + s * n
 
 
 def cpu_baseline(eps, k_full, impl="port", budget_cols=16):
@@ -214,6 +215,75 @@ def _ref_available():
         return False
 
 
+def serving_mix(S, count, max_n, seed=4):
+    """The serving mix of seeded requests: random-geometric or ER graphs (equiprobable), n log-uniform in
+    [1e3, max_n], average degree uniform in 8..32, weights uniform [0.1, 10] rounded to FP32, eps 0.3 or 0.5."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(count):
+        n = int(10 ** rng.uniform(3.0, math.log10(max_n)))
+        d = float(rng.integers(8, 33))
+        eps = float(rng.choice([0.3, 0.5]))
+        G = S.gen_rgg(n, d, 0.1, 10.0, 1000 + i) if rng.random() < 0.5 else S.gen_er(n, d, 0.1, 10.0, 1000 + i)
+        prm = S.SparsifierParameters.baseline(eps, pcg_tol=PCG_TOL, sampling_seed=i)
+        reqs.append((G, prm))
+    return reqs
+
+
+def run_serve(args):
+    """--serve: the serving mix through the persistent request loop (ssp_server_*).  A closed-loop pass
+    (everything submitted at once) measures the capacity; the timed pass submits at Poisson arrivals at 80% of
+    that rate and reports throughput and per-request latency (submit -> done) percentiles."""
+    import numpy as np
+    import spec_spars_b200 as S
+    reqs = serving_mix(S, args.serve_requests, args.serve_max_n)
+    m_total = sum(G.nnz // 2 for G, _ in reqs)
+    if args.precision == "mixed":
+        for _, prm in reqs:
+            prm.precision = S.SSP_PRECISION_MIXED
+
+    def run_pass(srv, arrivals):
+        t0 = time.perf_counter()
+        tickets = [None] * len(reqs)
+
+        def submitter():
+            for i, (G, prm) in enumerate(reqs):
+                delay = t0 + arrivals[i] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                tickets[i] = srv.submit(G, prm)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        lat = []
+        for t in tickets:
+            _, st, tm = srv.wait(t)
+            lat.append(tm["latency_ms"])
+        return time.perf_counter() - t0, lat
+
+    with S.Server(0, slots=args.serve_slots) as srv:
+        run_pass(srv, [0.0] * len(reqs))  # warm-up: workspaces grow, modules load
+        cap_s, _ = run_pass(srv, [0.0] * len(reqs))
+        rate = 0.8 * len(reqs) / cap_s
+        rng = np.random.default_rng(5)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs))).tolist()
+        wall, lat = run_pass(srv, arrivals)
+        info = srv.info()
+    line = {"metric": "serving mix: input edges sparsified/sec", "value": m_total / wall, "unit": "edges/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f64" if args.precision == "fp64" else "mixed",
+            "data": "synthetic",
+            "config": {"workload": "serving mix", "requests": len(reqs), "n_range": [1000, args.serve_max_n],
+                       "degree_range": [8, 32], "eps": [0.3, 0.5], "slots": args.serve_slots,
+                       "arrivals": f"Poisson at {rate:.2f} req/s (0.8 x closed-loop capacity)",
+                       "precision": args.precision},
+            "closed_loop_edges_per_s": m_total / cap_s, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(np.mean(lat)), "edges": m_total,
+            "peak_inflight": info["peak_inflight"], "peak_inflight_bytes": info["peak_inflight_bytes"]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -223,9 +293,18 @@ def main():
     ap.add_argument("--workload", default="er_n1M_deg20", choices=list(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="PCG arithmetic: fp64, or FP32 inner solves inside FP64 refinement to the same tolerance")
     ap.add_argument("--jl-cols", type=int, default=0,
                     help="use this many JL columns instead of ceil(24 ln n / eps^2) (smaller profiling cases)")
+    ap.add_argument("--serve", action="store_true", help="run the serving mix through the request loop")
+    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-max-n", type=int, default=100_000)
+    ap.add_argument("--serve-slots", type=int, default=4)
     args = ap.parse_args()
+    if args.serve:
+        run_serve(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -246,6 +325,8 @@ def main():
     prm = S.SparsifierParameters.baseline(eps, pcg_tol=PCG_TOL)
     if args.jl_cols > 0:
         prm.jl_dim_override = args.jl_cols
+    if args.precision == "mixed":
+        prm.precision = S.SSP_PRECISION_MIXED
     ctx = S.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
@@ -319,26 +400,30 @@ def main():
     pc_ms = sum(s["ms_precond"] for s in stats) / max(1, sum(s["n_precond"] for s in stats))
     sp_tot = sum(s["ms_spmm"] for s in stats)
     pc_tot = sum(s["ms_precond"] for s in stats)
+    vs = 4 if args.precision == "mixed" else 8
     if pc_tot >= sp_tot:
         kern, byts, kms = "precond (fwd+bwd level-set triangular solves, all k columns)", \
-            precond_bytes(n, st["nnz_factor"], k), pc_ms
+            precond_bytes(n, st["nnz_factor"], k, vs), pc_ms
     else:
-        kern, byts, kms = "spmm (Laplacian x n-by-k block)", spmm_bytes(n, st["nnz_laplacian"], k), sp_ms
+        kern, byts, kms = "spmm (Laplacian x n-by-k block)", spmm_bytes(n, st["nnz_laplacian"], k, vs), sp_ms
     achieved = byts / (kms / 1000.0) / 1e9 if kms > 0 else None
     traffic = None
-    if kern.startswith("spmm"):
+    if kern.startswith("spmm") and vs == 8:
         # scaled from the small-case capture by the units one launch processes
         traffic = SPMM_TRAFFIC_PER_NNZ_TILE * st["nnz_laplacian"] * math.ceil(k / 8)
     roof = {"kernel": kern, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_source": src,
             "algorithmic_bytes_per_launch": byts, "avg_launch_ms": kms,
             "spmm_avg_ms": sp_ms, "precond_avg_ms": pc_ms,
-            "spmm_GBps": spmm_bytes(n, st["nnz_laplacian"], k) / (sp_ms / 1000.0) / 1e9 if sp_ms > 0 else None,
-            "precond_GBps": precond_bytes(n, st["nnz_factor"], k) / (pc_ms / 1000.0) / 1e9 if pc_ms > 0 else None}
+            "spmm_GBps": spmm_bytes(n, st["nnz_laplacian"], k, vs) / (sp_ms / 1000.0) / 1e9 if sp_ms > 0 else None,
+            "precond_GBps": precond_bytes(n, st["nnz_factor"], k, vs) / (pc_ms / 1000.0) / 1e9 if pc_ms > 0 else None}
     line = {"metric": "input edges sparsified/sec", "value": value, "unit": "edges/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 inner PCG, f64 dots + refinement",
+            "data": "synthetic",
             "config": {"workload": args.workload, "n": n, "m": m, "eps": eps, "k": k, "pcg_tol": PCG_TOL,
+                       "precision": args.precision,
                        "l2": "inputs and n-by-k working set larger than L2; no flush",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "gpu_launches": launches,
@@ -346,6 +431,7 @@ def main():
                                              "ms_sample", "ms_total")},
             "kept_fraction": st["m_out"] / st["m_in"], "pcg_iters_max": st["pcg_max_iters_used"],
             "pcg_iters_mean": st["pcg_mean_iters"], "pcg_max_relres": st["pcg_max_relres"],
+            "pcg_refinements": st["pcg_refinements"], "pcg_fp64_rounds": st["pcg_fp64_rounds"],
             "factor_nnz": st["nnz_factor"], "factor_levels": st["factor_levels"],
             "roofline": roof, "clocks": clocks.summary(), "e2e": e2e}
     if rank == 0 and not args.no_cpu_baseline:

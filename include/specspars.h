@@ -43,6 +43,7 @@ extern "C" {
 #define SSP_ERR_CAPACITY (-5)      /* internal pool capacity exceeded */
 #define SSP_ERR_IO (-6)            /* file I/O or .mtx parse error */
 #define SSP_ERR_NO_DEVICE (-7)     /* no CUDA device visible */
+#define SSP_ERR_PENDING (-8)       /* ssp_poll / ssp_wait: the request has not finished yet */
 
 #define SSP_MEM_HOST 0
 #define SSP_MEM_DEVICE 1
@@ -53,6 +54,10 @@ extern "C" {
 /* sketch entry scale */
 #define SSP_JL_SCALE_FIXED 0      /* entries +-jl_scaling_factor (lib.rs:151)   */
 #define SSP_JL_SCALE_INV_SQRT_K 1 /* entries +-1/sqrt(k)                        */
+/* arithmetic of the PCG solve */
+#define SSP_PRECISION_FP64 0  /* every vector and matrix in FP64                                     */
+#define SSP_PRECISION_MIXED 1 /* SpMM, triangular solves and vectors in FP32 with FP64 dot products,
+                                 inside FP64 iterative refinement to the same tolerance                */
 /* reweighting of kept edges */
 #define SSP_REWEIGHT_INV_SQRT_P 0 /* w / sqrt(p)  (sparsifier.rs:657)           */
 #define SSP_REWEIGHT_INV_P 1      /* w / p        (stream_sparsify.jl:135)      */
@@ -109,6 +114,7 @@ typedef struct {
                                   this; the rest is preconditioned by its diagonal (0 = eliminate all,
                                   -1 = choose by the autotuner) */
     int32_t jl_dim_override;   /* > 0: use exactly this many JL columns instead of jl_dim_rule */
+    int32_t precision;         /* SSP_PRECISION_* of the PCG solve */
 } ssp_params;
 
 typedef struct {
@@ -133,6 +139,8 @@ typedef struct {
     int64_t nnz_laplacian;
     int64_t factor_max_degree_used; /* truncation actually used (autotuner's choice when requested) */
     double ms_autotune;             /* device time spent choosing it (included in ms_factor) */
+    int32_t pcg_refinements;        /* SSP_PRECISION_MIXED: FP64 refinement rounds (0 in FP64 mode) */
+    int32_t pcg_fp64_rounds;        /* ... of which ran an FP64 inner solve after FP32 stopped contracting */
 } ssp_stats;
 
 typedef struct {
@@ -143,6 +151,7 @@ typedef struct {
     int64_t dense_threshold;
     int32_t verbose;
     int64_t factor_max_degree;
+    int32_t precision;       /* SSP_PRECISION_* */
 } ssp_solve_opts;
 
 typedef struct {
@@ -156,6 +165,8 @@ typedef struct {
     double ms_factor;
     double ms_solve;
     int64_t factor_max_degree_used;
+    int32_t refinements;     /* SSP_PRECISION_MIXED: FP64 refinement rounds */
+    int32_t fp64_rounds;
 } ssp_solve_report;
 
 /* ---- errors ---- */
@@ -168,6 +179,8 @@ int ssp_context_destroy(ssp_context* ctx);
 int ssp_context_set_stream(ssp_context* ctx, void* stream);
 int64_t ssp_context_kernels_launched(const ssp_context* ctx);
 int64_t ssp_context_workspace_bytes(const ssp_context* ctx);
+/* free the context's cached device workspace (it grows again on the next call) */
+int ssp_context_release_workspace(ssp_context* ctx);
 
 /* ---- parameters ---- */
 void ssp_params_default(ssp_params* p);
@@ -203,6 +216,70 @@ int ssp_sparsify(ssp_context* ctx, const ssp_csc* graph, const ssp_params* param
                  ssp_csc_out* out, ssp_stats* stats);
 int ssp_csc_free(ssp_csc_out* out);
 
+/* ---- the JL columns split across ranks (one GPU each) ----
+ * The k sketch columns are independent once the factor exists (every rank builds the same deterministic
+ * factor; with factor_max_degree = -1 the choice is probed on the global columns 0..7 on every rank).
+ * Phase 1, every rank: sketch the global columns [col_begin, col_end) of the k that params implies, solve
+ * them, and write sq[e] = sum over those columns of (Z[v1_e, j] - Z[v2_e, j])^2 into the device buffer sq
+ * (m doubles).  With sq == NULL only *m (the edge count) is computed.
+ * The caller sums sq over ranks (an all-reduce), then phase 2 (on any rank) takes d_e = sqrt(sum) and runs
+ * probabilities, coins, reweighting and L_H exactly as ssp_sparsify does.  d_e differs from ssp_sparsify's
+ * only in the order of the final sum over columns.  Replaces the per-column loop of example.cc:551-568
+ * and sparsifier.rs:565-583 when the columns live on several GPUs. */
+int ssp_shard_leverage(ssp_context* ctx, const ssp_csc* graph, const ssp_params* params, int32_t col_begin,
+                       int32_t col_end, double* sq, int64_t* m, ssp_stats* stats);
+int ssp_shard_finish(ssp_context* ctx, const ssp_csc* graph, const ssp_params* params, const double* sq_total,
+                     int32_t out_mem, ssp_csc_out* out, ssp_stats* stats);
+
+/* ---- serving: a persistent request loop on one device ----
+ * No counterpart in the reference, which sparsifies one graph per process (sparsify_dataset, lib.rs:158-168).
+ * Requests of uneven size are submitted from any host thread and served by `slots` workers, each with its
+ * own stream and workspace, so admitted requests overlap on the device.  The oldest pending request is
+ * admitted as soon as a slot is free and its estimated device footprint (ssp_request_footprint) fits beside
+ * those in flight within hbm_budget_bytes; a request whose footprint alone exceeds the budget is refused
+ * at submit (SSP_ERR_CAPACITY).  Each request runs exactly ssp_sparsify, so its result is the same as a
+ * lone call's.  Results are collected once with ssp_wait / ssp_poll (which then own res->out: free it
+ * with ssp_csc_free). */
+#define SSP_REQ_SPARSIFY 0
+typedef struct ssp_server ssp_server;
+typedef struct {
+    int32_t device;
+    int32_t slots;            /* requests on the device at once */
+    int64_t hbm_budget_bytes; /* admission limit on in-flight footprints; <= 0: 85% of free memory at creation */
+    int32_t max_pending;      /* queue length beyond which ssp_submit refuses (0: unbounded) */
+} ssp_server_opts;
+typedef struct {
+    int32_t kind;             /* SSP_REQ_SPARSIFY */
+    ssp_csc graph;            /* host CSC; copied by ssp_submit */
+    ssp_params params;        /* copied by ssp_submit (output_file too) */
+} ssp_request;
+typedef struct {
+    int32_t status;           /* the request's own status code */
+    char error[256];
+    ssp_csc_out out;          /* L_H on the host */
+    ssp_stats stats;
+    int64_t est_bytes;        /* the footprint estimate used for admission */
+    double queue_ms;          /* submit -> admitted */
+    double run_ms;            /* admitted -> done */
+    double latency_ms;        /* submit -> done */
+    int32_t slot;
+} ssp_result;
+typedef struct {
+    int64_t submitted, completed, failed, rejected, pending;
+    int32_t inflight, peak_inflight, slots;
+    int64_t peak_inflight_bytes, budget_bytes;
+} ssp_server_info;
+void ssp_server_opts_default(ssp_server_opts* opts);
+int64_t ssp_request_footprint(const ssp_csc* graph, const ssp_params* params);
+int ssp_server_create(const ssp_server_opts* opts, ssp_server** server);
+int ssp_submit(ssp_server* server, const ssp_request* req, uint64_t* ticket);
+/* timeout_ms < 0 waits without limit; SSP_ERR_PENDING if the request is not done in time */
+int ssp_wait(ssp_server* server, uint64_t ticket, int64_t timeout_ms, ssp_result* res);
+int ssp_poll(ssp_server* server, uint64_t ticket, ssp_result* res);
+int ssp_server_info_get(ssp_server* server, ssp_server_info* info);
+/* drops pending requests, lets admitted ones finish, frees uncollected results */
+int ssp_server_destroy(ssp_server* server);
+
 /* ---- .mtx path (sparsify_dataset) ---- */
 int ssp_sparsify_mtx(const char* input_file, const char* output_file, const ssp_params* params, ssp_stats* stats);
 int ssp_read_mtx(const char* path, ssp_csc_out* out);             /* host CSC, duplicates summed */
@@ -213,6 +290,8 @@ int ssp_gen_grid2d(int64_t nx, int64_t ny, double w, ssp_csc_out* out);
 int ssp_gen_grid3d(int64_t nx, int64_t ny, int64_t nz, double wlog10_lo, double wlog10_hi, uint64_t seed,
                    ssp_csc_out* out);
 int ssp_gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, ssp_csc_out* out);
+/* random geometric graph in the unit square, radius sqrt(avg_degree / (pi n)), weights uniform [wlo, whi] */
+int ssp_gen_rgg(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, ssp_csc_out* out);
 
 /* ---- stage entry points (device-resident, for parity tests) ---- */
 /* edges of the input (v1 < v2, weights, CSC order) and L_G, copied to caller-allocated host buffers;

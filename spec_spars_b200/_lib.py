@@ -14,6 +14,7 @@ SSP_MEM_HOST, SSP_MEM_DEVICE = 0, 1
 SSP_JL_DIM_REF, SSP_JL_DIM_24 = 0, 1
 SSP_JL_SCALE_FIXED, SSP_JL_SCALE_INV_SQRT_K = 0, 1
 SSP_REWEIGHT_INV_SQRT_P, SSP_REWEIGHT_INV_P = 0, 1
+SSP_PRECISION_FP64, SSP_PRECISION_MIXED = 0, 1
 
 ERROR_NAMES = {-1: "SSP_ERR_INVALID", -2: "SSP_ERR_CUDA", -3: "SSP_ERR_NOMEM", -4: "SSP_ERR_NOT_CONVERGED",
                -5: "SSP_ERR_CAPACITY", -6: "SSP_ERR_IO", -7: "SSP_ERR_NO_DEVICE"}
@@ -56,7 +57,8 @@ class _Params(ctypes.Structure):
                 ("prob_variance_correction", ctypes.c_int32), ("reweight", ctypes.c_int32),
                 ("pcg_tol", ctypes.c_double), ("pcg_abs_tol", ctypes.c_double), ("pcg_max_iters", ctypes.c_int32),
                 ("factor_seed", ctypes.c_uint64), ("dense_threshold", ctypes.c_int64),
-                ("factor_max_degree", ctypes.c_int64), ("jl_dim_override", ctypes.c_int32)]
+                ("factor_max_degree", ctypes.c_int64), ("jl_dim_override", ctypes.c_int32),
+                ("precision", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -68,20 +70,44 @@ class _Stats(ctypes.Structure):
                 ("ms_leverage", ctypes.c_double), ("ms_sample", ctypes.c_double), ("ms_total", ctypes.c_double),
                 ("kernels_launched", ctypes.c_int64), ("ms_spmm", ctypes.c_double), ("n_spmm", ctypes.c_int64),
                 ("ms_precond", ctypes.c_double), ("n_precond", ctypes.c_int64), ("nnz_laplacian", ctypes.c_int64),
-                ("factor_max_degree_used", ctypes.c_int64), ("ms_autotune", ctypes.c_double)]
+                ("factor_max_degree_used", ctypes.c_int64), ("ms_autotune", ctypes.c_double),
+                ("pcg_refinements", ctypes.c_int32), ("pcg_fp64_rounds", ctypes.c_int32)]
 
 
 class _SolveOpts(ctypes.Structure):
     _fields_ = [("tol", ctypes.c_double), ("abs_tol", ctypes.c_double), ("max_iters", ctypes.c_int32),
                 ("factor_seed", ctypes.c_uint64), ("dense_threshold", ctypes.c_int64), ("verbose", ctypes.c_int32),
-                ("factor_max_degree", ctypes.c_int64)]
+                ("factor_max_degree", ctypes.c_int64), ("precision", ctypes.c_int32)]
 
 
 class _SolveReport(ctypes.Structure):
     _fields_ = [("k", ctypes.c_int32), ("max_iters_used", ctypes.c_int32), ("mean_iters", ctypes.c_double),
                 ("max_relres", ctypes.c_double), ("not_converged", ctypes.c_int32),
                 ("nnz_factor", ctypes.c_int64), ("factor_levels", ctypes.c_int32), ("ms_factor", ctypes.c_double),
-                ("ms_solve", ctypes.c_double), ("factor_max_degree_used", ctypes.c_int64)]
+                ("ms_solve", ctypes.c_double), ("factor_max_degree_used", ctypes.c_int64),
+                ("refinements", ctypes.c_int32), ("fp64_rounds", ctypes.c_int32)]
+
+
+class _ServerOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("slots", ctypes.c_int32), ("hbm_budget_bytes", ctypes.c_int64),
+                ("max_pending", ctypes.c_int32)]
+
+
+class _Request(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("graph", _Csc), ("params", _Params)]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("error", ctypes.c_char * 256), ("out", _CscOut), ("stats", _Stats),
+                ("est_bytes", ctypes.c_int64), ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double), ("slot", ctypes.c_int32)]
+
+
+class _ServerInfo(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("rejected", ctypes.c_int64), ("pending", ctypes.c_int64), ("inflight", ctypes.c_int32),
+                ("peak_inflight", ctypes.c_int32), ("slots", ctypes.c_int32),
+                ("peak_inflight_bytes", ctypes.c_int64), ("budget_bytes", ctypes.c_int64)]
 
 
 _LIB = None
@@ -125,6 +151,16 @@ def lib():
             "ssp_gen_grid2d": ([I64, I64, DBL, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_grid3d": ([I64, I64, I64, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_er": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
+            "ssp_gen_rgg": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
+            "ssp_context_release_workspace": ([P], ctypes.c_int),
+            "ssp_server_opts_default": ([ctypes.POINTER(_ServerOpts)], None),
+            "ssp_request_footprint": ([ctypes.POINTER(_Csc), ctypes.POINTER(_Params)], I64),
+            "ssp_server_create": ([ctypes.POINTER(_ServerOpts), ctypes.POINTER(P)], ctypes.c_int),
+            "ssp_submit": ([P, ctypes.POINTER(_Request), ctypes.POINTER(U64)], ctypes.c_int),
+            "ssp_wait": ([P, U64, I64, ctypes.POINTER(_Result)], ctypes.c_int),
+            "ssp_poll": ([P, U64, ctypes.POINTER(_Result)], ctypes.c_int),
+            "ssp_server_info_get": ([P, ctypes.POINTER(_ServerInfo)], ctypes.c_int),
+            "ssp_server_destroy": ([P], ctypes.c_int),
             "ssp_stage_graph": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(I64), ctypes.POINTER(I64), P, P, P, P, P, P],
                                 ctypes.c_int),
             "ssp_stage_sketch": ([P, I64, I64, P, P, P, I32, I32, DBL, U64, I32, P], ctypes.c_int),
@@ -137,6 +173,10 @@ def lib():
             "ssp_stage_sample_apply": ([P, ctypes.POINTER(_Csc), P, P, I32, I32, P, ctypes.POINTER(_CscOut)],
                                        ctypes.c_int),
             "ssp_stage_leverage_probs_static": ([P, I64, I64, P, P, P, I32, P, DBL, DBL, P], ctypes.c_int),
+            "ssp_shard_leverage": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(_Params), I32, I32, P,
+                                    ctypes.POINTER(I64), ctypes.POINTER(_Stats)], ctypes.c_int),
+            "ssp_shard_finish": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(_Params), P, I32, ctypes.POINTER(_CscOut),
+                                  ctypes.POINTER(_Stats)], ctypes.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -243,6 +283,12 @@ def gen_grid3d(nx, ny, nz, wlog10_lo=-3.0, wlog10_hi=3.0, seed=2):
 def gen_er(n, avg_degree, wlo=0.5, whi=2.0, seed=1):
     out = _CscOut()
     _check(lib().ssp_gen_er(n, avg_degree, wlo, whi, seed, ctypes.byref(out)))
+    return _take_out(out)
+
+
+def gen_rgg(n, avg_degree, wlo=0.1, whi=10.0, seed=1):
+    out = _CscOut()
+    _check(lib().ssp_gen_rgg(n, avg_degree, wlo, whi, seed, ctypes.byref(out)))
     return _take_out(out)
 
 
@@ -389,12 +435,38 @@ class Context:
                                   ctypes.byref(out), ctypes.byref(st)))
         return (out.nnz, out.colptr, out.rowidx, out.values), _stats_dict(st)
 
+    def num_edges(self, graph):
+        """Edges of a host graph as the sparsifier counts them (upper triangle, value != 0)."""
+        m = I64(0)
+        g = graph._struct()
+        _check(lib().ssp_shard_leverage(self._h, ctypes.byref(g), None, 0, 0, None, ctypes.byref(m), None))
+        return m.value
+
+    def shard_leverage(self, graph, params, col_begin, col_end, sq_ptr):
+        """Phase 1 of a column-split sparsification: solve the global JL columns [col_begin, col_end) and
+        write the per-edge partial sums of squared differences into the device buffer at sq_ptr."""
+        g = graph._struct()
+        m = I64(0)
+        st = _Stats()
+        _check(lib().ssp_shard_leverage(self._h, ctypes.byref(g), ctypes.byref(params._s), col_begin, col_end,
+                                        sq_ptr, ctypes.byref(m), ctypes.byref(st)))
+        return _stats_dict(st)
+
+    def shard_finish(self, graph, params, sq_total_ptr):
+        """Phase 2: probabilities, coins and L_H from the per-edge squares summed over all columns."""
+        g = graph._struct()
+        out = _CscOut()
+        st = _Stats()
+        _check(lib().ssp_shard_finish(self._h, ctypes.byref(g), ctypes.byref(params._s), sq_total_ptr,
+                                      SSP_MEM_HOST, ctypes.byref(out), ctypes.byref(st)))
+        return _take_out(out), _stats_dict(st)
+
     def solve_lap(self, lap, Y, tol=0.0, abs_tol=np.sqrt(2e-7), max_iters=400, factor_seed=0,
-                  dense_threshold=4096, max_degree=-1, raise_on_failure=True):
+                  dense_threshold=4096, max_degree=-1, raise_on_failure=True, precision=0, verbose=False):
         Y = np.ascontiguousarray(Y, np.float64)
         n, k = Y.shape
         Z = np.zeros_like(Y)
-        o = _SolveOpts(tol, abs_tol, max_iters, factor_seed, dense_threshold, 0, max_degree)
+        o = _SolveOpts(tol, abs_tol, max_iters, factor_seed, dense_threshold, int(verbose), max_degree, precision)
         rep = _SolveReport()
         s = lap._struct()
         rc = lib().ssp_solve_lap(self._h, ctypes.byref(s), _ptr(Y), k, _ptr(Z), SSP_MEM_HOST, ctypes.byref(o),
@@ -557,3 +629,70 @@ def stage_sample_apply(ctx, graph, p, coins, reweight):
     _check(lib().ssp_stage_sample_apply(ctx._h, ctypes.byref(g), _ptr(p), _ptr(coins), int(reweight), SSP_MEM_HOST,
                                         _ptr(keep), ctypes.byref(out)))
     return _take_out(out), keep[:len(p)].astype(bool)
+
+
+# ---------------------------------------------------------------- serving
+SSP_ERR_PENDING = -8
+
+
+def request_footprint(graph, params):
+    """Estimated device bytes of one sparsification (what the server admits against its HBM budget)."""
+    g = graph._struct()
+    return lib().ssp_request_footprint(ctypes.byref(g), ctypes.byref(params._s))
+
+
+class Server:
+    """Persistent request loop on one device (ssp_server_*): submit from any thread, collect with wait/poll."""
+
+    def __init__(self, device=0, slots=4, hbm_budget_bytes=0, max_pending=0):
+        o = _ServerOpts(device, slots, hbm_budget_bytes, max_pending)
+        h = P()
+        _check(lib().ssp_server_create(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+
+    def submit(self, graph, params):
+        req = _Request(0, graph._struct(), params._s)
+        t = U64(0)
+        _check(lib().ssp_submit(self._h, ctypes.byref(req), ctypes.byref(t)))
+        return t.value
+
+    def _collect(self, res):
+        info = {"queue_ms": res.queue_ms, "run_ms": res.run_ms, "latency_ms": res.latency_ms, "slot": res.slot,
+                "est_bytes": res.est_bytes}
+        if res.status != SSP_OK:
+            raise SspError(res.status, res.error.decode(errors="replace"))
+        return _take_out(res.out), _stats_dict(res.stats), info
+
+    def wait(self, ticket, timeout_ms=-1):
+        """(L_H, stats, timing) of a finished request; None if timeout_ms passes first."""
+        res = _Result()
+        rc = lib().ssp_wait(self._h, ticket, timeout_ms, ctypes.byref(res))
+        if rc == SSP_ERR_PENDING:
+            return None
+        _check(rc)
+        return self._collect(res)
+
+    def poll(self, ticket):
+        return self.wait(ticket, 0)
+
+    def info(self):
+        i = _ServerInfo()
+        _check(lib().ssp_server_info_get(self._h, ctypes.byref(i)))
+        return {f: getattr(i, f) for f, _ in _ServerInfo._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ssp_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -166,8 +166,17 @@ __global__ void k_count_diag(int64_t n, const int64_t* ptr, const int32_t* idx, 
             if (idx[p] == v) atomicAdd((unsigned long long*)out, 1ull);
 }
 
+// Splitting the JL columns across ranks (multi-GPU): phase 1 solves the global columns
+// [col_lo, col_hi) and leaves the per-edge sums of squared differences in sq_out; the caller sums them
+// over ranks; phase 2 takes the summed squares (sq_in) and runs probabilities, coins and L_H.
+struct ShardArgs {
+    int32_t col_lo = 0, col_hi = 0;
+    double* sq_out = nullptr;
+    const double* sq_in = nullptr;
+};
+
 static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* prm, int32_t out_mem, ssp_csc_out* out,
-                          ssp_stats* st) {
+                          ssp_stats* st, const ShardArgs* sh = nullptr) {
     SSP_REQUIRE(prm, SSP_ERR_INVALID, "params is NULL");
     SSP_REQUIRE(prm->epsilon > 0 && std::isfinite(prm->epsilon), SSP_ERR_INVALID, "epsilon must be positive");
     SSP_CUDA(cudaSetDevice(C.device));
@@ -180,9 +189,20 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     const int64_t n = G.n;
     const int32_t k = jl_dim(prm, n);
     const double scale = jl_scale(prm, k);
-    const int64_t ld = tile_ld(k);
-    double* Y = C.ws.get_t<double>("sp_Y", (size_t)n * ld);
-    sketch_device(C, G, k, scale, prm->sketch_seed, prm->sketch_uniform, Y, ld, 1);
+    const bool finish_only = sh && sh->sq_in;
+    int32_t col_lo = 0, kl = k;  // the global columns solved here
+    if (sh && !finish_only) {
+        SSP_REQUIRE(sh->col_lo >= 0 && sh->col_lo < sh->col_hi && sh->col_hi <= k, SSP_ERR_INVALID,
+                    "shard column range must satisfy 0 <= begin < end <= k");
+        col_lo = sh->col_lo;
+        kl = sh->col_hi - sh->col_lo;
+    }
+    const int64_t ld = tile_ld(kl);
+    double* Y = nullptr;
+    if (!finish_only) {
+        Y = C.ws.get_t<double>("sp_Y", (size_t)n * ld);
+        sketch_device(C, G, kl, scale, prm->sketch_seed, prm->sketch_uniform, Y, ld, 1, col_lo);
+    }
     T.mark();  // 2
     DevFactor F;
     FactorOptions fo;
@@ -194,21 +214,70 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     po.abs_tol = prm->pcg_abs_tol;
     po.max_iters = prm->pcg_max_iters;
     po.verbose = prm->verbose;
+    po.precision = prm->precision;
     double ms_tune = 0.0;
     int64_t deg_used = fo.max_degree;
-    if (fo.max_degree < 0)
-        deg_used = autotune_factor(C, n, G.lap_ptr, G.lap_idx, G.lap_val, 2 * G.m, Y, k, fo, po, F, &ms_tune);
-    else
+    if (finish_only) {
+        deg_used = 0;
+    } else if (fo.max_degree < 0) {
+        // the probe always uses global columns [0, min(k, 8)), so every rank of a split run picks the same
+        const double* probe = Y;
+        const int32_t kp = std::min<int32_t>(k, SSP_TILE);
+        if (col_lo != 0 || kl < kp) {
+            double* Yp = C.ws.get_t<double>("sp_Yprobe", (size_t)n * SSP_TILE);
+            sketch_device(C, G, kp, scale, prm->sketch_seed, prm->sketch_uniform, Yp, SSP_TILE, 1, 0);
+            probe = Yp;
+        }
+        deg_used = autotune_factor(C, n, G.lap_ptr, G.lap_idx, G.lap_val, 2 * G.m, probe, kp, fo, po, F, &ms_tune);
+    } else {
         factor_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, fo, F, "f");
+    }
     T.mark();  // 3
     PcgReport rep;
     const double* Zt = nullptr;
-    pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, k, &Zt, po, rep);
+    if (!finish_only) pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, kl, &Zt, po, rep);
     T.mark();  // 4
+    if (sh && sh->sq_out) {
+        diff_sq_device(C, G.m, G.v1, G.v2, Zt, kl, n, sh->sq_out);
+        T.mark();  // 5
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+        if (st) {
+            memset(st, 0, sizeof(*st));
+            st->n = n;
+            st->m_in = G.m;
+            st->k = k;
+            st->beta = beta_of(prm, n);
+            st->nnz_factor = F.nnz;
+            st->factor_levels = F.num_levels;
+            st->pcg_max_iters_used = rep.max_iters_used;
+            st->pcg_mean_iters = rep.mean_iters;
+            st->pcg_max_relres = rep.max_relres;
+            st->ms_assembly = T.ms(0, 1);
+            st->ms_sketch = T.ms(1, 2);
+            st->ms_factor = T.ms(2, 3);
+            st->ms_solve = T.ms(3, 4);
+            st->ms_leverage = T.ms(4, 5);
+            st->ms_total = T.ms(0, 5);
+            st->kernels_launched = C.kernels_launched;
+            st->ms_spmm = rep.ms_spmm;
+            st->n_spmm = rep.n_spmm;
+            st->ms_precond = rep.ms_precond;
+            st->n_precond = rep.n_precond;
+            st->nnz_laplacian = G.lap_nnz;
+            st->factor_max_degree_used = deg_used;
+            st->ms_autotune = ms_tune;
+            st->pcg_refinements = rep.refinements;
+            st->pcg_fp64_rounds = rep.fp64_rounds;
+        }
+        return;
+    }
     double* d = C.ws.get_t<double>("sp_d", G.m + 1);
     double* p = C.ws.get_t<double>("sp_p", G.m + 1);
     double* coins = C.ws.get_t<double>("sp_coins", G.m + 1);
-    diff_norms_device(C, G.m, G.v1, G.v2, Zt, k, ld, d, n);
+    if (finish_only)
+        sqrt_device(C, G.m, sh->sq_in, d);
+    else
+        diff_norms_device(C, G.m, G.v1, G.v2, Zt, k, ld, d, n);
     const double beta = beta_of(prm, n);
     const double denom = prm->prob_variance_correction ? (double)k * scale * scale : (double)k;
     probs_device(C, G.m, G.w, d, beta, denom, p);
@@ -287,6 +356,8 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
         st->nnz_laplacian = G.lap_nnz;
         st->factor_max_degree_used = deg_used;
         st->ms_autotune = ms_tune;
+        st->pcg_refinements = rep.refinements;
+        st->pcg_fp64_rounds = rep.fp64_rounds;
     }
     if (prm->verbose) {
         fprintf(stderr, "[ssp] n=%lld m=%lld k=%d nnz(L)=%lld levels=%d (sparse %zu, dense %d, truncated %lld, compactions %d) "
@@ -341,6 +412,7 @@ static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t 
     po.abs_tol = o->abs_tol;
     po.max_iters = o->max_iters;
     po.verbose = o->verbose;
+    po.precision = o->precision;
     int64_t deg_used = fo.max_degree;
     if (fo.max_degree < 0) {
         const int64_t offdiag = L.nnz - n;  // every vertex of a connected Laplacian stores its diagonal
@@ -373,6 +445,8 @@ static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t 
         rep->ms_factor = T.ms(0, 1);
         rep->ms_solve = T.ms(1, 2);
         rep->factor_max_degree_used = deg_used;
+        rep->refinements = pr.refinements;
+        rep->fp64_rounds = pr.fp64_rounds;
     }
     if (pr.not_converged > 0)
         throw Error(SSP_ERR_NOT_CONVERGED, "solver did not converge: " + std::to_string(pr.not_converged) +
@@ -465,6 +539,7 @@ void ssp_params_new(ssp_params* p, double epsilon, int32_t beta_constant, int32_
     p->dense_threshold = 4096;
     p->factor_max_degree = -1;
     p->jl_dim_override = 0;
+    p->precision = SSP_PRECISION_FP64;
 }
 
 void ssp_params_default(ssp_params* p) {
@@ -489,6 +564,7 @@ void ssp_solve_opts_default(ssp_solve_opts* o) {
     o->dense_threshold = 4096;
     o->verbose = 0;
     o->factor_max_degree = -1;
+    o->precision = SSP_PRECISION_FP64;
 }
 
 int ssp_run_solve_lap(const double* shared_jl_cols, size_t num_rows, size_t num_cols, const int32_t* col_ptrs,
@@ -526,6 +602,40 @@ int ssp_sparsify(ssp_context* c, const ssp_csc* graph, const ssp_params* params,
     return guarded([&] {
         SSP_REQUIRE(c, SSP_ERR_INVALID, "ctx is NULL");
         sparsify_impl(c->ctx, graph, params, out_mem, out, stats);
+    });
+}
+
+int ssp_shard_leverage(ssp_context* c, const ssp_csc* graph, const ssp_params* params, int32_t col_begin,
+                       int32_t col_end, double* sq, int64_t* m, ssp_stats* stats) {
+    return guarded([&] {
+        SSP_REQUIRE(c, SSP_ERR_INVALID, "ctx is NULL");
+        Context& C = c->ctx;
+        if (!sq) {
+            SSP_REQUIRE(m, SSP_ERR_INVALID, "need sq or m");
+            SSP_CUDA(cudaSetDevice(C.device));
+            DevCsc g = to_device(C, graph, "in");
+            DevGraph G;
+            build_graph_from_csc(C, g.n, g.colptr, g.rowidx, g.val, g.nnz, G);
+            SSP_CUDA(cudaStreamSynchronize(C.stream));
+            *m = G.m;
+            return;
+        }
+        ShardArgs sh;
+        sh.col_lo = col_begin;
+        sh.col_hi = col_end;
+        sh.sq_out = sq;
+        sparsify_impl(C, graph, params, SSP_MEM_DEVICE, nullptr, stats, &sh);
+        if (m && stats) *m = stats->m_in;
+    });
+}
+
+int ssp_shard_finish(ssp_context* c, const ssp_csc* graph, const ssp_params* params, const double* sq_total,
+                     int32_t out_mem, ssp_csc_out* out, ssp_stats* stats) {
+    return guarded([&] {
+        SSP_REQUIRE(c && sq_total, SSP_ERR_INVALID, "ctx and sq_total are required");
+        ShardArgs sh;
+        sh.sq_in = sq_total;
+        sparsify_impl(c->ctx, graph, params, out_mem, out, stats, &sh);
     });
 }
 
@@ -617,6 +727,23 @@ int ssp_gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t se
         HostCsc h;
         gen_er(n, avg_degree, wlo, whi, seed, h);
         host_out(h, out);
+    });
+}
+int ssp_gen_rgg(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, ssp_csc_out* out) {
+    return guarded([&] {
+        SSP_REQUIRE(n > 1 && avg_degree > 0 && out, SSP_ERR_INVALID, "bad arguments");
+        HostCsc h;
+        gen_rgg(n, avg_degree, wlo, whi, seed, h);
+        host_out(h, out);
+    });
+}
+
+int ssp_context_release_workspace(ssp_context* c) {
+    return guarded([&] {
+        SSP_REQUIRE(c, SSP_ERR_INVALID, "ctx is NULL");
+        SSP_CUDA(cudaSetDevice(c->ctx.device));
+        SSP_CUDA(cudaStreamSynchronize(c->ctx.stream));
+        c->ctx.ws.release();
     });
 }
 

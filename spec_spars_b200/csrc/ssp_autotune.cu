@@ -38,6 +38,7 @@ int64_t autotune_factor(Context& C, int64_t n, const int64_t* lap_ptr, const int
     po.abs_tol = 0.0;
     po.max_iters = TUNE_PROBE_ITERS;
     po.verbose = 0;
+    po.precision = SSP_PRECISION_FP64;  // the choice must not depend on the solve's precision
     std::vector<double> hist;
     po.history = &hist;
     PcgReport rep;

@@ -136,6 +136,48 @@ void gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed,
     out.from_upper_edges(n, a, b, ww);
 }
 
+// Random geometric graph: n points uniform in the unit square (Philox counters (i, 2) and (i, 3)), an edge
+// between every pair closer than r = sqrt(avg_degree / (pi n)); weight uniform [wlo, whi] rounded to FP32
+// from the counter (a * n + b, 4).  Pairs are found through a grid of r-sized cells.
+void gen_rgg(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, HostCsc& out) {
+    const double r = std::sqrt(avg_degree / (M_PI * (double)n));
+    std::vector<double> px(n), py(n);
+    for (int64_t i = 0; i < n; i++) {
+        px[i] = gen_u53(seed, (uint64_t)i, 2);
+        py[i] = gen_u53(seed, (uint64_t)i, 3);
+    }
+    const int64_t g = std::max<int64_t>(1, std::min<int64_t>((int64_t)(1.0 / r), 1 << 15));
+    auto cell = [&](double x) { return std::min<int64_t>(g - 1, (int64_t)(x * (double)g)); };
+    std::vector<int64_t> start(g * g + 1, 0), order(n);
+    for (int64_t i = 0; i < n; i++) start[cell(py[i]) * g + cell(px[i]) + 1]++;
+    for (int64_t c = 0; c < g * g; c++) start[c + 1] += start[c];
+    std::vector<int64_t> fill(start.begin(), start.end() - 1);
+    for (int64_t i = 0; i < n; i++) order[fill[cell(py[i]) * g + cell(px[i])]++] = i;
+    std::vector<std::pair<int32_t, int32_t>> e;  // (b, a), a < b
+    const double r2 = r * r;
+    for (int64_t i = 0; i < n; i++) {
+        const int64_t cx = cell(px[i]), cy = cell(py[i]);
+        for (int64_t yy = std::max<int64_t>(0, cy - 1); yy <= std::min<int64_t>(g - 1, cy + 1); yy++)
+            for (int64_t xx = std::max<int64_t>(0, cx - 1); xx <= std::min<int64_t>(g - 1, cx + 1); xx++)
+                for (int64_t t = start[yy * g + xx]; t < start[yy * g + xx + 1]; t++) {
+                    const int64_t j = order[t];
+                    if (j <= i) continue;
+                    const double dx = px[i] - px[j], dy = py[i] - py[j];
+                    if (dx * dx + dy * dy < r2) e.push_back({(int32_t)j, (int32_t)i});
+                }
+    }
+    std::sort(e.begin(), e.end());
+    std::vector<int32_t> a(e.size()), b(e.size());
+    std::vector<double> w(e.size());
+    for (size_t t = 0; t < e.size(); t++) {
+        b[t] = e[t].first;
+        a[t] = e[t].second;
+        const double u = gen_u53(seed, (uint64_t)a[t] * (uint64_t)n + (uint64_t)b[t], 4);
+        w[t] = (double)(float)(wlo + (whi - wlo) * u);
+    }
+    out.from_upper_edges(n, a, b, w);
+}
+
 // ---------------------------------------------------------------- Matrix Market
 static bool lower_eq(const std::string& a, const char* b) {
     if (a.size() != strlen(b)) return false;

@@ -19,6 +19,7 @@ struct HostCsc {
 void gen_grid2d(int64_t nx, int64_t ny, double w, HostCsc& out);
 void gen_grid3d(int64_t nx, int64_t ny, int64_t nz, double lo, double hi, uint64_t seed, HostCsc& out);
 void gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, HostCsc& out);
+void gen_rgg(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, HostCsc& out);
 
 int read_mtx(const char* path, HostCsc& out, std::string& err);
 int write_mtx(const char* path, int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,

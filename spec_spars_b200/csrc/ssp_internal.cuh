@@ -229,7 +229,7 @@ void build_graph_from_edges(Context& C, DevGraph& G);
 
 // a4: Y = B^T Q, columns [0,k): row-major with leading dimension ldy, or tile-major (8-column slabs)
 void sketch_device(Context& C, const DevGraph& G, int32_t k, double scale, uint64_t seed, int uniform,
-                   double* Y, int64_t ldy, int tile_major);
+                   double* Y, int64_t ldy, int tile_major, int32_t col_lo = 0);
 
 // a7: factor
 struct DevFactor {
@@ -284,6 +284,7 @@ struct PcgOptions {
     int32_t max_iters = 400;
     int verbose = 0;
     std::vector<double>* history = nullptr;  // per iteration: max over columns of ||r|| / ||b||
+    int precision = SSP_PRECISION_FP64;      // SSP_PRECISION_MIXED: FP32 inner solves, FP64 refinement
 };
 struct PcgReport {
     int32_t max_iters_used = 0;
@@ -296,6 +297,10 @@ struct PcgReport {
     int64_t n_precond = 0;
     double ms_loop = 0;      // device time of the iteration loop
     int32_t iters_run = 0;   // iterations of the loop (all columns)
+    int32_t refinements = 0; // mixed precision: outer rounds (true FP64 residual recomputations)
+    int32_t fp64_rounds = 0; // mixed precision: rounds that fell back to an FP64 inner solve
+    double ms_resid = 0;     // mixed precision: device time of the FP64 residual products
+    int64_t n_resid = 0;
 };
 // Picks the elimination truncation (FactorOptions::max_degree) for this Laplacian and right-hand sides
 // by factoring a few candidates and timing a short PCG probe on the first column tile of Y.  Leaves
@@ -314,6 +319,10 @@ void precond_apply_device(Context& C, const DevFactor& F, const double* R, doubl
 // Z row-major (leading dimension ldz) or, when n_tile_major > 0, tile-major with that many rows
 void diff_norms_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z, int32_t k,
                        int64_t ldz, double* d, int64_t n_tile_major = 0);
+// per-edge sum over the k columns of (Z[v1,j] - Z[v2,j])^2, Z tile-major with n_tile_major rows
+void diff_sq_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z, int32_t k,
+                    int64_t n_tile_major, double* sq);
+void sqrt_device(Context& C, int64_t m, const double* sq, double* d);
 void probs_device(Context& C, int64_t m, const double* w, const double* d, double beta, double denom, double* p);
 void coins_device(Context& C, int64_t m, uint64_t seed, double* coins);
 // returns nnz(L_H); writes L_H CSC into workspace buffers returned through pointers

@@ -6,18 +6,36 @@
 // ||r|| <= max(abs_tol, tol ||b||) (the reference's own rule is ||r||^2 <= 2e-7, :159,213), at most
 // max_iters iterations (:153), and success iff ||b - A x|| / ||b|| < 0.01 (:251-258).
 //
-// Layout ("tile-major", tile_off): an n x k block is stored as slabs of n x SSP_TILE doubles.  Every
+// Layout ("tile-major", tile_off): an n x k block is stored as slabs of n x SSP_TILE values.  Every
 // kernel works on one tile at a time across all rows, so the rows it gathers (one slab) stay resident
 // in L2 while the sparse matrix streams.  Column reductions are two-stage with a fixed order
-// (deterministic run to run).
+// (deterministic run to run) and always accumulate in FP64.
+//
+// Precision.  SSP_PRECISION_FP64 runs the whole iteration in FP64.  SSP_PRECISION_MIXED runs FP64
+// iterative refinement around FP32 inner PCG solves: the inner SpMM, triangular solves and vector
+// updates read and write FP32 (half the bytes of every gather and stream), the inner dot products
+// accumulate in FP64, and after each inner solve the true residual b - A x is recomputed with the FP64
+// matrix and FP64 x, so the stopping rule is checked on the same FP64 residual as in the FP64 mode.
+// An inner solve stops at a fixed relative reduction (or at half the outer threshold); once a round
+// fails to contract the FP64 residual by a large factor, the remaining rounds use an FP64 inner solve
+// that goes straight to the outer threshold.
+#include <algorithm>
+#include <cmath>
+
 #include "ssp_internal.cuh"
 
 namespace ssp {
 
 constexpr int TILE = SSP_TILE;    // columns per tile
 constexpr int SLOTS = 32 / TILE;  // nonzeros processed in parallel per warp
-constexpr int ROWS_PER_BLOCK = 8; // warps per 256-thread block, one row each
 constexpr int RED_THREADS = 256;  // column reductions: (256 / TILE) row lanes x TILE columns
+
+// mixed precision: relative reduction asked of one FP32 inner solve, and the round limit
+constexpr double MIXED_INNER_REDUCTION = 1e-4;
+constexpr int MIXED_MAX_ROUNDS = 40;
+// a round whose FP64 residual shrinks by less than this factor (max over columns) switches the remaining
+// rounds to FP64 inner solves
+constexpr double MIXED_MIN_CONTRACTION = 1e-2;
 
 __host__ __device__ __forceinline__ int64_t tm_off(int64_t n, int64_t r, int64_t c) { return tile_off(n, r, c); }
 
@@ -54,26 +72,26 @@ void tiles_to_rowmajor(Context& C, int64_t n, int32_t k, const double* src, doub
 enum ColOp { OP_SUM = 0, OP_DOT = 1, OP_SQ = 2, OP_SQDIFF_CENTERED = 3 };
 
 // grid (nparts, ntiles); thread = (row lane = tid / 8, column = tid % 8); part[blk][col]
-template <int OP>
-__global__ void __launch_bounds__(RED_THREADS) k_colred_partial(int64_t n, const double* __restrict__ a,
-                                                                const double* __restrict__ b,
+template <int OP, class T>
+__global__ void __launch_bounds__(RED_THREADS) k_colred_partial(int64_t n, const T* __restrict__ a,
+                                                                const T* __restrict__ b,
                                                                 const double* __restrict__ mean, int64_t rows_per_blk,
                                                                 int64_t ld, double* __restrict__ part) {
     __shared__ double s[RED_THREADS];
     const int64_t t = blockIdx.y;
     const int c = threadIdx.x % TILE, rl = threadIdx.x / TILE;
     const int64_t r0 = (int64_t)blockIdx.x * rows_per_blk, r1 = min(n, r0 + rows_per_blk);
-    const double* at = a + t * n * TILE;
-    const double* bt = b ? b + t * n * TILE : nullptr;
+    const T* at = a + t * n * TILE;
+    const T* bt = b ? b + t * n * TILE : nullptr;
     const double mu = (OP == OP_SQDIFF_CENTERED) ? mean[t * TILE + c] : 0.0;
     double acc = 0.0;
     for (int64_t r = r0 + rl; r < r1; r += RED_THREADS / TILE) {
-        const double x = at[r * TILE + c];
+        const double x = (double)at[r * TILE + c];
         if (OP == OP_SUM) acc += x;
-        else if (OP == OP_DOT) acc += x * bt[r * TILE + c];
+        else if (OP == OP_DOT) acc += x * (double)bt[r * TILE + c];
         else if (OP == OP_SQ) acc += x * x;
         else {
-            const double d = (x - mu) - bt[r * TILE + c];  // (Y - mean) - A x
+            const double d = (x - mu) - (double)bt[r * TILE + c];  // (Y - mean) - A x
             acc += d * d;
         }
     }
@@ -110,10 +128,10 @@ struct Reducer {
         nparts = (int)ceil_div<int64_t>(n, rows_per_blk);
         part = c.ws.get_t<double>(tag, (size_t)nparts * ld);
     }
-    template <int OP>
-    void run(const double* a, const double* b, double* out, const double* mean = nullptr) {
+    template <int OP, class T>
+    void run(const T* a, const T* b, double* out, const double* mean = nullptr) {
         dim3 grid((unsigned)nparts, (unsigned)(ld / TILE));
-        k_colred_partial<OP><<<grid, RED_THREADS, 0, C->stream>>>(n, a, b, mean, rows_per_blk, ld, part);
+        k_colred_partial<OP, T><<<grid, RED_THREADS, 0, C->stream>>>(n, a, b, mean, rows_per_blk, ld, part);
         k_colred_final<<<grid_for(ld, 256), 256, 0, C->stream>>>(ld, nparts, part, out);
         SSP_CHECK_LAUNCH();
         C->kernels_launched += 2;
@@ -140,27 +158,29 @@ __global__ void k_center(int64_t n, int32_t k, const double* __restrict__ Y, con
     }
 }
 
-// x += alpha p ; r -= alpha q ; partial ||r||^2 per column
+// x += alpha p ; r -= alpha q ; partial ||r||^2 per column (FP64 accumulation)
+template <class T>
 __global__ void __launch_bounds__(RED_THREADS) k_axpy_xr_rr(int64_t n, const double* __restrict__ alpha,
-                                                            const double* __restrict__ p, const double* __restrict__ q,
-                                                            double* __restrict__ x, double* __restrict__ r,
+                                                            const T* __restrict__ p, const T* __restrict__ q,
+                                                            T* __restrict__ x, T* __restrict__ r,
                                                             int64_t rows_per_blk, int64_t ld, double* __restrict__ part) {
     __shared__ double s[RED_THREADS];
     const int64_t t = blockIdx.y;
     const int c = threadIdx.x % TILE, rl = threadIdx.x / TILE;
     const int64_t r0 = (int64_t)blockIdx.x * rows_per_blk, r1 = min(n, r0 + rows_per_blk);
-    const double a = alpha[t * TILE + c];
+    const double a64 = alpha[t * TILE + c];
+    const T a = (T)a64;
     const int64_t base = t * n * TILE;
     double acc = 0.0;
     for (int64_t row = r0 + rl; row < r1; row += RED_THREADS / TILE) {
         const int64_t o = base + row * TILE + c;
-        double rv = r[o];
-        if (a != 0.0) {
+        T rv = r[o];
+        if (a64 != 0.0) {
             x[o] += a * p[o];
             rv -= a * q[o];
             r[o] = rv;
         }
-        acc += rv * rv;
+        acc += (double)rv * (double)rv;
     }
     s[threadIdx.x] = acc;
     __syncthreads();
@@ -171,13 +191,65 @@ __global__ void __launch_bounds__(RED_THREADS) k_axpy_xr_rr(int64_t n, const dou
     }
 }
 
-__global__ void k_update_p(int64_t n, const double* __restrict__ beta, const double* __restrict__ z,
-                           double* __restrict__ p) {
+template <class T>
+__global__ void k_update_p(int64_t n, const double* __restrict__ beta, const T* __restrict__ z, T* __restrict__ p) {
     const int64_t t = blockIdx.y;
     const int64_t cnt = n * TILE;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t o = t * cnt + i;
-        p[o] = z[o] + beta[t * TILE + (i % TILE)] * p[o];
+        p[o] = z[o] + (T)beta[t * TILE + (i % TILE)] * p[o];
+    }
+}
+
+// ---------------------------------------------------------------- mixed-precision helpers
+__global__ void k_d2f(int64_t count, const double* __restrict__ src, float* __restrict__ dst) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+
+// inner right-hand side: the FP64 residual of the columns still active, rounded to T; zero elsewhere
+// (runs in place when T is double)
+template <class T>
+__global__ void k_rhs_masked(int64_t n, const double* r64, const int32_t* __restrict__ active, T* rin) {
+    const int64_t t = blockIdx.y;
+    const int64_t cnt = n * TILE;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = t * cnt + i;
+        rin[o] = active[t * TILE + (i % TILE)] ? (T)r64[o] : (T)0;
+    }
+}
+
+template <class T>
+__global__ void k_add_into(int64_t count, const T* __restrict__ e, double* __restrict__ x) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] += (double)e[i];
+}
+
+// r = (Y - mean) - q with partial ||r||^2 per column: the true FP64 residual after a refinement round
+__global__ void __launch_bounds__(RED_THREADS) k_true_resid(int64_t n, int32_t k, const double* __restrict__ Y,
+                                                            const double* __restrict__ mean,
+                                                            const double* __restrict__ q, double* __restrict__ r,
+                                                            int64_t rows_per_blk, int64_t ld, double* __restrict__ part) {
+    __shared__ double s[RED_THREADS];
+    const int64_t t = blockIdx.y;
+    const int c = threadIdx.x % TILE, rl = threadIdx.x / TILE;
+    const int64_t r0 = (int64_t)blockIdx.x * rows_per_blk, r1 = min(n, r0 + rows_per_blk);
+    const int64_t col = t * TILE + c;
+    const double mu = mean[col];
+    const int64_t base = t * n * TILE;
+    double acc = 0.0;
+    for (int64_t row = r0 + rl; row < r1; row += RED_THREADS / TILE) {
+        const int64_t o = base + row * TILE + c;
+        const double rv = col < k ? (Y[o] - mu) - q[o] : 0.0;
+        r[o] = rv;
+        acc += rv * rv;
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x < TILE) {
+        double tt = s[threadIdx.x];
+        for (int i = 1; i < RED_THREADS / TILE; i++) tt += s[i * TILE + threadIdx.x];
+        part[(int64_t)blockIdx.x * ld + t * TILE + threadIdx.x] = tt;
     }
 }
 
@@ -196,6 +268,13 @@ struct ColState {
     int64_t* nactive;
 };
 
+static ColState make_colstate(Context& C, int64_t ld, const std::string& tag) {
+    double* v = C.ws.get_t<double>(tag + "_cols", 8 * ld);
+    int32_t* iv = C.ws.get_t<int32_t>(tag + "_coli", 2 * ld);
+    int64_t* na = C.ws.get_t<int64_t>(tag + "_nactive", 1);
+    return ColState{v, v + ld, v + 2 * ld, v + 3 * ld, v + 4 * ld, v + 5 * ld, v + 6 * ld, v + 7 * ld, iv, iv + ld, na};
+}
+
 __global__ void k_cols_init(int64_t ld, int32_t k, double tol, double abs_tol, ColState S) {
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x) {
         double bn = sqrt(S.bnorm2[c]);
@@ -204,6 +283,26 @@ __global__ void k_cols_init(int64_t ld, int32_t k, double tol, double abs_tol, C
         S.thr[c] = thr;
         S.rr[c] = S.bnorm2[c];
         int act = (c < k) && (bn > thr);
+        S.active[c] = act;
+        S.iters[c] = 0;
+        S.alpha[c] = 0.0;
+        S.beta[c] = 0.0;
+        if (act) atomicAdd((unsigned long long*)S.nactive, 1ull);
+    }
+}
+
+// inner solve of a refinement round: stop at a relative reduction `reduction` of its right-hand side, or
+// once below half the outer threshold of the column (no point solving past what the outer test needs)
+__global__ void k_cols_init_inner(int64_t ld, int32_t k, double reduction, const double* __restrict__ thr_out,
+                                  ColState S) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x) {
+        const double bn = sqrt(S.bnorm2[c]);
+        double thr = reduction * bn;
+        const double half_out = 0.5 * thr_out[c];
+        if (half_out > thr) thr = half_out;
+        S.thr[c] = thr;
+        S.rr[c] = S.bnorm2[c];
+        const int act = (c < k) && (bn > thr);
         S.active[c] = act;
         S.iters[c] = 0;
         S.alpha[c] = 0.0;
@@ -235,97 +334,48 @@ __global__ void k_cols_beta(int64_t ld, ColState S) {
     }
 }
 
+// outer test of a refinement round on the true residual: adds the round's inner iterations to the
+// column's count, deactivates converged columns, and records the largest residual ratio new/old
+__global__ void k_cols_outer(int64_t ld, const int32_t* __restrict__ inner_iters, const double* __restrict__ rr_new,
+                             ColState S, double* __restrict__ worst_ratio) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x) {
+        if (!S.active[c]) continue;
+        S.iters[c] += inner_iters[c];
+        const double before = S.rr[c], after = rr_new[c];
+        S.rr[c] = after;
+        if (sqrt(after) <= S.thr[c]) {
+            S.active[c] = 0;
+        } else {
+            atomicAdd((unsigned long long*)S.nactive, 1ull);
+            const double ratio = before > 0 ? sqrt(after / before) : 1.0;
+            // ratios are non-negative: their IEEE bit patterns order like the values
+            atomicMax((unsigned long long*)worst_ratio, (unsigned long long)__double_as_longlong(ratio));
+        }
+    }
+}
+
 // ---------------------------------------------------------------- SpMM and triangular solves
-// Warp per row; lane = slot * TILE + column.  xt points at the tile's slab (row stride TILE doubles).
+// Warp per row; lane = slot * TILE + column.  xt points at the tile's slab (row stride TILE values).
 // Two independent gathers per lane per step keep more loads in flight.
-__device__ __forceinline__ double warp_row_gather(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                                  const double* __restrict__ val, int64_t row, const double* xt,
-                                                  int lane) {
+template <class T>
+__device__ __forceinline__ T warp_row_gather(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                             const T* __restrict__ val, int64_t row, const T* xt, int lane) {
     const int slot = lane / TILE, c = lane % TILE;
     const int64_t e = ptr[row + 1];
-    double acc0 = 0.0, acc1 = 0.0;
+    T acc0 = 0, acc1 = 0;
     int64_t p = ptr[row] + slot;
     for (; p + SLOTS < e; p += 2 * SLOTS) {
         const int32_t i0 = idx[p], i1 = idx[p + SLOTS];
-        const double v0 = val[p], v1 = val[p + SLOTS];
+        const T v0 = val[p], v1 = val[p + SLOTS];
         acc0 += v0 * xt[(int64_t)i0 * TILE + c];
         acc1 += v1 * xt[(int64_t)i1 * TILE + c];
     }
     if (p < e) acc0 += val[p] * xt[(int64_t)idx[p] * TILE + c];
-    double acc = acc0 + acc1;
+    T acc = acc0 + acc1;
 #pragma unroll
     for (int o = TILE; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     return acc;
 }
-
-// q = A p for one tile per blockIdx.y; the epilogue accumulates p.q per column into part[blockIdx.x]
-__global__ void __launch_bounds__(256) k_spmm_pq(int64_t n, const int64_t* __restrict__ ptr,
-                                                 const int32_t* __restrict__ idx, const double* __restrict__ val,
-                                                 const double* __restrict__ x, double* __restrict__ y, int64_t ld,
-                                                 double* __restrict__ part) {
-    __shared__ double s[ROWS_PER_BLOCK][TILE];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t t = blockIdx.y;
-    const double* xt = x + t * n * TILE;
-    double* yt = y + t * n * TILE;
-    const int64_t wstride = (int64_t)gridDim.x * ROWS_PER_BLOCK;
-    double dot = 0.0;
-    for (int64_t row = (int64_t)blockIdx.x * ROWS_PER_BLOCK + warp; row < n; row += wstride) {
-        const double acc = warp_row_gather(ptr, idx, val, row, xt, lane);
-        if (lane < TILE) {
-            yt[row * TILE + lane] = acc;
-            dot += acc * xt[row * TILE + lane];
-        }
-    }
-    if (part) {
-        if (lane < TILE) s[warp][lane] = dot;
-        __syncthreads();
-        if (threadIdx.x < TILE) {
-            double tt = s[0][threadIdx.x];
-            for (int i = 1; i < ROWS_PER_BLOCK; i++) tt += s[i][threadIdx.x];
-            part[(int64_t)blockIdx.x * ld + t * TILE + threadIdx.x] = tt;
-        }
-    }
-}
-
-// forward: y[u] = r[u] - sum_{v<u} L[u,v] y[v]  for the rows of one level
-__global__ void __launch_bounds__(256) k_trsv_fwd(int64_t n, const int32_t* __restrict__ rows, int32_t nrows,
-                                                  const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                                  const double* __restrict__ val, const double* __restrict__ r,
-                                                  double* y) {
-    const int lane = threadIdx.x & 31;
-    const int64_t toff = (int64_t)blockIdx.y * n * TILE;
-    const int wstride = gridDim.x * ROWS_PER_BLOCK;
-    for (int i = blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5); i < nrows; i += wstride) {
-        const int64_t u = rows[i];
-        const double acc = warp_row_gather(ptr, idx, val, u, y + toff, lane);
-        if (lane < TILE) {
-            const int64_t o = toff + u * TILE + lane;
-            y[o] = r[o] - acc;
-        }
-    }
-}
-
-// backward (in place over y): z[u] = y[u]/D[u] - sum_{v>u} L[v,u] z[v]
-__global__ void __launch_bounds__(256) k_trsv_bwd(int64_t n, const int32_t* __restrict__ rows, int32_t nrows,
-                                                  const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                                  const double* __restrict__ val, const double* __restrict__ D,
-                                                  double* yz) {
-    const int lane = threadIdx.x & 31;
-    const int64_t toff = (int64_t)blockIdx.y * n * TILE;
-    const int wstride = gridDim.x * ROWS_PER_BLOCK;
-    for (int i = blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5); i < nrows; i += wstride) {
-        const int64_t u = rows[i];
-        const double acc = warp_row_gather(ptr, idx, val, u, yz + toff, lane);
-        if (lane < TILE) {
-            const int64_t o = toff + u * TILE + lane;
-            const double d = D[u];
-            const double yu = yz[o];
-            yz[o] = (d != 0.0 ? yu / d : yu) - acc;
-        }
-    }
-}
-
 
 // ---------------------------------------------------------------- chunked gather (SpMM-shaped work)
 // A chunk is a run of consecutive stored rows with at most CHUNK_CAP entries and CHUNK_ROWS rows (or
@@ -338,40 +388,40 @@ enum { M_SPMM = 0, M_FWD = 1, M_BWD = 2 };
 constexpr int CH_THREADS = 256;
 constexpr int CH_WARPS = CH_THREADS / 32;
 
-template <int MODE>
-__device__ __forceinline__ void chunk_epilogue(double* out, const double* aux, const double* xt, int64_t toff,
-                                               int64_t v, int col, double acc, double& dot) {
+template <int MODE, class T>
+__device__ __forceinline__ void chunk_epilogue(T* out, const T* aux, const T* xt, int64_t toff, int64_t v, int col,
+                                               T acc, double& dot) {
     const int64_t o = toff + v * TILE + col;
     if (MODE == M_SPMM) {
         out[o] = acc;
-        dot += acc * xt[v * TILE + col];
+        dot += (double)acc * (double)xt[v * TILE + col];
     } else if (MODE == M_FWD) {
         out[o] = aux[o] - acc;
     } else {
-        const double d = aux[v];
-        const double yu = out[o];
-        out[o] = (d != 0.0 ? yu / d : yu) - acc;
+        const T d = aux[v];
+        const T yu = out[o];
+        out[o] = (d != (T)0 ? yu / d : yu) - acc;
     }
 }
 
-template <int MODE>
+template <int MODE, class T>
 __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks,
                                                         const int64_t* __restrict__ ptr,
                                                         const int32_t* __restrict__ idx,
-                                                        const double* __restrict__ val,
-                                                        const int32_t* __restrict__ rowmap, const double* xsrc,
-                                                        double* out, const double* __restrict__ aux, int64_t ld,
+                                                        const T* __restrict__ val,
+                                                        const int32_t* __restrict__ rowmap, const T* xsrc,
+                                                        T* out, const T* __restrict__ aux, int64_t ld,
                                                         double* __restrict__ part) {
     __shared__ int32_t s_idx[CH_WARPS][CHUNK_CAP];
-    __shared__ double s_val[CH_WARPS][CHUNK_CAP];
+    __shared__ T s_val[CH_WARPS][CHUNK_CAP];
     __shared__ int32_t s_ptr[CH_WARPS][CHUNK_ROWS + 1];
     __shared__ double s_red[CH_THREADS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t t = blockIdx.y;
     const int64_t toff = t * n * TILE;
-    const double* xt = xsrc + toff;
+    const T* xt = xsrc + toff;
     int32_t* si = s_idx[w];
-    double* sv = s_val[w];
+    T* sv = s_val[w];
     int32_t* sp = s_ptr[w];
     double dot = 0.0;  // SpMM: per-lane partial of p.q for column (lane % TILE)
     for (int32_t c = blockIdx.x * CH_WARPS + w; c < nchunks; c += gridDim.x * CH_WARPS) {
@@ -389,7 +439,7 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
             for (int32_t pr = lane; pr < pairs; pr += 32) {
                 const int32_t rr = pr / TILE, col = pr % TILE;
                 const int32_t q0 = sp[rr], q1 = sp[rr + 1];
-                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+                T a0 = 0, a1 = 0, a2 = 0, a3 = 0;
                 int32_t q = q0;
                 for (; q + 3 < q1; q += 4) {
                     a0 += sv[q] * xt[(int64_t)si[q] * TILE + col];
@@ -399,23 +449,24 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
                 }
                 for (; q < q1; q++) a0 += sv[q] * xt[(int64_t)si[q] * TILE + col];
                 const int64_t row = r0 + rr;
-                chunk_epilogue<MODE>(out, aux, xt, toff, rowmap ? rowmap[row] : row, col, (a0 + a1) + (a2 + a3), dot);
+                chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[row] : row, col, (a0 + a1) + (a2 + a3),
+                                        dot);
             }
             __syncwarp();
         } else {
             // one long row: (32 / TILE) entry slots x TILE columns per step, then a reduction over the slots
             const int slot = lane / TILE, col = lane % TILE;
-            double a0 = 0.0, a1 = 0.0;
+            T a0 = 0, a1 = 0;
             int64_t q = e0 + slot;
             for (; q + SLOTS < e1; q += 2 * SLOTS) {
                 a0 += __ldcs(val + q) * xt[(int64_t)__ldcs(idx + q) * TILE + col];
                 a1 += __ldcs(val + q + SLOTS) * xt[(int64_t)__ldcs(idx + q + SLOTS) * TILE + col];
             }
             if (q < e1) a0 += __ldcs(val + q) * xt[(int64_t)__ldcs(idx + q) * TILE + col];
-            double acc = a0 + a1;
+            T acc = a0 + a1;
 #pragma unroll
             for (int o = TILE; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane < TILE) chunk_epilogue<MODE>(out, aux, xt, toff, rowmap ? rowmap[r0] : r0, col, acc, dot);
+            if (lane < TILE) chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[r0] : r0, col, acc, dot);
         }
     }
     if (MODE == M_SPMM && part) {
@@ -442,19 +493,20 @@ constexpr int RUN_THREADS = 512;
 constexpr int THIN_ROWS = 64;
 
 // rows[i] is the vertex of stored row i; ptr/idx/val are in storage order
+template <class T>
 __global__ void __launch_bounds__(RUN_THREADS) k_trsv_fwd_run(int64_t n, const int32_t* __restrict__ rows,
                                                               const int32_t* __restrict__ lptr, int32_t l0,
                                                               int32_t l1, const int64_t* __restrict__ ptr,
                                                               const int32_t* __restrict__ idx,
-                                                              const double* __restrict__ val,
-                                                              const double* __restrict__ r, double* y) {
+                                                              const T* __restrict__ val, const T* __restrict__ r,
+                                                              T* y) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = RUN_THREADS / 32;
     const int64_t toff = (int64_t)blockIdx.x * n * TILE;
     for (int32_t l = l0; l < l1; l++) {
         const int32_t s = lptr[l], e = lptr[l + 1];
         for (int32_t i = s + warp; i < e; i += nwarp) {
             const int64_t u = rows[i];
-            const double acc = warp_row_gather(ptr, idx, val, i, y + toff, lane);
+            const T acc = warp_row_gather<T>(ptr, idx, val, i, y + toff, lane);
             if (lane < TILE) {
                 const int64_t o = toff + u * TILE + lane;
                 y[o] = r[o] - acc;
@@ -464,24 +516,25 @@ __global__ void __launch_bounds__(RUN_THREADS) k_trsv_fwd_run(int64_t n, const i
     }
 }
 
+template <class T>
 __global__ void __launch_bounds__(RUN_THREADS) k_trsv_bwd_run(int64_t n, const int32_t* __restrict__ rows,
                                                               const int32_t* __restrict__ lptr, int32_t l0,
                                                               int32_t l1, const int64_t* __restrict__ ptr,
                                                               const int32_t* __restrict__ idx,
-                                                              const double* __restrict__ val,
-                                                              const double* __restrict__ D, double* yz) {
+                                                              const T* __restrict__ val, const T* __restrict__ D,
+                                                              T* yz) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = RUN_THREADS / 32;
     const int64_t toff = (int64_t)blockIdx.x * n * TILE;
     for (int32_t l = l1 - 1; l >= l0; l--) {
         const int32_t s = lptr[l], e = lptr[l + 1];
         for (int32_t i = s + warp; i < e; i += nwarp) {
             const int64_t u = rows[i];
-            const double acc = warp_row_gather(ptr, idx, val, i, yz + toff, lane);
+            const T acc = warp_row_gather<T>(ptr, idx, val, i, yz + toff, lane);
             if (lane < TILE) {
                 const int64_t o = toff + u * TILE + lane;
-                const double d = D[u];
-                const double yu = yz[o];
-                yz[o] = (d != 0.0 ? yu / d : yu) - acc;
+                const T d = D[u];
+                const T yu = yz[o];
+                yz[o] = (d != (T)0 ? yu / d : yu) - acc;
             }
         }
         __syncthreads();
@@ -489,6 +542,14 @@ __global__ void __launch_bounds__(RUN_THREADS) k_trsv_bwd_run(int64_t n, const i
 }
 
 // ---------------------------------------------------------------- preconditioner as a CUDA graph
+// values of the factor in the precision of the solve (the structure is shared)
+template <class T>
+struct FactorVals {
+    const T* prow_val;
+    const T* pcol_val;
+    const T* D;
+};
+
 struct Precond {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -516,35 +577,37 @@ static std::vector<std::pair<int32_t, int32_t>> level_segments(const DevFactor& 
     return seg;
 }
 
-static int64_t launch_precond(Context& C, const DevFactor& F, int64_t n, const double* r, double* y, int64_t ld) {
+template <class T>
+static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
+                              int64_t ld) {
     const int ntiles = (int)(ld / TILE);
     int64_t launches = 0;
     const auto seg = level_segments(F);
     for (size_t i = 0; i < seg.size(); i++) {
         const int32_t l0 = seg[i].first, l1 = seg[i].second;
         if (l1 - l0 >= 2) {
-            k_trsv_fwd_run<<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.level_ptr_d, l0, l1, F.prow_ptr,
-                                                                  F.prow_idx, F.prow_val, r, y);
+            k_trsv_fwd_run<T><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.level_ptr_d, l0, l1,
+                                                                     F.prow_ptr, F.prow_idx, V.prow_val, r, y);
         } else {
             const int32_t c0 = F.fchunk_lvl[l0], nc = F.fchunk_lvl[l0 + 1] - c0;
             if (nc == 0) continue;
             dim3 grid((unsigned)chunk_blocks(nc), (unsigned)ntiles);
-            k_chunked<M_FWD><<<grid, CH_THREADS, 0, C.stream>>>(n, F.fchunk + c0, nc, F.prow_ptr, F.prow_idx,
-                                                                 F.prow_val, F.level_rows, y, y, r, ld, nullptr);
+            k_chunked<M_FWD, T><<<grid, CH_THREADS, 0, C.stream>>>(n, F.fchunk + c0, nc, F.prow_ptr, F.prow_idx,
+                                                                    V.prow_val, F.level_rows, y, y, r, ld, nullptr);
         }
         launches++;
     }
     for (size_t i = seg.size(); i-- > 0;) {
         const int32_t l0 = seg[i].first, l1 = seg[i].second;
         if (l1 - l0 >= 2) {
-            k_trsv_bwd_run<<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.level_ptr_d, l0, l1, F.pcol_ptr,
-                                                                  F.pcol_idx, F.pcol_val, F.D, y);
+            k_trsv_bwd_run<T><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.level_ptr_d, l0, l1,
+                                                                     F.pcol_ptr, F.pcol_idx, V.pcol_val, V.D, y);
         } else {
             const int32_t c0 = F.bchunk_lvl[l0], nc = F.bchunk_lvl[l0 + 1] - c0;
             if (nc == 0) continue;
             dim3 grid((unsigned)chunk_blocks(nc), (unsigned)ntiles);
-            k_chunked<M_BWD><<<grid, CH_THREADS, 0, C.stream>>>(n, F.bchunk + c0, nc, F.pcol_ptr, F.pcol_idx,
-                                                                 F.pcol_val, F.level_rows, y, y, F.D, ld, nullptr);
+            k_chunked<M_BWD, T><<<grid, CH_THREADS, 0, C.stream>>>(n, F.bchunk + c0, nc, F.pcol_ptr, F.pcol_idx,
+                                                                    V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr);
         }
         launches++;
     }
@@ -552,11 +615,12 @@ static int64_t launch_precond(Context& C, const DevFactor& F, int64_t n, const d
     return launches;
 }
 
-static void build_precond_graph(Context& C, const DevFactor& F, int64_t n, const double* r, double* y, int64_t ld,
-                                Precond& P, int64_t& launches) {
+template <class T>
+static void build_precond_graph(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
+                                int64_t ld, Precond& P, int64_t& launches) {
     SSP_CUDA(cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeThreadLocal));
     try {
-        launches = launch_precond(C, F, n, r, y, ld);
+        launches = launch_precond<T>(C, F, V, n, r, y, ld);
     } catch (...) {
         cudaGraph_t g;
         cudaStreamEndCapture(C.stream, &g);
@@ -567,9 +631,11 @@ static void build_precond_graph(Context& C, const DevFactor& F, int64_t n, const
     SSP_CUDA(cudaGraphInstantiate(&P.exec, P.graph, 0));
 }
 
+static FactorVals<double> fp64_vals(const DevFactor& F) { return FactorVals<double>{F.prow_val, F.pcol_val, F.D}; }
+
 // apply M^{-1} to R into Z once (tile-major n x ld blocks; stage entry point)
 void precond_apply_device(Context& C, const DevFactor& F, const double* R, double* Z, int64_t ld) {
-    int64_t l = launch_precond(C, F, F.n, R, Z, ld);
+    int64_t l = launch_precond<double>(C, F, fp64_vals(F), F.n, R, Z, ld);
     C.kernels_launched += l;
 }
 
@@ -603,6 +669,96 @@ struct EventPairs {
     }
 };
 
+// ---------------------------------------------------------------- one PCG solve in one precision
+// The Laplacian split into row-aligned chunks, about one wave of blocks per tile.
+struct SpmmPlan {
+    const int32_t* chunks = nullptr;
+    int32_t nchunks = 0;
+    dim3 grid;
+    double* part = nullptr;
+};
+
+template <class T>
+struct PcgBufs {
+    T* e;  // solution increment (zero on entry)
+    T* r;  // right-hand side on entry, residual on exit
+    T* z;
+    T* p;
+    T* q;
+};
+
+struct PcgTimers {
+    EventPairs spmm, pc, loop;
+};
+
+// Runs PCG on A e = r for every column that S marks active (S.thr, S.active, S.nactive set by the
+// caller; e zero).  Returns the iterations of the loop.
+template <class T>
+static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const SpmmPlan& A, const int64_t* aptr,
+                         const int32_t* aidx, const T* aval, const Precond& P, int64_t pc_launches, PcgBufs<T> B,
+                         ColState& S, Reducer& R, int32_t max_iters, const PcgOptions& opt, PcgTimers& tm) {
+    const int64_t ntiles = ld / TILE;
+    const int64_t total = n * ld;
+    const dim3 egrid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div<int64_t>(n * TILE, 256),
+                                                                      2048 / std::max<int64_t>(1, ntiles) + 4)),
+                     (unsigned)ntiles);
+    const int cg = grid_for(ld, 256);
+    int64_t active = read_i64(C, S.nactive);
+    int32_t it = 0;
+    if (active == 0) return 0;
+    tm.pc.begin(C.stream);
+    SSP_CUDA(cudaGraphLaunch(P.exec, C.stream));
+    tm.pc.end(C.stream);
+    C.kernels_launched += pc_launches;
+    R.run<OP_DOT, T>(B.r, B.z, S.rz);
+    SSP_CUDA(cudaMemcpyAsync(B.p, B.z, sizeof(T) * total, cudaMemcpyDeviceToDevice, C.stream));
+    tm.loop.begin(C.stream);
+    while (it < max_iters) {
+        tm.spmm.begin(C.stream);
+        k_chunked<M_SPMM, T><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks, A.nchunks, aptr, aidx, aval, nullptr,
+                                                                   B.p, B.q, nullptr, ld, A.part);
+        tm.spmm.end(C.stream);
+        k_colred_final<<<cg, 256, 0, C.stream>>>(ld, (int)A.grid.x, A.part, S.pq);
+        k_cols_alpha<<<cg, 256, 0, C.stream>>>(ld, S);
+        k_axpy_xr_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
+            n, S.alpha, B.p, B.q, B.e, B.r, R.rows_per_blk, ld, R.part);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched += 4;
+        R.finish(S.rr);
+        it++;
+        SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
+        k_cols_check<<<cg, 256, 0, C.stream>>>(ld, it, S);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched++;
+        active = read_i64(C, S.nactive);
+        if (opt.history) {
+            std::vector<double> hrr(k), hbb(k);
+            SSP_CUDA(cudaMemcpyAsync(hrr.data(), S.rr, sizeof(double) * k, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(hbb.data(), S.bnorm2, sizeof(double) * k, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaStreamSynchronize(C.stream));
+            double mx = 0.0;
+            for (int32_t j = 0; j < k; j++)
+                if (hbb[j] > 0) mx = std::max(mx, std::sqrt(hrr[j] / hbb[j]));
+            opt.history->push_back(mx);
+        }
+        if (opt.verbose && (it % 10 == 0 || active == 0))
+            fprintf(stderr, "[ssp] pcg%s iter %d: %lld columns active\n", sizeof(T) == 4 ? " (fp32 inner)" : "", it,
+                    (long long)active);
+        if (active == 0) break;
+        tm.pc.begin(C.stream);
+        SSP_CUDA(cudaGraphLaunch(P.exec, C.stream));
+        tm.pc.end(C.stream);
+        C.kernels_launched += pc_launches;
+        R.run<OP_DOT, T>(B.r, B.z, S.rz_new);
+        k_cols_beta<<<cg, 256, 0, C.stream>>>(ld, S);
+        k_update_p<T><<<egrid, 256, 0, C.stream>>>(n, S.beta, B.z, B.p);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched += 2;
+    }
+    tm.loop.end(C.stream);
+    return it;
+}
+
 // ---------------------------------------------------------------- driver
 // Y: tile-major n x ld (ld = round8(k)), read only.  The solution stays in the workspace buffer
 // "pcg_x" (tile-major); *x_out points at it.
@@ -610,6 +766,8 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 const DevFactor& F, const double* Y, int32_t k, const double** x_out, const PcgOptions& opt,
                 PcgReport& rep, int32_t* h_iters, double* h_relres) {
     SSP_REQUIRE(k > 0, SSP_ERR_INVALID, "pcg: k must be positive");
+    const bool mixed = opt.precision == SSP_PRECISION_MIXED;
+    SSP_REQUIRE(mixed || opt.precision == SSP_PRECISION_FP64, SSP_ERR_INVALID, "pcg: unknown precision");
     const int64_t ld = ((int64_t)k + TILE - 1) / TILE * TILE;
     const int64_t ntiles = ld / TILE;
     const int64_t total = n * ld;
@@ -619,118 +777,160 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
     double* z = W.get_t<double>("pcg_z", total);
     double* p = W.get_t<double>("pcg_p", total);
     double* q = W.get_t<double>("pcg_q", total);
-    double* colv = W.get_t<double>("pcg_cols", 11 * ld);
-    int32_t* coli = W.get_t<int32_t>("pcg_coli", 2 * ld);
-    int64_t* nact = W.get_t<int64_t>("pcg_nactive", 1);
-    ColState S{colv, colv + ld, colv + 2 * ld, colv + 3 * ld, colv + 4 * ld, colv + 5 * ld, colv + 6 * ld,
-               colv + 7 * ld, coli, coli + ld, nact};
-    double* colsum = colv + 8 * ld;
-    double* relres = colv + 9 * ld;
-    double* mean = colv + 10 * ld;
+    ColState S = make_colstate(C, ld, "pcg");
+    double* colv = W.get_t<double>("pcg_aux", 3 * ld);
+    double* colsum = colv;
+    double* relres = colv + ld;
+    double* mean = colv + 2 * ld;
     Reducer R;
     R.init(C, n, ld);
     // SpMM: row-aligned chunks of the Laplacian, about one wave of blocks per tile
     std::vector<int32_t> achunks;
+    int64_t lap_nnz = 0;
     {
         std::vector<int64_t> hp(n + 1);
         SSP_CUDA(cudaMemcpyAsync(hp.data(), lap_ptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, C.stream));
         SSP_CUDA(cudaStreamSynchronize(C.stream));
         make_chunks(hp, 0, (int32_t)n, achunks);
         achunks.push_back((int32_t)n);
+        lap_nnz = hp[n];
     }
-    const int32_t anch = (int32_t)achunks.size() - 1;
+    SpmmPlan A;
+    A.nchunks = (int32_t)achunks.size() - 1;
     int32_t* d_achunks = W.get_t<int32_t>("pcg_achunks", achunks.size());
     SSP_CUDA(cudaMemcpyAsync(d_achunks, achunks.data(), sizeof(int32_t) * achunks.size(), cudaMemcpyHostToDevice,
                              C.stream));
-    const int spmm_bx = chunk_blocks(anch);
-    double* spmm_part = W.get_t<double>("pcg_spmm_part", (size_t)spmm_bx * ld);
-    const dim3 sgrid((unsigned)spmm_bx, (unsigned)ntiles);
+    A.chunks = d_achunks;
+    const int spmm_bx = chunk_blocks(A.nchunks);
+    A.part = W.get_t<double>("pcg_spmm_part", (size_t)spmm_bx * ld);
+    A.grid = dim3((unsigned)spmm_bx, (unsigned)ntiles);
     const dim3 egrid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div<int64_t>(n * TILE, 256),
                                                                       2048 / std::max<int64_t>(1, ntiles) + 4)),
                      (unsigned)ntiles);
     const int cg = grid_for(ld, 256);
 
     // r = Y - mean(Y); x = 0; ||b||^2
-    R.run<OP_SUM>(Y, nullptr, colsum);
+    R.run<OP_SUM, double>(Y, nullptr, colsum);
     k_center<<<egrid, 256, 0, C.stream>>>(n, k, Y, colsum, r, x, mean);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
-    R.run<OP_SQ>(r, nullptr, S.bnorm2);
-    SSP_CUDA(cudaMemsetAsync(nact, 0, sizeof(int64_t), C.stream));
+    R.run<OP_SQ, double>(r, nullptr, S.bnorm2);
+    SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
     k_cols_init<<<cg, 256, 0, C.stream>>>(ld, k, opt.tol, opt.abs_tol, S);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
-    int64_t active = read_i64(C, nact);
 
-    Precond P;
-    int64_t pc_launches = 0;
+    PcgTimers tm;
+    EventPairs ev_resid;
     int32_t it = 0;
-    EventPairs ev_spmm, ev_pc, ev_loop;
-    if (active > 0) {
-        build_precond_graph(C, F, n, r, z, ld, P, pc_launches);
-        ev_pc.begin(C.stream);
-        SSP_CUDA(cudaGraphLaunch(P.exec, C.stream));
-        ev_pc.end(C.stream);
-        C.kernels_launched += pc_launches;
-        R.run<OP_DOT>(r, z, S.rz);
-        SSP_CUDA(cudaMemcpyAsync(p, z, sizeof(double) * total, cudaMemcpyDeviceToDevice, C.stream));
-        ev_loop.begin(C.stream);
-        while (it < opt.max_iters) {
-            ev_spmm.begin(C.stream);
-            k_chunked<M_SPMM><<<sgrid, CH_THREADS, 0, C.stream>>>(n, d_achunks, anch, lap_ptr, lap_idx, lap_val,
-                                                                   nullptr, p, q, nullptr, ld, spmm_part);
-            ev_spmm.end(C.stream);
-            k_colred_final<<<cg, 256, 0, C.stream>>>(ld, spmm_bx, spmm_part, S.pq);
-            k_cols_alpha<<<cg, 256, 0, C.stream>>>(ld, S);
-            k_axpy_xr_rr<<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
-                n, S.alpha, p, q, x, r, R.rows_per_blk, ld, R.part);
-            SSP_CHECK_LAUNCH();
-            C.kernels_launched += 4;
-            R.finish(S.rr);
-            it++;
-            SSP_CUDA(cudaMemsetAsync(nact, 0, sizeof(int64_t), C.stream));
-            k_cols_check<<<cg, 256, 0, C.stream>>>(ld, it, S);
+    rep = PcgReport();
+    if (!mixed) {
+        Precond P;
+        int64_t pc_launches = 0;
+        if (read_i64(C, S.nactive) > 0) {
+            build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, P, pc_launches);
+            it = pcg_solve<double>(C, n, k, ld, A, lap_ptr, lap_idx, lap_val, P, pc_launches,
+                                   PcgBufs<double>{x, r, z, p, q}, S, R, opt.max_iters, opt, tm);
+        }
+    } else {
+        // FP32 copies of the Laplacian and factor values, and the FP32 inner vectors
+        float* aval32 = W.get_t<float>("pcgm_aval", lap_nnz + 1);
+        float* fval32 = W.get_t<float>("pcgm_fval", 2 * F.nnz + n + 1);
+        auto to_f32 = [&](int64_t count, const double* src, float* dst) {
+            if (count <= 0) return;
+            k_d2f<<<grid_for(count, 256, 148 * 16), 256, 0, C.stream>>>(count, src, dst);
             SSP_CHECK_LAUNCH();
             C.kernels_launched++;
-            active = read_i64(C, nact);
-            if (opt.history) {
-                std::vector<double> hrr(k), hbb(k);
-                SSP_CUDA(cudaMemcpyAsync(hrr.data(), S.rr, sizeof(double) * k, cudaMemcpyDeviceToHost, C.stream));
-                SSP_CUDA(cudaMemcpyAsync(hbb.data(), S.bnorm2, sizeof(double) * k, cudaMemcpyDeviceToHost, C.stream));
-                SSP_CUDA(cudaStreamSynchronize(C.stream));
-                double mx = 0.0;
-                for (int32_t j = 0; j < k; j++)
-                    if (hbb[j] > 0) mx = std::max(mx, std::sqrt(hrr[j] / hbb[j]));
-                opt.history->push_back(mx);
+        };
+        to_f32(lap_nnz, lap_val, aval32);
+        to_f32(F.nnz, F.prow_val, fval32);
+        to_f32(F.nnz, F.pcol_val, fval32 + F.nnz);
+        to_f32(n, F.D, fval32 + 2 * F.nnz);
+        const FactorVals<float> V32{fval32, fval32 + F.nnz, fval32 + 2 * F.nnz};
+        float* e32 = W.get_t<float>("pcgm_e", total);
+        float* r32 = W.get_t<float>("pcgm_r", total);
+        float* z32 = W.get_t<float>("pcgm_z", total);
+        float* p32 = W.get_t<float>("pcgm_p", total);
+        float* q32 = W.get_t<float>("pcgm_q", total);
+        ColState Si = make_colstate(C, ld, "pcgm_in");
+        double* worst = W.get_t<double>("pcgm_worst", 1);
+        double* e64 = nullptr;  // FP64 inner increment, only if a round falls back
+        Precond P32, P64;
+        int64_t pc32 = 0, pc64 = 0;
+        bool use64 = false;
+        int64_t active = read_i64(C, S.nactive);
+        while (active > 0 && rep.refinements < MIXED_MAX_ROUNDS && it < opt.max_iters) {
+            int32_t its;
+            SSP_CUDA(cudaMemsetAsync(Si.nactive, 0, sizeof(int64_t), C.stream));
+            if (!use64) {
+                k_rhs_masked<float><<<egrid, 256, 0, C.stream>>>(n, r, S.active, r32);
+                SSP_CUDA(cudaMemsetAsync(e32, 0, sizeof(float) * total, C.stream));
+                R.run<OP_SQ, float>(r32, nullptr, Si.bnorm2);
+                k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, MIXED_INNER_REDUCTION, S.thr, Si);
+                SSP_CHECK_LAUNCH();
+                C.kernels_launched += 2;
+                if (!P32.exec) build_precond_graph<float>(C, F, V32, n, r32, z32, ld, P32, pc32);
+                its = pcg_solve<float>(C, n, k, ld, A, lap_ptr, lap_idx, aval32, P32, pc32,
+                                       PcgBufs<float>{e32, r32, z32, p32, q32}, Si, R, opt.max_iters - it, opt, tm);
+                k_add_into<float><<<grid_for(total, 256, 148 * 16), 256, 0, C.stream>>>(total, e32, x);
+            } else {
+                if (!e64) e64 = W.get_t<double>("pcgm_e64", total);
+                // the FP64 inner solve runs in place on the residual of the active columns and goes straight
+                // to (half) the outer threshold
+                k_rhs_masked<double><<<egrid, 256, 0, C.stream>>>(n, r, S.active, r);
+                SSP_CUDA(cudaMemsetAsync(e64, 0, sizeof(double) * total, C.stream));
+                R.run<OP_SQ, double>(r, nullptr, Si.bnorm2);
+                k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, 0.0, S.thr, Si);
+                SSP_CHECK_LAUNCH();
+                C.kernels_launched += 2;
+                if (!P64.exec) build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, P64, pc64);
+                its = pcg_solve<double>(C, n, k, ld, A, lap_ptr, lap_idx, lap_val, P64, pc64,
+                                        PcgBufs<double>{e64, r, z, p, q}, Si, R, opt.max_iters - it, opt, tm);
+                k_add_into<double><<<grid_for(total, 256, 148 * 16), 256, 0, C.stream>>>(total, e64, x);
+                rep.fp64_rounds++;
             }
-            if (opt.verbose && (it % 10 == 0 || active == 0))
-                fprintf(stderr, "[ssp] pcg iter %d: %lld columns active\n", it, (long long)active);
-            if (active == 0) break;
-            ev_pc.begin(C.stream);
-            SSP_CUDA(cudaGraphLaunch(P.exec, C.stream));
-            ev_pc.end(C.stream);
-            C.kernels_launched += pc_launches;
-            R.run<OP_DOT>(r, z, S.rz_new);
-            k_cols_beta<<<cg, 256, 0, C.stream>>>(ld, S);
-            k_update_p<<<egrid, 256, 0, C.stream>>>(n, S.beta, z, p);
+            SSP_CHECK_LAUNCH();
+            C.kernels_launched++;
+            it += its;
+            rep.refinements++;
+            // true residual with the FP64 matrix and FP64 x
+            ev_resid.begin(C.stream);
+            k_chunked<M_SPMM, double><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks, A.nchunks, lap_ptr, lap_idx,
+                                                                            lap_val, nullptr, x, q, nullptr, ld,
+                                                                            nullptr);
+            ev_resid.end(C.stream);
+            k_true_resid<<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
+                n, k, Y, mean, q, r, R.rows_per_blk, ld, R.part);
             SSP_CHECK_LAUNCH();
             C.kernels_launched += 2;
+            R.finish(relres);
+            SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
+            SSP_CUDA(cudaMemsetAsync(worst, 0, sizeof(double), C.stream));
+            k_cols_outer<<<cg, 256, 0, C.stream>>>(ld, Si.iters, relres, S, worst);
+            SSP_CHECK_LAUNCH();
+            C.kernels_launched++;
+            active = read_i64(C, S.nactive);
+            double hw = 0.0;
+            SSP_CUDA(cudaMemcpyAsync(&hw, worst, sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaStreamSynchronize(C.stream));
+            if (opt.verbose)
+                fprintf(stderr, "[ssp] refinement %d (%s inner, %d iterations): %lld columns active, worst ratio %.3g\n",
+                        rep.refinements, use64 ? "fp64" : "fp32", its, (long long)active, hw);
+            if (active > 0 && !use64 && (hw > MIXED_MIN_CONTRACTION || its == 0)) use64 = true;
         }
-        ev_loop.end(C.stream);
     }
     // true relative residual ||(Y - mean) - A x|| / ||Y - mean||
-    k_chunked<M_SPMM><<<sgrid, CH_THREADS, 0, C.stream>>>(n, d_achunks, anch, lap_ptr, lap_idx, lap_val, nullptr, x,
-                                                           q, nullptr, ld, nullptr);
+    k_chunked<M_SPMM, double><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks, A.nchunks, lap_ptr, lap_idx, lap_val,
+                                                                    nullptr, x, q, nullptr, ld, nullptr);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
-    R.run<OP_SQDIFF_CENTERED>(Y, q, relres, mean);
+    R.run<OP_SQDIFF_CENTERED, double>(Y, q, relres, mean);
     std::vector<double> hb(ld), hr(ld);
     std::vector<int32_t> hi(ld);
     SSP_CUDA(cudaMemcpyAsync(hb.data(), S.bnorm2, sizeof(double) * ld, cudaMemcpyDeviceToHost, C.stream));
     SSP_CUDA(cudaMemcpyAsync(hr.data(), relres, sizeof(double) * ld, cudaMemcpyDeviceToHost, C.stream));
     SSP_CUDA(cudaMemcpyAsync(hi.data(), S.iters, sizeof(int32_t) * ld, cudaMemcpyDeviceToHost, C.stream));
     SSP_CUDA(cudaStreamSynchronize(C.stream));
-    rep = PcgReport();
     double sum_it = 0;
     for (int32_t j = 0; j < k; j++) {
         double rel = hb[j] > 0 ? sqrt(hr[j]) / sqrt(hb[j]) : 0.0;
@@ -742,11 +942,13 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         if (!(rel < 0.01)) rep.not_converged++;
     }
     rep.mean_iters = sum_it / k;
-    rep.ms_spmm = ev_spmm.total_ms();
-    rep.n_spmm = (int64_t)ev_spmm.used;
-    rep.ms_precond = ev_pc.total_ms();
-    rep.n_precond = (int64_t)ev_pc.used;
-    rep.ms_loop = ev_loop.total_ms();
+    rep.ms_spmm = tm.spmm.total_ms();
+    rep.n_spmm = (int64_t)tm.spmm.used;
+    rep.ms_precond = tm.pc.total_ms();
+    rep.n_precond = (int64_t)tm.pc.used;
+    rep.ms_loop = tm.loop.total_ms();
+    rep.ms_resid = ev_resid.total_ms();
+    rep.n_resid = (int64_t)ev_resid.used;
     rep.iters_run = it;
     if (x_out) *x_out = x;
 }

@@ -11,7 +11,8 @@
 
 namespace ssp {
 
-template <bool TM>
+// ROOT = false leaves the sum of squares (one rank's share of the columns, summed across ranks later)
+template <bool TM, bool ROOT = true>
 __global__ void __launch_bounds__(256) k_diff_norms(int64_t m, const int32_t* __restrict__ v1,
                                                     const int32_t* __restrict__ v2, const double* __restrict__ Z,
                                                     int32_t k, int64_t ldz, int64_t n, double* __restrict__ d) {
@@ -28,8 +29,13 @@ __global__ void __launch_bounds__(256) k_diff_norms(int64_t m, const int32_t* __
         }
 #pragma unroll
         for (int o = 16; o >= 1; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
-        if (lane == 0) d[e] = sqrt(s);
+        if (lane == 0) d[e] = ROOT ? sqrt(s) : s;
     }
+}
+
+__global__ void k_sqrt_vec(int64_t m, const double* __restrict__ sq, double* __restrict__ d) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x)
+        d[e] = sqrt(sq[e]);
 }
 
 __global__ void k_probs(int64_t m, const double* __restrict__ w, const double* __restrict__ d, double beta,
@@ -124,6 +130,22 @@ void diff_norms_device(Context& C, int64_t m, const int32_t* v1, const int32_t* 
         k_diff_norms<true><<<grid_for(m * 32, 256, 148 * 16), 256, 0, C.stream>>>(m, v1, v2, Z, k, ldz, n_tile_major, d);
     else
         k_diff_norms<false><<<grid_for(m * 32, 256, 148 * 16), 256, 0, C.stream>>>(m, v1, v2, Z, k, ldz, 0, d);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+}
+
+void diff_sq_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z, int32_t k,
+                    int64_t n_tile_major, double* sq) {
+    if (m == 0) return;
+    k_diff_norms<true, false><<<grid_for(m * 32, 256, 148 * 16), 256, 0, C.stream>>>(m, v1, v2, Z, k, k,
+                                                                                     n_tile_major, sq);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+}
+
+void sqrt_device(Context& C, int64_t m, const double* sq, double* d) {
+    if (m == 0) return;
+    k_sqrt_vec<<<grid_for(m, 256), 256, 0, C.stream>>>(m, sq, d);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
 }

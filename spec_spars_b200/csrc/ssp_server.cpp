@@ -1,0 +1,296 @@
+// ssp_server.cpp -- a persistent request loop for sparsification on one device.
+//
+// The reference runs one graph per process (sparsify_dataset, lib.rs:158-168; InputStream::run_stream,
+// stream.rs:40-64).  Here requests of uneven size arrive from any host thread (ssp_submit) and are served by
+// `slots` worker threads, each owning one ssp_context (its own stream and grow-only workspace), so the
+// admitted requests run concurrently on the device.  Admission is first come, first served: the oldest
+// pending request is admitted as soon as a slot is free and its estimated device footprint fits beside the
+// footprints of the requests in flight (the HBM budget); a request whose footprint alone exceeds the budget
+// is refused at submit.  Each request runs the same ssp_sparsify as a lone call, so its result does not
+// depend on what else is in flight.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/specspars.h"
+
+namespace ssp {
+void set_last_error(const std::string& msg);
+}
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+struct Job {
+    uint64_t ticket = 0;
+    int64_t n = 0;
+    std::vector<int64_t> colptr;
+    std::vector<int32_t> rowidx;
+    std::vector<double> values;
+    ssp_params params;
+    std::string output_file;
+    int64_t est_bytes = 0;
+    Clock::time_point t_submit, t_admit, t_done;
+    bool done = false;
+    int32_t status = SSP_OK;
+    std::string error;
+    ssp_csc_out out;
+    ssp_stats stats;
+    int32_t slot = -1;
+};
+
+int fail(int code, const std::string& msg) {
+    ssp::set_last_error(msg);
+    return code;
+}
+
+}  // namespace
+
+struct ssp_server {
+    ssp_server_opts opts;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Job*> pending;
+    std::unordered_map<uint64_t, std::unique_ptr<Job>> jobs;
+    uint64_t next_ticket = 1;
+    int32_t inflight = 0, peak_inflight = 0;
+    int64_t inflight_bytes = 0, peak_inflight_bytes = 0;
+    int64_t submitted = 0, completed = 0, failed = 0, rejected = 0;
+    bool stopping = false;
+    std::vector<ssp_context*> ctxs;
+    std::vector<std::thread> workers;
+
+    void worker(int slot) {
+        ssp_context* ctx = ctxs[slot];
+        const int64_t keep_ws = opts.hbm_budget_bytes / std::max(1, opts.slots);
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+            cv_work.wait(lk, [&] {
+                if (stopping) return true;
+                if (pending.empty()) return false;
+                const Job* j = pending.front();
+                return inflight == 0 || inflight_bytes + j->est_bytes <= opts.hbm_budget_bytes;
+            });
+            if (stopping) return;
+            Job* j = pending.front();
+            pending.pop_front();
+            inflight++;
+            inflight_bytes += j->est_bytes;
+            peak_inflight = std::max(peak_inflight, inflight);
+            peak_inflight_bytes = std::max(peak_inflight_bytes, inflight_bytes);
+            j->t_admit = Clock::now();
+            j->slot = slot;
+            lk.unlock();
+
+            ssp_csc g;
+            g.n = j->n;
+            g.nnz = (int64_t)j->values.size();
+            g.colptr = j->colptr.data();
+            g.rowidx = j->rowidx.data();
+            g.values = j->values.data();
+            g.mem = SSP_MEM_HOST;
+            j->params.output_file = j->output_file.c_str();
+            memset(&j->out, 0, sizeof(j->out));
+            memset(&j->stats, 0, sizeof(j->stats));
+            const int rc = ssp_sparsify(ctx, &g, &j->params, SSP_MEM_HOST, &j->out, &j->stats);
+            std::string err = rc == SSP_OK ? std::string() : std::string(ssp_last_error());
+            // keep the slot's cached workspace within its share of the budget
+            if (ssp_context_workspace_bytes(ctx) > keep_ws) ssp_context_release_workspace(ctx);
+            // the input copy is no longer needed
+            std::vector<int64_t>().swap(j->colptr);
+            std::vector<int32_t>().swap(j->rowidx);
+            std::vector<double>().swap(j->values);
+
+            lk.lock();
+            j->status = rc;
+            j->error = err;
+            j->t_done = Clock::now();
+            j->done = true;
+            inflight--;
+            inflight_bytes -= j->est_bytes;
+            if (rc == SSP_OK) completed++;
+            else failed++;
+            cv_done.notify_all();
+            cv_work.notify_all();
+        }
+    }
+
+    void fill(Job* j, ssp_result* r) {
+        memset(r, 0, sizeof(*r));
+        r->status = j->status;
+        snprintf(r->error, sizeof r->error, "%s", j->error.c_str());
+        r->out = j->out;
+        r->stats = j->stats;
+        r->est_bytes = j->est_bytes;
+        r->queue_ms = ms_between(j->t_submit, j->t_admit);
+        r->run_ms = ms_between(j->t_admit, j->t_done);
+        r->latency_ms = ms_between(j->t_submit, j->t_done);
+        r->slot = j->slot;
+    }
+};
+
+extern "C" {
+
+void ssp_server_opts_default(ssp_server_opts* o) {
+    memset(o, 0, sizeof(*o));
+    o->device = 0;
+    o->slots = 4;
+    o->hbm_budget_bytes = 0;  // 85% of the device memory free at creation
+    o->max_pending = 0;       // unbounded
+}
+
+int64_t ssp_request_footprint(const ssp_csc* graph, const ssp_params* params) {
+    if (!graph || !params || graph->n <= 0) return -1;
+    const int64_t n = graph->n, nnz = graph->nnz;
+    const int64_t k = ssp_params_jl_dim(params, n);
+    const int64_t ld = (k + 7) / 8 * 8;
+    // n x ld blocks: sketch + x, r, z, p, q in FP64 (+ five FP32 blocks and an FP64 increment when mixed);
+    // graph, Laplacian, factor pools and sampling arrays per stored entry; a fixed allowance
+    const double blocks = params->precision == SSP_PRECISION_MIXED ? 6.0 + 2.5 + 1.0 : 6.0;
+    return (int64_t)(blocks * 8.0 * (double)n * (double)ld) + 200 * nnz + 96 * n + (16ll << 20);
+}
+
+int ssp_server_create(const ssp_server_opts* opts, ssp_server** out) {
+    if (!out) return fail(SSP_ERR_INVALID, "ssp_server_create: out is NULL");
+    *out = nullptr;
+    ssp_server_opts o;
+    if (opts) o = *opts;
+    else ssp_server_opts_default(&o);
+    if (o.slots < 1 || o.slots > 64) return fail(SSP_ERR_INVALID, "ssp_server_create: slots must be in [1, 64]");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(SSP_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    if (o.device < 0 || o.device >= count) return fail(SSP_ERR_INVALID, "ssp_server_create: device out of range");
+    if (o.hbm_budget_bytes <= 0) {
+        size_t fr = 0, tot = 0;
+        if (cudaSetDevice(o.device) != cudaSuccess || cudaMemGetInfo(&fr, &tot) != cudaSuccess)
+            return fail(SSP_ERR_CUDA, "ssp_server_create: cannot query device memory");
+        o.hbm_budget_bytes = (int64_t)(0.85 * (double)fr);
+    }
+    std::unique_ptr<ssp_server> s(new ssp_server());
+    s->opts = o;
+    for (int i = 0; i < o.slots; i++) {
+        ssp_context* c = nullptr;
+        const int rc = ssp_context_create(o.device, &c);
+        if (rc != SSP_OK) {
+            const std::string msg = ssp_last_error();
+            for (auto* x : s->ctxs) ssp_context_destroy(x);
+            return fail(rc, msg);
+        }
+        s->ctxs.push_back(c);
+    }
+    for (int i = 0; i < o.slots; i++) s->workers.emplace_back([srv = s.get(), i] { srv->worker(i); });
+    *out = s.release();
+    return SSP_OK;
+}
+
+int ssp_submit(ssp_server* s, const ssp_request* req, uint64_t* ticket) {
+    if (!s || !req || !ticket) return fail(SSP_ERR_INVALID, "ssp_submit: bad arguments");
+    if (req->kind != SSP_REQ_SPARSIFY) return fail(SSP_ERR_INVALID, "ssp_submit: unknown request kind");
+    const ssp_csc& g = req->graph;
+    if (g.mem != SSP_MEM_HOST || g.n <= 0 || g.nnz < 0 || !g.colptr || (g.nnz > 0 && (!g.rowidx || !g.values)) ||
+        g.colptr[0] != 0 || g.colptr[g.n] != g.nnz)
+        return fail(SSP_ERR_INVALID, "ssp_submit: the graph must be a valid host CSC");
+    const int64_t est = ssp_request_footprint(&g, &req->params);
+    std::unique_ptr<Job> j(new Job());
+    j->n = g.n;
+    j->colptr.assign(g.colptr, g.colptr + g.n + 1);
+    j->rowidx.assign(g.rowidx, g.rowidx + g.nnz);
+    j->values.assign(g.values, g.values + g.nnz);
+    j->params = req->params;
+    j->output_file = req->params.output_file ? req->params.output_file : "";
+    j->est_bytes = est;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) return fail(SSP_ERR_INVALID, "ssp_submit: server is shutting down");
+    if (est > s->opts.hbm_budget_bytes) {
+        s->rejected++;
+        return fail(SSP_ERR_CAPACITY, "ssp_submit: estimated footprint " + std::to_string(est) +
+                                          " bytes exceeds the HBM budget " + std::to_string(s->opts.hbm_budget_bytes));
+    }
+    if (s->opts.max_pending > 0 && (int64_t)s->pending.size() >= s->opts.max_pending) {
+        s->rejected++;
+        return fail(SSP_ERR_CAPACITY, "ssp_submit: pending queue is full");
+    }
+    j->ticket = s->next_ticket++;
+    j->t_submit = Clock::now();
+    *ticket = j->ticket;
+    s->pending.push_back(j.get());
+    s->jobs.emplace(j->ticket, std::move(j));
+    s->submitted++;
+    s->cv_work.notify_one();
+    return SSP_OK;
+}
+
+// On completion the result (including ownership of res->out) moves to the caller and the ticket is retired.
+int ssp_wait(ssp_server* s, uint64_t ticket, int64_t timeout_ms, ssp_result* res) {
+    if (!s || !res) return fail(SSP_ERR_INVALID, "ssp_wait: bad arguments");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end()) return fail(SSP_ERR_INVALID, "ssp_wait: unknown or already collected ticket");
+    Job* j = it->second.get();
+    auto ready = [&] { return j->done; };
+    if (timeout_ms < 0) s->cv_done.wait(lk, ready);
+    else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
+        return SSP_ERR_PENDING;
+    s->fill(j, res);
+    s->jobs.erase(it);
+    return SSP_OK;
+}
+
+int ssp_poll(ssp_server* s, uint64_t ticket, ssp_result* res) { return ssp_wait(s, ticket, 0, res); }
+
+int ssp_server_info_get(ssp_server* s, ssp_server_info* info) {
+    if (!s || !info) return fail(SSP_ERR_INVALID, "ssp_server_info_get: bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    memset(info, 0, sizeof(*info));
+    info->submitted = s->submitted;
+    info->completed = s->completed;
+    info->failed = s->failed;
+    info->rejected = s->rejected;
+    info->pending = (int64_t)s->pending.size();
+    info->inflight = s->inflight;
+    info->peak_inflight = s->peak_inflight;
+    info->peak_inflight_bytes = s->peak_inflight_bytes;
+    info->budget_bytes = s->opts.hbm_budget_bytes;
+    info->slots = s->opts.slots;
+    return SSP_OK;
+}
+
+// Requests still pending are dropped; admitted ones finish first.  Uncollected results are freed.
+int ssp_server_destroy(ssp_server* s) {
+    if (!s) return SSP_OK;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->pending.clear();
+        s->cv_done.wait(lk, [&] { return s->inflight == 0; });
+        s->stopping = true;
+        s->cv_work.notify_all();
+    }
+    for (auto& t : s->workers) t.join();
+    for (auto& kv : s->jobs)
+        if (kv.second->done && kv.second->status == SSP_OK) ssp_csc_free(&kv.second->out);
+    for (auto* c : s->ctxs) ssp_context_destroy(c);
+    delete s;
+    return SSP_OK;
+}
+
+}  // extern "C"

@@ -10,7 +10,8 @@
 // every store instruction writes 32 consecutive doubles.  The 256 sign bits of one edge come from
 // one Philox4x64 call; up to 32 edges are hashed at once (one per lane) and their words are
 // broadcast with shuffles.  The output is row-major (leading dimension ldy) or tile-major (the
-// PCG layout, see tile_off).
+// PCG layout, see tile_off).  A block may hold a range [col_lo, col_lo + k) of the global columns (one
+// rank's share when the columns are split across GPUs): every entry depends on its global column only.
 #include "ssp_internal.cuh"
 
 namespace ssp {
@@ -18,13 +19,14 @@ namespace ssp {
 __global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, const int64_t* __restrict__ adj_ptr,
                                                      const int32_t* __restrict__ adj_eid,
                                                      const int32_t* __restrict__ v2, const double* __restrict__ w,
-                                                     int32_t k, int32_t ntiles, double scale, uint64_t seed,
+                                                     int32_t col_lo, int32_t col_hi, int32_t tile_lo,
+                                                     int32_t ntiles, double scale, uint64_t seed,
                                                      double* __restrict__ Y, int64_t ldy, int tm) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t item = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < n * ntiles; item += nw) {
         const int64_t v = item / ntiles;
-        const int32_t tile = (int32_t)(item - v * ntiles);
+        const int32_t tile = tile_lo + (int32_t)(item - v * ntiles);
         double acc[8];
 #pragma unroll
         for (int t = 0; t < 8; t++) acc[t] = 0.0;
@@ -59,7 +61,10 @@ __global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, const int64_t* _
 #pragma unroll
         for (int t = 0; t < 8; t++) {
             const int64_t col = (int64_t)tile * 256 + lane + 32 * t;
-            if (col < k) Y[tm ? tile_off(n, v, col) : v * ldy + col] = acc[t];
+            if (col >= col_lo && col < col_hi) {
+                const int64_t lc = col - col_lo;  // column of the stored block
+                Y[tm ? tile_off(n, v, lc) : v * ldy + lc] = acc[t];
+            }
         }
     }
 }
@@ -68,13 +73,14 @@ __global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, const int64_t* _
 __global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, const int64_t* __restrict__ adj_ptr,
                                                      const int32_t* __restrict__ adj_eid,
                                                      const int32_t* __restrict__ v2, const double* __restrict__ w,
-                                                     int32_t k, int32_t ntiles, double scale, uint64_t seed,
+                                                     int32_t col_lo, int32_t col_hi, int32_t tile_lo,
+                                                     int32_t ntiles, double scale, uint64_t seed,
                                                      double* __restrict__ Y, int64_t ldy, int tm) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t item = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < n * ntiles; item += nw) {
         const int64_t v = item / ntiles;
-        const int32_t tile = (int32_t)(item - v * ntiles);
+        const int32_t tile = tile_lo + (int32_t)(item - v * ntiles);
         double acc[8];
 #pragma unroll
         for (int t = 0; t < 8; t++) acc[t] = 0.0;
@@ -104,24 +110,30 @@ __global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, const int64_t* _
 #pragma unroll
         for (int t = 0; t < 8; t++) {
             const int64_t col = (int64_t)tile * 256 + lane + 32 * t;
-            if (col < k) Y[tm ? tile_off(n, v, col) : v * ldy + col] = acc[t];
+            if (col >= col_lo && col < col_hi) {
+                const int64_t lc = col - col_lo;  // column of the stored block
+                Y[tm ? tile_off(n, v, lc) : v * ldy + lc] = acc[t];
+            }
         }
     }
 }
 
 void sketch_device(Context& C, const DevGraph& G, int32_t k, double scale, uint64_t seed, int uniform, double* Y,
-                   int64_t ldy, int tile_major) {
+                   int64_t ldy, int tile_major, int32_t col_lo) {
     SSP_REQUIRE(k > 0 && (tile_major || ldy >= k), SSP_ERR_INVALID, "sketch: need 0 < k <= ld");
-    const int32_t ntiles = (k + 255) / 256;
+    SSP_REQUIRE(col_lo >= 0 && (int64_t)col_lo + k <= INT32_MAX, SSP_ERR_INVALID, "sketch: bad column range");
+    const int32_t col_hi = col_lo + k;
+    const int32_t tile_lo = col_lo >> 8;
+    const int32_t ntiles = ((col_hi - 1) >> 8) - tile_lo + 1;
     const int64_t items = G.n * ntiles;
     const int threads = 256;
     const int blocks = grid_for(items * 32, threads, 148 * 16);
     if (uniform)
-        k_sketch_unif<<<blocks, threads, 0, C.stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, k, ntiles, scale, seed,
-                                                        Y, ldy, tile_major);
+        k_sketch_unif<<<blocks, threads, 0, C.stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, col_lo, col_hi,
+                                                        tile_lo, ntiles, scale, seed, Y, ldy, tile_major);
     else
-        k_sketch_sign<<<blocks, threads, 0, C.stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, k, ntiles, scale, seed,
-                                                        Y, ldy, tile_major);
+        k_sketch_sign<<<blocks, threads, 0, C.stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, col_lo, col_hi,
+                                                        tile_lo, ntiles, scale, seed, Y, ldy, tile_major);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
 }

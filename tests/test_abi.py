@@ -115,3 +115,24 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(L, "_LIB", None)
     with pytest.raises(L.SspError):
         L.lib()
+
+
+def test_server_api_without_device(ssp):
+    """The serving entry points load and fail cleanly on a machine without a GPU; the footprint estimate
+    grows with the problem."""
+    G = ssp.gen_rgg(3000, 12.0, 0.1, 10.0, 5)
+    assert abs(G.nnz / G.n - 12.0) < 2.0
+    small = ssp.request_footprint(G, ssp.SparsifierParameters.baseline(0.5))
+    tight = ssp.request_footprint(G, ssp.SparsifierParameters.baseline(0.3))
+    mixed = ssp.SparsifierParameters.baseline(0.5)
+    mixed.precision = ssp.SSP_PRECISION_MIXED
+    assert 0 < small < tight and ssp.request_footprint(G, mixed) > small
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if not has_gpu:
+        with pytest.raises(ssp.SspError) as e:
+            ssp.Server(0, slots=2)
+        assert e.value.code == -7

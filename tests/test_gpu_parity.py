@@ -115,6 +115,53 @@ def test_pcg_matches_oracle(ssp, ora, ctx, name):
     assert abs(rep["max_iters_used"] - it.max()) <= 2
 
 
+MIXED_CASES = {
+    "grid40": lambda ssp: ssp.gen_grid2d(40, 40),
+    "er5k": lambda ssp: ssp.gen_er(5000, 20.0, 0.5, 2.0, 1),
+    # weights spread over six decades: FP32 inner solves stop contracting and FP64 rounds take over
+    "grid3d_logw": lambda ssp: ssp.gen_grid3d(16, 16, 16, -3, 3, 2),
+}
+
+
+@pytest.mark.parametrize("name", list(MIXED_CASES))
+@pytest.mark.parametrize("max_degree", [0, -1])
+def test_mixed_precision_reaches_fp64_tolerance(ssp, ora, ctx, name, max_degree):
+    """SSP_PRECISION_MIXED: FP32 inner PCG inside FP64 refinement stops on the same FP64 residual test, so
+    the solution matches the FP64 oracle's to the solve tolerance (stated: diff norms within 1e-6)."""
+    G = MIXED_CASES[name](ssp)
+    (v1, v2, w), (cp, ri, va) = _oracle_graph(ora, G)
+    lap = ssp.CSC(G.n, cp, ri, va)
+    k = 21
+    Y = ora.sketch(G.n, v1, v2, w, k, 1 / math.sqrt(k), 5)
+    Zm, rm = ctx.solve_lap(lap, Y, tol=1e-9, abs_tol=0.0, max_iters=600, max_degree=max_degree, precision=1)
+    Zd, rd = ctx.solve_lap(lap, Y, tol=1e-9, abs_tol=0.0, max_iters=600, max_degree=max_degree, precision=0)
+    assert rm["not_converged"] == 0 and rm["refinements"] >= 1 and rd["refinements"] == 0
+    assert rm["max_relres"] <= 1e-9 * 1.0001 and rd["max_relres"] <= 1e-9 * 1.0001
+    # the true residual of the mixed solution, computed here in FP64
+    Lg = sp.csc_matrix((va, ri, cp), shape=(G.n, G.n))
+    b = Y - Y.mean(0)
+    rel = np.linalg.norm(b - Lg @ Zm, axis=0) / np.linalg.norm(b, axis=0)
+    assert rel.max() <= 1.01e-9
+    F = ora.Factor(G.n, cp, ri, va, 0, 4096, rd["factor_max_degree_used"])
+    Zo, it, _, rc = ora.pcg(G.n, cp, ri, va, F, Y, 1e-9, 0.0, 600)
+    assert rc == 0
+    dm, do = ora.diff_norms(v1, v2, Zm), ora.diff_norms(v1, v2, Zo)
+    live = do > 1e-12 * do.max()
+    assert np.max(np.abs(dm[live] - do[live]) / do[live]) < 1e-6
+
+
+def test_mixed_precision_sparsify_end_to_end(ssp, ctx):
+    G = ssp.gen_er(4000, 80.0, 0.5, 2.0, 2)
+    prm = ssp.SparsifierParameters.baseline(1.5, pcg_tol=1e-8)
+    H0, s0 = ctx.sparsify(G, prm)
+    prm.precision = ssp.SSP_PRECISION_MIXED
+    H1, s1 = ctx.sparsify(G, prm)
+    assert s1["pcg_refinements"] >= 1 and s0["pcg_refinements"] == 0
+    assert s1["pcg_max_relres"] <= 1e-8 * 1.0001
+    # probabilities move by ~1e-8 relative: at most a handful of coin decisions can flip
+    assert abs(s1["m_out"] - s0["m_out"]) <= 3 and 0 < s0["m_out"] < s0["m_in"]
+
+
 def test_run_solve_lap_dropin(ssp, ora, ctx):
     """ffi::run_solve_lap semantics (lib.rs:103, example.cc:668-703): FlattenedVec row-major n x k in and
     out, ||r||^2 <= 2e-7 stop, success iff relative residual < 0.01."""
@@ -271,3 +318,40 @@ def test_sparsify_dataset_mtx(ssp, tmp_path):
     assert H.num_edges() == st.final_num_edges
     Lh = H.to_scipy()
     assert np.abs(np.asarray(Lh.sum(axis=0))).max() < 1e-9
+
+
+@pytest.mark.parametrize("split", [(0, 16, 37), (0, 8, 37), (0, 37, 37)])
+def test_column_split_phases_match_single_call(ssp, ora, ctx, split):
+    """ssp_shard_leverage over two column shares + ssp_shard_finish on their summed squares equals
+    ssp_sparsify up to the order of the final sum over columns; the autotuned factor is the same."""
+    import torch
+    G = ssp.gen_er(3000, 60.0, 0.5, 2.0, 9)
+    prm = ssp.SparsifierParameters.baseline(1.5, pcg_tol=1e-10)
+    prm.jl_dim_override = 37
+    H1, st1 = ctx.sparsify(G, prm)
+    m = ctx.num_edges(G)
+    assert m == st1["m_in"]
+    a, b, k = split
+    dev = torch.device("cuda", 0)
+    sq = torch.zeros((2, m), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    sa = ctx.shard_leverage(G, prm, a, b, sq[0].data_ptr())
+    degs = [sa["factor_max_degree_used"]]
+    if b < k:
+        sb = ctx.shard_leverage(G, prm, b, k, sq[1].data_ptr())
+        degs.append(sb["factor_max_degree_used"])
+    assert all(dg == st1["factor_max_degree_used"] for dg in degs)
+    tot = (sq[0] + sq[1]).contiguous()
+    torch.cuda.synchronize()
+    H2, st2 = ctx.shard_finish(G, prm, tot.data_ptr())
+    assert st2["m_out"] == st1["m_out"] and 0 < st1["m_out"] < m
+    assert np.array_equal(H2.colptr, H1.colptr) and np.array_equal(H2.rowidx, H1.rowidx)
+    np.testing.assert_allclose(H2.values, H1.values, rtol=1e-12, atol=1e-12)
+    # the summed squares against the oracle's solve of all 37 columns with the same factor
+    v1, v2, w = ora.extract_edges(G.n, G.colptr, G.rowidx, G.values)
+    cp, ri, va = ora.laplacian(G.n, v1, v2, w)
+    Y = ora.sketch(G.n, v1, v2, w, k, prm.jl_scale(k), prm.sketch_seed)
+    F = ora.Factor(G.n, cp, ri, va, prm.factor_seed, prm.dense_threshold, st1["factor_max_degree_used"])
+    Z, _, _, rc = ora.pcg(G.n, cp, ri, va, F, Y, prm.pcg_tol, prm.pcg_abs_tol, prm.pcg_max_iters)
+    assert rc == 0
+    np.testing.assert_allclose(tot.cpu().numpy(), ora.diff_norms(v1, v2, Z) ** 2, rtol=1e-7)
