@@ -216,6 +216,16 @@ int ssp_sparsify(ssp_context* ctx, const ssp_csc* graph, const ssp_params* param
                  ssp_csc_out* out, ssp_stats* stats);
 int ssp_csc_free(ssp_csc_out* out);
 
+/* ---- streaming: sparsify again after inserting edges (Sparsifier::insert + sparsify, sparsifier.rs:357-376,
+ * 735-790) ----
+ * laplacian: the current L_H (n x n, nnz may be 0); new_edges: the edges inserted since (a symmetric CSC
+ * whose upper triangle holds them, as for ssp_sparsify).  As form_laplacian (sparsifier.rs:693-709) the two are
+ * summed; the JL sketch covers only the new edges (the reference sketches new_entries, :736-741), the solve
+ * and the sampling run over every edge of the sum.  The sum's diagonal is rebuilt from its edges (equal to
+ * the reference's L_cur + L_new up to rounding). */
+int ssp_sparsify_update(ssp_context* ctx, const ssp_csc* laplacian, const ssp_csc* new_edges, const ssp_params* params,
+                        int32_t out_mem, ssp_csc_out* out, ssp_stats* stats);
+
 /* ---- the JL columns split across ranks (one GPU each) ----
  * The k sketch columns are independent once the factor exists (every rank builds the same deterministic
  * factor; with factor_max_degree = -1 the choice is probed on the global columns 0..7 on every rank).
@@ -252,6 +262,7 @@ typedef struct {
     int32_t kind;             /* SSP_REQ_SPARSIFY */
     ssp_csc graph;            /* host CSC; copied by ssp_submit */
     ssp_params params;        /* copied by ssp_submit (output_file too) */
+    int32_t check_probes;     /* > 0: check the result inline with this many quadratic-form probes (a15) */
 } ssp_request;
 typedef struct {
     int32_t status;           /* the request's own status code */
@@ -263,6 +274,13 @@ typedef struct {
     double run_ms;            /* admitted -> done */
     double latency_ms;        /* submit -> done */
     int32_t slot;
+    /* inline check when check_probes > 0 (ssp_probe_quadratic_form with the request's epsilon and the
+     * probes seeded by its sampling_seed, and ssp_connected_components of the graph and of L_H) */
+    int32_t checked;
+    int64_t probe_upper_violations, probe_lower_violations;
+    double probe_mean_relative_error, probe_max_relative_error;
+    int64_t components_graph, components_sparsifier;
+    double check_ms;
 } ssp_result;
 typedef struct {
     int64_t submitted, completed, failed, rejected, pending;
@@ -279,6 +297,33 @@ int ssp_poll(ssp_server* server, uint64_t ticket, ssp_result* res);
 int ssp_server_info_get(ssp_server* server, ssp_server_info* info);
 /* drops pending requests, lets admitted ones finish, frees uncollected results */
 int ssp_server_destroy(ssp_server* server);
+
+/* ---- checks of a Laplacian and of a sparsifier (a15) ----
+ * ssp_check_laplacian      <- Sparsifier::check_diagonal        src/sparsifier.rs:806-817
+ *   counts columns whose sum exceeds tol in magnitude, the largest |column sum|, and entries whose mirror
+ *   (j, i) is missing or differs (exact symmetry, as sprs::is_symmetric)
+ * ssp_quadratic_forms      <- Sparsifier::compute_quadratic_form src/sparsifier.rs:820-826
+ *   out[j] = x_j^T L x_j for the p columns of X (column-major n x p)
+ * ssp_probe_vectors        the probe vectors: X[i + n j] = 2u - 1, u uniform from Philox((i, j)) (the reference
+ *                          draws uniform(-1, 1) from thread_rng, tests.rs:50-59)
+ * ssp_probe_quadratic_form <- probe_quadratic_form              src/experiments.rs:88-122
+ * ssp_connected_components <- petgraph connected_components in verify_ccs, src/experiments.rs:58-64
+ *   over the off-diagonal nonzeros; labels (optional) = the smallest vertex of each component */
+typedef struct {
+    int64_t upper_bound_violations;  /* x^T L_H x >= (1 + eps) x^T L_G x */
+    int64_t lower_bound_violations;  /* x^T L_H x <= (1 - eps) x^T L_G x */
+    double mean_relative_error;      /* of |qH - qG| / |qG| over the probes */
+    double std_dev_relative_error;   /* population standard deviation */
+    double max_relative_error;
+    int32_t probes;
+} ssp_probe_result;
+int ssp_check_laplacian(ssp_context* ctx, const ssp_csc* lap, double tol, int64_t* bad_columns,
+                        double* max_abs_colsum, int64_t* asymmetric_entries);
+int ssp_probe_vectors(ssp_context* ctx, int64_t n, int32_t p, uint64_t seed, int32_t mem, double* X);
+int ssp_quadratic_forms(ssp_context* ctx, const ssp_csc* lap, const double* X, int32_t p, int32_t mem, double* out);
+int ssp_probe_quadratic_form(ssp_context* ctx, const ssp_csc* lap_g, const ssp_csc* lap_h, double epsilon,
+                             int32_t probes, uint64_t seed, ssp_probe_result* res);
+int ssp_connected_components(ssp_context* ctx, const ssp_csc* m, int32_t mem, int32_t* labels, int64_t* count);
 
 /* ---- .mtx path (sparsify_dataset) ---- */
 int ssp_sparsify_mtx(const char* input_file, const char* output_file, const ssp_params* params, ssp_stats* stats);

@@ -1,5 +1,6 @@
 """ctypes bindings of include/specspars.h and the reference-shaped Python API on top of them."""
 import ctypes
+import math
 import os
 import re
 
@@ -94,13 +95,17 @@ class _ServerOpts(ctypes.Structure):
 
 
 class _Request(ctypes.Structure):
-    _fields_ = [("kind", ctypes.c_int32), ("graph", _Csc), ("params", _Params)]
+    _fields_ = [("kind", ctypes.c_int32), ("graph", _Csc), ("params", _Params), ("check_probes", ctypes.c_int32)]
 
 
 class _Result(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int32), ("error", ctypes.c_char * 256), ("out", _CscOut), ("stats", _Stats),
                 ("est_bytes", ctypes.c_int64), ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
-                ("latency_ms", ctypes.c_double), ("slot", ctypes.c_int32)]
+                ("latency_ms", ctypes.c_double), ("slot", ctypes.c_int32), ("checked", ctypes.c_int32),
+                ("probe_upper_violations", ctypes.c_int64), ("probe_lower_violations", ctypes.c_int64),
+                ("probe_mean_relative_error", ctypes.c_double), ("probe_max_relative_error", ctypes.c_double),
+                ("components_graph", ctypes.c_int64), ("components_sparsifier", ctypes.c_int64),
+                ("check_ms", ctypes.c_double)]
 
 
 class _ServerInfo(ctypes.Structure):
@@ -108,6 +113,12 @@ class _ServerInfo(ctypes.Structure):
                 ("rejected", ctypes.c_int64), ("pending", ctypes.c_int64), ("inflight", ctypes.c_int32),
                 ("peak_inflight", ctypes.c_int32), ("slots", ctypes.c_int32),
                 ("peak_inflight_bytes", ctypes.c_int64), ("budget_bytes", ctypes.c_int64)]
+
+
+class _ProbeResult(ctypes.Structure):
+    _fields_ = [("upper_bound_violations", ctypes.c_int64), ("lower_bound_violations", ctypes.c_int64),
+                ("mean_relative_error", ctypes.c_double), ("std_dev_relative_error", ctypes.c_double),
+                ("max_relative_error", ctypes.c_double), ("probes", ctypes.c_int32)]
 
 
 _LIB = None
@@ -152,6 +163,13 @@ def lib():
             "ssp_gen_grid3d": ([I64, I64, I64, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_er": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_rgg": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
+            "ssp_check_laplacian": ([P, ctypes.POINTER(_Csc), DBL, ctypes.POINTER(I64), ctypes.POINTER(DBL),
+                                     ctypes.POINTER(I64)], ctypes.c_int),
+            "ssp_probe_vectors": ([P, I64, I32, U64, I32, P], ctypes.c_int),
+            "ssp_quadratic_forms": ([P, ctypes.POINTER(_Csc), P, I32, I32, P], ctypes.c_int),
+            "ssp_probe_quadratic_form": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(_Csc), DBL, I32, U64,
+                                          ctypes.POINTER(_ProbeResult)], ctypes.c_int),
+            "ssp_connected_components": ([P, ctypes.POINTER(_Csc), I32, P, ctypes.POINTER(I64)], ctypes.c_int),
             "ssp_context_release_workspace": ([P], ctypes.c_int),
             "ssp_server_opts_default": ([ctypes.POINTER(_ServerOpts)], None),
             "ssp_request_footprint": ([ctypes.POINTER(_Csc), ctypes.POINTER(_Params)], I64),
@@ -175,6 +193,8 @@ def lib():
             "ssp_stage_leverage_probs_static": ([P, I64, I64, P, P, P, I32, P, DBL, DBL, P], ctypes.c_int),
             "ssp_shard_leverage": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(_Params), I32, I32, P,
                                     ctypes.POINTER(I64), ctypes.POINTER(_Stats)], ctypes.c_int),
+            "ssp_sparsify_update": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(_Csc), ctypes.POINTER(_Params), I32,
+                                     ctypes.POINTER(_CscOut), ctypes.POINTER(_Stats)], ctypes.c_int),
             "ssp_shard_finish": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(_Params), P, I32, ctypes.POINTER(_CscOut),
                                   ctypes.POINTER(_Stats)], ctypes.c_int),
         }
@@ -435,6 +455,63 @@ class Context:
                                   ctypes.byref(out), ctypes.byref(st)))
         return (out.nnz, out.colptr, out.rowidx, out.values), _stats_dict(st)
 
+    # ---- checks (a15): check_diagonal, compute_quadratic_form, probe_quadratic_form, verify_ccs
+    def check_laplacian(self, lap, tol=1e-10):
+        """Sparsifier::check_diagonal (sparsifier.rs:806-817) as counts instead of asserts."""
+        bad, mx, asym = I64(0), DBL(0), I64(0)
+        g = lap._struct()
+        _check(lib().ssp_check_laplacian(self._h, ctypes.byref(g), tol, ctypes.byref(bad), ctypes.byref(mx),
+                                         ctypes.byref(asym)))
+        return {"bad_columns": bad.value, "max_abs_colsum": mx.value, "asymmetric_entries": asym.value,
+                "ok": bad.value == 0 and asym.value == 0}
+
+    def probe_vectors(self, n, p, seed=0):
+        X = np.zeros((p, n), np.float64)  # column-major n x p = p contiguous vectors
+        _check(lib().ssp_probe_vectors(self._h, n, p, seed, SSP_MEM_HOST, _ptr(X)))
+        return X.T
+
+    def quadratic_forms(self, lap, X):
+        """x_j^T L x_j for the columns of X (n x p)."""
+        X = np.asarray(X, np.float64)
+        if X.ndim == 1:
+            X = X[:, None]
+        Xc = np.ascontiguousarray(X.T)
+        out = np.zeros(X.shape[1], np.float64)
+        g = lap._struct()
+        _check(lib().ssp_quadratic_forms(self._h, ctypes.byref(g), _ptr(Xc), X.shape[1], SSP_MEM_HOST, _ptr(out)))
+        return out
+
+    def probe_quadratic_form(self, lap_g, lap_h, epsilon, probes=100, seed=0):
+        """probe_quadratic_form (experiments.rs:88-122) with Philox probes."""
+        r = _ProbeResult()
+        g, h = lap_g._struct(), lap_h._struct()
+        _check(lib().ssp_probe_quadratic_form(self._h, ctypes.byref(g), ctypes.byref(h), epsilon, probes, seed,
+                                              ctypes.byref(r)))
+        return {f: getattr(r, f) for f, _ in _ProbeResult._fields_}
+
+    def connected_components(self, m):
+        """(number of components, label = smallest vertex of the component) over off-diagonal nonzeros."""
+        labels = np.zeros(m.n, np.int32)
+        cnt = I64(0)
+        g = m._struct()
+        _check(lib().ssp_connected_components(self._h, ctypes.byref(g), SSP_MEM_HOST, _ptr(labels),
+                                              ctypes.byref(cnt)))
+        return cnt.value, labels
+
+    def verify_ccs(self, graph, sparsifier):
+        """verify_ccs (experiments.rs:58-64): the sparsifier keeps the number of connected components."""
+        return self.connected_components(graph)[0] == self.connected_components(sparsifier)[0]
+
+    def sparsify_update(self, laplacian, new_edges, params):
+        """Sparsify again after inserting edges: current L_H + the new edges (sketched alone), as
+        Sparsifier::insert + sparsify (sparsifier.rs:357-376,735-790).  Returns (L_H, stats)."""
+        a, b = laplacian._struct(), new_edges._struct()
+        out = _CscOut()
+        st = _Stats()
+        _check(lib().ssp_sparsify_update(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(params._s),
+                                         SSP_MEM_HOST, ctypes.byref(out), ctypes.byref(st)))
+        return _take_out(out), _stats_dict(st)
+
     def num_edges(self, graph):
         """Edges of a host graph as the sparsifier counts them (upper triangle, value != 0)."""
         m = I64(0)
@@ -505,17 +582,63 @@ def run_solve_lap(shared_jl_cols, col_ptrs, row_indices, values, solver_output_f
 
 
 class Sparsifier:
-    """Holds the current Laplacian of a graph; sparsify() runs the GPU path (sparsifier.rs:722-770)."""
+    """Sparsifier (sparsifier.rs:244-297, 357-376, 735-790): a current Laplacian plus the edges inserted since
+    the last sparsification.  Built from a graph (all its edges pending) or from a vertex count (empty).
+
+    insert() skips zero values and checks the reference's streaming trigger: with params.streaming set, it
+    sparsifies when the current Laplacian has more than threshold = n * round(beta) * row_constant edges
+    (sparsifier.rs:266,370-374; as there, the count is of the current Laplacian, not of the pending edges).
+    sparsify() adds the pending edges and runs the GPU path; the JL sketch covers the pending edges only."""
 
     def __init__(self, graph, parameters, ctx=None):
-        self.graph = graph
         self.params = parameters
         self.ctx = ctx or _ctx()
-        self.current_laplacian = None
         self.stats = None
+        if isinstance(graph, (int, np.integer)):
+            self.num_nodes = int(graph)
+            self._rows, self._cols, self._vals = [], [], []
+        else:
+            self.num_nodes = graph.n
+            A = graph.to_scipy().tocoo()
+            up = A.row < A.col
+            self._rows, self._cols, self._vals = list(A.row[up]), list(A.col[up]), list(A.data[up])
+        beta = parameters.beta(self.num_nodes)
+        # f64::round rounds half away from zero (sparsifier.rs:266)
+        self.threshold = self.num_nodes * int(math.floor(beta + 0.5)) * parameters.row_constant
+        self.current_laplacian = None
+
+    @property
+    def graph(self):
+        return self._pending_csc()
+
+    def insert(self, v1, v2, value):
+        if not (0 <= v1 < self.num_nodes and 0 <= v2 < self.num_nodes):
+            raise SspError(-1, "vertex id out of range")
+        if value != 0.0 and v1 != v2:
+            a, b = (v1, v2) if v1 < v2 else (v2, v1)
+            self._rows.append(a)
+            self._cols.append(b)
+            self._vals.append(float(value))
+        if self.params.streaming and (self.num_edges() or 0) > self.threshold:
+            self.sparsify()
+
+    def _pending_csc(self):
+        import scipy.sparse as sp
+        n = self.num_nodes
+        U = sp.coo_matrix((np.asarray(self._vals, np.float64), (np.asarray(self._rows, np.int64),
+                                                                 np.asarray(self._cols, np.int64))), shape=(n, n))
+        A = (U + U.T).tocsc()  # duplicates summed, as Triplet::to_csc
+        A.sum_duplicates()
+        A.sort_indices()
+        return CSC.from_scipy(A)
 
     def sparsify(self):
-        self.current_laplacian, st = self.ctx.sparsify(self.graph, self.params)
+        new = self._pending_csc()
+        if self.current_laplacian is None:
+            self.current_laplacian, st = self.ctx.sparsify(new, self.params)
+        else:
+            self.current_laplacian, st = self.ctx.sparsify_update(self.current_laplacian, new, self.params)
+        self._rows, self._cols, self._vals = [], [], []
         self.stats = SparsificationStats(st)
         return self.stats
 
@@ -650,8 +773,9 @@ class Server:
         _check(lib().ssp_server_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h
 
-    def submit(self, graph, params):
-        req = _Request(0, graph._struct(), params._s)
+    def submit(self, graph, params, check_probes=0):
+        """Queue one sparsification; check_probes > 0 also checks the result on the device (a15)."""
+        req = _Request(0, graph._struct(), params._s, check_probes)
         t = U64(0)
         _check(lib().ssp_submit(self._h, ctypes.byref(req), ctypes.byref(t)))
         return t.value
@@ -659,6 +783,15 @@ class Server:
     def _collect(self, res):
         info = {"queue_ms": res.queue_ms, "run_ms": res.run_ms, "latency_ms": res.latency_ms, "slot": res.slot,
                 "est_bytes": res.est_bytes}
+        if res.checked:
+            info["check"] = {"upper_bound_violations": res.probe_upper_violations,
+                             "lower_bound_violations": res.probe_lower_violations,
+                             "mean_relative_error": res.probe_mean_relative_error,
+                             "max_relative_error": res.probe_max_relative_error,
+                             "components_graph": res.components_graph,
+                             "components_sparsifier": res.components_sparsifier,
+                             "ccs_equal": res.components_graph == res.components_sparsifier,
+                             "check_ms": res.check_ms}
         if res.status != SSP_OK:
             raise SspError(res.status, res.error.decode(errors="replace"))
         return _take_out(res.out), _stats_dict(res.stats), info

@@ -169,10 +169,13 @@ __global__ void k_count_diag(int64_t n, const int64_t* ptr, const int32_t* idx, 
 // Splitting the JL columns across ranks (multi-GPU): phase 1 solves the global columns
 // [col_lo, col_hi) and leaves the per-edge sums of squared differences in sq_out; the caller sums them
 // over ranks; phase 2 takes the summed squares (sq_in) and runs probabilities, coins and L_H.
+// A streaming update (ssp_sparsify_update) instead sketches only the edges inserted since the last
+// sparsification (sketch_graph) while solving and sampling over the whole current graph.
 struct ShardArgs {
     int32_t col_lo = 0, col_hi = 0;
     double* sq_out = nullptr;
     const double* sq_in = nullptr;
+    const DevGraph* sketch_graph = nullptr;
 };
 
 static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* prm, int32_t out_mem, ssp_csc_out* out,
@@ -191,7 +194,8 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     const double scale = jl_scale(prm, k);
     const bool finish_only = sh && sh->sq_in;
     int32_t col_lo = 0, kl = k;  // the global columns solved here
-    if (sh && !finish_only) {
+    const DevGraph& SG = (sh && sh->sketch_graph) ? *sh->sketch_graph : G;
+    if (sh && sh->sq_out) {
         SSP_REQUIRE(sh->col_lo >= 0 && sh->col_lo < sh->col_hi && sh->col_hi <= k, SSP_ERR_INVALID,
                     "shard column range must satisfy 0 <= begin < end <= k");
         col_lo = sh->col_lo;
@@ -201,7 +205,7 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     double* Y = nullptr;
     if (!finish_only) {
         Y = C.ws.get_t<double>("sp_Y", (size_t)n * ld);
-        sketch_device(C, G, kl, scale, prm->sketch_seed, prm->sketch_uniform, Y, ld, 1, col_lo);
+        sketch_device(C, SG, kl, scale, prm->sketch_seed, prm->sketch_uniform, Y, ld, 1, col_lo);
     }
     T.mark();  // 2
     DevFactor F;
@@ -225,7 +229,7 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
         const int32_t kp = std::min<int32_t>(k, SSP_TILE);
         if (col_lo != 0 || kl < kp) {
             double* Yp = C.ws.get_t<double>("sp_Yprobe", (size_t)n * SSP_TILE);
-            sketch_device(C, G, kp, scale, prm->sketch_seed, prm->sketch_uniform, Yp, SSP_TILE, 1, 0);
+            sketch_device(C, SG, kp, scale, prm->sketch_seed, prm->sketch_uniform, Yp, SSP_TILE, 1, 0);
             probe = Yp;
         }
         deg_used = autotune_factor(C, n, G.lap_ptr, G.lap_idx, G.lap_val, 2 * G.m, probe, kp, fo, po, F, &ms_tune);
@@ -629,6 +633,35 @@ int ssp_shard_leverage(ssp_context* c, const ssp_csc* graph, const ssp_params* p
     });
 }
 
+int ssp_sparsify_update(ssp_context* c, const ssp_csc* laplacian, const ssp_csc* new_edges, const ssp_params* params,
+                        int32_t out_mem, ssp_csc_out* out, ssp_stats* stats) {
+    return guarded([&] {
+        SSP_REQUIRE(c && laplacian && new_edges, SSP_ERR_INVALID, "bad arguments");
+        SSP_REQUIRE(laplacian->n == new_edges->n, SSP_ERR_INVALID, "the Laplacian and the new edges differ in size");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        DevCsc L = to_device(C, laplacian, "ul");
+        DevCsc B = to_device(C, new_edges, "ub");
+        DevGraph Gn;
+        build_graph_from_csc(C, B.n, B.colptr, B.rowidx, B.val, B.nnz, Gn, "gn");
+        int64_t* mp;
+        int32_t* mi;
+        double* mv;
+        const int64_t mnnz =
+            laplacian_plus_graph_device(C, L.n, L.colptr, L.rowidx, L.val, B.colptr, B.rowidx, B.val, &mp, &mi, &mv);
+        ssp_csc merged;
+        merged.n = L.n;
+        merged.nnz = mnnz;
+        merged.colptr = mp;
+        merged.rowidx = mi;
+        merged.values = mv;
+        merged.mem = SSP_MEM_DEVICE;
+        ShardArgs sh;
+        sh.sketch_graph = &Gn;
+        sparsify_impl(C, &merged, params, out_mem, out, stats, &sh);
+    });
+}
+
 int ssp_shard_finish(ssp_context* c, const ssp_csc* graph, const ssp_params* params, const double* sq_total,
                      int32_t out_mem, ssp_csc_out* out, ssp_stats* stats) {
     return guarded([&] {
@@ -636,6 +669,104 @@ int ssp_shard_finish(ssp_context* c, const ssp_csc* graph, const ssp_params* par
         ShardArgs sh;
         sh.sq_in = sq_total;
         sparsify_impl(c->ctx, graph, params, out_mem, out, stats, &sh);
+    });
+}
+
+// ---------------------------------------------------------------- a15: checks
+int ssp_check_laplacian(ssp_context* c, const ssp_csc* lap, double tol, int64_t* bad_columns,
+                        double* max_abs_colsum, int64_t* asymmetric_entries) {
+    return guarded([&] {
+        SSP_REQUIRE(c && bad_columns && max_abs_colsum && asymmetric_entries, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        DevCsc L = to_device(C, lap, "qc");
+        laplacian_check_device(C, L.n, L.colptr, L.rowidx, L.val, tol, bad_columns, max_abs_colsum,
+                               asymmetric_entries);
+    });
+}
+
+int ssp_probe_vectors(ssp_context* c, int64_t n, int32_t p, uint64_t seed, int32_t mem, double* X) {
+    return guarded([&] {
+        SSP_REQUIRE(c && X && n > 0 && p > 0, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        double* d = mem == SSP_MEM_DEVICE ? X : C.ws.get_t<double>("q_X", (size_t)n * p);
+        probe_vectors_device(C, n, p, seed, d);
+        if (mem == SSP_MEM_HOST)
+            SSP_CUDA(cudaMemcpyAsync(X, d, sizeof(double) * n * p, cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int ssp_quadratic_forms(ssp_context* c, const ssp_csc* lap, const double* X, int32_t p, int32_t mem, double* out) {
+    return guarded([&] {
+        SSP_REQUIRE(c && X && out && p > 0, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        DevCsc L = to_device(C, lap, "qf");
+        const double* dX = stage_in(C, X, L.n * (int64_t)p, mem, "qf_X");
+        double* dout = mem == SSP_MEM_DEVICE ? out : C.ws.get_t<double>("qf_out", p);
+        quadratic_forms_device(C, L.n, L.colptr, L.rowidx, L.val, dX, p, dout);
+        if (mem == SSP_MEM_HOST)
+            SSP_CUDA(cudaMemcpyAsync(out, dout, sizeof(double) * p, cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int ssp_probe_quadratic_form(ssp_context* c, const ssp_csc* lap_g, const ssp_csc* lap_h, double epsilon,
+                             int32_t probes, uint64_t seed, ssp_probe_result* res) {
+    return guarded([&] {
+        SSP_REQUIRE(c && lap_g && lap_h && res && probes > 0, SSP_ERR_INVALID, "bad arguments");
+        SSP_REQUIRE(lap_g->n == lap_h->n, SSP_ERR_INVALID, "L_G and L_H must have the same size");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        const int64_t n = lap_g->n;
+        double* X = C.ws.get_t<double>("q_X", (size_t)n * probes);
+        double* q = C.ws.get_t<double>("q_forms", 2 * (size_t)probes);
+        probe_vectors_device(C, n, probes, seed, X);
+        DevCsc G = to_device(C, lap_g, "qg");
+        quadratic_forms_device(C, n, G.colptr, G.rowidx, G.val, X, probes, q);
+        DevCsc H = to_device(C, lap_h, "qh");
+        quadratic_forms_device(C, n, H.colptr, H.rowidx, H.val, X, probes, q + probes);
+        std::vector<double> h(2 * (size_t)probes);
+        SSP_CUDA(cudaMemcpyAsync(h.data(), q, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+        // experiments.rs:95-121: non-strict bound tests, relative error against the graph's form
+        memset(res, 0, sizeof(*res));
+        res->probes = probes;
+        std::vector<double> err(probes);
+        for (int32_t j = 0; j < probes; j++) {
+            const double og = h[j], sh = h[probes + j];
+            if (sh >= og * (1.0 + epsilon)) res->upper_bound_violations++;
+            if (sh <= og * (1.0 - epsilon)) res->lower_bound_violations++;
+            err[j] = std::fabs(sh - og) / std::fabs(og);
+        }
+        double mean = 0.0, mx = err[0];
+        for (double e : err) {
+            mean += e;
+            mx = std::max(mx, e);
+        }
+        mean /= probes;
+        double var = 0.0;
+        for (double e : err) var += (e - mean) * (e - mean);
+        res->mean_relative_error = mean;
+        res->std_dev_relative_error = std::sqrt(var / probes);
+        res->max_relative_error = mx;
+    });
+}
+
+int ssp_connected_components(ssp_context* c, const ssp_csc* m, int32_t mem, int32_t* labels, int64_t* count) {
+    return guarded([&] {
+        SSP_REQUIRE(c && count, SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        DevCsc M = to_device(C, m, "cc");
+        int32_t* d = (labels && mem == SSP_MEM_DEVICE) ? labels : C.ws.get_t<int32_t>("cc_labels", M.n);
+        *count = components_device(C, M.n, M.colptr, M.rowidx, M.val, d);
+        if (labels && mem == SSP_MEM_HOST) {
+            SSP_CUDA(cudaMemcpyAsync(labels, d, sizeof(int32_t) * M.n, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaStreamSynchronize(C.stream));
+        }
     });
 }
 

@@ -171,14 +171,14 @@ static void check_err(Context& C, int32_t* d_err, const char* what) {
                     std::string(what) + ": edge weights must be finite and positive (upper-triangle entries)");
 }
 
-void build_graph_from_edges(Context& C, DevGraph& G) {
+void build_graph_from_edges(Context& C, DevGraph& G, const std::string& tag) {
     const int64_t n = G.n, m = G.m;
     Workspace& W = C.ws;
-    int32_t* lowcnt = W.get_t<int32_t>("g_lowcnt", n + 1);
-    int32_t* highcnt = W.get_t<int32_t>("g_highcnt", n + 1);
-    int32_t* deg = W.get_t<int32_t>("g_deg", n + 1);
-    int32_t* cursor = W.get_t<int32_t>("g_cursor", n + 1);
-    int32_t* err = W.get_t<int32_t>("g_err", 2);
+    int32_t* lowcnt = W.get_t<int32_t>(tag + "_lowcnt", n + 1);
+    int32_t* highcnt = W.get_t<int32_t>(tag + "_highcnt", n + 1);
+    int32_t* deg = W.get_t<int32_t>(tag + "_deg", n + 1);
+    int32_t* cursor = W.get_t<int32_t>(tag + "_cursor", n + 1);
+    int32_t* err = W.get_t<int32_t>(tag + "_err", 2);
     SSP_CUDA(cudaMemsetAsync(lowcnt, 0, sizeof(int32_t) * (n + 1), C.stream));
     SSP_CUDA(cudaMemsetAsync(highcnt, 0, sizeof(int32_t) * (n + 1), C.stream));
     SSP_CUDA(cudaMemsetAsync(cursor, 0, sizeof(int32_t) * (n + 1), C.stream));
@@ -194,20 +194,20 @@ void build_graph_from_edges(Context& C, DevGraph& G) {
     SSP_CUDA(cudaStreamSynchronize(C.stream));
     G.max_deg = hmax;
 
-    int64_t* eoff = W.get_t<int64_t>("g_eoff", n + 1);
+    int64_t* eoff = W.get_t<int64_t>(tag + "_eoff", n + 1);
     exclusive_scan_i32_to_i64(C, lowcnt, eoff, n, nullptr);
-    G.adj_ptr = W.get_t<int64_t>("g_adj_ptr", n + 1);
+    G.adj_ptr = W.get_t<int64_t>(tag + "_adj_ptr", n + 1);
     SSP_CUDA(cudaMemsetAsync(deg + n, 0, sizeof(int32_t), C.stream));
     exclusive_scan_i32_to_i64(C, deg, G.adj_ptr, n + 1, nullptr);  // deg[n] == 0 -> adj_ptr[n] = 2m
-    G.adj_nbr = W.get_t<int32_t>("g_adj_nbr", 2 * m + 1);
-    G.adj_eid = W.get_t<int32_t>("g_adj_eid", 2 * m + 1);
+    G.adj_nbr = W.get_t<int32_t>(tag + "_adj_nbr", 2 * m + 1);
+    G.adj_eid = W.get_t<int32_t>(tag + "_adj_eid", 2 * m + 1);
     k_adj_place<<<grid_for(m, 256), 256, 0, C.stream>>>(m, G.v1, G.v2, eoff, G.adj_ptr, lowcnt, cursor, G.adj_nbr,
                                                          G.adj_eid);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
     // upper parts: sort edge ids (edge id order == neighbour order)
-    int64_t* seg_start = W.get_t<int64_t>("g_seg_start", n + 1);
-    int32_t* seg_len = W.get_t<int32_t>("g_seg_len", n + 1);
+    int64_t* seg_start = W.get_t<int64_t>(tag + "_seg_start", n + 1);
+    int32_t* seg_len = W.get_t<int32_t>(tag + "_seg_len", n + 1);
     k_upper_seg<<<grid_for(n, 256), 256, 0, C.stream>>>(n, G.adj_ptr, lowcnt, highcnt, seg_start, seg_len);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
@@ -217,16 +217,16 @@ void build_graph_from_edges(Context& C, DevGraph& G) {
     C.kernels_launched++;
 
     // Laplacian
-    int32_t* lapcnt = W.get_t<int32_t>("g_lapcnt", n + 1);
+    int32_t* lapcnt = W.get_t<int32_t>(tag + "_lapcnt", n + 1);
     k_lap_count<<<grid_for(n, 256), 256, 0, C.stream>>>(n, deg, lapcnt);
     SSP_CHECK_LAUNCH();
     SSP_CUDA(cudaMemsetAsync(lapcnt + n, 0, sizeof(int32_t), C.stream));
-    G.lap_ptr = W.get_t<int64_t>("g_lap_ptr", n + 1);
-    int64_t* d_tot = W.get_t<int64_t>("g_lap_tot", 1);
+    G.lap_ptr = W.get_t<int64_t>(tag + "_lap_ptr", n + 1);
+    int64_t* d_tot = W.get_t<int64_t>(tag + "_lap_tot", 1);
     exclusive_scan_i32_to_i64(C, lapcnt, G.lap_ptr, n + 1, d_tot);
     G.lap_nnz = read_i64(C, d_tot);
-    G.lap_idx = W.get_t<int32_t>("g_lap_idx", G.lap_nnz + 1);
-    G.lap_val = W.get_t<double>("g_lap_val", G.lap_nnz + 1);
+    G.lap_idx = W.get_t<int32_t>(tag + "_lap_idx", G.lap_nnz + 1);
+    G.lap_val = W.get_t<double>(tag + "_lap_val", G.lap_nnz + 1);
     k_lap_fill<<<grid_for(n, 128), 128, 0, C.stream>>>(n, G.adj_ptr, G.adj_nbr, G.adj_eid, G.w, G.lap_ptr,
                                                        G.lap_idx, G.lap_val);
     SSP_CHECK_LAUNCH();
@@ -234,12 +234,12 @@ void build_graph_from_edges(Context& C, DevGraph& G) {
 }
 
 void build_graph_from_csc(Context& C, int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,
-                          int64_t nnz, DevGraph& G) {
+                          int64_t nnz, DevGraph& G, const std::string& tag) {
     (void)nnz;
     Workspace& W = C.ws;
     G.n = n;
-    int32_t* upcnt = W.get_t<int32_t>("g_upcnt", n + 1);
-    int32_t* err = W.get_t<int32_t>("g_err", 2);
+    int32_t* upcnt = W.get_t<int32_t>(tag + "_upcnt", n + 1);
+    int32_t* err = W.get_t<int32_t>(tag + "_err", 2);
     SSP_CUDA(cudaMemsetAsync(err, 0, sizeof(int32_t) * 2, C.stream));
     int threads = 256;
     int blocks = grid_for(n * 32, threads, 148 * 64);
@@ -247,18 +247,127 @@ void build_graph_from_csc(Context& C, int64_t n, const int64_t* colptr, const in
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
     check_err(C, err, "input matrix");
-    int64_t* eoff = W.get_t<int64_t>("g_eoff_in", n + 1);
-    int64_t* d_m = W.get_t<int64_t>("g_m", 1);
+    int64_t* eoff = W.get_t<int64_t>(tag + "_eoff_in", n + 1);
+    int64_t* d_m = W.get_t<int64_t>(tag + "_m", 1);
     exclusive_scan_i32_to_i64(C, upcnt, eoff, n, d_m);
     G.m = read_i64(C, d_m);
     SSP_REQUIRE(G.m < (int64_t)INT32_MAX, SSP_ERR_INVALID, "more than 2^31-1 edges");
-    G.v1 = W.get_t<int32_t>("g_v1", G.m + 1);
-    G.v2 = W.get_t<int32_t>("g_v2", G.m + 1);
-    G.w = W.get_t<double>("g_w", G.m + 1);
+    G.v1 = W.get_t<int32_t>(tag + "_v1", G.m + 1);
+    G.v2 = W.get_t<int32_t>(tag + "_v2", G.m + 1);
+    G.w = W.get_t<double>(tag + "_w", G.m + 1);
     k_col_emit<<<blocks, threads, 0, C.stream>>>(n, colptr, rowidx, val, eoff, G.v1, G.v2, G.w);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
-    build_graph_from_edges(C, G);
+    build_graph_from_edges(C, G, tag);
+}
+
+
+// ---------------------------------------------------------------- streaming update
+// Sparsifier::form_laplacian (sparsifier.rs:693-709) adds the Laplacian of the edges inserted since the last
+// sparsification to the current one.  Here the sum is formed as a graph: the current Laplacian's
+// off-diagonal nonzeros become edges of weight -value, the new batch's entries are added column by column
+// (duplicates summed current + new, which is exactly -(L_cur + L_new) off the diagonal), and the Laplacian is
+// rebuilt from that graph, its diagonal summed in edge order.
+namespace {
+__global__ void k_lap_graph_count(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                  const double* __restrict__ val, int32_t* __restrict__ cnt) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        int32_t c = 0;
+        for (int64_t t = ptr[j]; t < ptr[j + 1]; t++) c += (idx[t] != (int32_t)j && val[t] != 0.0);
+        cnt[j] = c;
+    }
+}
+__global__ void k_lap_graph_fill(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                 const double* __restrict__ val, const int64_t* __restrict__ optr,
+                                 int32_t* __restrict__ oidx, double* __restrict__ oval) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        int64_t o = optr[j];
+        for (int64_t t = ptr[j]; t < ptr[j + 1]; t++)
+            if (idx[t] != (int32_t)j && val[t] != 0.0) {
+                oidx[o] = idx[t];
+                oval[o] = -val[t];
+                o++;
+            }
+    }
+}
+// C = A + B column by column; rows are sorted within each column of A and B
+__global__ void k_csc_add_count(int64_t n, const int64_t* __restrict__ ap, const int32_t* __restrict__ ai,
+                                const int64_t* __restrict__ bp, const int32_t* __restrict__ bi,
+                                int32_t* __restrict__ cnt) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        int64_t x = ap[j], y = bp[j];
+        const int64_t xe = ap[j + 1], ye = bp[j + 1];
+        int32_t c = 0;
+        while (x < xe || y < ye) {
+            if (y >= ye || (x < xe && ai[x] < bi[y])) x++;
+            else if (x >= xe || bi[y] < ai[x]) y++;
+            else {
+                x++;
+                y++;
+            }
+            c++;
+        }
+        cnt[j] = c;
+    }
+}
+__global__ void k_csc_add_fill(int64_t n, const int64_t* __restrict__ ap, const int32_t* __restrict__ ai,
+                               const double* __restrict__ av, const int64_t* __restrict__ bp,
+                               const int32_t* __restrict__ bi, const double* __restrict__ bv,
+                               const int64_t* __restrict__ cp, int32_t* __restrict__ ci, double* __restrict__ cv) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        int64_t x = ap[j], y = bp[j], o = cp[j];
+        const int64_t xe = ap[j + 1], ye = bp[j + 1];
+        while (x < xe || y < ye) {
+            if (y >= ye || (x < xe && ai[x] < bi[y])) {
+                ci[o] = ai[x];
+                cv[o] = av[x];
+                x++;
+            } else if (x >= xe || bi[y] < ai[x]) {
+                ci[o] = bi[y];
+                cv[o] = bv[y];
+                y++;
+            } else {
+                ci[o] = ai[x];
+                cv[o] = __dadd_rn(av[x], bv[y]);
+                x++;
+                y++;
+            }
+            o++;
+        }
+    }
+}
+}  // namespace
+
+int64_t laplacian_plus_graph_device(Context& C, int64_t n, const int64_t* lptr, const int32_t* lidx,
+                                    const double* lval, const int64_t* bptr, const int32_t* bidx, const double* bval,
+                                    int64_t** mptr, int32_t** midx, double** mval) {
+    Workspace& W = C.ws;
+    int32_t* cnt = W.get_t<int32_t>("u_cnt", n + 1);
+    int64_t* gptr = W.get_t<int64_t>("u_gptr", n + 1);
+    int64_t* tot = W.get_t<int64_t>("u_tot", 1);
+    k_lap_graph_count<<<grid_for(n, 256), 256, 0, C.stream>>>(n, lptr, lidx, lval, cnt);
+    SSP_CHECK_LAUNCH();
+    SSP_CUDA(cudaMemsetAsync(cnt + n, 0, sizeof(int32_t), C.stream));
+    exclusive_scan_i32_to_i64(C, cnt, gptr, n + 1, tot);
+    const int64_t gnnz = read_i64(C, tot);
+    int32_t* gidx = W.get_t<int32_t>("u_gidx", gnnz + 1);
+    double* gval = W.get_t<double>("u_gval", gnnz + 1);
+    k_lap_graph_fill<<<grid_for(n, 256), 256, 0, C.stream>>>(n, lptr, lidx, lval, gptr, gidx, gval);
+    k_csc_add_count<<<grid_for(n, 256), 256, 0, C.stream>>>(n, gptr, gidx, bptr, bidx, cnt);
+    SSP_CHECK_LAUNCH();
+    int64_t* cptr = W.get_t<int64_t>("u_mptr", n + 1);
+    SSP_CUDA(cudaMemsetAsync(cnt + n, 0, sizeof(int32_t), C.stream));
+    exclusive_scan_i32_to_i64(C, cnt, cptr, n + 1, tot);
+    const int64_t cnnz = read_i64(C, tot);
+    int32_t* cidx = W.get_t<int32_t>("u_midx", cnnz + 1);
+    double* cval = W.get_t<double>("u_mval", cnnz + 1);
+    k_csc_add_fill<<<grid_for(n, 256), 256, 0, C.stream>>>(n, gptr, gidx, gval, bptr, bidx, bval, cptr, cidx, cval);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched += 4;
+    *mptr = cptr;
+    *midx = cidx;
+    *mval = cval;
+    return cnnz;
 }
 
 }  // namespace ssp

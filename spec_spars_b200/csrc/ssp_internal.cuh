@@ -222,10 +222,17 @@ struct DevGraph {
 };
 
 // a2+a5: build edges, adjacency and L_G from an input CSC already on the device.
+// tag prefixes the workspace buffers, so that two graphs can be held at once
 void build_graph_from_csc(Context& C, int64_t n, const int64_t* colptr, const int32_t* rowidx,
-                          const double* val, int64_t nnz, DevGraph& G);
+                          const double* val, int64_t nnz, DevGraph& G, const std::string& tag = "g");
 // adjacency + Laplacian for a given device edge list (v1<v2, CSC order)
-void build_graph_from_edges(Context& C, DevGraph& G);
+void build_graph_from_edges(Context& C, DevGraph& G, const std::string& tag = "g");
+
+// the current Laplacian's off-diagonals as a graph plus a batch of new edges (a symmetric CSC), duplicates
+// summed; returns nnz of the merged graph CSC, left in workspace buffers
+int64_t laplacian_plus_graph_device(Context& C, int64_t n, const int64_t* lptr, const int32_t* lidx,
+                                    const double* lval, const int64_t* bptr, const int32_t* bidx, const double* bval,
+                                    int64_t** mptr, int32_t** midx, double** mval);
 
 // a4: Y = B^T Q, columns [0,k): row-major with leading dimension ldy, or tile-major (8-column slabs)
 void sketch_device(Context& C, const DevGraph& G, int32_t k, double scale, uint64_t seed, int uniform,
@@ -325,6 +332,15 @@ void diff_sq_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2,
 void sqrt_device(Context& C, int64_t m, const double* sq, double* d);
 void probs_device(Context& C, int64_t m, const double* w, const double* d, double beta, double denom, double* p);
 void coins_device(Context& C, int64_t m, uint64_t seed, double* coins);
+
+// a15: checks (ssp_quality.cu)
+void laplacian_check_device(Context& C, int64_t n, const int64_t* ptr, const int32_t* idx, const double* val,
+                            double tol, int64_t* bad_cols, double* max_abs_colsum, int64_t* asym_entries);
+void probe_vectors_device(Context& C, int64_t n, int32_t p, uint64_t seed, double* X);
+void quadratic_forms_device(Context& C, int64_t n, const int64_t* ptr, const int32_t* idx, const double* val,
+                            const double* X, int32_t p, double* out);
+int64_t components_device(Context& C, int64_t n, const int64_t* ptr, const int32_t* idx, const double* val,
+                          int32_t* labels);
 // returns nnz(L_H); writes L_H CSC into workspace buffers returned through pointers
 int64_t sample_apply_device(Context& C, const DevGraph& G, const double* p, const double* coins, int reweight,
                             int64_t** lh_ptr, int32_t** lh_idx, double** lh_val, uint8_t* keep_out);

@@ -36,6 +36,11 @@ constexpr int MIXED_MAX_ROUNDS = 40;
 // a round whose FP64 residual shrinks by less than this factor (max over columns) switches the remaining
 // rounds to FP64 inner solves
 constexpr double MIXED_MIN_CONTRACTION = 1e-2;
+// FP32 rounds after the first may take at most this many times the first round's iterations (at least
+// MIXED_MIN_ROUND_ITERS); on ill-conditioned systems the FP32 recurrence stalls short of its target, and a
+// round that runs into the cap hands the rest to FP64
+constexpr int MIXED_ROUND_ITER_FACTOR = 2;
+constexpr int MIXED_MIN_ROUND_ITERS = 20;
 
 __host__ __device__ __forceinline__ int64_t tm_off(int64_t n, int64_t r, int64_t c) { return tile_off(n, r, c); }
 
@@ -858,9 +863,11 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         Precond P32, P64;
         int64_t pc32 = 0, pc64 = 0;
         bool use64 = false;
+        int32_t first_its = -1;
         int64_t active = read_i64(C, S.nactive);
         while (active > 0 && rep.refinements < MIXED_MAX_ROUNDS && it < opt.max_iters) {
             int32_t its;
+            bool hit_cap = false;
             SSP_CUDA(cudaMemsetAsync(Si.nactive, 0, sizeof(int64_t), C.stream));
             if (!use64) {
                 k_rhs_masked<float><<<egrid, 256, 0, C.stream>>>(n, r, S.active, r32);
@@ -870,8 +877,13 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
                 if (!P32.exec) build_precond_graph<float>(C, F, V32, n, r32, z32, ld, P32, pc32);
+                int32_t cap = opt.max_iters - it;
+                if (first_its >= 0)
+                    cap = std::min(cap, std::max(MIXED_MIN_ROUND_ITERS, MIXED_ROUND_ITER_FACTOR * first_its));
                 its = pcg_solve<float>(C, n, k, ld, A, lap_ptr, lap_idx, aval32, P32, pc32,
-                                       PcgBufs<float>{e32, r32, z32, p32, q32}, Si, R, opt.max_iters - it, opt, tm);
+                                       PcgBufs<float>{e32, r32, z32, p32, q32}, Si, R, cap, opt, tm);
+                if (first_its < 0) first_its = its;
+                hit_cap = its >= cap;
                 k_add_into<float><<<grid_for(total, 256, 148 * 16), 256, 0, C.stream>>>(total, e32, x);
             } else {
                 if (!e64) e64 = W.get_t<double>("pcgm_e64", total);
@@ -916,7 +928,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
             if (opt.verbose)
                 fprintf(stderr, "[ssp] refinement %d (%s inner, %d iterations): %lld columns active, worst ratio %.3g\n",
                         rep.refinements, use64 ? "fp64" : "fp32", its, (long long)active, hw);
-            if (active > 0 && !use64 && (hw > MIXED_MIN_CONTRACTION || its == 0)) use64 = true;
+            if (active > 0 && !use64 && (hw > MIXED_MIN_CONTRACTION || its == 0 || hit_cap)) use64 = true;
         }
     }
     // true relative residual ||(Y - mean) - A x|| / ||Y - mean||

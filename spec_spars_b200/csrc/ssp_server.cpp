@@ -45,6 +45,7 @@ struct Job {
     std::vector<int32_t> rowidx;
     std::vector<double> values;
     ssp_params params;
+    int32_t check_probes = 0;
     std::string output_file;
     int64_t est_bytes = 0;
     Clock::time_point t_submit, t_admit, t_done;
@@ -54,7 +55,32 @@ struct Job {
     ssp_csc_out out;
     ssp_stats stats;
     int32_t slot = -1;
+    // inline check (a15)
+    bool checked = false;
+    ssp_probe_result probe{};
+    int64_t cc_graph = 0, cc_sparsifier = 0;
+    double check_ms = 0.0;
 };
+
+// x^T L_H x against x^T L_G x on the request's own graph, and the component counts of both (a15)
+int check_result(ssp_context* ctx, const ssp_csc& g, const ssp_params& prm, int32_t probes, const ssp_csc_out& out,
+                 Job* j) {
+    int64_t m = 0, lnnz = 0;
+    int rc = ssp_stage_graph(ctx, &g, &m, &lnnz, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    if (rc != SSP_OK) return rc;
+    std::vector<int32_t> v1(m + 1), v2(m + 1), ri(lnnz + 1);
+    std::vector<double> w(m + 1), va(lnnz + 1);
+    std::vector<int64_t> cp(g.n + 1);
+    rc = ssp_stage_graph(ctx, &g, &m, &lnnz, v1.data(), v2.data(), w.data(), cp.data(), ri.data(), va.data());
+    if (rc != SSP_OK) return rc;
+    ssp_csc lg{g.n, lnnz, cp.data(), ri.data(), va.data(), SSP_MEM_HOST};
+    ssp_csc lh{out.n, out.nnz, out.colptr, out.rowidx, out.values, SSP_MEM_HOST};
+    rc = ssp_probe_quadratic_form(ctx, &lg, &lh, prm.epsilon, probes, prm.sampling_seed, &j->probe);
+    if (rc != SSP_OK) return rc;
+    rc = ssp_connected_components(ctx, &g, SSP_MEM_HOST, nullptr, &j->cc_graph);
+    if (rc != SSP_OK) return rc;
+    return ssp_connected_components(ctx, &lh, SSP_MEM_HOST, nullptr, &j->cc_sparsifier);
+}
 
 int fail(int code, const std::string& msg) {
     ssp::set_last_error(msg);
@@ -111,6 +137,19 @@ struct ssp_server {
             memset(&j->stats, 0, sizeof(j->stats));
             const int rc = ssp_sparsify(ctx, &g, &j->params, SSP_MEM_HOST, &j->out, &j->stats);
             std::string err = rc == SSP_OK ? std::string() : std::string(ssp_last_error());
+            int status = rc;
+            if (rc == SSP_OK && j->check_probes > 0) {
+                const Clock::time_point t0 = Clock::now();
+                const int crc = check_result(ctx, g, j->params, j->check_probes, j->out, j);
+                j->check_ms = ms_between(t0, Clock::now());
+                if (crc == SSP_OK) {
+                    j->checked = true;
+                } else {
+                    status = crc;
+                    err = std::string("inline check: ") + ssp_last_error();
+                    ssp_csc_free(&j->out);
+                }
+            }
             // keep the slot's cached workspace within its share of the budget
             if (ssp_context_workspace_bytes(ctx) > keep_ws) ssp_context_release_workspace(ctx);
             // the input copy is no longer needed
@@ -119,13 +158,13 @@ struct ssp_server {
             std::vector<double>().swap(j->values);
 
             lk.lock();
-            j->status = rc;
+            j->status = status;
             j->error = err;
             j->t_done = Clock::now();
             j->done = true;
             inflight--;
             inflight_bytes -= j->est_bytes;
-            if (rc == SSP_OK) completed++;
+            if (status == SSP_OK) completed++;
             else failed++;
             cv_done.notify_all();
             cv_work.notify_all();
@@ -143,6 +182,14 @@ struct ssp_server {
         r->run_ms = ms_between(j->t_admit, j->t_done);
         r->latency_ms = ms_between(j->t_submit, j->t_done);
         r->slot = j->slot;
+        r->checked = j->checked ? 1 : 0;
+        r->probe_upper_violations = j->probe.upper_bound_violations;
+        r->probe_lower_violations = j->probe.lower_bound_violations;
+        r->probe_mean_relative_error = j->probe.mean_relative_error;
+        r->probe_max_relative_error = j->probe.max_relative_error;
+        r->components_graph = j->cc_graph;
+        r->components_sparsifier = j->cc_sparsifier;
+        r->check_ms = j->check_ms;
     }
 };
 
@@ -217,6 +264,7 @@ int ssp_submit(ssp_server* s, const ssp_request* req, uint64_t* ticket) {
     j->rowidx.assign(g.rowidx, g.rowidx + g.nnz);
     j->values.assign(g.values, g.values + g.nnz);
     j->params = req->params;
+    j->check_probes = req->check_probes;
     j->output_file = req->params.output_file ? req->params.output_file : "";
     j->est_bytes = est;
     std::lock_guard<std::mutex> lk(s->mu);

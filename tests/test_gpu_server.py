@@ -86,3 +86,21 @@ def test_failed_request_does_not_stop_the_server(ssp):
         H, st, _ = srv.wait(tg)
         assert st["m_in"] == 2 * 30 * 29
         assert srv.info()["failed"] == 1 and srv.info()["completed"] == 1
+
+
+@pytest.mark.gpu
+def test_inline_check_matches_direct_probe(ssp, ora, ctx):
+    G = ssp.gen_er(3000, 60.0, 0.5, 2.0, 12)
+    prm = ssp.SparsifierParameters.baseline(0.5, pcg_tol=1e-8, sampling_seed=3)
+    prm.reweight = ssp.SSP_REWEIGHT_INV_P
+    with ssp.Server(0, slots=2) as srv:
+        H, st, info = srv.wait(srv.submit(G, prm, check_probes=40))
+    chk = info["check"]
+    v1, v2, w = ora.extract_edges(G.n, G.colptr, G.rowidx, G.values)
+    cp, ri, va = ora.laplacian(G.n, v1, v2, w)
+    direct = ctx.probe_quadratic_form(ssp.CSC(G.n, cp, ri, va), H, 0.5, probes=40, seed=3)
+    assert chk["upper_bound_violations"] == direct["upper_bound_violations"]
+    assert chk["lower_bound_violations"] == direct["lower_bound_violations"]
+    assert chk["mean_relative_error"] == direct["mean_relative_error"]
+    assert chk["ccs_equal"] and chk["components_graph"] == ctx.connected_components(G)[0]
+    assert chk["max_relative_error"] < 0.5 and chk["check_ms"] > 0
