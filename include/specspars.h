@@ -329,6 +329,9 @@ int ssp_connected_components(ssp_context* ctx, const ssp_csc* m, int32_t mem, in
 int ssp_sparsify_mtx(const char* input_file, const char* output_file, const ssp_params* params, ssp_stats* stats);
 int ssp_read_mtx(const char* path, ssp_csc_out* out);             /* host CSC, duplicates summed */
 int ssp_write_mtx(const char* path, const ssp_csc* m);            /* coordinate real general */
+/* edge list ("<n> <m>" then "u v [w]" lines) -> symmetric .mtx, first weight of a repeated pair wins
+ * (edge_list_to_matrix_market, src/utils.rs:413-526) */
+int ssp_edgelist_to_mtx(const char* input_path, const char* output_path, double default_weight);
 
 /* ---- synthetic graphs (seeded, identical on every host) as symmetric host CSC ---- */
 int ssp_gen_grid2d(int64_t nx, int64_t ny, double w, ssp_csc_out* out);

@@ -162,6 +162,7 @@ def lib():
             "ssp_gen_grid2d": ([I64, I64, DBL, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_grid3d": ([I64, I64, I64, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_er": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
+            "ssp_edgelist_to_mtx": ([ctypes.c_char_p, ctypes.c_char_p, DBL], ctypes.c_int),
             "ssp_gen_rgg": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_check_laplacian": ([P, ctypes.POINTER(_Csc), DBL, ctypes.POINTER(I64), ctypes.POINTER(DBL),
                                      ctypes.POINTER(I64)], ctypes.c_int),
@@ -304,6 +305,11 @@ def gen_er(n, avg_degree, wlo=0.5, whi=2.0, seed=1):
     out = _CscOut()
     _check(lib().ssp_gen_er(n, avg_degree, wlo, whi, seed, ctypes.byref(out)))
     return _take_out(out)
+
+
+def edge_list_to_matrix_market(input_path, output_path, default_weight=1.0):
+    """edge_list_to_matrix_market (utils.rs:413-526)."""
+    _check(lib().ssp_edgelist_to_mtx(str(input_path).encode(), str(output_path).encode(), default_weight))
 
 
 def gen_rgg(n, avg_degree, wlo=0.1, whi=10.0, seed=1):

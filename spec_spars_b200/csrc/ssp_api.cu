@@ -860,6 +860,14 @@ int ssp_gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t se
         host_out(h, out);
     });
 }
+int ssp_edgelist_to_mtx(const char* input_path, const char* output_path, double default_weight) {
+    return guarded([&] {
+        SSP_REQUIRE(input_path && output_path, SSP_ERR_INVALID, "bad arguments");
+        std::string err;
+        if (edgelist_to_mtx(input_path, output_path, default_weight, err) != 0) throw Error(SSP_ERR_IO, err);
+    });
+}
+
 int ssp_gen_rgg(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, ssp_csc_out* out) {
     return guarded([&] {
         SSP_REQUIRE(n > 1 && avg_degree > 0 && out, SSP_ERR_INVALID, "bad arguments");

@@ -7,6 +7,8 @@
 // Generators produce the symmetric adjacency of the synthetic graphs used by the benchmark
 // configurations, seeded through Philox so every host builds the same graph.
 #include <algorithm>
+#include <cerrno>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -176,6 +178,103 @@ void gen_rgg(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed
         w[t] = (double)(float)(wlo + (whi - wlo) * u);
     }
     out.from_upper_edges(n, a, b, w);
+}
+
+// Edge list -> Matrix Market (edge_list_to_matrix_market, utils.rs:413-526).  The first line holds
+// "<num_nodes> <num_edges>" (the edge count is not used); each further non-blank line "u v [w]", w defaulting
+// to default_weight.  Pairs are stored as (min, max); for repeated pairs the first weight wins.  The output is
+// a symmetric real coordinate file with the pairs sorted, indices written as read, and weights in the
+// shortest round-trip decimal without an exponent (how Rust displays an f64).
+int edgelist_to_mtx(const char* in_path, const char* out_path, double default_weight, std::string& err) {
+    FILE* f = fopen(in_path, "r");
+    if (!f) {
+        err = std::string("cannot open ") + in_path;
+        return -1;
+    }
+    std::vector<char> buf(1 << 16);
+    std::string line;
+    auto getline = [&](std::string& out) -> bool {
+        out.clear();
+        for (;;) {
+            if (!fgets(buf.data(), (int)buf.size(), f)) return !out.empty();
+            out += buf.data();
+            if (!out.empty() && out.back() == '\n') return true;
+        }
+    };
+    if (!getline(line)) {
+        fclose(f);
+        err = "empty input file";
+        return -1;
+    }
+    unsigned long long n_nodes = 0, n_decl = 0;
+    if (sscanf(line.c_str(), "%llu %llu", &n_nodes, &n_decl) != 2) {
+        fclose(f);
+        err = "first line must hold the node and edge counts";
+        return -1;
+    }
+    std::vector<std::pair<std::pair<uint64_t, uint64_t>, double>> edges;
+    std::vector<std::pair<std::pair<uint64_t, uint64_t>, size_t>> keys;
+    size_t lineno = 1;
+    while (getline(line)) {
+        lineno++;
+        size_t p = line.find_first_not_of(" \t\r\n");
+        if (p == std::string::npos) continue;
+        const char* c = line.c_str() + p;
+        char* end = nullptr;
+        errno = 0;
+        const unsigned long long u = strtoull(c, &end, 10);
+        if (end == c || errno) {
+            fclose(f);
+            err = "line " + std::to_string(lineno) + ": missing first endpoint";
+            return -1;
+        }
+        c = end;
+        const unsigned long long v = strtoull(c, &end, 10);
+        if (end == c || errno) {
+            fclose(f);
+            err = "line " + std::to_string(lineno) + ": missing second endpoint";
+            return -1;
+        }
+        c = end;
+        while (*c == ' ' || *c == '\t') c++;
+        double w = default_weight;
+        if (*c && *c != '\n' && *c != '\r') {
+            w = strtod(c, &end);
+            if (end == c) {
+                fclose(f);
+                err = "line " + std::to_string(lineno) + ": bad weight";
+                return -1;
+            }
+        }
+        const uint64_t i = std::min(u, v), j = std::max(u, v);
+        keys.push_back({{i, j}, edges.size()});
+        edges.push_back({{i, j}, w});
+    }
+    fclose(f);
+    // first occurrence wins: stable order by (pair, position), keep the first of each pair
+    std::sort(keys.begin(), keys.end());
+    FILE* o = fopen(out_path, "w");
+    if (!o) {
+        err = std::string("cannot write ") + out_path;
+        return -1;
+    }
+    size_t unique = 0;
+    for (size_t t = 0; t < keys.size(); t++)
+        if (t == 0 || keys[t].first != keys[t - 1].first) unique++;
+    fprintf(o, "%%%%MatrixMarket matrix coordinate real symmetric\n%% Converted from %s\n%llu %llu %zu\n", in_path,
+            n_nodes, n_nodes, unique);
+    char num[512];
+    for (size_t t = 0; t < keys.size(); t++) {
+        if (t > 0 && keys[t].first == keys[t - 1].first) continue;
+        const double w = edges[keys[t].second].second;
+        auto r = std::to_chars(num, num + sizeof num - 1, w, std::chars_format::fixed);
+        *r.ptr = 0;
+        fprintf(o, "%llu %llu %s\n", (unsigned long long)keys[t].first.first,
+                (unsigned long long)keys[t].first.second, num);
+    }
+    const bool ok = fclose(o) == 0;
+    if (!ok) err = std::string("error writing ") + out_path;
+    return ok ? 0 : -1;
 }
 
 // ---------------------------------------------------------------- Matrix Market

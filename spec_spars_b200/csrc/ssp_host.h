@@ -22,6 +22,7 @@ void gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed,
 void gen_rgg(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, HostCsc& out);
 
 int read_mtx(const char* path, HostCsc& out, std::string& err);
+int edgelist_to_mtx(const char* in_path, const char* out_path, double default_weight, std::string& err);
 int write_mtx(const char* path, int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,
               std::string& err);
 

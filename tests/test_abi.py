@@ -136,3 +136,29 @@ def test_server_api_without_device(ssp):
         with pytest.raises(ssp.SspError) as e:
             ssp.Server(0, slots=2)
         assert e.value.code == -7
+
+
+def test_edge_list_to_matrix_market(ssp, tmp_path):
+    """edge_list_to_matrix_market (utils.rs:413-526): header line, optional weights, (min, max) pairs,
+    first weight of a repeated pair wins, sorted output, weights printed as Rust displays an f64."""
+    src = tmp_path / "g.txt"
+    lines = ["6 9", "0 1 2.5", "1 0 7.0", "", "3 2", "2 4 0.0025", "5 5 1e-10", "4 2 9", "1 3 12345678.5",
+             "0 5 0.1"]
+    src.write_text("\n".join(lines) + "\n")
+    dst = tmp_path / "g.mtx"
+    ssp.edge_list_to_matrix_market(src, dst, 1.5)
+    first = {}
+    for ln in lines[1:]:
+        if not ln.strip():
+            continue
+        t = ln.split()
+        u, v = int(t[0]), int(t[1])
+        w = float(t[2]) if len(t) > 2 else 1.5
+        first.setdefault((min(u, v), max(u, v)), w)
+    expect = ["%%MatrixMarket matrix coordinate real symmetric", f"% Converted from {src}", f"6 6 {len(first)}"]
+    expect += [f"{i} {j} {np.format_float_positional(w, trim='-')}" for (i, j), w in sorted(first.items())]
+    assert dst.read_text().splitlines() == expect
+    assert "0 1 2.5" in expect and "5 5 0.0000000001" in expect and "2 3 1.5" in expect
+    with pytest.raises(ssp.SspError) as e:
+        ssp.edge_list_to_matrix_market(tmp_path / "missing.txt", dst, 1.0)
+    assert e.value.code == -6
