@@ -338,6 +338,9 @@ int ssp_gen_grid2d(int64_t nx, int64_t ny, double w, ssp_csc_out* out);
 int ssp_gen_grid3d(int64_t nx, int64_t ny, int64_t nz, double wlog10_lo, double wlog10_hi, uint64_t seed,
                    ssp_csc_out* out);
 int ssp_gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, ssp_csc_out* out);
+/* R-MAT: edge_factor * 2^scale samples with quadrant probabilities (a, b, c, 1-a-b-c), self-loops dropped,
+ * symmetrized and deduplicated, LogNormal(0,1) weights rounded to FP32, largest connected component only */
+int ssp_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed, ssp_csc_out* out);
 /* random geometric graph in the unit square, radius sqrt(avg_degree / (pi n)), weights uniform [wlo, whi] */
 int ssp_gen_rgg(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, ssp_csc_out* out);
 

@@ -163,6 +163,7 @@ def lib():
             "ssp_gen_grid3d": ([I64, I64, I64, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_er": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_edgelist_to_mtx": ([ctypes.c_char_p, ctypes.c_char_p, DBL], ctypes.c_int),
+            "ssp_gen_rmat": ([I32, I32, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_rgg": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_check_laplacian": ([P, ctypes.POINTER(_Csc), DBL, ctypes.POINTER(I64), ctypes.POINTER(DBL),
                                      ctypes.POINTER(I64)], ctypes.c_int),
@@ -271,11 +272,36 @@ class CSC:
         return (self.nnz - diag) // 2
 
 
+class _HostOut:
+    """Owns a library-allocated host CSC; frees it once no array views it any more."""
+
+    def __init__(self, out):
+        self.out = out
+
+    def __del__(self):
+        try:
+            lib().ssp_csc_free(ctypes.byref(self.out))
+        except Exception:
+            pass
+
+
 def _take_out(out):
-    try:
-        return CSC._from_out(out)
-    finally:
-        lib().ssp_csc_free(ctypes.byref(out))
+    """Host CSC result as numpy arrays viewing the library's buffers (no copy); they are freed with the
+    last array."""
+    if out.mem != SSP_MEM_HOST or out.nnz == 0:
+        try:
+            return CSC._from_out(out)
+        finally:
+            lib().ssp_csc_free(ctypes.byref(out))
+    holder = _HostOut(out)
+    views = []
+    for addr, ct, cnt, dt in ((out.colptr, ctypes.c_int64, out.n + 1, np.int64),
+                              (out.rowidx, ctypes.c_int32, out.nnz, np.int32),
+                              (out.values, ctypes.c_double, out.nnz, np.float64)):
+        buf = (ct * cnt).from_address(addr)
+        buf._owner = holder
+        views.append(np.frombuffer(buf, dtype=dt))
+    return CSC(out.n, *views)
 
 
 def read_mtx(path):
@@ -310,6 +336,13 @@ def gen_er(n, avg_degree, wlo=0.5, whi=2.0, seed=1):
 def edge_list_to_matrix_market(input_path, output_path, default_weight=1.0):
     """edge_list_to_matrix_market (utils.rs:413-526)."""
     _check(lib().ssp_edgelist_to_mtx(str(input_path).encode(), str(output_path).encode(), default_weight))
+
+
+def gen_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=3):
+    """R-MAT graph, largest connected component (the R-MAT configuration: scale 22, edge factor 16)."""
+    out = _CscOut()
+    _check(lib().ssp_gen_rmat(scale, edge_factor, a, b, c, seed, ctypes.byref(out)))
+    return _take_out(out)
 
 
 def gen_rgg(n, avg_degree, wlo=0.1, whi=10.0, seed=1):

@@ -224,12 +224,13 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     if (finish_only) {
         deg_used = 0;
     } else if (fo.max_degree < 0) {
-        // the probe always uses global columns [0, min(k, 8)), so every rank of a split run picks the same
+        // the probe always uses global columns [0, min(k, SSP_PROBE_COLS)), so every rank of a split run picks
+        // the same factor
         const double* probe = Y;
-        const int32_t kp = std::min<int32_t>(k, SSP_TILE);
+        const int32_t kp = std::min<int32_t>(k, SSP_PROBE_COLS);
         if (col_lo != 0 || kl < kp) {
-            double* Yp = C.ws.get_t<double>("sp_Yprobe", (size_t)n * SSP_TILE);
-            sketch_device(C, SG, kp, scale, prm->sketch_seed, prm->sketch_uniform, Yp, SSP_TILE, 1, 0);
+            double* Yp = C.ws.get_t<double>("sp_Yprobe", (size_t)n * tile_ld(kp));
+            sketch_device(C, SG, kp, scale, prm->sketch_seed, prm->sketch_uniform, Yp, tile_ld(kp), 1, 0);
             probe = Yp;
         }
         deg_used = autotune_factor(C, n, G.lap_ptr, G.lap_idx, G.lap_val, 2 * G.m, probe, kp, fo, po, F, &ms_tune);
@@ -865,6 +866,17 @@ int ssp_edgelist_to_mtx(const char* input_path, const char* output_path, double 
         SSP_REQUIRE(input_path && output_path, SSP_ERR_INVALID, "bad arguments");
         std::string err;
         if (edgelist_to_mtx(input_path, output_path, default_weight, err) != 0) throw Error(SSP_ERR_IO, err);
+    });
+}
+
+int ssp_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed, ssp_csc_out* out) {
+    return guarded([&] {
+        SSP_REQUIRE(scale >= 1 && scale <= 30 && edge_factor > 0 && a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0 &&
+                        out,
+                    SSP_ERR_INVALID, "bad arguments");
+        HostCsc h;
+        gen_rmat(scale, edge_factor, a, b, c, seed, h);
+        host_out(h, out);
     });
 }
 

@@ -6,8 +6,8 @@
 // early Schur complement -- while every PCG iteration pays gathers proportional to nnz(A) + 2 nnz(L).
 //
 // Rule: factor with the lightest truncation (stop once the Schur complement's average degree exceeds
-// 1.05 d0 + 1, d0 the graph's average degree), run a 20-iteration PCG probe on the first column tile of
-// the actual right-hand sides, and estimate the iterations to reach the tolerance from the contraction
+// 1.05 d0 + 1, d0 the graph's average degree), run a 20-iteration PCG probe on the first SSP_PROBE_COLS
+// columns of the actual right-hand sides, and estimate the iterations to reach the tolerance from the contraction
 // rate of the last ten probe iterations.  A graph whose lightly preconditioned system converges within
 // 30 iterations keeps that factor; otherwise the elimination runs to completion.  Both factorizations
 // are deterministic.
@@ -42,7 +42,7 @@ int64_t autotune_factor(Context& C, int64_t n, const int64_t* lap_ptr, const int
     std::vector<double> hist;
     po.history = &hist;
     PcgReport rep;
-    const int32_t kp = std::min<int32_t>(k, SSP_TILE);
+    const int32_t kp = std::min<int32_t>(k, SSP_PROBE_COLS);
     pcg_device(C, n, lap_ptr, lap_idx, lap_val, F, Ytiles, kp, nullptr, po, rep);
     const double tol_rel = popt.tol > 0 ? popt.tol : 1e-6;
     double iters = 1e9;

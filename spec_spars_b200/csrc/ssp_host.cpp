@@ -180,6 +180,75 @@ void gen_rgg(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed
     out.from_upper_edges(n, a, b, w);
 }
 
+// R-MAT graph: edge_factor * 2^scale directed samples; each picks its quadrant bit by bit with probabilities
+// (a, b, c, 1 - a - b - c) from Philox counters (sample, bit) in stream 5.  Self-loops are dropped, pairs are
+// made undirected and deduplicated, each kept pair gets a LogNormal(0, 1) weight (Box-Muller from the
+// counter (min * 2^scale + max, 6), rounded to FP32), and only the largest connected component is kept, its
+// vertices renumbered in increasing order.
+void gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed, HostCsc& out) {
+    const uint64_t nv = 1ull << scale;
+    const uint64_t samples = (uint64_t)edge_factor << scale;
+    std::vector<uint64_t> keys;
+    keys.reserve(samples);
+    for (uint64_t t = 0; t < samples; t++) {
+        uint64_t u = 0, v = 0;
+        for (int32_t bit = 0; bit < scale; bit++) {
+            const double r = gen_u53(seed, t * 64 + (uint64_t)bit, 5);
+            const int q = r < a ? 0 : r < a + b ? 1 : r < a + b + c ? 2 : 3;
+            u = (u << 1) | (uint64_t)(q >> 1);
+            v = (v << 1) | (uint64_t)(q & 1);
+        }
+        if (u == v) continue;
+        const uint64_t lo = std::min(u, v), hi = std::max(u, v);
+        keys.push_back(lo * nv + hi);
+    }
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    // largest connected component by union-find (smaller root wins, so labels are deterministic)
+    std::vector<uint64_t> parent(nv);
+    for (uint64_t i = 0; i < nv; i++) parent[i] = i;
+    auto find = [&](uint64_t x) {
+        while (parent[x] != x) x = parent[x] = parent[parent[x]];
+        return x;
+    };
+    for (uint64_t k : keys) {
+        uint64_t ra = find(k / nv), rb = find(k % nv);
+        if (ra != rb) parent[std::max(ra, rb)] = std::min(ra, rb);
+    }
+    std::vector<uint64_t> size(nv, 0);
+    for (uint64_t i = 0; i < nv; i++) size[find(i)]++;
+    uint64_t best = 0;
+    for (uint64_t i = 0; i < nv; i++)
+        if (size[i] > size[best]) best = i;
+    std::vector<int64_t> newid(nv, -1);
+    int64_t n = 0;
+    for (uint64_t i = 0; i < nv; i++)
+        if (find(i) == best) newid[i] = n++;
+    // kept pairs in CSC-upper order (by (hi, lo)) with their weights
+    std::vector<std::pair<int64_t, int64_t>> e;
+    std::vector<uint64_t> ek;
+    for (uint64_t k : keys) {
+        const uint64_t lo = k / nv, hi = k % nv;
+        if (newid[lo] < 0) continue;
+        e.push_back({newid[hi], newid[lo]});
+        ek.push_back(k);
+    }
+    std::vector<size_t> order(e.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](size_t x, size_t y) { return e[x] < e[y]; });
+    std::vector<int32_t> va(e.size()), vb(e.size());
+    std::vector<double> w(e.size());
+    for (size_t t = 0; t < order.size(); t++) {
+        const size_t i = order[t];
+        vb[t] = (int32_t)e[i].first;
+        va[t] = (int32_t)e[i].second;
+        const double u1 = gen_u53(seed, ek[i], 6), u2 = gen_u53(seed ^ 0x9e3779b97f4a7c15ull, ek[i], 6);
+        const double z = std::sqrt(-2.0 * std::log(1.0 - u1)) * std::cos(2.0 * M_PI * u2);
+        w[t] = (double)(float)std::exp(z);
+    }
+    out.from_upper_edges(n, va, vb, w);
+}
+
 // Edge list -> Matrix Market (edge_list_to_matrix_market, utils.rs:413-526).  The first line holds
 // "<num_nodes> <num_edges>" (the edge count is not used); each further non-blank line "u v [w]", w defaulting
 // to default_weight.  Pairs are stored as (min, max); for repeated pairs the first weight wins.  The output is

@@ -20,6 +20,7 @@ void gen_grid2d(int64_t nx, int64_t ny, double w, HostCsc& out);
 void gen_grid3d(int64_t nx, int64_t ny, int64_t nz, double lo, double hi, uint64_t seed, HostCsc& out);
 void gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, HostCsc& out);
 void gen_rgg(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, HostCsc& out);
+void gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed, HostCsc& out);
 
 int read_mtx(const char* path, HostCsc& out, std::string& err);
 int edgelist_to_mtx(const char* in_path, const char* out_path, double default_weight, std::string& err);

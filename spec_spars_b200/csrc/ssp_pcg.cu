@@ -27,7 +27,6 @@
 namespace ssp {
 
 constexpr int TILE = SSP_TILE;    // columns per tile
-constexpr int SLOTS = 32 / TILE;  // nonzeros processed in parallel per warp
 constexpr int RED_THREADS = 256;  // column reductions: (256 / TILE) row lanes x TILE columns
 
 // mixed precision: relative reduction asked of one FP32 inner solve, and the round limit
@@ -360,25 +359,29 @@ __global__ void k_cols_outer(int64_t ld, const int32_t* __restrict__ inner_iters
 }
 
 // ---------------------------------------------------------------- SpMM and triangular solves
-// Warp per row; lane = slot * TILE + column.  xt points at the tile's slab (row stride TILE values).
-// Two independent gathers per lane per step keep more loads in flight.
-template <class T>
+// Warp per row; lane = slot * W + column, W = the columns handled (TILE, or 8 when at most 8 are real).
+// xt points at the tile's slab (row stride TILE values).  Two independent gathers per lane per step keep
+// more loads in flight.  Lanes of padding columns (past the k real ones, in the last tile) are not live and
+// load nothing.
+template <class T, int W>
 __device__ __forceinline__ T warp_row_gather(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                             const T* __restrict__ val, int64_t row, const T* xt, int lane) {
-    const int slot = lane / TILE, c = lane % TILE;
-    const int64_t e = ptr[row + 1];
+                                             const T* __restrict__ val, int64_t row, const T* xt, int lane,
+                                             bool live) {
+    constexpr int SLOTS_W = 32 / W;
+    const int slot = lane / W, c = lane % W;
+    const int64_t e = live ? ptr[row + 1] : 0;
     T acc0 = 0, acc1 = 0;
-    int64_t p = ptr[row] + slot;
-    for (; p + SLOTS < e; p += 2 * SLOTS) {
-        const int32_t i0 = idx[p], i1 = idx[p + SLOTS];
-        const T v0 = val[p], v1 = val[p + SLOTS];
+    int64_t p = live ? ptr[row] + slot : 0;
+    for (; p + SLOTS_W < e; p += 2 * SLOTS_W) {
+        const int32_t i0 = idx[p], i1 = idx[p + SLOTS_W];
+        const T v0 = val[p], v1 = val[p + SLOTS_W];
         acc0 += v0 * xt[(int64_t)i0 * TILE + c];
         acc1 += v1 * xt[(int64_t)i1 * TILE + c];
     }
     if (p < e) acc0 += val[p] * xt[(int64_t)idx[p] * TILE + c];
     T acc = acc0 + acc1;
 #pragma unroll
-    for (int o = TILE; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    for (int o = W; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     return acc;
 }
 
@@ -409,14 +412,14 @@ __device__ __forceinline__ void chunk_epilogue(T* out, const T* aux, const T* xt
     }
 }
 
-template <int MODE, class T>
+template <int MODE, class T, int W>
 __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks,
                                                         const int64_t* __restrict__ ptr,
                                                         const int32_t* __restrict__ idx,
                                                         const T* __restrict__ val,
                                                         const int32_t* __restrict__ rowmap, const T* xsrc,
                                                         T* out, const T* __restrict__ aux, int64_t ld,
-                                                        double* __restrict__ part) {
+                                                        double* __restrict__ part, int32_t kcols) {
     __shared__ int32_t s_idx[CH_WARPS][CHUNK_CAP];
     __shared__ T s_val[CH_WARPS][CHUNK_CAP];
     __shared__ int32_t s_ptr[CH_WARPS][CHUNK_ROWS + 1];
@@ -428,7 +431,8 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
     int32_t* si = s_idx[w];
     T* sv = s_val[w];
     int32_t* sp = s_ptr[w];
-    double dot = 0.0;  // SpMM: per-lane partial of p.q for column (lane % TILE)
+    constexpr int SLOTS_W = 32 / W;
+    double dot = 0.0;  // SpMM: per-lane partial of p.q for column (lane % W)
     for (int32_t c = blockIdx.x * CH_WARPS + w; c < nchunks; c += gridDim.x * CH_WARPS) {
         const int32_t r0 = cstart[c], r1 = cstart[c + 1];
         const int64_t e0 = ptr[r0], e1 = ptr[r1];
@@ -440,10 +444,11 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
             }
             for (int32_t i = lane; i <= r1 - r0; i += 32) sp[i] = (int32_t)(ptr[r0 + i] - e0);
             __syncwarp();
-            const int32_t pairs = (r1 - r0) * TILE;
+            const int32_t pairs = (r1 - r0) * W;
             for (int32_t pr = lane; pr < pairs; pr += 32) {
-                const int32_t rr = pr / TILE, col = pr % TILE;
-                const int32_t q0 = sp[rr], q1 = sp[rr + 1];
+                const int32_t rr = pr / W, col = pr % W;
+                const bool live = t * TILE + col < kcols;
+                const int32_t q0 = sp[rr], q1 = live ? sp[rr + 1] : q0;
                 T a0 = 0, a1 = 0, a2 = 0, a3 = 0;
                 int32_t q = q0;
                 for (; q + 3 < q1; q += 4) {
@@ -459,19 +464,20 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
             }
             __syncwarp();
         } else {
-            // one long row: (32 / TILE) entry slots x TILE columns per step, then a reduction over the slots
-            const int slot = lane / TILE, col = lane % TILE;
+            // one long row: (32 / W) entry slots x W columns per step, then a reduction over the slots
+            const int slot = lane / W, col = lane % W;
+            const int64_t qe = t * TILE + col < kcols ? e1 : e0;
             T a0 = 0, a1 = 0;
             int64_t q = e0 + slot;
-            for (; q + SLOTS < e1; q += 2 * SLOTS) {
+            for (; q + SLOTS_W < qe; q += 2 * SLOTS_W) {
                 a0 += __ldcs(val + q) * xt[(int64_t)__ldcs(idx + q) * TILE + col];
-                a1 += __ldcs(val + q + SLOTS) * xt[(int64_t)__ldcs(idx + q + SLOTS) * TILE + col];
+                a1 += __ldcs(val + q + SLOTS_W) * xt[(int64_t)__ldcs(idx + q + SLOTS_W) * TILE + col];
             }
-            if (q < e1) a0 += __ldcs(val + q) * xt[(int64_t)__ldcs(idx + q) * TILE + col];
+            if (q < qe) a0 += __ldcs(val + q) * xt[(int64_t)__ldcs(idx + q) * TILE + col];
             T acc = a0 + a1;
 #pragma unroll
-            for (int o = TILE; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane < TILE) chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[r0] : r0, col, acc, dot);
+            for (int o = W; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane < W) chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[r0] : r0, col, acc, dot);
         }
     }
     if (MODE == M_SPMM && part) {
@@ -479,7 +485,8 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
         __syncthreads();
         if (threadIdx.x < TILE) {
             double tt = 0.0;
-            for (int i = 0; i < CH_THREADS / TILE; i++) tt += s_red[i * TILE + threadIdx.x];
+            if (threadIdx.x < W)
+                for (int i = 0; i < CH_THREADS / W; i++) tt += s_red[i * W + threadIdx.x];
             part[(int64_t)blockIdx.x * ld + t * TILE + threadIdx.x] = tt;
         }
     }
@@ -491,28 +498,29 @@ static int chunk_blocks(int32_t nchunks) {
     return std::max(1, std::min((nchunks + CH_WARPS - 1) / CH_WARPS, 148 * 6));
 }
 
-// Runs of thin levels: the k columns are independent, so one block per 8-column tile can walk a run
+// Runs of thin levels: the k columns are independent, so one block per column tile can walk a run
 // of consecutive levels on its own, with only a block barrier between levels (its own writes are the
 // only values it reads back).  y is read and written in place: no read-only cache path.
 constexpr int RUN_THREADS = 512;
 constexpr int THIN_ROWS = 64;
 
 // rows[i] is the vertex of stored row i; ptr/idx/val are in storage order
-template <class T>
+template <class T, int W>
 __global__ void __launch_bounds__(RUN_THREADS) k_trsv_fwd_run(int64_t n, const int32_t* __restrict__ rows,
                                                               const int32_t* __restrict__ lptr, int32_t l0,
                                                               int32_t l1, const int64_t* __restrict__ ptr,
                                                               const int32_t* __restrict__ idx,
                                                               const T* __restrict__ val, const T* __restrict__ r,
-                                                              T* y) {
+                                                              T* y, int32_t kcols) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = RUN_THREADS / 32;
     const int64_t toff = (int64_t)blockIdx.x * n * TILE;
+    const bool live = (int64_t)blockIdx.x * TILE + lane % W < kcols;
     for (int32_t l = l0; l < l1; l++) {
         const int32_t s = lptr[l], e = lptr[l + 1];
         for (int32_t i = s + warp; i < e; i += nwarp) {
             const int64_t u = rows[i];
-            const T acc = warp_row_gather<T>(ptr, idx, val, i, y + toff, lane);
-            if (lane < TILE) {
+            const T acc = warp_row_gather<T, W>(ptr, idx, val, i, y + toff, lane, live);
+            if (lane < W) {
                 const int64_t o = toff + u * TILE + lane;
                 y[o] = r[o] - acc;
             }
@@ -521,21 +529,22 @@ __global__ void __launch_bounds__(RUN_THREADS) k_trsv_fwd_run(int64_t n, const i
     }
 }
 
-template <class T>
+template <class T, int W>
 __global__ void __launch_bounds__(RUN_THREADS) k_trsv_bwd_run(int64_t n, const int32_t* __restrict__ rows,
                                                               const int32_t* __restrict__ lptr, int32_t l0,
                                                               int32_t l1, const int64_t* __restrict__ ptr,
                                                               const int32_t* __restrict__ idx,
                                                               const T* __restrict__ val, const T* __restrict__ D,
-                                                              T* yz) {
+                                                              T* yz, int32_t kcols) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = RUN_THREADS / 32;
     const int64_t toff = (int64_t)blockIdx.x * n * TILE;
+    const bool live = (int64_t)blockIdx.x * TILE + lane % W < kcols;
     for (int32_t l = l1 - 1; l >= l0; l--) {
         const int32_t s = lptr[l], e = lptr[l + 1];
         for (int32_t i = s + warp; i < e; i += nwarp) {
             const int64_t u = rows[i];
-            const T acc = warp_row_gather<T>(ptr, idx, val, i, yz + toff, lane);
-            if (lane < TILE) {
+            const T acc = warp_row_gather<T, W>(ptr, idx, val, i, yz + toff, lane, live);
+            if (lane < W) {
                 const int64_t o = toff + u * TILE + lane;
                 const T d = D[u];
                 const T yu = yz[o];
@@ -582,37 +591,43 @@ static std::vector<std::pair<int32_t, int32_t>> level_segments(const DevFactor& 
     return seg;
 }
 
-template <class T>
-static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
-                              int64_t ld) {
+// columns a warp handles per row: all TILE, or 8 when no more than 8 are real (the autotuner's probe), so
+// that a warp still covers four rows per step; the padding columns of y must then be zero already
+constexpr int NARROW_W = 8;
+
+template <class T, int W>
+static int64_t launch_precond_w(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
+                                int64_t ld, int32_t kcols) {
     const int ntiles = (int)(ld / TILE);
     int64_t launches = 0;
     const auto seg = level_segments(F);
     for (size_t i = 0; i < seg.size(); i++) {
         const int32_t l0 = seg[i].first, l1 = seg[i].second;
         if (l1 - l0 >= 2) {
-            k_trsv_fwd_run<T><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.level_ptr_d, l0, l1,
-                                                                     F.prow_ptr, F.prow_idx, V.prow_val, r, y);
+            k_trsv_fwd_run<T, W><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.level_ptr_d, l0, l1,
+                                                                     F.prow_ptr, F.prow_idx, V.prow_val, r, y, kcols);
         } else {
             const int32_t c0 = F.fchunk_lvl[l0], nc = F.fchunk_lvl[l0 + 1] - c0;
             if (nc == 0) continue;
             dim3 grid((unsigned)chunk_blocks(nc), (unsigned)ntiles);
-            k_chunked<M_FWD, T><<<grid, CH_THREADS, 0, C.stream>>>(n, F.fchunk + c0, nc, F.prow_ptr, F.prow_idx,
-                                                                    V.prow_val, F.level_rows, y, y, r, ld, nullptr);
+            k_chunked<M_FWD, T, W><<<grid, CH_THREADS, 0, C.stream>>>(n, F.fchunk + c0, nc, F.prow_ptr, F.prow_idx,
+                                                                    V.prow_val, F.level_rows, y, y, r, ld, nullptr,
+                                                                    kcols);
         }
         launches++;
     }
     for (size_t i = seg.size(); i-- > 0;) {
         const int32_t l0 = seg[i].first, l1 = seg[i].second;
         if (l1 - l0 >= 2) {
-            k_trsv_bwd_run<T><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.level_ptr_d, l0, l1,
-                                                                     F.pcol_ptr, F.pcol_idx, V.pcol_val, V.D, y);
+            k_trsv_bwd_run<T, W><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.level_ptr_d, l0, l1,
+                                                                     F.pcol_ptr, F.pcol_idx, V.pcol_val, V.D, y, kcols);
         } else {
             const int32_t c0 = F.bchunk_lvl[l0], nc = F.bchunk_lvl[l0 + 1] - c0;
             if (nc == 0) continue;
             dim3 grid((unsigned)chunk_blocks(nc), (unsigned)ntiles);
-            k_chunked<M_BWD, T><<<grid, CH_THREADS, 0, C.stream>>>(n, F.bchunk + c0, nc, F.pcol_ptr, F.pcol_idx,
-                                                                    V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr);
+            k_chunked<M_BWD, T, W><<<grid, CH_THREADS, 0, C.stream>>>(n, F.bchunk + c0, nc, F.pcol_ptr, F.pcol_idx,
+                                                                    V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr,
+                                                                    kcols);
         }
         launches++;
     }
@@ -621,11 +636,31 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
 }
 
 template <class T>
+static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
+                              int64_t ld, int32_t kcols) {
+    if (TILE > NARROW_W && kcols <= NARROW_W) return launch_precond_w<T, NARROW_W>(C, F, V, n, r, y, ld, kcols);
+    return launch_precond_w<T, TILE>(C, F, V, n, r, y, ld, kcols);
+}
+
+// SpMM q = A p (+ p.q partials into part when part != nullptr)
+template <class T>
+static void launch_spmm(Context& C, int64_t n, const int32_t* chunks, int32_t nchunks, dim3 grid, const int64_t* aptr,
+                        const int32_t* aidx, const T* aval, const T* p, T* q, int64_t ld, double* part,
+                        int32_t kcols) {
+    if (TILE > NARROW_W && kcols <= NARROW_W)
+        k_chunked<M_SPMM, T, NARROW_W><<<grid, CH_THREADS, 0, C.stream>>>(n, chunks, nchunks, aptr, aidx, aval, nullptr,
+                                                                           p, q, nullptr, ld, part, kcols);
+    else
+        k_chunked<M_SPMM, T, TILE><<<grid, CH_THREADS, 0, C.stream>>>(n, chunks, nchunks, aptr, aidx, aval, nullptr, p,
+                                                                       q, nullptr, ld, part, kcols);
+}
+
+template <class T>
 static void build_precond_graph(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
-                                int64_t ld, Precond& P, int64_t& launches) {
+                                int64_t ld, int32_t kcols, Precond& P, int64_t& launches) {
     SSP_CUDA(cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeThreadLocal));
     try {
-        launches = launch_precond<T>(C, F, V, n, r, y, ld);
+        launches = launch_precond<T>(C, F, V, n, r, y, ld, kcols);
     } catch (...) {
         cudaGraph_t g;
         cudaStreamEndCapture(C.stream, &g);
@@ -640,7 +675,7 @@ static FactorVals<double> fp64_vals(const DevFactor& F) { return FactorVals<doub
 
 // apply M^{-1} to R into Z once (tile-major n x ld blocks; stage entry point)
 void precond_apply_device(Context& C, const DevFactor& F, const double* R, double* Z, int64_t ld) {
-    int64_t l = launch_precond<double>(C, F, fp64_vals(F), F.n, R, Z, ld);
+    int64_t l = launch_precond<double>(C, F, fp64_vals(F), F.n, R, Z, ld, (int32_t)ld);
     C.kernels_launched += l;
 }
 
@@ -720,8 +755,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
     tm.loop.begin(C.stream);
     while (it < max_iters) {
         tm.spmm.begin(C.stream);
-        k_chunked<M_SPMM, T><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks, A.nchunks, aptr, aidx, aval, nullptr,
-                                                                   B.p, B.q, nullptr, ld, A.part);
+        launch_spmm<T>(C, n, A.chunks, A.nchunks, A.grid, aptr, aidx, aval, B.p, B.q, ld, A.part, k);
         tm.spmm.end(C.stream);
         k_colred_final<<<cg, 256, 0, C.stream>>>(ld, (int)A.grid.x, A.part, S.pq);
         k_cols_alpha<<<cg, 256, 0, C.stream>>>(ld, S);
@@ -825,6 +859,12 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
 
+    // a narrow solve leaves the padding columns of its gathered outputs untouched: start them at zero
+    if (TILE > NARROW_W && k <= NARROW_W) {
+        SSP_CUDA(cudaMemsetAsync(z, 0, sizeof(double) * total, C.stream));
+        SSP_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * total, C.stream));
+        SSP_CUDA(cudaMemsetAsync(q, 0, sizeof(double) * total, C.stream));
+    }
     PcgTimers tm;
     EventPairs ev_resid;
     int32_t it = 0;
@@ -833,7 +873,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         Precond P;
         int64_t pc_launches = 0;
         if (read_i64(C, S.nactive) > 0) {
-            build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, P, pc_launches);
+            build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P, pc_launches);
             it = pcg_solve<double>(C, n, k, ld, A, lap_ptr, lap_idx, lap_val, P, pc_launches,
                                    PcgBufs<double>{x, r, z, p, q}, S, R, opt.max_iters, opt, tm);
         }
@@ -876,7 +916,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, MIXED_INNER_REDUCTION, S.thr, Si);
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
-                if (!P32.exec) build_precond_graph<float>(C, F, V32, n, r32, z32, ld, P32, pc32);
+                if (!P32.exec) build_precond_graph<float>(C, F, V32, n, r32, z32, ld, k, P32, pc32);
                 int32_t cap = opt.max_iters - it;
                 if (first_its >= 0)
                     cap = std::min(cap, std::max(MIXED_MIN_ROUND_ITERS, MIXED_ROUND_ITER_FACTOR * first_its));
@@ -895,7 +935,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, 0.0, S.thr, Si);
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
-                if (!P64.exec) build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, P64, pc64);
+                if (!P64.exec) build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P64, pc64);
                 its = pcg_solve<double>(C, n, k, ld, A, lap_ptr, lap_idx, lap_val, P64, pc64,
                                         PcgBufs<double>{e64, r, z, p, q}, Si, R, opt.max_iters - it, opt, tm);
                 k_add_into<double><<<grid_for(total, 256, 148 * 16), 256, 0, C.stream>>>(total, e64, x);
@@ -907,9 +947,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
             rep.refinements++;
             // true residual with the FP64 matrix and FP64 x
             ev_resid.begin(C.stream);
-            k_chunked<M_SPMM, double><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks, A.nchunks, lap_ptr, lap_idx,
-                                                                            lap_val, nullptr, x, q, nullptr, ld,
-                                                                            nullptr);
+            launch_spmm<double>(C, n, A.chunks, A.nchunks, A.grid, lap_ptr, lap_idx, lap_val, x, q, ld, nullptr, k);
             ev_resid.end(C.stream);
             k_true_resid<<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
                 n, k, Y, mean, q, r, R.rows_per_blk, ld, R.part);
@@ -932,8 +970,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         }
     }
     // true relative residual ||(Y - mean) - A x|| / ||Y - mean||
-    k_chunked<M_SPMM, double><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks, A.nchunks, lap_ptr, lap_idx, lap_val,
-                                                                    nullptr, x, q, nullptr, ld, nullptr);
+    launch_spmm<double>(C, n, A.chunks, A.nchunks, A.grid, lap_ptr, lap_idx, lap_val, x, q, ld, nullptr, k);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
     R.run<OP_SQDIFF_CENTERED, double>(Y, q, relres, mean);

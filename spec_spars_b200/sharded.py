@@ -17,7 +17,7 @@ only one this package provides.
 import torch
 import torch.distributed as dist
 
-TILE = 8  # columns per PCG tile: shares are whole tiles so no rank pays for a partial tile twice
+TILE = 32  # columns per PCG tile (SSP_TILE): shares are whole tiles so no rank pays for a partial tile twice
 
 
 def column_range(k, world, rank, align=TILE):

@@ -162,3 +162,17 @@ def test_edge_list_to_matrix_market(ssp, tmp_path):
     with pytest.raises(ssp.SspError) as e:
         ssp.edge_list_to_matrix_market(tmp_path / "missing.txt", dst, 1.0)
     assert e.value.code == -6
+
+
+def test_rmat_generator(ssp):
+    """R-MAT (the scale-22 configuration, run small): symmetric, one connected component (the LCC),
+    FP32-rounded lognormal weights, deterministic for a seed."""
+    import scipy.sparse.csgraph as csg
+    g = ssp.gen_rmat(11, 16, 0.57, 0.19, 0.19, 3)
+    A = g.to_scipy()
+    assert abs(A - A.T).max() == 0 and A.diagonal().max() == 0
+    assert csg.connected_components(A, directed=False)[0] == 1
+    assert np.all(g.values == g.values.astype(np.float32).astype(np.float64)) and g.values.min() > 0
+    assert np.diff(g.colptr).max() > 20 * np.diff(g.colptr).mean()  # skewed degrees
+    h = ssp.gen_rmat(11, 16, 0.57, 0.19, 0.19, 3)
+    assert np.array_equal(g.rowidx, h.rowidx) and np.array_equal(g.values, h.values)

@@ -254,6 +254,19 @@ def test_sparsify_config_grid2d_100(ssp, ora, ctx):
     assert st["m_out"] == int(o["keep"].sum())
 
 
+def test_sparsify_config_rmat_small(ssp, ora, ctx):
+    """The R-MAT configuration (power-law LCC, lognormal weights, eps 0.3) at scale 12: hubs of degree
+    > 1000 take the long-row path of every gather kernel.  End to end against the oracle."""
+    G = ssp.gen_rmat(12, 16, 0.57, 0.19, 0.19, 3)
+    prm = ssp.SparsifierParameters.baseline(0.3, pcg_tol=1e-8)
+    H, st = ctx.sparsify(G, prm)
+    o = _oracle_pipeline(ora, ssp, G, prm, st["factor_max_degree_used"])
+    assert st["pcg_max_relres"] < 1e-7 and st["m_in"] == len(o["keep"])
+    assert st["m_out"] == int(o["keep"].sum()) and st["m_out"] < st["m_in"]
+    Hm, Ho = H.to_scipy(), sp.csc_matrix((o["H"][2], o["H"][1], o["H"][0]), shape=(G.n, G.n))
+    assert (Hm != 0).nnz == (Ho != 0).nnz and abs(Hm - Ho).max() <= 1e-12 * abs(Ho).max()
+
+
 def test_spectral_check_dense_graph(ssp, ora, ctx):
     """A graph that actually gets sparsified: K_300 with eps = 0.7 and unbiased w/p reweighting.
     Every probe x^T L_H x / x^T L_G x and every eigenvalue of L_G^+ L_H must lie within 1 +- eps."""

@@ -63,7 +63,7 @@ class OracleStages:
 
 def _params(ssp):
     prm = ssp.SparsifierParameters.baseline(1.5, pcg_tol=1e-10)  # large eps: some edges are dropped
-    prm.jl_dim_override = 37  # not a multiple of the 8-column tile: the last share is ragged
+    prm.jl_dim_override = 37  # not a multiple of the column tile: the last share is ragged
     prm.factor_max_degree = 0
     prm.dense_threshold = 64
     return prm
@@ -91,15 +91,15 @@ def _worker(rank, world, port, outdir):
 
 
 def test_column_range_partitions_k():
-    from spec_spars_b200.sharded import column_range
+    from spec_spars_b200.sharded import column_range, TILE
     for k in (1, 7, 8, 37, 885, 1327):
         for world in (1, 2, 3, 8, 200):
             shares = [column_range(k, world, r) for r in range(world)]
             assert shares[0][0] == 0 and shares[-1][1] == k
             for (a0, a1), (b0, b1) in zip(shares, shares[1:]):
                 assert a1 == b0 and a0 <= a1
-            tiles = [(b - a + 7) // 8 for a, b in shares]
-            assert all(a % 8 == 0 for a, b in shares if b > a)
+            tiles = [(b - a + TILE - 1) // TILE for a, b in shares]
+            assert all(a % TILE == 0 for a, b in shares if b > a)
             assert max(tiles) - min(tiles) <= 1
     with pytest.raises(ValueError):
         column_range(10, 2, 2)
