@@ -27,6 +27,9 @@ WORKLOADS = {
     "grid2d_100": ("grid2d", dict(nx=100, ny=100), 0.5),
     "er_n100k_deg20": ("er", dict(n=100_000, avg_degree=20.0, wlo=0.5, whi=2.0, seed=1), 0.5),
     "er_n250k_deg20": ("er", dict(n=250_000, avg_degree=20.0, wlo=0.5, whi=2.0, seed=1), 0.5),
+    # 3-D 7-point grids with log-uniform weights in [1e-3, 1e3] (the ill-conditioned mesh configuration)
+    "grid3d_64": ("grid3d", dict(nx=64, ny=64, nz=64, lo=-3.0, hi=3.0, seed=2), 0.5),
+    "grid3d_128": ("grid3d", dict(nx=128, ny=128, nz=128, lo=-3.0, hi=3.0, seed=2), 0.5),
 }
 PCG_TOL = 1e-8
 
@@ -37,6 +40,8 @@ def make_graph(S, name, rank=0):
     if kind == "er":
         kw["seed"] = kw["seed"] + rank
         return S.gen_er(kw["n"], kw["avg_degree"], kw["wlo"], kw["whi"], kw["seed"]), eps
+    if kind == "grid3d":
+        return S.gen_grid3d(kw["nx"], kw["ny"], kw["nz"], kw["lo"], kw["hi"], kw["seed"]), eps
     return S.gen_grid2d(kw["nx"], kw["ny"]), eps
 
 
@@ -106,9 +111,11 @@ def peaks():
         return 6650.0, "fallback"
 
 
-# DRAM bytes per (Laplacian nonzero, 8-column tile) of one FP64 SpMM launch, from the ncu capture of
-# ER n=250K, k=256 (profiles/k_chunked_spmm_er_n250k_k256.md: 3.86 GB / (5.25M nonzeros x 32 tiles))
-SPMM_TRAFFIC_PER_NNZ_TILE = 3.86e9 / (5.25e6 * 32)
+# DRAM bytes per (Laplacian nonzero, 32-column tile) of one FP64 SpMM launch at ER n=1M, from the ncu
+# capture of a one-tile solve of that graph (profiles/k_chunked_spmm_er_n1M_k32.md: 4.31 GB for
+# nnz(L_G) = 21.0M nonzeros x 1 tile); every tile of a full launch does the same work
+SPMM_TRAFFIC_PER_NNZ_TILE = 4.31e9 / 21.0e6
+SPMM_TILE = 32
 
 
 def spmm_bytes(n, nnz_lap, k, s=8):
@@ -412,7 +419,7 @@ def main():
     traffic = None
     if kern.startswith("spmm") and vs == 8:
         # scaled from the small-case capture by the units one launch processes
-        traffic = SPMM_TRAFFIC_PER_NNZ_TILE * st["nnz_laplacian"] * math.ceil(k / 8)
+        traffic = SPMM_TRAFFIC_PER_NNZ_TILE * st["nnz_laplacian"] * math.ceil(k / SPMM_TILE)
     roof = {"kernel": kern, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_source": src,
             "algorithmic_bytes_per_launch": byts, "avg_launch_ms": kms,
@@ -434,7 +441,7 @@ def main():
             "kept_fraction": st["m_out"] / st["m_in"], "pcg_iters_max": st["pcg_max_iters_used"],
             "pcg_iters_mean": st["pcg_mean_iters"], "pcg_max_relres": st["pcg_max_relres"],
             "pcg_refinements": st["pcg_refinements"], "pcg_fp64_rounds": st["pcg_fp64_rounds"],
-            "factor_nnz": st["nnz_factor"], "factor_levels": st["factor_levels"],
+            "spmm_slabs": st["spmm_slabs"], "factor_nnz": st["nnz_factor"], "factor_levels": st["factor_levels"],
             "roofline": roof, "clocks": clocks.summary(), "e2e": e2e}
     if args.precision == "fp64" and not args.no_mixed:
         # the same workload with FP32 inner solves inside FP64 refinement (same PCG tolerance), beside the
@@ -457,7 +464,7 @@ def main():
         line["mixed_precision"] = {"value": m * world / (mms / 1000.0), "unit": "edges/s", "ms_per_step": mms,
                                    "dtype": "f32 inner PCG, f64 dots + refinement",
                                    "pcg_max_relres": stm["pcg_max_relres"], "pcg_iters_max": stm["pcg_max_iters_used"],
-                                   "pcg_refinements": stm["pcg_refinements"],
+                                   "pcg_refinements": stm["pcg_refinements"], "spmm_slabs": stm["spmm_slabs"],
                                    "spmm_avg_ms": stm["ms_spmm"] / max(1, stm["n_spmm"])}
         prm.precision = S.SSP_PRECISION_FP64
     if rank == 0 and not args.no_cpu_baseline:

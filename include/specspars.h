@@ -141,6 +141,7 @@ typedef struct {
     double ms_autotune;             /* device time spent choosing it (included in ms_factor) */
     int32_t pcg_refinements;        /* SSP_PRECISION_MIXED: FP64 refinement rounds (0 in FP64 mode) */
     int32_t pcg_fp64_rounds;        /* ... of which ran an FP64 inner solve after FP32 stopped contracting */
+    int32_t spmm_slabs;             /* column slabs of the PCG's Laplacian product (1 = one pass) */
 } ssp_stats;
 
 typedef struct {
@@ -167,6 +168,7 @@ typedef struct {
     int64_t factor_max_degree_used;
     int32_t refinements;     /* SSP_PRECISION_MIXED: FP64 refinement rounds */
     int32_t fp64_rounds;
+    int32_t spmm_slabs;      /* column slabs of the Laplacian product (1 = one pass) */
 } ssp_solve_report;
 
 /* ---- errors ---- */

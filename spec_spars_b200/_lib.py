@@ -72,7 +72,8 @@ class _Stats(ctypes.Structure):
                 ("kernels_launched", ctypes.c_int64), ("ms_spmm", ctypes.c_double), ("n_spmm", ctypes.c_int64),
                 ("ms_precond", ctypes.c_double), ("n_precond", ctypes.c_int64), ("nnz_laplacian", ctypes.c_int64),
                 ("factor_max_degree_used", ctypes.c_int64), ("ms_autotune", ctypes.c_double),
-                ("pcg_refinements", ctypes.c_int32), ("pcg_fp64_rounds", ctypes.c_int32)]
+                ("pcg_refinements", ctypes.c_int32), ("pcg_fp64_rounds", ctypes.c_int32),
+                ("spmm_slabs", ctypes.c_int32)]
 
 
 class _SolveOpts(ctypes.Structure):
@@ -86,7 +87,7 @@ class _SolveReport(ctypes.Structure):
                 ("max_relres", ctypes.c_double), ("not_converged", ctypes.c_int32),
                 ("nnz_factor", ctypes.c_int64), ("factor_levels", ctypes.c_int32), ("ms_factor", ctypes.c_double),
                 ("ms_solve", ctypes.c_double), ("factor_max_degree_used", ctypes.c_int64),
-                ("refinements", ctypes.c_int32), ("fp64_rounds", ctypes.c_int32)]
+                ("refinements", ctypes.c_int32), ("fp64_rounds", ctypes.c_int32), ("spmm_slabs", ctypes.c_int32)]
 
 
 class _ServerOpts(ctypes.Structure):

@@ -273,6 +273,7 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
             st->ms_autotune = ms_tune;
             st->pcg_refinements = rep.refinements;
             st->pcg_fp64_rounds = rep.fp64_rounds;
+            st->spmm_slabs = rep.spmm_slabs;
         }
         return;
     }
@@ -363,6 +364,7 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
         st->ms_autotune = ms_tune;
         st->pcg_refinements = rep.refinements;
         st->pcg_fp64_rounds = rep.fp64_rounds;
+        st->spmm_slabs = rep.spmm_slabs;
     }
     if (prm->verbose) {
         fprintf(stderr, "[ssp] n=%lld m=%lld k=%d nnz(L)=%lld levels=%d (sparse %zu, dense %d, truncated %lld, compactions %d) "
@@ -452,6 +454,7 @@ static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t 
         rep->factor_max_degree_used = deg_used;
         rep->refinements = pr.refinements;
         rep->fp64_rounds = pr.fp64_rounds;
+        rep->spmm_slabs = pr.spmm_slabs;
     }
     if (pr.not_converged > 0)
         throw Error(SSP_ERR_NOT_CONVERGED, "solver did not converge: " + std::to_string(pr.not_converged) +

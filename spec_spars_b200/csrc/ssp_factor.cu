@@ -586,6 +586,106 @@ __global__ void k_level_prep(int64_t* ctr) {
     ctr[C_MAXLIVE] = 0;
 }
 
+// ---------------------------------------------------------------- solve schedule
+// Thin-level runs (DevFactor::SolveRun) and their step schedules.  Row t of a run depends, in the forward
+// solve, on the rows of the same run that its L row reads (lower levels), and in the backward solve on the
+// rows its L column reaches (higher levels); its step is one more than the deepest of those (0 if none).
+// Steps list the run's storage rows by (step, storage row).  Built on the host from the runs' own rows.
+static void build_solve_schedule(Context& C, DevFactor& out, const std::vector<int64_t>& lp, const std::string& tag) {
+    const int32_t NL = out.num_levels;
+    out.runs.clear();
+    for (int32_t l = 0; l < NL;) {
+        int32_t r = l;
+        while (r < NL && lp[r + 1] - lp[r] <= THIN_ROWS) r++;
+        if (r - l >= 2) {
+            out.runs.push_back({l, r, 0, 0, 0, 0});
+            l = r;
+        } else {
+            l++;
+        }
+    }
+    if (out.runs.empty()) return;
+    // the runs' vertices, row pointers and entries
+    struct Host {
+        std::vector<int32_t> vert, fidx, bidx;
+        std::vector<int64_t> fptr, bptr;
+    };
+    std::vector<Host> h(out.runs.size());
+    auto get = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) SSP_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, C.stream));
+    };
+    for (size_t u = 0; u < out.runs.size(); u++) {
+        const int64_t r0 = lp[out.runs[u].l0], r1 = lp[out.runs[u].l1];
+        h[u].vert.resize(r1 - r0);
+        h[u].fptr.resize(r1 - r0 + 1);
+        h[u].bptr.resize(r1 - r0 + 1);
+        get(h[u].vert.data(), out.level_rows + r0, sizeof(int32_t) * (r1 - r0));
+        get(h[u].fptr.data(), out.prow_ptr + r0, sizeof(int64_t) * (r1 - r0 + 1));
+        get(h[u].bptr.data(), out.pcol_ptr + r0, sizeof(int64_t) * (r1 - r0 + 1));
+    }
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    for (auto& x : h) {
+        x.fidx.resize(x.fptr.back() - x.fptr.front());
+        x.bidx.resize(x.bptr.back() - x.bptr.front());
+        get(x.fidx.data(), out.prow_idx + x.fptr.front(), sizeof(int32_t) * x.fidx.size());
+        get(x.bidx.data(), out.pcol_idx + x.bptr.front(), sizeof(int32_t) * x.bidx.size());
+    }
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    std::vector<int32_t> fsched, bsched, fstep{0}, bstep{0};
+    std::vector<int32_t> where(out.n, -1);  // vertex -> local row of the run being scheduled
+    // depth of every local row, then a counting sort by depth
+    auto schedule = [&](const Host& x, int64_t r0, bool fwd, std::vector<int32_t>& sched, std::vector<int32_t>& step,
+                        int32_t& s0, int32_t& s1) {
+        const int32_t R = (int32_t)x.vert.size();
+        const auto& ptr = fwd ? x.fptr : x.bptr;
+        const auto& idx = fwd ? x.fidx : x.bidx;
+        std::vector<int32_t> d(R, 0);
+        int32_t depth = 0;
+        for (int32_t k = 0; k < R; k++) {
+            const int32_t t = fwd ? k : R - 1 - k;  // dependencies come first in this order
+            int32_t dt = 0;
+            for (int64_t e = ptr[t] - ptr[0]; e < ptr[t + 1] - ptr[0]; e++) {
+                const int32_t j = where[idx[e]];
+                if (j < 0) continue;
+                if (fwd ? j >= t : j <= t) throw Error(SSP_ERR_INVALID, "factor: solve schedule out of order");
+                dt = std::max(dt, d[j] + 1);
+            }
+            d[t] = dt;
+            depth = std::max(depth, dt + 1);
+        }
+        std::vector<int32_t> cnt(depth + 1, 0);
+        for (int32_t t = 0; t < R; t++) cnt[d[t] + 1]++;
+        for (int32_t s = 0; s < depth; s++) cnt[s + 1] += cnt[s];
+        const size_t base = sched.size();
+        sched.resize(base + R);
+        for (int32_t t = 0; t < R; t++) sched[base + cnt[d[t]]++] = (int32_t)(r0 + t);
+        s0 = (int32_t)step.size() - 1;
+        int32_t acc = (int32_t)base;
+        std::vector<int32_t> sz(depth, 0);
+        for (int32_t t = 0; t < R; t++) sz[d[t]]++;
+        for (int32_t s = 0; s < depth; s++) step.push_back(acc += sz[s]);
+        s1 = (int32_t)step.size() - 1;
+    };
+    for (size_t u = 0; u < out.runs.size(); u++) {
+        auto& run = out.runs[u];
+        const int64_t r0 = lp[run.l0];
+        for (int32_t t = 0; t < (int32_t)h[u].vert.size(); t++) where[h[u].vert[t]] = t;
+        schedule(h[u], r0, true, fsched, fstep, run.fs0, run.fs1);
+        schedule(h[u], r0, false, bsched, bstep, run.bs0, run.bs1);
+        for (int32_t v : h[u].vert) where[v] = -1;
+    }
+    auto put = [&](const std::vector<int32_t>& v, const char* name) {
+        int32_t* d = C.ws.get_t<int32_t>(tag + "_" + name, v.size());
+        SSP_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(int32_t) * v.size(), cudaMemcpyHostToDevice, C.stream));
+        return d;
+    };
+    out.fsched = put(fsched, "fsched");
+    out.fstep = put(fstep, "fstep");
+    out.bsched = put(bsched, "bsched");
+    out.bstep = put(bstep, "bstep");
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+}
+
 // ---------------------------------------------------------------- dense tail
 __global__ void k_collect_live(int64_t n, const int32_t* level, int32_t* rem, int64_t* cnt) {
     for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
@@ -1300,6 +1400,7 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
         build(out.col_ptr, out.col_idx, out.col_val, "pcol", &out.pcol_ptr, &out.pcol_idx, &out.pcol_val,
               &out.bchunk, out.bchunk_lvl);
     }
+    build_solve_schedule(C, out, lp, tag);
 }
 
 }  // namespace ssp

@@ -199,9 +199,15 @@ void read_i64s(Context& C, const int64_t* d_ptr, int64_t* host, int cnt);
 
 // Row-aligned chunks of a CSR row range: each holds at most CHUNK_CAP entries and CHUNK_ROWS rows
 // (a longer row is a chunk of its own).  Appends chunk starts for rows [r0, r1).
-constexpr int CHUNK_CAP = 256;
+#ifndef SSP_CHUNK_CAP
+#define SSP_CHUNK_CAP 256
+#endif
+constexpr int CHUNK_CAP = SSP_CHUNK_CAP;
 constexpr int CHUNK_ROWS = 32;
 void make_chunks(const std::vector<int64_t>& ptr, int32_t r0, int32_t r1, std::vector<int32_t>& starts);
+void make_chunks(const int64_t* ptr, int32_t r0, int32_t r1, std::vector<int32_t>& starts);
+// L2 share (MB) of one column slab of the PCG's Laplacian product (SSP_SPMM_SLAB_MB; 0 = one pass)
+double spmm_slab_mb();
 
 // Segmented sort of int32 keys in place (ascending).  Segments [start[i], start[i]+len[i]).
 void segsort_i32(Context& C, int32_t* keys, const int64_t* seg_start, const int32_t* seg_len, int64_t nseg,
@@ -278,7 +284,23 @@ struct DevFactor {
     std::vector<int64_t> frontier_sizes;  // rows of each sparse level
     int32_t compactions = 0;
     int64_t truncated_rows = 0;           // vertices left to the diagonal final level
+    // Solve schedule.  Maximal runs of consecutive thin levels (at most THIN_ROWS rows each, two or more
+    // levels) are solved by one launch that walks "steps": the run's rows grouped by their dependency depth
+    // inside the run (a row's depth is one more than the deepest row of the same run it reads), which is
+    // often far smaller than the run's level count (the dense tail eliminates one vertex per level).  The
+    // factor and its levels are unchanged; only the order rows are solved in differs, and each row's own
+    // sum is formed the same way whatever step it lands in.
+    struct SolveRun {
+        int32_t l0, l1;  // levels [l0, l1)
+        int32_t fs0, fs1, bs0, bs1;  // step ranges of the forward and backward schedules
+    };
+    std::vector<SolveRun> runs;
+    int32_t* fsched = nullptr;  // storage rows of all runs, forward step order
+    int32_t* fstep = nullptr;   // step pointers into fsched
+    int32_t* bsched = nullptr;
+    int32_t* bstep = nullptr;
 };
+constexpr int THIN_ROWS = 64;  // a level with at most this many rows is "thin"
 struct FactorOptions {
     uint64_t seed = 0;
     int64_t dense_threshold = 4096;
@@ -311,6 +333,7 @@ struct PcgReport {
     int32_t iters_run = 0;   // iterations of the loop (all columns)
     int32_t refinements = 0; // mixed precision: outer rounds (true FP64 residual recomputations)
     int32_t fp64_rounds = 0; // mixed precision: rounds that fell back to an FP64 inner solve
+    int32_t spmm_slabs = 1;  // column slabs of the Laplacian product
     double ms_resid = 0;     // mixed precision: device time of the FP64 residual products
     int64_t n_resid = 0;
 };

@@ -21,6 +21,7 @@
 // that goes straight to the outer threshold.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "ssp_internal.cuh"
 
@@ -40,6 +41,10 @@ constexpr double MIXED_MIN_CONTRACTION = 1e-2;
 // round that runs into the cap hands the rest to FP64
 constexpr int MIXED_ROUND_ITER_FACTOR = 2;
 constexpr int MIXED_MIN_ROUND_ITERS = 20;
+// the first FP32 round may take at most max_iters / MIXED_FIRST_ROUND_DIV iterations (at least
+// MIXED_MIN_ROUND_ITERS): an FP32 recurrence that stalls above its target (3-D grid, n = 64^3, weights over
+// six decades: still at relative residual 0.26 after 400 iterations) then leaves the rest to FP64 rounds
+constexpr int MIXED_FIRST_ROUND_DIV = 4;
 
 __host__ __device__ __forceinline__ int64_t tm_off(int64_t n, int64_t r, int64_t c) { return tile_off(n, r, c); }
 
@@ -358,51 +363,68 @@ __global__ void k_cols_outer(int64_t ld, const int32_t* __restrict__ inner_iters
     }
 }
 
-// ---------------------------------------------------------------- SpMM and triangular solves
-// Warp per row; lane = slot * W + column, W = the columns handled (TILE, or 8 when at most 8 are real).
-// xt points at the tile's slab (row stride TILE values).  Two independent gathers per lane per step keep
-// more loads in flight.  Lanes of padding columns (past the k real ones, in the last tile) are not live and
-// load nothing.
-template <class T, int W>
-__device__ __forceinline__ T warp_row_gather(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                             const T* __restrict__ val, int64_t row, const T* xt, int lane,
-                                             bool live) {
-    constexpr int SLOTS_W = 32 / W;
-    const int slot = lane / W, c = lane % W;
-    const int64_t e = live ? ptr[row + 1] : 0;
-    T acc0 = 0, acc1 = 0;
-    int64_t p = live ? ptr[row] + slot : 0;
-    for (; p + SLOTS_W < e; p += 2 * SLOTS_W) {
-        const int32_t i0 = idx[p], i1 = idx[p + SLOTS_W];
-        const T v0 = val[p], v1 = val[p + SLOTS_W];
-        acc0 += v0 * xt[(int64_t)i0 * TILE + c];
-        acc1 += v1 * xt[(int64_t)i1 * TILE + c];
+// ---------------------------------------------------------------- the iteration loop on the device
+// The PCG iterations after the first run as the body of a CUDA-graph WHILE node: the body advances the
+// iteration counter on the device, runs the convergence check, and k_loop_ctl keeps the loop going only while
+// some column is active and fewer than max_iters iterations have run, so the loop ends by itself without a
+// host round trip per iteration.
+__global__ void k_it_set(int32_t* it, int32_t v) { *it = v; }
+__global__ void k_it_next(int32_t* it) { *it += 1; }
+
+__global__ void k_cols_check_at(int64_t ld, const int32_t* __restrict__ it, ColState S) {
+    const int32_t i = *it;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x) {
+        if (!S.active[c]) continue;
+        S.iters[c] = i;
+        if (sqrt(S.rr[c]) <= S.thr[c]) S.active[c] = 0;
+        else atomicAdd((unsigned long long*)S.nactive, 1ull);
     }
-    if (p < e) acc0 += val[p] * xt[(int64_t)idx[p] * TILE + c];
-    T acc = acc0 + acc1;
-#pragma unroll
-    for (int o = W; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    return acc;
 }
 
+__global__ void k_loop_ctl(cudaGraphConditionalHandle h, const int64_t* __restrict__ nactive,
+                           const int32_t* __restrict__ it, int32_t max_iters) {
+    cudaGraphSetConditional(h, (*nactive > 0 && *it < max_iters) ? 1u : 0u);
+}
+
+struct LoopGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~LoopGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+// ---------------------------------------------------------------- SpMM and triangular solves
+// Warp per row; lane = slot * W + column, W = the columns handled (TILE, or 8 when at most 8 are real).
 // ---------------------------------------------------------------- chunked gather (SpMM-shaped work)
 // A chunk is a run of consecutive stored rows with at most CHUNK_CAP entries and CHUNK_ROWS rows (or
 // one longer row).  Each warp owns whole chunks: it stages the chunk's (index, value) pairs in its own
 // shared-memory slice with coalesced streaming loads (the matrix is read once per tile and should not
 // evict the gathered slab from L2), then every (row, column) lane pair sums its row with independent
-// gathers from the tile slab.  Warps never wait for each other.  Modes: SpMM (+ p.q partials),
-// forward solve, backward solve.
-enum { M_SPMM = 0, M_FWD = 1, M_BWD = 2 };
+// gathers from the tile slab.  Warps never wait for each other.  Modes: SpMM (+ p.q partials), SpMM
+// adding into its output (the second and later column slabs of the matrix), forward solve, backward solve.
+enum { M_SPMM = 0, M_FWD = 1, M_BWD = 2, M_SPMM_ACC = 3 };
 constexpr int CH_THREADS = 256;
+// independent gathers in flight per lane in the chunk kernels (powers of two).  Measured on B200 at ER n = 1M,
+// k = 1327: 8 for the SpMM takes it from 48 to 38 ms; the level solves are faster with 4 (19 against 22 ms).
+#ifndef SSP_GATHER_UNROLL_SPMM
+#define SSP_GATHER_UNROLL_SPMM 8
+#endif
+#ifndef SSP_GATHER_UNROLL_SOLVE
+#define SSP_GATHER_UNROLL_SOLVE 4
+#endif
 constexpr int CH_WARPS = CH_THREADS / 32;
 
 template <int MODE, class T>
 __device__ __forceinline__ void chunk_epilogue(T* out, const T* aux, const T* xt, int64_t toff, int64_t v, int col,
-                                               T acc, double& dot) {
+                                               T acc, double& dot, bool want_dot) {
     const int64_t o = toff + v * TILE + col;
-    if (MODE == M_SPMM) {
-        out[o] = acc;
-        dot += (double)acc * (double)xt[v * TILE + col];
+    if (MODE == M_SPMM || MODE == M_SPMM_ACC) {
+        // q streams out (evict-first), so it does not push the gathered slab out of L2
+        if (MODE == M_SPMM_ACC) acc += __ldcs(out + o);
+        __stcs(out + o, acc);
+        if (want_dot) dot += (double)acc * (double)xt[v * TILE + col];
     } else if (MODE == M_FWD) {
         out[o] = aux[o] - acc;
     } else {
@@ -432,6 +454,8 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
     T* sv = s_val[w];
     int32_t* sp = s_ptr[w];
     constexpr int SLOTS_W = 32 / W;
+    constexpr bool SPMM = MODE == M_SPMM || MODE == M_SPMM_ACC;
+    const bool want_dot = SPMM && part != nullptr;
     double dot = 0.0;  // SpMM: per-lane partial of p.q for column (lane % W)
     for (int32_t c = blockIdx.x * CH_WARPS + w; c < nchunks; c += gridDim.x * CH_WARPS) {
         const int32_t r0 = cstart[c], r1 = cstart[c + 1];
@@ -449,18 +473,28 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
                 const int32_t rr = pr / W, col = pr % W;
                 const bool live = t * TILE + col < kcols;
                 const int32_t q0 = sp[rr], q1 = live ? sp[rr + 1] : q0;
-                T a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+                // GATHER_UNROLL independent accumulators, summed as a pairwise tree
+                constexpr int GATHER_UNROLL = SPMM ? SSP_GATHER_UNROLL_SPMM : SSP_GATHER_UNROLL_SOLVE;
+                T a[GATHER_UNROLL];
+#pragma unroll
+                for (int u = 0; u < GATHER_UNROLL; u++) a[u] = 0;
                 int32_t q = q0;
-                for (; q + 3 < q1; q += 4) {
-                    a0 += sv[q] * xt[(int64_t)si[q] * TILE + col];
-                    a1 += sv[q + 1] * xt[(int64_t)si[q + 1] * TILE + col];
-                    a2 += sv[q + 2] * xt[(int64_t)si[q + 2] * TILE + col];
-                    a3 += sv[q + 3] * xt[(int64_t)si[q + 3] * TILE + col];
+                for (; q + GATHER_UNROLL - 1 < q1; q += GATHER_UNROLL) {
+#pragma unroll
+                    for (int u = 0; u < GATHER_UNROLL; u++) a[u] += sv[q + u] * xt[(int64_t)si[q + u] * TILE + col];
                 }
-                for (; q < q1; q++) a0 += sv[q] * xt[(int64_t)si[q] * TILE + col];
+                if (GATHER_UNROLL > 4 && q + 3 < q1) {  // short rows (a slab's share of a row) still get 4 in flight
+#pragma unroll
+                    for (int u = 0; u < 4; u++) a[u] += sv[q + u] * xt[(int64_t)si[q + u] * TILE + col];
+                    q += 4;
+                }
+                for (; q < q1; q++) a[0] += sv[q] * xt[(int64_t)si[q] * TILE + col];
+#pragma unroll
+                for (int h = 1; h < GATHER_UNROLL; h <<= 1)
+#pragma unroll
+                    for (int u = 0; u < GATHER_UNROLL; u += 2 * h) a[u] += a[u + h];
                 const int64_t row = r0 + rr;
-                chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[row] : row, col, (a0 + a1) + (a2 + a3),
-                                        dot);
+                chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[row] : row, col, a[0], dot, want_dot);
             }
             __syncwarp();
         } else {
@@ -477,10 +511,11 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
             T acc = a0 + a1;
 #pragma unroll
             for (int o = W; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane < W) chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[r0] : r0, col, acc, dot);
+            if (lane < W)
+                chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[r0] : r0, col, acc, dot, want_dot);
         }
     }
-    if (MODE == M_SPMM && part) {
+    if (want_dot) {
         s_red[threadIdx.x] = dot;
         __syncthreads();
         if (threadIdx.x < TILE) {
@@ -498,57 +533,85 @@ static int chunk_blocks(int32_t nchunks) {
     return std::max(1, std::min((nchunks + CH_WARPS - 1) / CH_WARPS, 148 * 6));
 }
 
-// Runs of thin levels: the k columns are independent, so one block per column tile can walk a run
-// of consecutive levels on its own, with only a block barrier between levels (its own writes are the
-// only values it reads back).  y is read and written in place: no read-only cache path.
+// Runs of thin levels: the k columns are independent, so one block per column tile walks the run's steps
+// (rows grouped by dependency depth, DevFactor::SolveRun) on its own, with only block barriers between
+// steps (its own writes are the only values it reads back).  y is read and written in place: no read-only
+// cache path.  A step with fewer rows than warps splits each row's entries over several warps (partial sums
+// added in warp order), so a lone row costs about one gather latency instead of one per entry.
 constexpr int RUN_THREADS = 512;
-constexpr int THIN_ROWS = 64;
+constexpr int RUN_WARPS = RUN_THREADS / 32;
 
-// rows[i] is the vertex of stored row i; ptr/idx/val are in storage order
+// one warp's share of a row: entries ptr[row] + sub * SLOTS_W + slot, stepping g * SLOTS_W, four in flight,
+// summed over the slots; every lane returns its column's partial
 template <class T, int W>
-__global__ void __launch_bounds__(RUN_THREADS) k_trsv_fwd_run(int64_t n, const int32_t* __restrict__ rows,
-                                                              const int32_t* __restrict__ lptr, int32_t l0,
-                                                              int32_t l1, const int64_t* __restrict__ ptr,
-                                                              const int32_t* __restrict__ idx,
-                                                              const T* __restrict__ val, const T* __restrict__ r,
-                                                              T* y, int32_t kcols) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = RUN_THREADS / 32;
-    const int64_t toff = (int64_t)blockIdx.x * n * TILE;
-    const bool live = (int64_t)blockIdx.x * TILE + lane % W < kcols;
-    for (int32_t l = l0; l < l1; l++) {
-        const int32_t s = lptr[l], e = lptr[l + 1];
-        for (int32_t i = s + warp; i < e; i += nwarp) {
-            const int64_t u = rows[i];
-            const T acc = warp_row_gather<T, W>(ptr, idx, val, i, y + toff, lane, live);
-            if (lane < W) {
-                const int64_t o = toff + u * TILE + lane;
-                y[o] = r[o] - acc;
-            }
-        }
-        __syncthreads();
+__device__ __forceinline__ T warp_row_share(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                            const T* __restrict__ val, int64_t row, const T* xt, int lane,
+                                            bool live, int sub, int g) {
+    constexpr int SLOTS_W = 32 / W;
+    const int slot = lane / W, c = lane % W;
+    const int64_t e = live ? ptr[row + 1] : 0;
+    const int64_t st = (int64_t)g * SLOTS_W;
+    int64_t p = live ? ptr[row] + (int64_t)sub * SLOTS_W + slot : 0;
+    T a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (; p + 3 * st < e; p += 4 * st) {
+        const int32_t i0 = idx[p], i1 = idx[p + st], i2 = idx[p + 2 * st], i3 = idx[p + 3 * st];
+        const T v0 = val[p], v1 = val[p + st], v2 = val[p + 2 * st], v3 = val[p + 3 * st];
+        a0 += v0 * xt[(int64_t)i0 * TILE + c];
+        a1 += v1 * xt[(int64_t)i1 * TILE + c];
+        a2 += v2 * xt[(int64_t)i2 * TILE + c];
+        a3 += v3 * xt[(int64_t)i3 * TILE + c];
     }
+    for (; p < e; p += st) a0 += val[p] * xt[(int64_t)idx[p] * TILE + c];
+    T acc = (a0 + a1) + (a2 + a3);
+#pragma unroll
+    for (int o = W; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    return acc;
 }
 
-template <class T, int W>
-__global__ void __launch_bounds__(RUN_THREADS) k_trsv_bwd_run(int64_t n, const int32_t* __restrict__ rows,
-                                                              const int32_t* __restrict__ lptr, int32_t l0,
-                                                              int32_t l1, const int64_t* __restrict__ ptr,
-                                                              const int32_t* __restrict__ idx,
-                                                              const T* __restrict__ val, const T* __restrict__ D,
-                                                              T* yz, int32_t kcols) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = RUN_THREADS / 32;
+// FWD: y_u = r_u - L[u, :] y (row form).  BWD: y_u = y_u / D_u (D_u != 0) - L[:, u]^T y (column form).
+template <class T, int W, bool FWD>
+__global__ void __launch_bounds__(RUN_THREADS) k_trsv_run(int64_t n, const int32_t* __restrict__ rows,
+                                                          const int32_t* __restrict__ sched,
+                                                          const int32_t* __restrict__ step, int32_t s0, int32_t s1,
+                                                          const int64_t* __restrict__ ptr,
+                                                          const int32_t* __restrict__ idx,
+                                                          const T* __restrict__ val, const T* __restrict__ aux, T* y,
+                                                          int32_t kcols) {
+    __shared__ T s_part[RUN_WARPS][W];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t toff = (int64_t)blockIdx.x * n * TILE;
     const bool live = (int64_t)blockIdx.x * TILE + lane % W < kcols;
-    for (int32_t l = l1 - 1; l >= l0; l--) {
-        const int32_t s = lptr[l], e = lptr[l + 1];
-        for (int32_t i = s + warp; i < e; i += nwarp) {
-            const int64_t u = rows[i];
-            const T acc = warp_row_gather<T, W>(ptr, idx, val, i, yz + toff, lane, live);
-            if (lane < W) {
-                const int64_t o = toff + u * TILE + lane;
-                const T d = D[u];
-                const T yu = yz[o];
-                yz[o] = (d != (T)0 ? yu / d : yu) - acc;
+    auto finish = [&](int32_t i, T acc) {
+        const int64_t u = rows[i];
+        const int64_t o = toff + u * TILE + lane;
+        if (FWD) {
+            y[o] = aux[o] - acc;
+        } else {
+            const T d = aux[u];
+            const T yu = y[o];
+            y[o] = (d != (T)0 ? yu / d : yu) - acc;
+        }
+    };
+    for (int32_t s = s0; s < s1; s++) {
+        const int32_t a = step[s], b = step[s + 1];
+        const int g = RUN_WARPS / max(1, b - a);  // warps per row
+        if (g <= 1) {
+            for (int32_t q = a + warp; q < b; q += RUN_WARPS) {
+                const int32_t i = sched[q];
+                const T acc = warp_row_share<T, W>(ptr, idx, val, i, y + toff, lane, live, 0, 1);
+                if (lane < W) finish(i, acc);
+            }
+        } else {
+            const int q = warp / g, sub = warp % g;
+            const bool mine = a + q < b;
+            const T acc = mine ? warp_row_share<T, W>(ptr, idx, val, sched[a + q], y + toff, lane, live, sub, g)
+                               : (T)0;
+            if (lane < W) s_part[warp][lane] = acc;
+            __syncthreads();
+            if (mine && sub == 0 && lane < W) {
+                T tot = s_part[warp][lane];
+                for (int u = 1; u < g; u++) tot += s_part[warp + u][lane];
+                finish(sched[a + q], tot);
             }
         }
         __syncthreads();
@@ -573,24 +636,6 @@ struct Precond {
     }
 };
 
-// level schedule: maximal runs of thin levels become one launch; wide levels launch on their own
-static std::vector<std::pair<int32_t, int32_t>> level_segments(const DevFactor& F) {
-    std::vector<std::pair<int32_t, int32_t>> seg;
-    int32_t l = 0;
-    while (l < F.num_levels) {
-        int32_t r = l;
-        while (r < F.num_levels && F.level_ptr[r + 1] - F.level_ptr[r] <= THIN_ROWS) r++;
-        if (r - l >= 2) {
-            seg.push_back({l, r});  // run [l, r)
-            l = r;
-        } else {
-            seg.push_back({l, l + 1});
-            l++;
-        }
-    }
-    return seg;
-}
-
 // columns a warp handles per row: all TILE, or 8 when no more than 8 are real (the autotuner's probe), so
 // that a warp still covers four rows per step; the padding columns of y must then be zero already
 constexpr int NARROW_W = 8;
@@ -600,12 +645,23 @@ static int64_t launch_precond_w(Context& C, const DevFactor& F, const FactorVals
                                 int64_t ld, int32_t kcols) {
     const int ntiles = (int)(ld / TILE);
     int64_t launches = 0;
-    const auto seg = level_segments(F);
+    // segments in level order: the thin-level runs (by index into F.runs) and single wide levels (-1)
+    std::vector<std::pair<int32_t, int32_t>> seg;  // (level, run or -1)
+    for (int32_t l = 0, u = 0; l < F.num_levels;) {
+        if (u < (int32_t)F.runs.size() && F.runs[u].l0 == l) {
+            seg.push_back({l, u});
+            l = F.runs[u++].l1;
+        } else {
+            seg.push_back({l++, -1});
+        }
+    }
     for (size_t i = 0; i < seg.size(); i++) {
-        const int32_t l0 = seg[i].first, l1 = seg[i].second;
-        if (l1 - l0 >= 2) {
-            k_trsv_fwd_run<T, W><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.level_ptr_d, l0, l1,
-                                                                     F.prow_ptr, F.prow_idx, V.prow_val, r, y, kcols);
+        const int32_t l0 = seg[i].first;
+        if (seg[i].second >= 0) {
+            const auto& run = F.runs[seg[i].second];
+            k_trsv_run<T, W, true><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.fsched, F.fstep, run.fs0,
+                                                                       run.fs1, F.prow_ptr, F.prow_idx, V.prow_val,
+                                                                       r, y, kcols);
         } else {
             const int32_t c0 = F.fchunk_lvl[l0], nc = F.fchunk_lvl[l0 + 1] - c0;
             if (nc == 0) continue;
@@ -617,10 +673,12 @@ static int64_t launch_precond_w(Context& C, const DevFactor& F, const FactorVals
         launches++;
     }
     for (size_t i = seg.size(); i-- > 0;) {
-        const int32_t l0 = seg[i].first, l1 = seg[i].second;
-        if (l1 - l0 >= 2) {
-            k_trsv_bwd_run<T, W><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.level_ptr_d, l0, l1,
-                                                                     F.pcol_ptr, F.pcol_idx, V.pcol_val, V.D, y, kcols);
+        const int32_t l0 = seg[i].first;
+        if (seg[i].second >= 0) {
+            const auto& run = F.runs[seg[i].second];
+            k_trsv_run<T, W, false><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.bsched, F.bstep,
+                                                                        run.bs0, run.bs1, F.pcol_ptr, F.pcol_idx,
+                                                                        V.pcol_val, V.D, y, kcols);
         } else {
             const int32_t c0 = F.bchunk_lvl[l0], nc = F.bchunk_lvl[l0 + 1] - c0;
             if (nc == 0) continue;
@@ -642,17 +700,185 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
     return launch_precond_w<T, TILE>(C, F, V, n, r, y, ld, kcols);
 }
 
-// SpMM q = A p (+ p.q partials into part when part != nullptr)
+// ---------------------------------------------------------------- SpMM plan
+// The Laplacian as the SpMM reads it.  When one tile of the gathered operand (n rows of TILE values) is
+// far larger than L2 and the matrix has no locality to exploit (random graphs: a row's neighbours are
+// anywhere), the columns are cut into nslabs equal ranges and the entries stored slab-major: slab b,
+// row i holds row i's entries with a column in slab b, in their stored order, at ptr[b n + i] ..
+// ptr[b n + i + 1].  The SpMM then makes one pass per slab (the first writes q, the others add into it),
+// and each pass gathers from a 1/nslabs share of the tile that stays resident in L2; the price is
+// 2 nslabs - 1 streaming passes over q instead of 1.  Measured on B200 (ER n = 1M, average degree 20,
+// 1327 columns, FP64): one pass 39.5 ms; 3, 4, 6, 8, 11 slabs 48.0, 52.6, 63.4, 75.4, 93.7 ms -- the extra q
+// passes cost more than the L2 hits save, so slabs are off unless SSP_SPMM_SLAB_MB (the L2 share of one
+// slab, MB) asks for them.
+constexpr int MAX_SLABS = 16;
+
+double spmm_slab_mb() {
+    const char* e = getenv("SSP_SPMM_SLAB_MB");
+    return e ? atof(e) : 0.0;
+}
+
+struct SpmmPlan {
+    int32_t nslabs = 1;
+    int64_t nnz = 0;
+    const int64_t* ptr = nullptr;  // nslabs * n + 1 row pointers
+    const int32_t* idx = nullptr;
+    const double* val = nullptr;  // FP64 values in this entry order
+    const int32_t* chunks[MAX_SLABS] = {};
+    int32_t nchunks[MAX_SLABS] = {};
+    dim3 grid;
+    double* part = nullptr;
+};
+
+// entries farther than `window` from the diagonal, summed per block into *far
+__global__ void k_far_count(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                            int64_t window, unsigned long long* far) {
+    __shared__ unsigned long long s_far;
+    if (threadIdx.x == 0) s_far = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    unsigned c = 0;
+    if (i < n)
+        for (int64_t e = ptr[i] + lane; e < ptr[i + 1]; e += 32) c += llabs((int64_t)idx[e] - i) > window;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0 && c) atomicAdd(&s_far, (unsigned long long)c);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_far) atomicAdd(far, s_far);
+}
+
+// per (slab, row) entry counts; one warp per row, lane b keeps slab b's count
+__global__ void k_slab_count(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                             int64_t slab_rows, int32_t nslabs, int32_t* __restrict__ cnt) {
+    const int lane = threadIdx.x & 31;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;
+    int32_t mine = 0;
+    for (int64_t e0 = ptr[i]; e0 < ptr[i + 1]; e0 += 32) {
+        const int64_t e = e0 + lane;
+        const int b = e < ptr[i + 1] ? (int)(idx[e] / slab_rows) : -1;
+        for (int s = 0; s < nslabs; s++) {
+            const int c = __popc(__ballot_sync(0xffffffffu, b == s));
+            if (lane == s) mine += c;
+        }
+    }
+    if (lane < nslabs) cnt[(int64_t)lane * n + i] = mine;
+}
+
+// stable partition of each row's entries into the slab-major copy
+__global__ void k_slab_fill(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                            const double* __restrict__ val, int64_t slab_rows, int32_t nslabs,
+                            const int64_t* __restrict__ sptr, int32_t* __restrict__ sidx,
+                            double* __restrict__ sval) {
+    const int lane = threadIdx.x & 31;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;
+    int64_t base = lane < nslabs ? sptr[(int64_t)lane * n + i] : 0;  // lane b: next free slot of slab b
+    const unsigned lt = (1u << lane) - 1u;
+    for (int64_t e0 = ptr[i]; e0 < ptr[i + 1]; e0 += 32) {
+        const int64_t e = e0 + lane;
+        const bool in = e < ptr[i + 1];
+        const int b = in ? (int)(idx[e] / slab_rows) : -1;
+        for (int s = 0; s < nslabs; s++) {
+            const unsigned bal = __ballot_sync(0xffffffffu, b == s);
+            const int64_t at = __shfl_sync(0xffffffffu, base, s);
+            if (b == s) {
+                const int64_t pos = at + __popc(bal & lt);
+                sidx[pos] = idx[e];
+                sval[pos] = val[e];
+            }
+            if (lane == s) base += __popc(bal);
+        }
+    }
+}
+
+static int32_t spmm_slab_count(Context& C, int64_t n, const int64_t* ptr, const int32_t* idx, int64_t nnz) {
+    const double mb = spmm_slab_mb();
+    if (!(mb > 0) || nnz == 0) return 1;
+    // slabs are cut for the FP64 operand (TILE doubles per row); FP32 solves use the same cut
+    const int64_t slab_rows = std::max<int64_t>(1, (int64_t)(mb * 1048576.0 / (TILE * sizeof(double))));
+    if (n <= slab_rows) return 1;
+    unsigned long long* far = C.ws.get_t<unsigned long long>("pcg_slab_far", 1);
+    SSP_CUDA(cudaMemsetAsync(far, 0, sizeof(unsigned long long), C.stream));
+    k_far_count<<<(unsigned)ceil_div<int64_t>(n * 32, 256), 256, 0, C.stream>>>(n, ptr, idx, slab_rows / 2, far);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+    // a matrix whose entries mostly sit near the diagonal already reuses L2 in a row sweep
+    if (read_i64(C, reinterpret_cast<const int64_t*>(far)) * 4 < nnz) return 1;
+    return (int32_t)std::min<int64_t>(MAX_SLABS, ceil_div<int64_t>(n, slab_rows));
+}
+
+static SpmmPlan make_spmm_plan(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx,
+                               const double* lap_val, int64_t ld) {
+    Workspace& W = C.ws;
+    SpmmPlan A;
+    A.nnz = read_i64(C, lap_ptr + n);
+    A.nslabs = spmm_slab_count(C, n, lap_ptr, lap_idx, A.nnz);
+    const int32_t m = A.nslabs;
+    std::vector<int64_t> hp((size_t)m * n + 1);
+    if (m == 1) {
+        A.ptr = lap_ptr;
+        A.idx = lap_idx;
+        A.val = lap_val;
+    } else {
+        const int64_t slab_rows = ceil_div<int64_t>(n, m);
+        int32_t* cnt = W.get_t<int32_t>("pcg_slab_cnt", (size_t)m * n);
+        int64_t* sptr = W.get_t<int64_t>("pcg_slab_ptr", (size_t)m * n + 1);
+        int32_t* sidx = W.get_t<int32_t>("pcg_slab_idx", A.nnz + 1);
+        double* sval = W.get_t<double>("pcg_slab_val", A.nnz + 1);
+        const unsigned blocks = (unsigned)ceil_div<int64_t>(n * 32, 256);
+        k_slab_count<<<blocks, 256, 0, C.stream>>>(n, lap_ptr, lap_idx, slab_rows, m, cnt);
+        SSP_CHECK_LAUNCH();
+        exclusive_scan_i32_to_i64(C, cnt, sptr, (int64_t)m * n, sptr + (int64_t)m * n);
+        k_slab_fill<<<blocks, 256, 0, C.stream>>>(n, lap_ptr, lap_idx, lap_val, slab_rows, m, sptr, sidx, sval);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched += 2;
+        A.ptr = sptr;
+        A.idx = sidx;
+        A.val = sval;
+    }
+    SSP_CUDA(cudaMemcpyAsync(hp.data(), A.ptr, sizeof(int64_t) * hp.size(), cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    std::vector<int32_t> all;
+    std::vector<size_t> off(m);
+    int32_t most = 0;
+    for (int32_t b = 0; b < m; b++) {
+        off[b] = all.size();
+        const size_t before = all.size();
+        make_chunks(hp.data() + (size_t)b * n, 0, (int32_t)n, all);
+        A.nchunks[b] = (int32_t)(all.size() - before);
+        most = std::max(most, A.nchunks[b]);
+        all.push_back((int32_t)n);
+    }
+    int32_t* d = W.get_t<int32_t>("pcg_achunks", all.size());
+    SSP_CUDA(cudaMemcpyAsync(d, all.data(), sizeof(int32_t) * all.size(), cudaMemcpyHostToDevice, C.stream));
+    for (int32_t b = 0; b < m; b++) A.chunks[b] = d + off[b];
+    const int bx = chunk_blocks(most);
+    A.grid = dim3((unsigned)bx, (unsigned)(ld / TILE));
+    A.part = W.get_t<double>("pcg_spmm_part", (size_t)bx * ld);
+    return A;
+}
+
+// SpMM q = A p over the plan's slabs (+ p.q partials into A.part when dot)
 template <class T>
-static void launch_spmm(Context& C, int64_t n, const int32_t* chunks, int32_t nchunks, dim3 grid, const int64_t* aptr,
-                        const int32_t* aidx, const T* aval, const T* p, T* q, int64_t ld, double* part,
-                        int32_t kcols) {
-    if (TILE > NARROW_W && kcols <= NARROW_W)
-        k_chunked<M_SPMM, T, NARROW_W><<<grid, CH_THREADS, 0, C.stream>>>(n, chunks, nchunks, aptr, aidx, aval, nullptr,
-                                                                           p, q, nullptr, ld, part, kcols);
-    else
-        k_chunked<M_SPMM, T, TILE><<<grid, CH_THREADS, 0, C.stream>>>(n, chunks, nchunks, aptr, aidx, aval, nullptr, p,
-                                                                       q, nullptr, ld, part, kcols);
+static void launch_spmm(Context& C, int64_t n, const SpmmPlan& A, const T* aval, const T* p, T* q, int64_t ld,
+                        bool dot, int32_t kcols) {
+    const bool narrow = TILE > NARROW_W && kcols <= NARROW_W;
+    for (int32_t b = 0; b < A.nslabs; b++) {
+        const int64_t* ptr = A.ptr + (int64_t)b * n;
+        double* part = dot && b == A.nslabs - 1 ? A.part : nullptr;
+#define SSP_SPMM_LAUNCH(MODE, W_)                                                                                  \
+    k_chunked<MODE, T, W_><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks[b], A.nchunks[b], ptr, A.idx, aval,    \
+                                                                 nullptr, p, q, nullptr, ld, part, kcols)
+        if (b == 0) {
+            if (narrow) SSP_SPMM_LAUNCH(M_SPMM, NARROW_W);
+            else SSP_SPMM_LAUNCH(M_SPMM, TILE);
+        } else {
+            if (narrow) SSP_SPMM_LAUNCH(M_SPMM_ACC, NARROW_W);
+            else SSP_SPMM_LAUNCH(M_SPMM_ACC, TILE);
+        }
+#undef SSP_SPMM_LAUNCH
+    }
 }
 
 template <class T>
@@ -710,14 +936,6 @@ struct EventPairs {
 };
 
 // ---------------------------------------------------------------- one PCG solve in one precision
-// The Laplacian split into row-aligned chunks, about one wave of blocks per tile.
-struct SpmmPlan {
-    const int32_t* chunks = nullptr;
-    int32_t nchunks = 0;
-    dim3 grid;
-    double* part = nullptr;
-};
-
 template <class T>
 struct PcgBufs {
     T* e;  // solution increment (zero on entry)
@@ -734,9 +952,16 @@ struct PcgTimers {
 // Runs PCG on A e = r for every column that S marks active (S.thr, S.active, S.nactive set by the
 // caller; e zero).  Returns the iterations of the loop.
 template <class T>
-static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const SpmmPlan& A, const int64_t* aptr,
-                         const int32_t* aidx, const T* aval, const Precond& P, int64_t pc_launches, PcgBufs<T> B,
-                         ColState& S, Reducer& R, int32_t max_iters, const PcgOptions& opt, PcgTimers& tm) {
+static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const SpmmPlan& A, const T* aval,
+                         const DevFactor& F, const FactorVals<T>& V,
+                         const Precond& P, int64_t pc_launches, PcgBufs<T> B, ColState& S, Reducer& R,
+                         int32_t max_iters, const PcgOptions& opt, PcgTimers& tm) {
+    // without a residual history or progress output the iterations after the first run on the device
+#ifdef SSP_HOST_PCG_LOOP
+    const bool device_loop = false;
+#else
+    const bool device_loop = !opt.history && !opt.verbose;
+#endif
     const int64_t ntiles = ld / TILE;
     const int64_t total = n * ld;
     const dim3 egrid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div<int64_t>(n * TILE, 256),
@@ -755,14 +980,14 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
     tm.loop.begin(C.stream);
     while (it < max_iters) {
         tm.spmm.begin(C.stream);
-        launch_spmm<T>(C, n, A.chunks, A.nchunks, A.grid, aptr, aidx, aval, B.p, B.q, ld, A.part, k);
+        launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, true, k);
         tm.spmm.end(C.stream);
         k_colred_final<<<cg, 256, 0, C.stream>>>(ld, (int)A.grid.x, A.part, S.pq);
         k_cols_alpha<<<cg, 256, 0, C.stream>>>(ld, S);
         k_axpy_xr_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
             n, S.alpha, B.p, B.q, B.e, B.r, R.rows_per_blk, ld, R.part);
         SSP_CHECK_LAUNCH();
-        C.kernels_launched += 4;
+        C.kernels_launched += 3 + A.nslabs;
         R.finish(S.rr);
         it++;
         SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
@@ -784,6 +1009,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
             fprintf(stderr, "[ssp] pcg%s iter %d: %lld columns active\n", sizeof(T) == 4 ? " (fp32 inner)" : "", it,
                     (long long)active);
         if (active == 0) break;
+        if (device_loop) break;
         tm.pc.begin(C.stream);
         SSP_CUDA(cudaGraphLaunch(P.exec, C.stream));
         tm.pc.end(C.stream);
@@ -793,6 +1019,70 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         k_update_p<T><<<egrid, 256, 0, C.stream>>>(n, S.beta, B.z, B.p);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += 2;
+    }
+    if (device_loop && active > 0 && it < max_iters) {
+        // one iteration = preconditioner, r.z, beta, p update, SpMM, alpha, x/r update, check, control
+        int32_t* d_it = C.ws.get_t<int32_t>("pcg_loop_it", 1);
+        k_it_set<<<1, 1, 0, C.stream>>>(d_it, it);
+        SSP_CHECK_LAUNCH();
+        LoopGraph L;
+        cudaGraphConditionalHandle h;
+        const int64_t k_before = C.kernels_launched;
+        int64_t body_kernels = 0;
+        SSP_CUDA(cudaGraphCreate(&L.graph, 0));
+        SSP_CUDA(cudaGraphConditionalHandleCreate(&h, L.graph, 0, cudaGraphCondAssignDefault));
+        auto capture = [&](cudaGraph_t g, auto&& fn) {
+            SSP_CUDA(cudaStreamBeginCaptureToGraph(C.stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            try {
+                fn();
+            } catch (...) {
+                cudaGraph_t tmp;
+                cudaStreamEndCapture(C.stream, &tmp);
+                throw;
+            }
+            SSP_CUDA(cudaStreamEndCapture(C.stream, &g));
+        };
+        capture(L.graph, [&] {
+            k_loop_ctl<<<1, 1, 0, C.stream>>>(h, S.nactive, d_it, max_iters);
+            SSP_CHECK_LAUNCH();
+        });
+        size_t nn = 0;
+        SSP_CUDA(cudaGraphGetNodes(L.graph, nullptr, &nn));
+        std::vector<cudaGraphNode_t> roots(nn);
+        SSP_CUDA(cudaGraphGetNodes(L.graph, roots.data(), &nn));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t wnode;
+        SSP_CUDA(cudaGraphAddNode(&wnode, L.graph, roots.data(), nn, &cp));
+        capture(cp.conditional.phGraph_out[0], [&] {
+            body_kernels += launch_precond<T>(C, F, V, n, B.r, B.z, ld, k);
+            R.run<OP_DOT, T>(B.r, B.z, S.rz_new);
+            k_cols_beta<<<cg, 256, 0, C.stream>>>(ld, S);
+            k_update_p<T><<<egrid, 256, 0, C.stream>>>(n, S.beta, B.z, B.p);
+            launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, true, k);
+            k_colred_final<<<cg, 256, 0, C.stream>>>(ld, (int)A.grid.x, A.part, S.pq);
+            k_cols_alpha<<<cg, 256, 0, C.stream>>>(ld, S);
+            k_axpy_xr_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
+                n, S.alpha, B.p, B.q, B.e, B.r, R.rows_per_blk, ld, R.part);
+            R.finish(S.rr);
+            k_it_next<<<1, 1, 0, C.stream>>>(d_it);
+            SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
+            k_cols_check_at<<<cg, 256, 0, C.stream>>>(ld, d_it, S);
+            k_loop_ctl<<<1, 1, 0, C.stream>>>(h, S.nactive, d_it, max_iters);
+            SSP_CHECK_LAUNCH();
+        });
+        body_kernels += (C.kernels_launched - k_before) + 9 + A.nslabs;  // the helpers count theirs
+        C.kernels_launched = k_before;
+        SSP_CUDA(cudaGraphInstantiate(&L.exec, L.graph, 0));
+        SSP_CUDA(cudaGraphLaunch(L.exec, C.stream));
+        int32_t it_end = it;
+        SSP_CUDA(cudaMemcpyAsync(&it_end, d_it, sizeof(int32_t), cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+        C.kernels_launched += 1 + body_kernels * (int64_t)(it_end - it);
+        it = it_end;
     }
     tm.loop.end(C.stream);
     return it;
@@ -823,26 +1113,10 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
     double* mean = colv + 2 * ld;
     Reducer R;
     R.init(C, n, ld);
-    // SpMM: row-aligned chunks of the Laplacian, about one wave of blocks per tile
-    std::vector<int32_t> achunks;
-    int64_t lap_nnz = 0;
-    {
-        std::vector<int64_t> hp(n + 1);
-        SSP_CUDA(cudaMemcpyAsync(hp.data(), lap_ptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, C.stream));
-        SSP_CUDA(cudaStreamSynchronize(C.stream));
-        make_chunks(hp, 0, (int32_t)n, achunks);
-        achunks.push_back((int32_t)n);
-        lap_nnz = hp[n];
-    }
-    SpmmPlan A;
-    A.nchunks = (int32_t)achunks.size() - 1;
-    int32_t* d_achunks = W.get_t<int32_t>("pcg_achunks", achunks.size());
-    SSP_CUDA(cudaMemcpyAsync(d_achunks, achunks.data(), sizeof(int32_t) * achunks.size(), cudaMemcpyHostToDevice,
-                             C.stream));
-    A.chunks = d_achunks;
-    const int spmm_bx = chunk_blocks(A.nchunks);
-    A.part = W.get_t<double>("pcg_spmm_part", (size_t)spmm_bx * ld);
-    A.grid = dim3((unsigned)spmm_bx, (unsigned)ntiles);
+    // SpMM: row-aligned chunks of the Laplacian (column slabs on large random graphs), about one wave of
+    // blocks per tile
+    const SpmmPlan A = make_spmm_plan(C, n, lap_ptr, lap_idx, lap_val, ld);
+    const int64_t lap_nnz = A.nnz;
     const dim3 egrid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div<int64_t>(n * TILE, 256),
                                                                       2048 / std::max<int64_t>(1, ntiles) + 4)),
                      (unsigned)ntiles);
@@ -874,7 +1148,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         int64_t pc_launches = 0;
         if (read_i64(C, S.nactive) > 0) {
             build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P, pc_launches);
-            it = pcg_solve<double>(C, n, k, ld, A, lap_ptr, lap_idx, lap_val, P, pc_launches,
+            it = pcg_solve<double>(C, n, k, ld, A, A.val, F, fp64_vals(F), P, pc_launches,
                                    PcgBufs<double>{x, r, z, p, q}, S, R, opt.max_iters, opt, tm);
         }
     } else {
@@ -887,7 +1161,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
             SSP_CHECK_LAUNCH();
             C.kernels_launched++;
         };
-        to_f32(lap_nnz, lap_val, aval32);
+        to_f32(lap_nnz, A.val, aval32);
         to_f32(F.nnz, F.prow_val, fval32);
         to_f32(F.nnz, F.pcol_val, fval32 + F.nnz);
         to_f32(n, F.D, fval32 + 2 * F.nnz);
@@ -920,7 +1194,9 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 int32_t cap = opt.max_iters - it;
                 if (first_its >= 0)
                     cap = std::min(cap, std::max(MIXED_MIN_ROUND_ITERS, MIXED_ROUND_ITER_FACTOR * first_its));
-                its = pcg_solve<float>(C, n, k, ld, A, lap_ptr, lap_idx, aval32, P32, pc32,
+                else
+                    cap = std::min(cap, std::max(MIXED_MIN_ROUND_ITERS, opt.max_iters / MIXED_FIRST_ROUND_DIV));
+                its = pcg_solve<float>(C, n, k, ld, A, aval32, F, V32, P32, pc32,
                                        PcgBufs<float>{e32, r32, z32, p32, q32}, Si, R, cap, opt, tm);
                 if (first_its < 0) first_its = its;
                 hit_cap = its >= cap;
@@ -936,7 +1212,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
                 if (!P64.exec) build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P64, pc64);
-                its = pcg_solve<double>(C, n, k, ld, A, lap_ptr, lap_idx, lap_val, P64, pc64,
+                its = pcg_solve<double>(C, n, k, ld, A, A.val, F, fp64_vals(F), P64, pc64,
                                         PcgBufs<double>{e64, r, z, p, q}, Si, R, opt.max_iters - it, opt, tm);
                 k_add_into<double><<<grid_for(total, 256, 148 * 16), 256, 0, C.stream>>>(total, e64, x);
                 rep.fp64_rounds++;
@@ -947,12 +1223,12 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
             rep.refinements++;
             // true residual with the FP64 matrix and FP64 x
             ev_resid.begin(C.stream);
-            launch_spmm<double>(C, n, A.chunks, A.nchunks, A.grid, lap_ptr, lap_idx, lap_val, x, q, ld, nullptr, k);
+            launch_spmm<double>(C, n, A, A.val, x, q, ld, false, k);
             ev_resid.end(C.stream);
             k_true_resid<<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
                 n, k, Y, mean, q, r, R.rows_per_blk, ld, R.part);
             SSP_CHECK_LAUNCH();
-            C.kernels_launched += 2;
+            C.kernels_launched += 1 + A.nslabs;
             R.finish(relres);
             SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
             SSP_CUDA(cudaMemsetAsync(worst, 0, sizeof(double), C.stream));
@@ -970,9 +1246,9 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         }
     }
     // true relative residual ||(Y - mean) - A x|| / ||Y - mean||
-    launch_spmm<double>(C, n, A.chunks, A.nchunks, A.grid, lap_ptr, lap_idx, lap_val, x, q, ld, nullptr, k);
+    launch_spmm<double>(C, n, A, A.val, x, q, ld, false, k);
     SSP_CHECK_LAUNCH();
-    C.kernels_launched++;
+    C.kernels_launched += A.nslabs;
     R.run<OP_SQDIFF_CENTERED, double>(Y, q, relres, mean);
     std::vector<double> hb(ld), hr(ld);
     std::vector<int32_t> hi(ld);
@@ -999,6 +1275,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
     rep.ms_resid = ev_resid.total_ms();
     rep.n_resid = (int64_t)ev_resid.used;
     rep.iters_run = it;
+    rep.spmm_slabs = A.nslabs;
     if (x_out) *x_out = x;
 }
 

@@ -27,6 +27,10 @@
 #include "../../include/specspars.h"
 
 namespace ssp {
+double spmm_slab_mb();  // ssp_pcg.cu
+}
+
+namespace ssp {
 void set_last_error(const std::string& msg);
 }
 
@@ -207,11 +211,17 @@ int64_t ssp_request_footprint(const ssp_csc* graph, const ssp_params* params) {
     if (!graph || !params || graph->n <= 0) return -1;
     const int64_t n = graph->n, nnz = graph->nnz;
     const int64_t k = ssp_params_jl_dim(params, n);
-    const int64_t ld = (k + 7) / 8 * 8;
+    const int64_t ld = (k + 31) / 32 * 32;  // whole 32-column tiles
     // n x ld blocks: sketch + x, r, z, p, q in FP64 (+ five FP32 blocks and an FP64 increment when mixed);
-    // graph, Laplacian, factor pools and sampling arrays per stored entry; a fixed allowance
+    // graph, Laplacian, factor pools and sampling arrays per stored entry; the SpMM's column-slab copy of
+    // the Laplacian when slabs are on and the graph has more rows than one slab holds (256-byte rows, at
+    // most 16 slabs); a fixed allowance
     const double blocks = params->precision == SSP_PRECISION_MIXED ? 6.0 + 2.5 + 1.0 : 6.0;
-    return (int64_t)(blocks * 8.0 * (double)n * (double)ld) + 200 * nnz + 96 * n + (16ll << 20);
+    const int64_t slab_rows = std::max<int64_t>(1, (int64_t)(ssp::spmm_slab_mb() * 1048576.0 / 256));
+    const int64_t slabs = ssp::spmm_slab_mb() > 0 && n > slab_rows
+                              ? std::min<int64_t>(16, (n + slab_rows - 1) / slab_rows) : 0;
+    const int64_t slab_bytes = slabs ? 12 * (nnz + n) + 12 * slabs * n : 0;
+    return (int64_t)(blocks * 8.0 * (double)n * (double)ld) + 200 * nnz + 96 * n + slab_bytes + (16ll << 20);
 }
 
 int ssp_server_create(const ssp_server_opts* opts, ssp_server** out) {

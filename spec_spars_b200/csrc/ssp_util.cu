@@ -114,6 +114,10 @@ void exclusive_scan_i32_to_i64(Context& C, const int32_t* in, int64_t* out, int6
 }
 
 void make_chunks(const std::vector<int64_t>& ptr, int32_t r0, int32_t r1, std::vector<int32_t>& starts) {
+    make_chunks(ptr.data(), r0, r1, starts);
+}
+
+void make_chunks(const int64_t* ptr, int32_t r0, int32_t r1, std::vector<int32_t>& starts) {
     int32_t r = r0;
     while (r < r1) {
         starts.push_back(r);
