@@ -331,6 +331,26 @@ int ssp_connected_components(ssp_context* ctx, const ssp_csc* m, int32_t mem, in
 int ssp_sparsify_mtx(const char* input_file, const char* output_file, const ssp_params* params, ssp_stats* stats);
 int ssp_read_mtx(const char* path, ssp_csc_out* out);             /* host CSC, duplicates summed */
 int ssp_write_mtx(const char* path, const ssp_csc* m);            /* coordinate real general */
+
+/* ---- Matrix Market on the device (the GPU .mtx ingest / egest; replaces read_mtx / write_mtx,
+ * utils.rs:149-154,189-191, whose parsing and formatting run on one host core) ----
+ * ssp_read_mtx_device: the same CSC as ssp_read_mtx, parsed on the GPU (newline index, one thread per line,
+ * exact decimal conversion, stable radix sort by (column, row), duplicates summed in file order).  A file
+ * whose body the per-line parser cannot mirror exactly is read by the host reader instead, so both entry
+ * points always return the same matrix and the same errors.  out_mem SSP_MEM_DEVICE leaves the arrays in
+ * the context (owned_by_context = 1, valid until the context's next read).
+ * ssp_write_mtx_device: the bytes ssp_write_mtx writes, formatted on the GPU; m in host or device memory.
+ * ssp_sparsify_mtx uses both. */
+int ssp_read_mtx_device(ssp_context* ctx, const char* path, int32_t out_mem, ssp_csc_out* out);
+int ssp_write_mtx_device(ssp_context* ctx, const char* path, const ssp_csc* m);
+/* the exact conversions those kernels use, on the host: ssp_parse_decimal returns 1 with the correctly rounded
+ * binary64 of the token s[0, len) (as strtod), 0 when the token is outside the exact converter's domain
+ * (more than 19 significant digits, |decimal exponent| > 38, subnormal results, inf/nan/hex), -1 on a
+ * malformed token; ssp_format_g17 writes printf("%.17g", v) into buf (cap >= 33, NUL-terminated) and returns
+ * its length, or -1 for values outside the device formatter's range (decimal exponent outside [-20, 38],
+ * subnormals, inf, nan). */
+int ssp_parse_decimal(const char* s, size_t len, double* out);
+int ssp_format_g17(double v, char* buf, size_t cap);
 /* edge list ("<n> <m>" then "u v [w]" lines) -> symmetric .mtx, first weight of a repeated pair wins
  * (edge_list_to_matrix_market, src/utils.rs:413-526) */
 int ssp_edgelist_to_mtx(const char* input_path, const char* output_path, double default_weight);

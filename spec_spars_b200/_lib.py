@@ -159,6 +159,10 @@ def lib():
             "ssp_sparsify_mtx": ([ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_Params),
                                   ctypes.POINTER(_Stats)], ctypes.c_int),
             "ssp_read_mtx": ([ctypes.c_char_p, ctypes.POINTER(_CscOut)], ctypes.c_int),
+            "ssp_read_mtx_device": ([P, ctypes.c_char_p, I32, ctypes.POINTER(_CscOut)], ctypes.c_int),
+            "ssp_write_mtx_device": ([P, ctypes.c_char_p, ctypes.POINTER(_Csc)], ctypes.c_int),
+            "ssp_parse_decimal": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+            "ssp_format_g17": ([ctypes.c_double, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
             "ssp_write_mtx": ([ctypes.c_char_p, ctypes.POINTER(_Csc)], ctypes.c_int),
             "ssp_gen_grid2d": ([I64, I64, DBL, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_grid3d": ([I64, I64, I64, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
@@ -316,6 +320,21 @@ def write_mtx(path, m):
     _check(lib().ssp_write_mtx(path.encode(), ctypes.byref(s)))
 
 
+def parse_decimal(token):
+    """(status, value): status 1 = exact device conversion, 0 = left to the host's strtod, -1 = malformed."""
+    b = token.encode() if isinstance(token, str) else bytes(token)
+    v = ctypes.c_double(0.0)
+    rc = lib().ssp_parse_decimal(b, len(b), ctypes.byref(v))
+    return rc, v.value
+
+
+def format_g17(x):
+    """printf("%.17g", x) as the device formats it, or None where the host formats it."""
+    buf = ctypes.create_string_buffer(40)
+    n = lib().ssp_format_g17(float(x), buf, 40)
+    return None if n < 0 else buf.raw[:n].decode()
+
+
 def gen_grid2d(nx, ny, w=1.0):
     out = _CscOut()
     _check(lib().ssp_gen_grid2d(nx, ny, w, ctypes.byref(out)))
@@ -465,6 +484,17 @@ class Context:
 
     def __exit__(self, *a):
         self.close()
+
+    def read_mtx(self, path):
+        """utils::read_mtx parsed on the GPU (host CSC result, identical to read_mtx)."""
+        out = _CscOut()
+        _check(lib().ssp_read_mtx_device(self._h, path.encode(), SSP_MEM_HOST, ctypes.byref(out)))
+        return _take_out(out)
+
+    def write_mtx(self, path, m):
+        """utils::write_mtx formatted on the GPU (the bytes write_mtx writes)."""
+        s = m._struct()
+        _check(lib().ssp_write_mtx_device(self._h, path.encode(), ctypes.byref(s)))
 
     def set_stream(self, stream_ptr):
         _check(lib().ssp_context_set_stream(self._h, stream_ptr))

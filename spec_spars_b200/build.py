@@ -18,9 +18,9 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 # Translation units whose results must be bit-identical to the CPU oracle: no FMA contraction.
 EXACT = {"ssp_graph.cu", "ssp_sketch.cu", "ssp_factor.cu", "ssp_sample.cu", "ssp_noalloc.cu"}
 SOURCES = ["ssp_util.cu", "ssp_graph.cu", "ssp_sketch.cu", "ssp_factor.cu", "ssp_pcg.cu", "ssp_sample.cu",
-           "ssp_autotune.cu", "ssp_noalloc.cu", "ssp_quality.cu", "ssp_api.cu", "ssp_host.cpp",
+           "ssp_autotune.cu", "ssp_noalloc.cu", "ssp_quality.cu", "ssp_mtxio.cu", "ssp_api.cu", "ssp_host.cpp",
            "ssp_server.cpp"]
-HEADERS = ["ssp_internal.cuh", "ssp_sort.cuh", "ssp_host.h"]
+HEADERS = ["ssp_internal.cuh", "ssp_sort.cuh", "ssp_host.h", "ssp_decimal.cuh"]
 
 
 def _nvcc():

@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include "ssp_decimal.cuh"
 #include "ssp_host.h"
 #include "ssp_internal.cuh"
 
@@ -377,16 +378,7 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
                 fprintf(stderr, " %zu:%lld", i, (long long)F.frontier_sizes[i]);
         fprintf(stderr, "\n");
     }
-    if (prm->output_file && prm->output_file[0]) {
-        std::vector<int64_t> cp(n + 1);
-        std::vector<int32_t> ri(nnz);
-        std::vector<double> va(nnz);
-        SSP_CUDA(cudaMemcpy(cp.data(), lh_ptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost));
-        SSP_CUDA(cudaMemcpy(ri.data(), lh_idx, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost));
-        SSP_CUDA(cudaMemcpy(va.data(), lh_val, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
-        std::string err;
-        if (write_mtx(prm->output_file, n, cp.data(), ri.data(), va.data(), err) != 0) throw Error(SSP_ERR_IO, err);
-    }
+    if (prm->output_file && prm->output_file[0]) write_mtx_device(C, prm->output_file, n, lh_ptr, lh_idx, lh_val, "mtxw");
 }
 
 static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t k, double* Z, int32_t mem,
@@ -823,21 +815,99 @@ int ssp_write_mtx(const char* path, const ssp_csc* m) {
     });
 }
 
+// the file parsed on the device when it can be (read_mtx_device), else by the host reader and copied up
+static ssp_csc read_mtx_to_device(Context& C, const char* path, HostCsc& h) {
+    int64_t n = 0, nnz = 0;
+    int64_t* cp = nullptr;
+    int32_t* ri = nullptr;
+    double* va = nullptr;
+    if (read_mtx_device(C, path, &n, &nnz, &cp, &ri, &va, "mtxr")) return ssp_csc{n, nnz, cp, ri, va, SSP_MEM_DEVICE};
+    std::string err;
+    if (read_mtx(path, h, err) != 0) throw Error(SSP_ERR_IO, err);
+    return ssp_csc{h.n, h.colptr[h.n], h.colptr.data(), h.rowidx.data(), h.val.data(), SSP_MEM_HOST};
+}
+
 int ssp_sparsify_mtx(const char* input_file, const char* output_file, const ssp_params* params, ssp_stats* stats) {
     return guarded([&] {
         SSP_REQUIRE(input_file && params, SSP_ERR_INVALID, "bad arguments");
-        HostCsc h;
-        std::string err;
-        if (read_mtx(input_file, h, err) != 0) throw Error(SSP_ERR_IO, err);
         // InputStream::new zeroes the stored diagonal (stream.rs:23-28): the edge extraction only
         // reads row < col, so the diagonal never reaches the sparsifier.
         ssp_params p = *params;
         p.output_file = output_file;
         std::lock_guard<std::mutex> lk(g_default_mu);
         Context& C = default_context();
-        ssp_csc g{h.n, h.colptr[h.n], h.colptr.data(), h.rowidx.data(), h.val.data(), SSP_MEM_HOST};
+        HostCsc h;
+        const ssp_csc g = read_mtx_to_device(C, input_file, h);
         sparsify_impl(C, &g, &p, SSP_MEM_HOST, nullptr, stats);
     });
+}
+
+int ssp_read_mtx_device(ssp_context* ctx, const char* path, int32_t out_mem, ssp_csc_out* out) {
+    return guarded([&] {
+        SSP_REQUIRE(ctx && path && out, SSP_ERR_INVALID, "bad arguments");
+        SSP_REQUIRE(out_mem == SSP_MEM_HOST || out_mem == SSP_MEM_DEVICE, SSP_ERR_INVALID, "bad out_mem");
+        Context& C = ctx->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        HostCsc h;
+        const ssp_csc g = read_mtx_to_device(C, path, h);
+        if (g.mem == SSP_MEM_HOST && out_mem == SSP_MEM_HOST) {
+            host_out(h, out);
+            return;
+        }
+        memset(out, 0, sizeof(*out));
+        out->n = g.n;
+        out->nnz = g.nnz;
+        if (out_mem == SSP_MEM_HOST) {
+            out->colptr = (int64_t*)malloc(sizeof(int64_t) * (g.n + 1));
+            out->rowidx = (int32_t*)malloc(sizeof(int32_t) * (g.nnz + 1));
+            out->values = (double*)malloc(sizeof(double) * (g.nnz + 1));
+            if (!out->colptr || !out->rowidx || !out->values) throw std::bad_alloc();
+            SSP_CUDA(cudaMemcpyAsync(out->colptr, g.colptr, sizeof(int64_t) * (g.n + 1), cudaMemcpyDeviceToHost,
+                                     C.stream));
+            SSP_CUDA(cudaMemcpyAsync(out->rowidx, g.rowidx, sizeof(int32_t) * g.nnz, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(out->values, g.values, sizeof(double) * g.nnz, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaStreamSynchronize(C.stream));
+            out->mem = SSP_MEM_HOST;
+            return;
+        }
+        // device result in the context's buffers (a host-read file is copied into them)
+        int64_t* cp = (int64_t*)C.ws.get("mtxr_colptr", sizeof(int64_t) * (g.n + 1));
+        int32_t* ri = (int32_t*)C.ws.get("mtxr_rowidx", sizeof(int32_t) * (g.nnz + 1));
+        double* va = (double*)C.ws.get("mtxr_val", sizeof(double) * (g.nnz + 1));
+        if (g.mem == SSP_MEM_HOST) {
+            SSP_CUDA(cudaMemcpyAsync(cp, g.colptr, sizeof(int64_t) * (g.n + 1), cudaMemcpyHostToDevice, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(ri, g.rowidx, sizeof(int32_t) * g.nnz, cudaMemcpyHostToDevice, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(va, g.values, sizeof(double) * g.nnz, cudaMemcpyHostToDevice, C.stream));
+            SSP_CUDA(cudaStreamSynchronize(C.stream));
+        }
+        out->colptr = cp;
+        out->rowidx = ri;
+        out->values = va;
+        out->mem = SSP_MEM_DEVICE;
+        out->owned_by_context = 1;
+    });
+}
+
+int ssp_write_mtx_device(ssp_context* ctx, const char* path, const ssp_csc* m) {
+    return guarded([&] {
+        SSP_REQUIRE(ctx && path && m, SSP_ERR_INVALID, "bad arguments");
+        Context& C = ctx->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        const DevCsc d = to_device(C, m, "mtxw_in");
+        write_mtx_device(C, path, d.n, d.colptr, d.rowidx, d.val, "mtxw");
+    });
+}
+
+int ssp_parse_decimal(const char* s, size_t len, double* out) {
+    if (!s || !out) return -1;
+    return dec::parse_decimal(s, s + len, out);
+}
+
+int ssp_format_g17(double v, char* buf, size_t cap) {
+    if (!buf || cap < 33) return -1;
+    const int len = dec::format_g17(v, buf);
+    if (len >= 0) buf[len] = 0;
+    return len;
 }
 
 int ssp_gen_grid2d(int64_t nx, int64_t ny, double w, ssp_csc_out* out) {

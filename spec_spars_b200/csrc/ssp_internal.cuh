@@ -206,6 +206,16 @@ constexpr int CHUNK_CAP = SSP_CHUNK_CAP;
 constexpr int CHUNK_ROWS = 32;
 void make_chunks(const std::vector<int64_t>& ptr, int32_t r0, int32_t r1, std::vector<int32_t>& starts);
 void make_chunks(const int64_t* ptr, int32_t r0, int32_t r1, std::vector<int32_t>& starts);
+// Matrix Market on the device (ssp_mtxio.cu).  read_mtx_device leaves the CSC in workspace buffers named
+// after tag and returns false when the file needs the host reader; write_mtx_device takes device arrays.
+bool read_mtx_device(Context& C, const char* path, int64_t* n, int64_t* nnz, int64_t** colptr, int32_t** rowidx,
+                     double** val, const std::string& tag);
+void write_mtx_device(Context& C, const char* path, int64_t n, const int64_t* colptr, const int32_t* rowidx,
+                      const double* val, const std::string& tag);
+// stable ascending sort of (key, value) pairs by the low key_bits bits of the keys (LSD radix, 8-bit digits);
+// tmp_* are scratch arrays of n items
+void radix_sort_u64(Context& C, uint64_t* keys, int32_t* vals, int64_t n, int key_bits, uint64_t* tmp_keys,
+                    int32_t* tmp_vals);
 // L2 share (MB) of one column slab of the PCG's Laplacian product (SSP_SPMM_SLAB_MB; 0 = one pass)
 double spmm_slab_mb();
 

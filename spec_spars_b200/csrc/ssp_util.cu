@@ -264,4 +264,98 @@ void segsort_pairs_i32_f64(Context& C, int32_t* keys, double* vals, const int64_
     segsort_impl<true>(C, keys, vals, seg_start, seg_len, nseg, max_len);
 }
 
+
+// ---------------------------------------------------------------- stable LSD radix sort (64-bit keys)
+// 8-bit digits.  Each block owns a tile of RS_TILE consecutive items: a histogram pass, a digit-major
+// scan of the block histograms, and a scatter that ranks equal digits in item order (warp match masks,
+// then a per-digit prefix over the block's warps), so items with equal keys keep their order.
+namespace {
+constexpr int RS_THREADS = 256;
+constexpr int RS_ROUNDS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ROUNDS;
+constexpr int RS_WARPS = RS_THREADS / 32;
+}  // namespace
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const uint64_t* __restrict__ keys, int64_t n, int shift,
+                                                        int32_t* __restrict__ hist, int64_t nblocks) {
+    __shared__ int32_t s_h[256];
+    s_h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * RS_TILE;
+    for (int r = 0; r < RS_ROUNDS; r++) {
+        const int64_t i = base + r * RS_THREADS + threadIdx.x;
+        if (i < n) atomicAdd(&s_h[(keys[i] >> shift) & 255], 1);
+    }
+    __syncthreads();
+    hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = s_h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t* __restrict__ kin,
+                                                           const int32_t* __restrict__ vin, uint64_t* __restrict__ kout,
+                                                           int32_t* __restrict__ vout, int64_t n, int shift,
+                                                           const int64_t* __restrict__ offs, int64_t nblocks) {
+    __shared__ int64_t s_run[256];
+    __shared__ int64_t s_wc[RS_WARPS][256];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    s_run[threadIdx.x] = offs[(int64_t)threadIdx.x * nblocks + blockIdx.x];
+    for (int w = 0; w < RS_WARPS; w++) s_wc[w][threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * RS_TILE;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int r = 0; r < RS_ROUNDS; r++) {
+        const int64_t i = base + r * RS_THREADS + threadIdx.x;
+        const bool valid = i < n;
+        const uint64_t key = valid ? kin[i] : 0;
+        const int d = valid ? (int)((key >> shift) & 255) : 256;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int rank = __popc(peers & lt);
+        if (valid && rank == 0) s_wc[warp][d] = __popc(peers);
+        __syncthreads();
+        {
+            const int t = threadIdx.x;
+            int64_t run = s_run[t];
+            for (int w = 0; w < RS_WARPS; w++) {
+                const int64_t c = s_wc[w][t];
+                s_wc[w][t] = run;
+                run += c;
+            }
+            s_run[t] = run;
+        }
+        __syncthreads();
+        if (valid) {
+            const int64_t pos = s_wc[warp][d] + rank;
+            kout[pos] = key;
+            vout[pos] = vin[i];
+        }
+        __syncthreads();
+        for (int w = 0; w < RS_WARPS; w++) s_wc[w][threadIdx.x] = 0;
+        __syncthreads();
+    }
+}
+
+void radix_sort_u64(Context& C, uint64_t* keys, int32_t* vals, int64_t n, int key_bits, uint64_t* tmp_keys,
+                    int32_t* tmp_vals) {
+    if (n <= 1 || key_bits <= 0) return;
+    const int64_t nblocks = ceil_div<int64_t>(n, RS_TILE);
+    int32_t* hist = C.ws.get_t<int32_t>("rs_hist", (size_t)256 * nblocks);
+    int64_t* offs = C.ws.get_t<int64_t>("rs_offs", (size_t)256 * nblocks);
+    uint64_t *ka = keys, *kb = tmp_keys;
+    int32_t *va = vals, *vb = tmp_vals;
+    int passes = 0;
+    for (int shift = 0; shift < key_bits; shift += 8, passes++) {
+        k_rs_hist<<<(unsigned)nblocks, RS_THREADS, 0, C.stream>>>(ka, n, shift, hist, nblocks);
+        SSP_CHECK_LAUNCH();
+        exclusive_scan_i32_to_i64(C, hist, offs, 256 * nblocks, nullptr);
+        k_rs_scatter<<<(unsigned)nblocks, RS_THREADS, 0, C.stream>>>(ka, va, kb, vb, n, shift, offs, nblocks);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched += 2;
+        std::swap(ka, kb);
+        std::swap(va, vb);
+    }
+    if (passes & 1) {
+        SSP_CUDA(cudaMemcpyAsync(keys, ka, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, C.stream));
+        SSP_CUDA(cudaMemcpyAsync(vals, va, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, C.stream));
+    }
+}
+
 }  // namespace ssp
