@@ -213,9 +213,9 @@ bool read_mtx_device(Context& C, const char* path, int64_t* n, int64_t* nnz, int
 void write_mtx_device(Context& C, const char* path, int64_t n, const int64_t* colptr, const int32_t* rowidx,
                       const double* val, const std::string& tag);
 // stable ascending sort of (key, value) pairs by the low key_bits bits of the keys (LSD radix, 8-bit digits);
-// tmp_* are scratch arrays of n items
+// tmp_* are scratch arrays of n items; a scatter outside [0, n) is skipped and recorded in *err (if given)
 void radix_sort_u64(Context& C, uint64_t* keys, int32_t* vals, int64_t n, int key_bits, uint64_t* tmp_keys,
-                    int32_t* tmp_vals);
+                    int32_t* tmp_vals, unsigned long long* err = nullptr);
 // L2 share (MB) of one column slab of the PCG's Laplacian product (SSP_SPMM_SLAB_MB; 0 = one pass)
 double spmm_slab_mb();
 

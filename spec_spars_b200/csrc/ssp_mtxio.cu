@@ -41,6 +41,22 @@ enum : int32_t { LN_BLANK = 0, LN_ENTRY = 1, LN_FALLBACK = 2 };
 enum : int32_t { VAL_OK = 0, VAL_HOST = 1 };
 }  // namespace
 
+// ---------------------------------------------------------------- self-checks
+// Every kernel below checks its writes against the sizes it was given; a violation records (check id, index)
+// in *err (the smallest wins) and skips the access.  The host reads *err after each stage.
+__device__ __forceinline__ void check_fail(unsigned long long* err, int id, int64_t i) {
+    atomicMin(err, ((unsigned long long)id << 48) | ((unsigned long long)i & ((1ull << 48) - 1)));
+}
+
+static void stage_check(Context& C, unsigned long long* err, const char* stage) {
+    unsigned long long h = ~0ull;
+    SSP_CUDA(cudaMemcpyAsync(&h, err, sizeof h, cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    if (h != ~0ull)
+        throw Error(SSP_ERR_INVALID, std::string("mtx ") + stage + ": device check " + std::to_string(h >> 48) +
+                                         " failed at index " + std::to_string(h & ((1ull << 48) - 1)));
+}
+
 // ---------------------------------------------------------------- line index
 __global__ void __launch_bounds__(NL_THREADS) k_nl_count(const char* __restrict__ buf, int64_t size,
                                                          int32_t* __restrict__ cnt) {
@@ -60,7 +76,8 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_count(const char* __restrict_
 // line l starts at 0 (l = 0) or one past the l-th newline; the tile's newlines are ranked in byte order
 __global__ void __launch_bounds__(NL_THREADS) k_nl_starts(const char* __restrict__ buf, int64_t size,
                                                           const int64_t* __restrict__ off,
-                                                          int64_t* __restrict__ starts) {
+                                                          int64_t* __restrict__ starts, int64_t nlines,
+                                                          unsigned long long* __restrict__ err) {
     __shared__ int32_t s_warp[NL_THREADS / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t b = (int64_t)blockIdx.x * NL_TILE + (int64_t)threadIdx.x * NL_BYTES;
@@ -78,7 +95,11 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_starts(const char* __restrict
     for (int w = 0; w < warp; w++) before += s_warp[w];
     int64_t r = off[blockIdx.x] + before + incl - c;  // newlines before this thread's bytes
     for (int i = 0; i < NL_BYTES; i++)
-        if (b + i < size && buf[b + i] == '\n') starts[1 + r++] = b + i + 1;
+        if (b + i < size && buf[b + i] == '\n') {
+            if (1 + r < nlines && r >= 0) starts[1 + r] = b + i + 1;
+            else check_fail(err, 1, r);
+            r++;
+        }
     if (blockIdx.x == 0 && threadIdx.x == 0) starts[0] = 0;
 }
 
@@ -199,11 +220,16 @@ __global__ void k_offdiag(int64_t nnz, const int32_t* __restrict__ ei, const int
 // expanded entries in the host reader's push order, keyed by (column, row)
 __global__ void k_expand(int64_t nnz, int symmetric, int rbits, const int32_t* __restrict__ ei,
                          const int32_t* __restrict__ ej, const int64_t* __restrict__ odpos,
-                         uint64_t* __restrict__ keys, int32_t* __restrict__ src) {
+                         uint64_t* __restrict__ keys, int32_t* __restrict__ src, int64_t E,
+                         unsigned long long* __restrict__ err) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nnz) return;
     const int64_t i = ei[t], j = ej[t];
     const int64_t s = t + (symmetric ? odpos[t] : 0);
+    if (s < 0 || s + (symmetric && i != j ? 1 : 0) >= E) {
+        check_fail(err, 2, t);
+        return;
+    }
     keys[s] = ((uint64_t)j << rbits) | (uint64_t)i;
     src[s] = (int32_t)t;
     if (symmetric && i != j) {
@@ -221,10 +247,14 @@ __global__ void k_run_heads(int64_t E, const uint64_t* __restrict__ keys, int32_
 __global__ void k_run_sum(int64_t E, int rbits, const uint64_t* __restrict__ keys, const int32_t* __restrict__ src,
                           const double* __restrict__ ev, const int32_t* __restrict__ head,
                           const int64_t* __restrict__ upos, int32_t* __restrict__ rowidx, double* __restrict__ val,
-                          int32_t* __restrict__ colcnt) {
+                          int32_t* __restrict__ colcnt, int64_t U, int64_t n, unsigned long long* __restrict__ err) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= E || !head[s]) return;
     const uint64_t k = keys[s];
+    if (upos[s] < 0 || upos[s] >= U || (int64_t)(k >> rbits) >= n || src[s] < 0) {
+        check_fail(err, 3, s);
+        return;
+    }
     double acc = ev[src[s]];
     for (int64_t q = s + 1; q < E && keys[q] == k; q++) acc += ev[src[q]];
     const int64_t u = upos[s];
@@ -332,6 +362,8 @@ bool read_mtx_device(Context& C, const char* path, int64_t* n_out, int64_t* nnz_
     const int64_t size = (int64_t)st.st_size - h.body;
     Workspace& W = C.ws;
     auto nm = [&](const char* s) { return tag + "_" + s; };
+    unsigned long long* derr = W.get_t<unsigned long long>(nm("err"), 1);
+    SSP_CUDA(cudaMemsetAsync(derr, 0xff, sizeof(unsigned long long), C.stream));
     char* dbuf = W.get_t<char>(nm("text"), (size_t)std::max<int64_t>(size, 1));
     // stream the body: fread into one pinned buffer while the other copies
     if (size > 0) {
@@ -375,9 +407,10 @@ bool read_mtx_device(Context& C, const char* path, int64_t* n_out, int64_t* nnz_
     const int64_t newlines = read_i64(C, toff + tiles);
     const int64_t nlines = newlines + 1;  // the last line may be empty
     int64_t* starts = W.get_t<int64_t>(nm("lstart"), nlines);
-    k_nl_starts<<<(unsigned)tiles, NL_THREADS, 0, C.stream>>>(dbuf, size, toff, starts);
+    k_nl_starts<<<(unsigned)tiles, NL_THREADS, 0, C.stream>>>(dbuf, size, toff, starts, nlines, derr);
     SSP_CHECK_LAUNCH();
     C.kernels_launched += 2;
+    stage_check(C, derr, "line index");
     // parse
     int32_t* kind = W.get_t<int32_t>(nm("kind"), nlines);
     int64_t* I = W.get_t<int64_t>(nm("li"), nlines);
@@ -387,6 +420,7 @@ bool read_mtx_device(Context& C, const char* path, int64_t* n_out, int64_t* nnz_
     const unsigned lb = (unsigned)ceil_div<int64_t>(nlines, 256);
     k_parse_lines<<<lb, 256, 0, C.stream>>>(dbuf, size, starts, nlines, h.pattern ? 1 : 0, kind, I, J, V, vflag);
     SSP_CHECK_LAUNCH();
+    stage_check(C, derr, "line parse");
     // entries: rank of every line among the entry lines
     int32_t* isent = W.get_t<int32_t>(nm("isent"), nlines);
     int64_t* rank = W.get_t<int64_t>(nm("rank"), nlines + 1);
@@ -474,12 +508,14 @@ bool read_mtx_device(Context& C, const char* path, int64_t* n_out, int64_t* nnz_
     int64_t U = 0;
     if (E > 0) {
         k_expand<<<(unsigned)ceil_div<int64_t>(nnz, 256), 256, 0, C.stream>>>(nnz, h.symmetric ? 1 : 0, rbits, ei,
-                                                                               ej, odpos, keys, src);
+                                                                               ej, odpos, keys, src, E, derr);
         SSP_CHECK_LAUNCH();
         C.kernels_launched++;
+        stage_check(C, derr, "expand");
         uint64_t* tk = W.get_t<uint64_t>(nm("tkeys"), E);
         int32_t* ts = W.get_t<int32_t>(nm("tsrc"), E);
-        radix_sort_u64(C, keys, src, E, 2 * rbits, tk, ts);
+        radix_sort_u64(C, keys, src, E, 2 * rbits, tk, ts, derr);
+        stage_check(C, derr, "sort");
         int32_t* head = W.get_t<int32_t>(nm("head"), E);
         int64_t* upos = W.get_t<int64_t>(nm("upos"), E + 1);
         const unsigned eb = (unsigned)ceil_div<int64_t>(E, 256);
@@ -489,9 +525,10 @@ bool read_mtx_device(Context& C, const char* path, int64_t* n_out, int64_t* nnz_
         U = read_i64(C, upos + E);
         *rowidx = W.get_t<int32_t>(nm("rowidx"), U + 1);
         *val = W.get_t<double>(nm("val"), U + 1);
-        k_run_sum<<<eb, 256, 0, C.stream>>>(E, rbits, keys, src, ev, head, upos, *rowidx, *val, colcnt);
+        k_run_sum<<<eb, 256, 0, C.stream>>>(E, rbits, keys, src, ev, head, upos, *rowidx, *val, colcnt, U, h.n, derr);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += 2;
+        stage_check(C, derr, "duplicate sums");
     } else {
         *rowidx = W.get_t<int32_t>(nm("rowidx"), 1);
         *val = W.get_t<double>(nm("val"), 1);
@@ -518,10 +555,18 @@ __device__ __forceinline__ int dec_len(int64_t x) {
 }
 
 __global__ void k_fmt_values(int64_t nnz, const double* __restrict__ val, char* __restrict__ vtxt,
-                             int32_t* __restrict__ vlen) {
+                             int32_t* __restrict__ vlen, unsigned long long* __restrict__ err) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nnz) return;
-    vlen[p] = dec::format_g17(val[p], vtxt + p * VSLOT);
+    char t[VSLOT];
+    const int len = dec::format_g17(val[p], t);
+    if (len > VSLOT) {
+        check_fail(err, 4, p);
+        vlen[p] = -1;
+        return;
+    }
+    for (int i = 0; i < len; i++) vtxt[p * VSLOT + i] = t[i];
+    vlen[p] = len;
 }
 
 __global__ void k_fmt_misses(int64_t nnz, const int32_t* __restrict__ vlen, int32_t* __restrict__ n,
@@ -533,16 +578,29 @@ __global__ void k_fmt_misses(int64_t nnz, const int32_t* __restrict__ vlen, int3
     }
 }
 
-__global__ void k_col_of(int64_t n, const int64_t* __restrict__ colptr, int32_t* __restrict__ col) {
+__global__ void k_col_of(int64_t n, int64_t nnz, const int64_t* __restrict__ colptr, int32_t* __restrict__ col,
+                         unsigned long long* __restrict__ err) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
-    for (int64_t p = colptr[c]; p < colptr[c + 1]; p++) col[p] = (int32_t)c;
+    const int64_t a = colptr[c], b = colptr[c + 1];
+    if (a < 0 || b < a || b > nnz) {
+        check_fail(err, 5, c);
+        return;
+    }
+    for (int64_t p = a; p < b; p++) col[p] = (int32_t)c;
 }
 
 __global__ void k_line_len(int64_t nnz, const int32_t* __restrict__ rowidx, const int32_t* __restrict__ col,
-                           const int32_t* __restrict__ vlen, int32_t* __restrict__ llen) {
+                           const int32_t* __restrict__ vlen, int32_t* __restrict__ llen,
+                           unsigned long long* __restrict__ err) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < nnz) llen[p] = dec_len((int64_t)rowidx[p] + 1) + 1 + dec_len((int64_t)col[p] + 1) + 1 + vlen[p] + 1;
+    if (p >= nnz) return;
+    if (vlen[p] < 0 || vlen[p] > VSLOT || rowidx[p] < 0 || col[p] < 0) {
+        check_fail(err, 6, p);
+        llen[p] = 0;
+        return;
+    }
+    llen[p] = dec_len((int64_t)rowidx[p] + 1) + 1 + dec_len((int64_t)col[p] + 1) + 1 + vlen[p] + 1;
 }
 
 __device__ __forceinline__ char* put_int(char* o, int64_t x) {
@@ -556,9 +614,14 @@ __device__ __forceinline__ char* put_int(char* o, int64_t x) {
 
 __global__ void k_line_write(int64_t nnz, const int32_t* __restrict__ rowidx, const int32_t* __restrict__ col,
                              const char* __restrict__ vtxt, const int32_t* __restrict__ vlen,
-                             const int64_t* __restrict__ loff, char* __restrict__ out) {
+                             const int32_t* __restrict__ llen, const int64_t* __restrict__ loff, char* __restrict__ out,
+                             int64_t bytes, unsigned long long* __restrict__ err) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nnz) return;
+    if (llen[p] <= 0 || loff[p] < 0 || loff[p] + llen[p] > bytes) {
+        check_fail(err, 7, p);
+        return;
+    }
     char* o = out + loff[p];
     o = put_int(o, (int64_t)rowidx[p] + 1);
     *o++ = ' ';
@@ -575,6 +638,8 @@ void write_mtx_device(Context& C, const char* path, int64_t n, const int64_t* co
     Workspace& W = C.ws;
     auto nm = [&](const char* s) { return tag + "_" + s; };
     const int64_t nnz = read_i64(C, colptr + n);
+    unsigned long long* derr = W.get_t<unsigned long long>(nm("err"), 1);
+    SSP_CUDA(cudaMemsetAsync(derr, 0xff, sizeof(unsigned long long), C.stream));
     File F;
     F.f = fopen(path, "wb");
     if (!F.f) throw Error(SSP_ERR_IO, std::string("cannot open ") + path + " for writing");
@@ -587,10 +652,11 @@ void write_mtx_device(Context& C, const char* path, int64_t n, const int64_t* co
         int32_t* llen = W.get_t<int32_t>(nm("llen"), nnz);
         int64_t* loff = W.get_t<int64_t>(nm("loff"), nnz + 1);
         const unsigned eb = (unsigned)ceil_div<int64_t>(nnz, 256);
-        k_fmt_values<<<eb, 256, 0, C.stream>>>(nnz, val, vtxt, vlen);
-        k_col_of<<<(unsigned)ceil_div<int64_t>(n, 256), 256, 0, C.stream>>>(n, colptr, col);
+        k_fmt_values<<<eb, 256, 0, C.stream>>>(nnz, val, vtxt, vlen, derr);
+        k_col_of<<<(unsigned)ceil_div<int64_t>(n, 256), 256, 0, C.stream>>>(n, nnz, colptr, col, derr);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += 2;
+        stage_check(C, derr, "format values");
         // values outside the device formatter's range: snprintf on the host
         {
             int32_t* nmiss = W.get_t<int32_t>(nm("nmiss"), 1);
@@ -627,14 +693,16 @@ void write_mtx_device(Context& C, const char* path, int64_t n, const int64_t* co
                 SSP_CUDA(cudaStreamSynchronize(C.stream));
             }
         }
-        k_line_len<<<eb, 256, 0, C.stream>>>(nnz, rowidx, col, vlen, llen);
+        k_line_len<<<eb, 256, 0, C.stream>>>(nnz, rowidx, col, vlen, llen, derr);
         SSP_CHECK_LAUNCH();
+        stage_check(C, derr, "line lengths");
         exclusive_scan_i32_to_i64(C, llen, loff, nnz, loff + nnz);
         const int64_t bytes = read_i64(C, loff + nnz);
         char* out = W.get_t<char>(nm("out"), (size_t)bytes);
-        k_line_write<<<eb, 256, 0, C.stream>>>(nnz, rowidx, col, vtxt, vlen, loff, out);
+        k_line_write<<<eb, 256, 0, C.stream>>>(nnz, rowidx, col, vtxt, vlen, llen, loff, out, bytes, derr);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += 2;
+        stage_check(C, derr, "line write");
         // stream back through two pinned buffers
         Pinned stage(2 * STAGE_BYTES);
         cudaEvent_t done[2];

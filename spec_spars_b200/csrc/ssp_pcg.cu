@@ -113,12 +113,34 @@ __global__ void __launch_bounds__(RED_THREADS) k_colred_partial(int64_t n, const
     }
 }
 
-__global__ void k_colred_final(int64_t ld, int nparts, const double* __restrict__ part, double* __restrict__ out) {
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x) {
+// out[c] = sum over parts of part[i][c]: a block per 32 columns, warp w sums the parts i = w (mod FIN_WARPS) two
+// at a time, then the warps' sums are added in warp order (fixed order: deterministic).  Hundreds of parts per
+// column (the SpMM's p.q partials) are then 16-way parallel instead of one thread's dependent chain.
+constexpr int FIN_WARPS = 16;
+__global__ void __launch_bounds__(FIN_WARPS * 32) k_colred_final(int64_t ld, int nparts, const double* __restrict__ part,
+                                                                  double* __restrict__ out) {
+    __shared__ double s[FIN_WARPS][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t c = (int64_t)blockIdx.x * 32 + lane;
+    double a0 = 0.0, a1 = 0.0;
+    if (c < ld) {
+        int i = w;
+        for (; i + FIN_WARPS < nparts; i += 2 * FIN_WARPS) {
+            a0 += part[(int64_t)i * ld + c];
+            a1 += part[(int64_t)(i + FIN_WARPS) * ld + c];
+        }
+        if (i < nparts) a0 += part[(int64_t)i * ld + c];
+    }
+    s[w][lane] = a0 + a1;
+    __syncthreads();
+    if (w == 0 && c < ld) {
         double t = 0.0;
-        for (int i = 0; i < nparts; i++) t += part[(int64_t)i * ld + c];
+        for (int j = 0; j < FIN_WARPS; j++) t += s[j][lane];
         out[c] = t;
     }
+}
+static void colred_final(Context& C, int64_t ld, int nparts, const double* part, double* out) {
+    k_colred_final<<<(unsigned)ceil_div<int64_t>(ld, 32), FIN_WARPS * 32, 0, C.stream>>>(ld, nparts, part, out);
 }
 
 struct Reducer {
@@ -141,12 +163,12 @@ struct Reducer {
     void run(const T* a, const T* b, double* out, const double* mean = nullptr) {
         dim3 grid((unsigned)nparts, (unsigned)(ld / TILE));
         k_colred_partial<OP, T><<<grid, RED_THREADS, 0, C->stream>>>(n, a, b, mean, rows_per_blk, ld, part);
-        k_colred_final<<<grid_for(ld, 256), 256, 0, C->stream>>>(ld, nparts, part, out);
+        colred_final(*C, ld, nparts, part, out);
         SSP_CHECK_LAUNCH();
         C->kernels_launched += 2;
     }
     void finish(double* out) {
-        k_colred_final<<<grid_for(ld, 256), 256, 0, C->stream>>>(ld, nparts, part, out);
+        colred_final(*C, ld, nparts, part, out);
         SSP_CHECK_LAUNCH();
         C->kernels_launched++;
     }
@@ -434,20 +456,21 @@ __device__ __forceinline__ void chunk_epilogue(T* out, const T* aux, const T* xt
     }
 }
 
+// Grid: x over chunks, y over (tile, sub-tile): a tile's TILE columns are covered by nsub = TILE / W warps'
+// column ranges (nsub = 1 for the full-width layout, or for the narrow one when only W columns are real).
 template <int MODE, class T, int W>
-__global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks,
-                                                        const int64_t* __restrict__ ptr,
-                                                        const int32_t* __restrict__ idx,
-                                                        const T* __restrict__ val,
-                                                        const int32_t* __restrict__ rowmap, const T* xsrc,
-                                                        T* out, const T* __restrict__ aux, int64_t ld,
-                                                        double* __restrict__ part, int32_t kcols) {
+__device__ __forceinline__ void chunked_body(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks,
+                                             const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                             const T* __restrict__ val, const int32_t* __restrict__ rowmap,
+                                             const T* xsrc, T* out, const T* __restrict__ aux, int64_t ld,
+                                             double* __restrict__ part, int32_t kcols, int nsub) {
     __shared__ int32_t s_idx[CH_WARPS][CHUNK_CAP];
     __shared__ T s_val[CH_WARPS][CHUNK_CAP];
     __shared__ int32_t s_ptr[CH_WARPS][CHUNK_ROWS + 1];
     __shared__ double s_red[CH_THREADS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t t = blockIdx.y;
+    const int64_t t = blockIdx.y / nsub;
+    const int c0 = (int)(blockIdx.y % nsub) * W;  // first column of this block's sub-tile
     const int64_t toff = t * n * TILE;
     const T* xt = xsrc + toff;
     int32_t* si = s_idx[w];
@@ -470,7 +493,7 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
             __syncwarp();
             const int32_t pairs = (r1 - r0) * W;
             for (int32_t pr = lane; pr < pairs; pr += 32) {
-                const int32_t rr = pr / W, col = pr % W;
+                const int32_t rr = pr / W, col = c0 + pr % W;
                 const bool live = t * TILE + col < kcols;
                 const int32_t q0 = sp[rr], q1 = live ? sp[rr + 1] : q0;
                 // GATHER_UNROLL independent accumulators, summed as a pairwise tree
@@ -499,7 +522,7 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
             __syncwarp();
         } else {
             // one long row: (32 / W) entry slots x W columns per step, then a reduction over the slots
-            const int slot = lane / W, col = lane % W;
+            const int slot = lane / W, col = c0 + lane % W;
             const int64_t qe = t * TILE + col < kcols ? e1 : e0;
             T a0 = 0, a1 = 0;
             int64_t q = e0 + slot;
@@ -525,6 +548,26 @@ __global__ void __launch_bounds__(CH_THREADS) k_chunked(int64_t n, const int32_t
             part[(int64_t)blockIdx.x * ld + t * TILE + threadIdx.x] = tt;
         }
     }
+}
+
+// The SpMM asks for six resident blocks per SM (its registers would otherwise allow five: FP32 SpMM 29.7 ->
+// 22.6 ms at ER n = 1M); the level solves keep the compiler's own register choice (six blocks cost them 7 %).
+template <int MODE, class T, int W>
+__global__ void __launch_bounds__(CH_THREADS, 6)
+    k_spmm_chunked(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks, const int64_t* __restrict__ ptr,
+                   const int32_t* __restrict__ idx, const T* __restrict__ val, const T* xsrc, T* out,
+                   int64_t ld, double* __restrict__ part, int32_t kcols) {
+    static_assert(MODE == M_SPMM || MODE == M_SPMM_ACC, "SpMM modes only");
+    chunked_body<MODE, T, W>(n, cstart, nchunks, ptr, idx, val, nullptr, xsrc, out, nullptr, ld, part, kcols, 1);
+}
+
+template <int MODE, class T, int W>
+__global__ void __launch_bounds__(CH_THREADS)
+    k_chunked(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks, const int64_t* __restrict__ ptr,
+              const int32_t* __restrict__ idx, const T* __restrict__ val, const int32_t* __restrict__ rowmap,
+              const T* xsrc, T* out, const T* __restrict__ aux, int64_t ld, int32_t kcols, int nsub) {
+    static_assert(MODE == M_FWD || MODE == M_BWD, "level-solve modes only");
+    chunked_body<MODE, T, W>(n, cstart, nchunks, ptr, idx, val, rowmap, xsrc, out, aux, ld, nullptr, kcols, nsub);
 }
 
 // blocks per tile: about one wave of resident blocks, so the gathered slab of the tile being worked
@@ -569,6 +612,20 @@ __device__ __forceinline__ T warp_row_share(const int64_t* __restrict__ ptr, con
 }
 
 // FWD: y_u = r_u - L[u, :] y (row form).  BWD: y_u = y_u / D_u (D_u != 0) - L[:, u]^T y (column form).
+template <class T, bool FWD>
+__device__ __forceinline__ void run_finish(const int32_t* __restrict__ rows, const T* __restrict__ aux, T* y,
+                                           int64_t toff, int c, int32_t i, T acc) {
+    const int64_t u = rows[i];
+    const int64_t o = toff + u * TILE + c;
+    if (FWD) {
+        y[o] = aux[o] - acc;
+    } else {
+        const T d = aux[u];
+        const T yu = y[o];
+        y[o] = (d != (T)0 ? yu / d : yu) - acc;
+    }
+}
+
 template <class T, int W, bool FWD>
 __global__ void __launch_bounds__(RUN_THREADS) k_trsv_run(int64_t n, const int32_t* __restrict__ rows,
                                                           const int32_t* __restrict__ sched,
@@ -576,42 +633,33 @@ __global__ void __launch_bounds__(RUN_THREADS) k_trsv_run(int64_t n, const int32
                                                           const int64_t* __restrict__ ptr,
                                                           const int32_t* __restrict__ idx,
                                                           const T* __restrict__ val, const T* __restrict__ aux, T* y,
-                                                          int32_t kcols) {
+                                                          int32_t kcols, int nsub) {
     __shared__ T s_part[RUN_WARPS][W];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t toff = (int64_t)blockIdx.x * n * TILE;
-    const bool live = (int64_t)blockIdx.x * TILE + lane % W < kcols;
-    auto finish = [&](int32_t i, T acc) {
-        const int64_t u = rows[i];
-        const int64_t o = toff + u * TILE + lane;
-        if (FWD) {
-            y[o] = aux[o] - acc;
-        } else {
-            const T d = aux[u];
-            const T yu = y[o];
-            y[o] = (d != (T)0 ? yu / d : yu) - acc;
-        }
-    };
+    const int64_t t = blockIdx.x / nsub;
+    const int c0 = (int)(blockIdx.x % nsub) * W;  // first column of this block's sub-tile
+    const int64_t toff = t * n * TILE;
+    const bool live = t * TILE + c0 + lane % W < kcols;
     for (int32_t s = s0; s < s1; s++) {
         const int32_t a = step[s], b = step[s + 1];
         const int g = RUN_WARPS / max(1, b - a);  // warps per row
         if (g <= 1) {
             for (int32_t q = a + warp; q < b; q += RUN_WARPS) {
                 const int32_t i = sched[q];
-                const T acc = warp_row_share<T, W>(ptr, idx, val, i, y + toff, lane, live, 0, 1);
-                if (lane < W) finish(i, acc);
+                const T acc = warp_row_share<T, W>(ptr, idx, val, i, y + toff + c0, lane, live, 0, 1);
+                if (lane < W) run_finish<T, FWD>(rows, aux, y, toff, c0 + lane, i, acc);
             }
         } else {
             const int q = warp / g, sub = warp % g;
             const bool mine = a + q < b;
-            const T acc = mine ? warp_row_share<T, W>(ptr, idx, val, sched[a + q], y + toff, lane, live, sub, g)
+            const T acc = mine ? warp_row_share<T, W>(ptr, idx, val, sched[a + q], y + toff + c0, lane, live, sub, g)
                                : (T)0;
             if (lane < W) s_part[warp][lane] = acc;
             __syncthreads();
             if (mine && sub == 0 && lane < W) {
                 T tot = s_part[warp][lane];
                 for (int u = 1; u < g; u++) tot += s_part[warp + u][lane];
-                finish(sched[a + q], tot);
+                run_finish<T, FWD>(rows, aux, y, toff, c0 + lane, sched[a + q], tot);
             }
         }
         __syncthreads();
@@ -636,14 +684,20 @@ struct Precond {
     }
 };
 
-// columns a warp handles per row: all TILE, or 8 when no more than 8 are real (the autotuner's probe), so
-// that a warp still covers four rows per step; the padding columns of y must then be zero already
+// Column layouts of the triangular-solve launches.  Big levels: a warp's lanes cover a tile's TILE columns of
+// one row (256-byte gathers).  Runs and levels of at most SPLIT_LEVEL_ROWS rows are latency-bound -- a lane
+// walks its rows one after another -- so there each tile is split into TILE / 8 sub-tiles of 8 columns, one
+// block each: four rows per warp step and four times the warps.  With no more than 8 real columns (the
+// autotuner's probe) every launch uses 8 columns and one sub-tile; the padding columns of y must then be zero.
 constexpr int NARROW_W = 8;
+constexpr int SPLIT_LEVEL_ROWS = 4096;
 
-template <class T, int W>
-static int64_t launch_precond_w(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
-                                int64_t ld, int32_t kcols) {
+template <class T>
+static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
+                              int64_t ld, int32_t kcols) {
     const int ntiles = (int)(ld / TILE);
+    const bool narrow = TILE > NARROW_W && kcols <= NARROW_W;
+    const int nsub = narrow ? 1 : TILE / NARROW_W;  // sub-tiles of the 8-column layout
     int64_t launches = 0;
     // segments in level order: the thin-level runs (by index into F.runs) and single wide levels (-1)
     std::vector<std::pair<int32_t, int32_t>> seg;  // (level, run or -1)
@@ -655,49 +709,52 @@ static int64_t launch_precond_w(Context& C, const DevFactor& F, const FactorVals
             seg.push_back({l++, -1});
         }
     }
+    auto level = [&](bool fwd, int32_t l) {
+        const auto& lvl = fwd ? F.fchunk_lvl : F.bchunk_lvl;
+        const int32_t c0 = lvl[l], nc = lvl[l + 1] - c0;
+        if (nc == 0) return;
+        const bool split = narrow || F.level_ptr[l + 1] - F.level_ptr[l] <= SPLIT_LEVEL_ROWS;
+        const dim3 grid((unsigned)chunk_blocks(nc), (unsigned)(split ? ntiles * nsub : ntiles));
+        const int32_t* ch = (fwd ? F.fchunk : F.bchunk) + c0;
+        if (fwd && split)
+            k_chunked<M_FWD, T, NARROW_W><<<grid, CH_THREADS, 0, C.stream>>>(
+                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, kcols, nsub);
+        else if (fwd)
+            k_chunked<M_FWD, T, TILE><<<grid, CH_THREADS, 0, C.stream>>>(
+                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, kcols, 1);
+        else if (split)
+            k_chunked<M_BWD, T, NARROW_W><<<grid, CH_THREADS, 0, C.stream>>>(
+                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, kcols, nsub);
+        else
+            k_chunked<M_BWD, T, TILE><<<grid, CH_THREADS, 0, C.stream>>>(
+                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, kcols, 1);
+        launches++;
+    };
+    const unsigned rgrid = (unsigned)(ntiles * nsub);
     for (size_t i = 0; i < seg.size(); i++) {
-        const int32_t l0 = seg[i].first;
-        if (seg[i].second >= 0) {
-            const auto& run = F.runs[seg[i].second];
-            k_trsv_run<T, W, true><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.fsched, F.fstep, run.fs0,
-                                                                       run.fs1, F.prow_ptr, F.prow_idx, V.prow_val,
-                                                                       r, y, kcols);
-        } else {
-            const int32_t c0 = F.fchunk_lvl[l0], nc = F.fchunk_lvl[l0 + 1] - c0;
-            if (nc == 0) continue;
-            dim3 grid((unsigned)chunk_blocks(nc), (unsigned)ntiles);
-            k_chunked<M_FWD, T, W><<<grid, CH_THREADS, 0, C.stream>>>(n, F.fchunk + c0, nc, F.prow_ptr, F.prow_idx,
-                                                                    V.prow_val, F.level_rows, y, y, r, ld, nullptr,
-                                                                    kcols);
+        if (seg[i].second < 0) {
+            level(true, seg[i].first);
+            continue;
         }
+        const auto& run = F.runs[seg[i].second];
+        k_trsv_run<T, NARROW_W, true><<<rgrid, RUN_THREADS, 0, C.stream>>>(
+            n, F.level_rows, F.fsched, F.fstep, run.fs0, run.fs1, F.prow_ptr, F.prow_idx, V.prow_val, r, y, kcols,
+            nsub);
         launches++;
     }
     for (size_t i = seg.size(); i-- > 0;) {
-        const int32_t l0 = seg[i].first;
-        if (seg[i].second >= 0) {
-            const auto& run = F.runs[seg[i].second];
-            k_trsv_run<T, W, false><<<ntiles, RUN_THREADS, 0, C.stream>>>(n, F.level_rows, F.bsched, F.bstep,
-                                                                        run.bs0, run.bs1, F.pcol_ptr, F.pcol_idx,
-                                                                        V.pcol_val, V.D, y, kcols);
-        } else {
-            const int32_t c0 = F.bchunk_lvl[l0], nc = F.bchunk_lvl[l0 + 1] - c0;
-            if (nc == 0) continue;
-            dim3 grid((unsigned)chunk_blocks(nc), (unsigned)ntiles);
-            k_chunked<M_BWD, T, W><<<grid, CH_THREADS, 0, C.stream>>>(n, F.bchunk + c0, nc, F.pcol_ptr, F.pcol_idx,
-                                                                    V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr,
-                                                                    kcols);
+        if (seg[i].second < 0) {
+            level(false, seg[i].first);
+            continue;
         }
+        const auto& run = F.runs[seg[i].second];
+        k_trsv_run<T, NARROW_W, false><<<rgrid, RUN_THREADS, 0, C.stream>>>(
+            n, F.level_rows, F.bsched, F.bstep, run.bs0, run.bs1, F.pcol_ptr, F.pcol_idx, V.pcol_val, V.D, y, kcols,
+            nsub);
         launches++;
     }
     SSP_CHECK_LAUNCH();
     return launches;
-}
-
-template <class T>
-static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
-                              int64_t ld, int32_t kcols) {
-    if (TILE > NARROW_W && kcols <= NARROW_W) return launch_precond_w<T, NARROW_W>(C, F, V, n, r, y, ld, kcols);
-    return launch_precond_w<T, TILE>(C, F, V, n, r, y, ld, kcols);
 }
 
 // ---------------------------------------------------------------- SpMM plan
@@ -868,8 +925,8 @@ static void launch_spmm(Context& C, int64_t n, const SpmmPlan& A, const T* aval,
         const int64_t* ptr = A.ptr + (int64_t)b * n;
         double* part = dot && b == A.nslabs - 1 ? A.part : nullptr;
 #define SSP_SPMM_LAUNCH(MODE, W_)                                                                                  \
-    k_chunked<MODE, T, W_><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks[b], A.nchunks[b], ptr, A.idx, aval,    \
-                                                                 nullptr, p, q, nullptr, ld, part, kcols)
+    k_spmm_chunked<MODE, T, W_><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks[b], A.nchunks[b], ptr, A.idx, aval, \
+                                                                      p, q, ld, part, kcols)
         if (b == 0) {
             if (narrow) SSP_SPMM_LAUNCH(M_SPMM, NARROW_W);
             else SSP_SPMM_LAUNCH(M_SPMM, TILE);
@@ -982,7 +1039,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         tm.spmm.begin(C.stream);
         launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, true, k);
         tm.spmm.end(C.stream);
-        k_colred_final<<<cg, 256, 0, C.stream>>>(ld, (int)A.grid.x, A.part, S.pq);
+        colred_final(C, ld, (int)A.grid.x, A.part, S.pq);
         k_cols_alpha<<<cg, 256, 0, C.stream>>>(ld, S);
         k_axpy_xr_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
             n, S.alpha, B.p, B.q, B.e, B.r, R.rows_per_blk, ld, R.part);
@@ -1063,7 +1120,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
             k_cols_beta<<<cg, 256, 0, C.stream>>>(ld, S);
             k_update_p<T><<<egrid, 256, 0, C.stream>>>(n, S.beta, B.z, B.p);
             launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, true, k);
-            k_colred_final<<<cg, 256, 0, C.stream>>>(ld, (int)A.grid.x, A.part, S.pq);
+            colred_final(C, ld, (int)A.grid.x, A.part, S.pq);
             k_cols_alpha<<<cg, 256, 0, C.stream>>>(ld, S);
             k_axpy_xr_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
                 n, S.alpha, B.p, B.q, B.e, B.r, R.rows_per_blk, ld, R.part);

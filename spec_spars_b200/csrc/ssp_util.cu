@@ -293,7 +293,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const uint64_t* __restri
 __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t* __restrict__ kin,
                                                            const int32_t* __restrict__ vin, uint64_t* __restrict__ kout,
                                                            int32_t* __restrict__ vout, int64_t n, int shift,
-                                                           const int64_t* __restrict__ offs, int64_t nblocks) {
+                                                           const int64_t* __restrict__ offs, int64_t nblocks,
+                                                           unsigned long long* __restrict__ err) {
     __shared__ int64_t s_run[256];
     __shared__ int64_t s_wc[RS_WARPS][256];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -324,8 +325,12 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t* __res
         __syncthreads();
         if (valid) {
             const int64_t pos = s_wc[warp][d] + rank;
-            kout[pos] = key;
-            vout[pos] = vin[i];
+            if (pos >= 0 && pos < n) {
+                kout[pos] = key;
+                vout[pos] = vin[i];
+            } else if (err) {
+                atomicMin(err, (8ull << 48) | ((unsigned long long)i & ((1ull << 48) - 1)));
+            }
         }
         __syncthreads();
         for (int w = 0; w < RS_WARPS; w++) s_wc[w][threadIdx.x] = 0;
@@ -334,7 +339,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t* __res
 }
 
 void radix_sort_u64(Context& C, uint64_t* keys, int32_t* vals, int64_t n, int key_bits, uint64_t* tmp_keys,
-                    int32_t* tmp_vals) {
+                    int32_t* tmp_vals, unsigned long long* err) {
     if (n <= 1 || key_bits <= 0) return;
     const int64_t nblocks = ceil_div<int64_t>(n, RS_TILE);
     int32_t* hist = C.ws.get_t<int32_t>("rs_hist", (size_t)256 * nblocks);
@@ -346,7 +351,7 @@ void radix_sort_u64(Context& C, uint64_t* keys, int32_t* vals, int64_t n, int ke
         k_rs_hist<<<(unsigned)nblocks, RS_THREADS, 0, C.stream>>>(ka, n, shift, hist, nblocks);
         SSP_CHECK_LAUNCH();
         exclusive_scan_i32_to_i64(C, hist, offs, 256 * nblocks, nullptr);
-        k_rs_scatter<<<(unsigned)nblocks, RS_THREADS, 0, C.stream>>>(ka, va, kb, vb, n, shift, offs, nblocks);
+        k_rs_scatter<<<(unsigned)nblocks, RS_THREADS, 0, C.stream>>>(ka, va, kb, vb, n, shift, offs, nblocks, err);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += 2;
         std::swap(ka, kb);
