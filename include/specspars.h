@@ -387,6 +387,9 @@ int ssp_stage_diff_norms(ssp_context* ctx, int64_t n, int64_t m, const int32_t* 
 int ssp_stage_probs(ssp_context* ctx, int64_t m, const double* w, const double* d, double beta, double denom,
                     int32_t mem, double* p);
 int ssp_stage_coins(ssp_context* ctx, int64_t m, uint64_t seed, int32_t mem, double* coins);
+/* the device-wide exclusive scan every stage builds its offsets with: out[i] = sum of in[0..i), out[n] = total
+ * (host arrays; out has n + 1 entries) */
+int ssp_stage_scan(ssp_context* ctx, const int32_t* in, int64_t n, int64_t* out);
 int ssp_stage_sample_apply(ssp_context* ctx, const ssp_csc* graph, const double* p, const double* coins,
                            int32_t reweight, int32_t mem, uint8_t* keep, ssp_csc_out* out);
 

@@ -161,6 +161,7 @@ def lib():
             "ssp_read_mtx": ([ctypes.c_char_p, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_read_mtx_device": ([P, ctypes.c_char_p, I32, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_write_mtx_device": ([P, ctypes.c_char_p, ctypes.POINTER(_Csc)], ctypes.c_int),
+            "ssp_stage_scan": ([P, P, I64, P], ctypes.c_int),
             "ssp_parse_decimal": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
             "ssp_format_g17": ([ctypes.c_double, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
             "ssp_write_mtx": ([ctypes.c_char_p, ctypes.POINTER(_Csc)], ctypes.c_int),
@@ -806,6 +807,13 @@ def stage_probs(ctx, w, d, beta, denom):
     p = np.zeros_like(w)
     _check(lib().ssp_stage_probs(ctx._h, len(w), _ptr(w), _ptr(d), beta, denom, SSP_MEM_HOST, _ptr(p)))
     return p
+
+
+def stage_scan(ctx, a):
+    a = np.ascontiguousarray(a, np.int32)
+    out = np.zeros(len(a) + 1, np.int64)
+    _check(lib().ssp_stage_scan(ctx._h, _ptr(a), len(a), _ptr(out)))
+    return out
 
 
 def stage_coins(ctx, m, seed):

@@ -1132,6 +1132,20 @@ int ssp_stage_coins(ssp_context* c, int64_t m, uint64_t seed, int32_t mem, doubl
     });
 }
 
+int ssp_stage_scan(ssp_context* c, const int32_t* in, int64_t n, int64_t* out) {
+    return guarded([&] {
+        SSP_REQUIRE(c && out && n >= 0 && (n == 0 || in), SSP_ERR_INVALID, "bad arguments");
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        int32_t* di = C.ws.get_t<int32_t>("scan_in", n + 1);
+        int64_t* dout = C.ws.get_t<int64_t>("scan_out", n + 1);
+        if (n) SSP_CUDA(cudaMemcpyAsync(di, in, sizeof(int32_t) * n, cudaMemcpyHostToDevice, C.stream));
+        exclusive_scan_i32_to_i64(C, di, dout, n, dout + n);
+        SSP_CUDA(cudaMemcpyAsync(out, dout, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
 int ssp_stage_sample_apply(ssp_context* c, const ssp_csc* graph, const double* p, const double* coins,
                            int32_t reweight, int32_t mem, uint8_t* keep, ssp_csc_out* out) {
     return guarded([&] {

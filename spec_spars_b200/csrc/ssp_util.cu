@@ -73,6 +73,10 @@ __global__ void k_tile_scan(const TIn* in, int64_t* out, int64_t n, const int64_
     }
 }
 
+// nesting depth of the running scan on this thread, shared by every input type: an int32 scan recurses into
+// the int64 one, and each level needs its own tile-sum buffer
+static thread_local int g_scan_depth = 0;
+
 template <class TIn>
 static void scan_impl(Context& C, const TIn* in, int64_t* out, int64_t n, int64_t* d_total) {
     if (n <= 0) {
@@ -87,7 +91,7 @@ static void scan_impl(Context& C, const TIn* in, int64_t* out, int64_t n, int64_
         return;
     }
     // tile sums are staged in a per-depth buffer: (in may alias out)
-    static thread_local int depth = 0;
+    int& depth = g_scan_depth;
     std::string tag = "scan_sums_" + std::to_string(depth);
     int64_t* sums = C.ws.get_t<int64_t>(tag, tiles + 1);
     k_tile_sums<TIn><<<(unsigned)tiles, SCAN_THREADS, 0, C.stream>>>(in, n, sums);

@@ -386,3 +386,14 @@ def test_column_split_phases_match_single_call(ssp, ora, ctx, split):
     Z, _, _, rc = ora.pcg(G.n, cp, ri, va, F, Y, prm.pcg_tol, prm.pcg_abs_tol, prm.pcg_max_iters)
     assert rc == 0
     np.testing.assert_allclose(tot.cpu().numpy(), ora.diff_norms(v1, v2, Z) ** 2, rtol=1e-7)
+
+
+@pytest.mark.parametrize("n", [0, 1, 4095, 4096, 4097, 16_777_216, 16_777_217, 40_000_123])
+def test_device_scan_every_depth(ssp, ctx, n):
+    """The exclusive scan every stage builds its offsets with: one tile, several, and past 4096^2 elements,
+    where an int32 scan recurses twice into the int64 one (each level with its own tile-sum buffer)."""
+    a = np.random.default_rng(n).integers(0, 100, n, dtype=np.int32)
+    out = ssp.stage_scan(ctx, a)
+    ref = np.zeros(n + 1, np.int64)
+    np.cumsum(a, dtype=np.int64, out=ref[1:])
+    assert np.array_equal(out, ref)
