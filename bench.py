@@ -112,9 +112,9 @@ def peaks():
 
 
 # DRAM bytes per (Laplacian nonzero, 32-column tile) of one FP64 SpMM launch at ER n=1M, from the ncu
-# capture of a one-tile solve of that graph (profiles/k_chunked_spmm_er_n1M_k32.md: 4.31 GB for
-# nnz(L_G) = 21.0M nonzeros x 1 tile); every tile of a full launch does the same work
-SPMM_TRAFFIC_PER_NNZ_TILE = 4.31e9 / 21.0e6
+# capture of a one-tile solve of that graph (profiles/k_chunked_spmm_er_n1M_k32.md: 4.123 GB read + 0.287 GB
+# written for nnz(L_G) = 21.003M nonzeros x 1 tile); every tile of a full launch does the same work
+SPMM_TRAFFIC_PER_NNZ_TILE = 4.4093e9 / 21.003e6
 SPMM_TILE = 32
 
 
@@ -291,6 +291,63 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def run_mtx(args):
+    """--mtx: the Matrix Market path of sparsify_dataset on the workload's graph.  Timed: the GPU reader and
+    writer (ssp_read_mtx_device / ssp_write_mtx_device, file in the page cache) and sparsify_dataset file to
+    file; beside them the host reader and writer they replace (one pass each).  Both readers must return the
+    same CSC and both writers the same bytes."""
+    import tempfile
+    import numpy as np
+    import spec_spars_b200 as S
+    G, eps = make_graph(S, args.workload)
+    d = tempfile.mkdtemp(prefix="ssp_mtx_")
+    src, out_h, out_d, out_s = (os.path.join(d, x) for x in ("g.mtx", "h.mtx", "d.mtx", "s.mtx"))
+    S.write_mtx(src, G)
+    size = os.path.getsize(src)
+    ctx = S.Context(0)
+    for _ in range(max(1, args.warmup)):
+        ctx.read_mtx(src)
+        ctx.write_mtx(out_d, G)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        Hd = ctx.read_mtx(src)
+    t_read = (time.perf_counter() - t) / args.steps
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.write_mtx(out_d, G)
+    t_write = (time.perf_counter() - t) / args.steps
+    wsize = os.path.getsize(out_d)
+    S.sparsify_dataset(src, args.workload, out_s, eps, False, 0, 0, False)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        st = S.sparsify_dataset(src, args.workload, out_s, eps, False, 0, 0, False)
+    t_ds = (time.perf_counter() - t) / args.steps
+    t = time.perf_counter()
+    Hh = S.read_mtx(src)
+    th_read = time.perf_counter() - t
+    t = time.perf_counter()
+    S.write_mtx(out_h, G)
+    th_write = time.perf_counter() - t
+    same_read = (np.array_equal(Hh.colptr, Hd.colptr) and np.array_equal(Hh.rowidx, Hd.rowidx)
+                 and np.array_equal(Hh.values.view(np.uint64), Hd.values.view(np.uint64)))
+    with open(out_h, "rb") as a, open(out_d, "rb") as b:
+        same_write = a.read() == b.read()
+    m = G.nnz // 2
+    line = {"metric": "Matrix Market read: file bytes/sec", "value": size / t_read, "unit": "B/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "text -> f64",
+            "data": "synthetic", "config": {"workload": args.workload, "file_bytes": size, "entries": int(G.nnz),
+                                            "written_bytes": wsize, "page_cache": "file read from the page cache"},
+            "read_s": t_read, "write_s": t_write, "write_bytes_per_s": wsize / t_write,
+            "sparsify_dataset": {"s": t_ds, "edges_per_s": m / t_ds, "m_out": st.final_num_edges},
+            "cpu_baseline": {"read_s": th_read, "write_s": th_write, "cores": 1, "kind": "port",
+                             "sample": "the same file, host reader and writer (read_mtx / write_mtx restated)"},
+            "same_csc": bool(same_read), "same_bytes": bool(same_write)}
+    print(json.dumps(line), flush=True)
+    for f in (src, out_h, out_d, out_s):
+        os.remove(f)
+    os.rmdir(d)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -310,9 +367,13 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--serve-max-n", type=int, default=100_000)
     ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--mtx", action="store_true", help="time the GPU Matrix Market reader/writer and sparsify_dataset")
     args = ap.parse_args()
     if args.serve:
         run_serve(args)
+        return
+    if args.mtx:
+        run_mtx(args)
         return
     if args.impl == "reference":
         run_reference(args)
@@ -422,6 +483,9 @@ def main():
         traffic = SPMM_TRAFFIC_PER_NNZ_TILE * st["nnz_laplacian"] * math.ceil(k / SPMM_TILE)
     roof = {"kernel": kern, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_source": src,
+            # the DRAM bytes the launch really moves (traffic) per second, against the same peak
+            "traffic_GBps": traffic / (kms / 1000.0) / 1e9 if traffic and kms > 0 else None,
+            "traffic_frac": traffic / (kms / 1000.0) / 1e9 / peak if traffic and kms > 0 else None,
             "algorithmic_bytes_per_launch": byts, "avg_launch_ms": kms,
             "spmm_avg_ms": sp_ms, "precond_avg_ms": pc_ms,
             "spmm_GBps": spmm_bytes(n, st["nnz_laplacian"], k, vs) / (sp_ms / 1000.0) / 1e9 if sp_ms > 0 else None,

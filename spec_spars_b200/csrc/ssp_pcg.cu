@@ -437,6 +437,7 @@ constexpr int CH_THREADS = 256;
 #define SSP_GATHER_UNROLL_SOLVE 4
 #endif
 constexpr int CH_WARPS = CH_THREADS / 32;
+constexpr int MINB_SPMM = 6, MINB_FWD = 6, MINB_BWD = 5;
 
 template <int MODE, class T>
 __device__ __forceinline__ void chunk_epilogue(T* out, const T* aux, const T* xt, int64_t toff, int64_t v, int col,
@@ -458,12 +459,17 @@ __device__ __forceinline__ void chunk_epilogue(T* out, const T* aux, const T* xt
 
 // Grid: x over chunks, y over (tile, sub-tile): a tile's TILE columns are covered by nsub = TILE / W warps'
 // column ranges (nsub = 1 for the full-width layout, or for the narrow one when only W columns are real).
-template <int MODE, class T, int W>
-__device__ __forceinline__ void chunked_body(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks,
-                                             const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                             const T* __restrict__ val, const int32_t* __restrict__ rowmap,
-                                             const T* xsrc, T* out, const T* __restrict__ aux, int64_t ld,
-                                             double* __restrict__ part, int32_t kcols, int nsub) {
+// MINB: resident blocks per SM asked of the compiler.  The SpMM asks for six (its registers would otherwise
+// allow five: FP32 SpMM 29.7 -> 22.6 ms at ER n = 1M); the level solves ask for what their own register
+// choice gives (forward 6, backward 5; forcing six on the backward solve cost the preconditioner 7 %).
+// Keeping the body in the kernel itself matters: moved into a __device__ function holding the shared
+// arrays, the FP32 SpMM took 39 ms instead of 22.6 (twice the long-scoreboard stalls per issue).
+template <int MODE, class T, int W, int MINB>
+__global__ void __launch_bounds__(CH_THREADS, MINB)
+    k_chunked(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks, const int64_t* __restrict__ ptr,
+              const int32_t* __restrict__ idx, const T* __restrict__ val, const int32_t* __restrict__ rowmap,
+              const T* xsrc, T* out, const T* __restrict__ aux, int64_t ld, double* __restrict__ part,
+              int32_t kcols, int nsub) {
     __shared__ int32_t s_idx[CH_WARPS][CHUNK_CAP];
     __shared__ T s_val[CH_WARPS][CHUNK_CAP];
     __shared__ int32_t s_ptr[CH_WARPS][CHUNK_ROWS + 1];
@@ -548,26 +554,6 @@ __device__ __forceinline__ void chunked_body(int64_t n, const int32_t* __restric
             part[(int64_t)blockIdx.x * ld + t * TILE + threadIdx.x] = tt;
         }
     }
-}
-
-// The SpMM asks for six resident blocks per SM (its registers would otherwise allow five: FP32 SpMM 29.7 ->
-// 22.6 ms at ER n = 1M); the level solves keep the compiler's own register choice (six blocks cost them 7 %).
-template <int MODE, class T, int W>
-__global__ void __launch_bounds__(CH_THREADS, 6)
-    k_spmm_chunked(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks, const int64_t* __restrict__ ptr,
-                   const int32_t* __restrict__ idx, const T* __restrict__ val, const T* xsrc, T* out,
-                   int64_t ld, double* __restrict__ part, int32_t kcols) {
-    static_assert(MODE == M_SPMM || MODE == M_SPMM_ACC, "SpMM modes only");
-    chunked_body<MODE, T, W>(n, cstart, nchunks, ptr, idx, val, nullptr, xsrc, out, nullptr, ld, part, kcols, 1);
-}
-
-template <int MODE, class T, int W>
-__global__ void __launch_bounds__(CH_THREADS)
-    k_chunked(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks, const int64_t* __restrict__ ptr,
-              const int32_t* __restrict__ idx, const T* __restrict__ val, const int32_t* __restrict__ rowmap,
-              const T* xsrc, T* out, const T* __restrict__ aux, int64_t ld, int32_t kcols, int nsub) {
-    static_assert(MODE == M_FWD || MODE == M_BWD, "level-solve modes only");
-    chunked_body<MODE, T, W>(n, cstart, nchunks, ptr, idx, val, rowmap, xsrc, out, aux, ld, nullptr, kcols, nsub);
 }
 
 // blocks per tile: about one wave of resident blocks, so the gathered slab of the tile being worked
@@ -717,17 +703,17 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
         const dim3 grid((unsigned)chunk_blocks(nc), (unsigned)(split ? ntiles * nsub : ntiles));
         const int32_t* ch = (fwd ? F.fchunk : F.bchunk) + c0;
         if (fwd && split)
-            k_chunked<M_FWD, T, NARROW_W><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, kcols, nsub);
+            k_chunked<M_FWD, T, NARROW_W, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
+                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, nsub);
         else if (fwd)
-            k_chunked<M_FWD, T, TILE><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, kcols, 1);
+            k_chunked<M_FWD, T, TILE, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
+                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, 1);
         else if (split)
-            k_chunked<M_BWD, T, NARROW_W><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, kcols, nsub);
+            k_chunked<M_BWD, T, NARROW_W, MINB_BWD><<<grid, CH_THREADS, 0, C.stream>>>(
+                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr, kcols, nsub);
         else
-            k_chunked<M_BWD, T, TILE><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, kcols, 1);
+            k_chunked<M_BWD, T, TILE, MINB_BWD><<<grid, CH_THREADS, 0, C.stream>>>(
+                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr, kcols, 1);
         launches++;
     };
     const unsigned rgrid = (unsigned)(ntiles * nsub);
@@ -925,8 +911,9 @@ static void launch_spmm(Context& C, int64_t n, const SpmmPlan& A, const T* aval,
         const int64_t* ptr = A.ptr + (int64_t)b * n;
         double* part = dot && b == A.nslabs - 1 ? A.part : nullptr;
 #define SSP_SPMM_LAUNCH(MODE, W_)                                                                                  \
-    k_spmm_chunked<MODE, T, W_><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks[b], A.nchunks[b], ptr, A.idx, aval, \
-                                                                      p, q, ld, part, kcols)
+    k_chunked<MODE, T, W_, MINB_SPMM><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks[b], A.nchunks[b], ptr, A.idx,  \
+                                                                            aval, nullptr, p, q, nullptr, ld, part,    \
+                                                                            kcols, 1)
         if (b == 0) {
             if (narrow) SSP_SPMM_LAUNCH(M_SPMM, NARROW_W);
             else SSP_SPMM_LAUNCH(M_SPMM, TILE);
@@ -1014,11 +1001,13 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
                          const Precond& P, int64_t pc_launches, PcgBufs<T> B, ColState& S, Reducer& R,
                          int32_t max_iters, const PcgOptions& opt, PcgTimers& tm) {
     // without a residual history or progress output the iterations after the first run on the device
-#ifdef SSP_HOST_PCG_LOOP
-    const bool device_loop = false;
-#else
-    const bool device_loop = !opt.history && !opt.verbose;
-#endif
+    // SSP_PCG_HOST_LOOP=1 keeps every iteration on the host loop (the same kernels, launched one by one), for
+    // profilers that do not look inside conditional graph nodes
+    static const bool host_loop = [] {
+        const char* e = getenv("SSP_PCG_HOST_LOOP");
+        return e && e[0] == '1';
+    }();
+    const bool device_loop = !opt.history && !opt.verbose && !host_loop;
     const int64_t ntiles = ld / TILE;
     const int64_t total = n * ld;
     const dim3 egrid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div<int64_t>(n * TILE, 256),
