@@ -676,7 +676,7 @@ struct Precond {
 // block each: four rows per warp step and four times the warps.  With no more than 8 real columns (the
 // autotuner's probe) every launch uses 8 columns and one sub-tile; the padding columns of y must then be zero.
 constexpr int NARROW_W = 8;
-constexpr int SPLIT_LEVEL_ROWS = 4096;
+constexpr int SPLIT_LEVEL_ROWS = 1024;
 
 template <class T>
 static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
