@@ -605,26 +605,30 @@ int ora_pcg(int64_t n, const int64_t* cp, const int32_t* ri, const double* va, c
 }
 
 /* ------------------------------------------------------------------------ */
-/* a9: d_e = ||Z[v1] - Z[v2]|| (sparsifier.rs:565-583).  Reduction order fixed to the
- * CUDA kernel's: lane l accumulates columns j = l, l+32, ... with fma(d,d,acc), then an
- * xor butterfly (16,8,4,2,1). */
+/* a9: d_e = ||Z[v1] - Z[v2]|| (sparsifier.rs:565-583).  Reduction order fixed to the CUDA
+ * kernels' (the 32-column tiles of the device layout): for each tile T, lane l squares the
+ * difference in column 32T + l (0 past k), the 32 squares are summed by an xor butterfly
+ * (16,8,4,2,1; lane 0's result), and the tile sums are added in tile order from 0. */
 void ora_diff_norms(int64_t n, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z,
                     int32_t k, int64_t ldz, double* d) {
     (void)n;
     for (int64_t e = 0; e < m; e++) {
         const double* za = Z + (int64_t)v1[e] * ldz;
         const double* zb = Z + (int64_t)v2[e] * ldz;
-        double acc[32], t[32];
-        for (int l = 0; l < 32; l++) {
-            double s = 0.0;
-            for (int32_t j = l; j < k; j += 32) { double x = za[j] - zb[j]; s = fma(x, x, s); }
-            acc[l] = s;
+        double acc = 0.0;
+        for (int32_t j0 = 0; j0 < k; j0 += 32) {
+            double s[32], t[32];
+            for (int l = 0; l < 32; l++) {
+                const double x = j0 + l < k ? za[j0 + l] - zb[j0 + l] : 0.0;
+                s[l] = x * x;
+            }
+            for (int h = 16; h >= 1; h >>= 1) {
+                for (int l = 0; l < 32; l++) t[l] = s[l] + s[l ^ h];
+                memcpy(s, t, sizeof(s));
+            }
+            acc = acc + s[0];
         }
-        for (int s = 16; s >= 1; s >>= 1) {
-            for (int l = 0; l < 32; l++) t[l] = acc[l] + acc[l ^ s];
-            memcpy(acc, t, sizeof(acc));
-        }
-        d[e] = sqrt(acc[0]);
+        d[e] = sqrt(acc);
     }
 }
 

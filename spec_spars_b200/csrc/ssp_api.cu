@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -179,6 +180,38 @@ struct ShardArgs {
     const DevGraph* sketch_graph = nullptr;
 };
 
+// Host output of a large sparsify: the L_H arrays are allocated and their pages touched on a host thread while
+// the device works (L_H has at most nnz(L_G) entries: it only reweights or drops edges of G), so the final
+// device-to-host copy lands in resident pages (4.8 GB/s into fresh pages against 11 GB/s at ER n = 1M).
+struct HostOutBuffers {
+    std::thread th;
+    int64_t* colptr = nullptr;
+    int32_t* rowidx = nullptr;
+    double* values = nullptr;
+    int64_t cap = 0;
+    void start(int64_t n, int64_t nnz_cap) {
+        cap = nnz_cap;
+        th = std::thread([this, n] {
+            colptr = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+            rowidx = (int32_t*)malloc(sizeof(int32_t) * (cap + 1));
+            values = (double*)malloc(sizeof(double) * (cap + 1));
+            if (colptr) memset(colptr, 0, sizeof(int64_t) * (n + 1));
+            if (rowidx) memset(rowidx, 0, sizeof(int32_t) * (cap + 1));
+            if (values) memset(values, 0, sizeof(double) * (cap + 1));
+        });
+    }
+    void join() {
+        if (th.joinable()) th.join();
+    }
+    ~HostOutBuffers() {
+        join();
+        free(colptr);
+        free(rowidx);
+        free(values);
+    }
+};
+constexpr int64_t HOST_OUT_PREFAULT_MIN = 1 << 20;  // entries; smaller outputs allocate at the end
+
 static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* prm, int32_t out_mem, ssp_csc_out* out,
                           ssp_stats* st, const ShardArgs* sh = nullptr) {
     SSP_REQUIRE(prm, SSP_ERR_INVALID, "params is NULL");
@@ -190,6 +223,8 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     DevGraph G;
     build_graph_from_csc(C, g.n, g.colptr, g.rowidx, g.val, g.nnz, G);
     T.mark();  // 1
+    HostOutBuffers hob;
+    if (out && out_mem == SSP_MEM_HOST && G.lap_nnz >= HOST_OUT_PREFAULT_MIN) hob.start(G.n, G.lap_nnz);
     const int64_t n = G.n;
     const int32_t k = jl_dim(prm, n);
     const double scale = jl_scale(prm, k);
@@ -241,10 +276,17 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     T.mark();  // 3
     PcgReport rep;
     const double* Zt = nullptr;
-    if (!finish_only) pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, kl, &Zt, po, rep);
+    // the final product of the solve also forms the squared diff norms (sharded: this rank's share);
+    // SSP_DIFF_FUSED=0 leaves them to the separate pass over the edges (the same sums, for comparison)
+    const char* fe = getenv("SSP_DIFF_FUSED");
+    const bool fuse = !(fe && fe[0] == '0');
+    double* d2 = (finish_only || !fuse) ? nullptr
+                 : (sh && sh->sq_out) ? sh->sq_out : C.ws.get_t<double>("sp_d2", G.m + 1);
+    if (!finish_only)
+        pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, kl, &Zt, po, rep, nullptr, nullptr, G.lap_eid, d2);
     T.mark();  // 4
     if (sh && sh->sq_out) {
-        diff_sq_device(C, G.m, G.v1, G.v2, Zt, kl, n, sh->sq_out);
+        if (!rep.diff_fused) diff_sq_device(C, G.m, G.v1, G.v2, Zt, kl, n, sh->sq_out);
         T.mark();  // 5
         SSP_CUDA(cudaStreamSynchronize(C.stream));
         if (st) {
@@ -283,6 +325,8 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     double* coins = C.ws.get_t<double>("sp_coins", G.m + 1);
     if (finish_only)
         sqrt_device(C, G.m, sh->sq_in, d);
+    else if (rep.diff_fused)
+        sqrt_device(C, G.m, d2, d);
     else
         diff_norms_device(C, G.m, G.v1, G.v2, Zt, k, ld, d, n);
     const double beta = beta_of(prm, n);
@@ -320,9 +364,19 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
             out->mem = SSP_MEM_DEVICE;
             out->owned_by_context = 1;
         } else {
-            out->colptr = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
-            out->rowidx = (int32_t*)malloc(sizeof(int32_t) * (nnz + 1));
-            out->values = (double*)malloc(sizeof(double) * (nnz + 1));
+            hob.join();
+            if (hob.colptr && hob.rowidx && hob.values && nnz <= hob.cap) {
+                out->colptr = hob.colptr;
+                out->rowidx = hob.rowidx;
+                out->values = hob.values;
+                hob.colptr = nullptr;
+                hob.rowidx = nullptr;
+                hob.values = nullptr;
+            } else {
+                out->colptr = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+                out->rowidx = (int32_t*)malloc(sizeof(int32_t) * (nnz + 1));
+                out->values = (double*)malloc(sizeof(double) * (nnz + 1));
+            }
             if (!out->colptr || !out->rowidx || !out->values) {
                 free(out->colptr); free(out->rowidx); free(out->values);
                 memset(out, 0, sizeof(*out));

@@ -133,8 +133,11 @@ __global__ void k_lap_count(int64_t n, const int32_t* deg, int32_t* lapcnt) {
 }
 
 // one thread per vertex: diagonal summed in edge order (Triplet::insert, sparsifier.rs:67-68)
+// lap_eid[q]: the edge of entry q when its row is the edge's smaller vertex (row < column), else -1; each edge
+// is named once, in the column of its larger vertex
 __global__ void k_lap_fill(int64_t n, const int64_t* adj_ptr, const int32_t* adj_nbr, const int32_t* adj_eid,
-                           const double* w, const int64_t* lap_ptr, int32_t* lap_idx, double* lap_val) {
+                           const double* w, const int64_t* lap_ptr, int32_t* lap_idx, double* lap_val,
+                           int32_t* lap_eid) {
     for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         int64_t s = adj_ptr[v], e = adj_ptr[v + 1];
         if (s == e) continue;
@@ -146,14 +149,17 @@ __global__ void k_lap_fill(int64_t n, const int64_t* adj_ptr, const int32_t* adj
             int32_t u = adj_nbr[p];
             if (!done && u > v) {
                 lap_idx[q] = (int32_t)v;
+                lap_eid[q] = -1;
                 lap_val[q++] = diag;
                 done = true;
             }
             lap_idx[q] = u;
+            lap_eid[q] = u < v ? adj_eid[p] : -1;
             lap_val[q++] = -w[adj_eid[p]];
         }
         if (!done) {
             lap_idx[q] = (int32_t)v;
+            lap_eid[q] = -1;
             lap_val[q] = diag;
         }
     }
@@ -227,8 +233,9 @@ void build_graph_from_edges(Context& C, DevGraph& G, const std::string& tag) {
     G.lap_nnz = read_i64(C, d_tot);
     G.lap_idx = W.get_t<int32_t>(tag + "_lap_idx", G.lap_nnz + 1);
     G.lap_val = W.get_t<double>(tag + "_lap_val", G.lap_nnz + 1);
+    G.lap_eid = W.get_t<int32_t>(tag + "_lap_eid", G.lap_nnz + 1);
     k_lap_fill<<<grid_for(n, 128), 128, 0, C.stream>>>(n, G.adj_ptr, G.adj_nbr, G.adj_eid, G.w, G.lap_ptr,
-                                                       G.lap_idx, G.lap_val);
+                                                       G.lap_idx, G.lap_val, G.lap_eid);
     SSP_CHECK_LAUNCH();
     C.kernels_launched += 2;
 }

@@ -240,6 +240,7 @@ struct DevGraph {
     int64_t* lap_ptr = nullptr;
     int32_t* lap_idx = nullptr;
     double* lap_val = nullptr;
+    int32_t* lap_eid = nullptr;  // [lap_nnz] edge of an entry with row < column, else -1
 };
 
 // a2+a5: build edges, adjacency and L_G from an input CSC already on the device.
@@ -346,6 +347,7 @@ struct PcgReport {
     int32_t spmm_slabs = 1;  // column slabs of the Laplacian product
     double ms_resid = 0;     // mixed precision: device time of the FP64 residual products
     int64_t n_resid = 0;
+    bool diff_fused = false; // the squared diff norms were formed by the final product (d2 filled)
 };
 // Picks the elimination truncation (FactorOptions::max_degree) for this Laplacian and right-hand sides
 // by factoring a few candidates and timing a short PCG probe on the first column tile of Y.  Leaves
@@ -353,9 +355,14 @@ struct PcgReport {
 int64_t autotune_factor(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx,
                         const double* lap_val, int64_t lap_offdiag_nnz, const double* Ytiles, int32_t k,
                         const FactorOptions& base, const PcgOptions& popt, DevFactor& F, double* ms_tuning);
+// With lap_eid (the graph's per-entry edge map) and d2 (m doubles), the final product A x also forms
+// d2[e] = sum over columns of (x[v1_e] - x[v2_e])^2 in the order of diff_norms_device (per 32-column tile a
+// butterfly over the tile's columns, tiles added in order) from the rows it gathers anyway, and sets
+// rep.diff_fused; without them, or with a slab plan, d2 is left alone.
 void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx, const double* lap_val,
                 const DevFactor& F, const double* Y, int32_t k, const double** x_out, const PcgOptions& opt,
-                PcgReport& rep, int32_t* h_iters = nullptr, double* h_relres = nullptr);
+                PcgReport& rep, int32_t* h_iters = nullptr, double* h_relres = nullptr,
+                const int32_t* lap_eid = nullptr, double* d2 = nullptr);
 void rowmajor_to_tiles(Context& C, int64_t n, int32_t k, int64_t ldr, const double* src, double* dst);
 void tiles_to_rowmajor(Context& C, int64_t n, int32_t k, const double* src, double* dst, int64_t ldr);
 void precond_apply_device(Context& C, const DevFactor& F, const double* R, double* Z, int64_t ld);

@@ -29,8 +29,9 @@ static __device__ __align__(256) double g_ssp_static_scratch[SSP_STATIC_SCRATCH_
 constexpr int kMaxDevices = 64;
 std::atomic<double*> g_scratch_addr[kMaxDevices];
 
-// d_e into the scratch: one warp per edge, lanes stride the k columns of row-major Z (leading dimension
-// k), a lane-local fused multiply-add chain, then a fixed xor-butterfly -- the order of k_diff_norms.
+// d_e into the scratch: one warp per edge over row-major Z (leading dimension k), 32 columns at a time: each
+// lane squares its column's difference, a fixed xor-butterfly sums the 32 squares, and the groups' sums are
+// added in order -- the order of k_diff_norms.
 // An edge with an endpoint outside [0, n) is not read and gets d_e = NaN.
 __global__ void __launch_bounds__(256) k_norms_static(int64_t n, int64_t m, const int32_t* __restrict__ v1,
                                                       const int32_t* __restrict__ v2, const double* __restrict__ Z,
@@ -43,14 +44,16 @@ __global__ void __launch_bounds__(256) k_norms_static(int64_t n, int64_t m, cons
             if (lane == 0) d[e] = __longlong_as_double(0x7ff8000000000000LL);
             continue;
         }
-        double s = 0.0;
-        for (int32_t j = lane; j < k; j += 32) {
-            const double x = __dsub_rn(Z[a * k + j], Z[b * k + j]);
-            s = __fma_rn(x, x, s);
-        }
+        double acc = 0.0;
+        for (int32_t j0 = 0; j0 < k; j0 += 32) {
+            const int32_t j = j0 + lane;
+            const double x = j < k ? __dsub_rn(Z[a * k + j], Z[b * k + j]) : 0.0;
+            double s = __dmul_rn(x, x);
 #pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
-        if (lane == 0) d[e] = sqrt(s);
+            for (int o = 16; o >= 1; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+            acc = __dadd_rn(acc, s);
+        }
+        if (lane == 0) d[e] = sqrt(acc);
     }
 }
 

@@ -556,6 +556,102 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
     }
 }
 
+// The final product of a solve, one tile per launch, also forming the squared diff norms of the edges from
+// the rows it gathers: the edge of an entry with row < column (eid >= 0) gets, per tile, the xor-butterfly
+// sum over the tile's 32 columns of (x[row] - x[col])^2 (0 for columns past k), added to d2 in tile order
+// (first: stored) -- diff_norms_device's order.  All 32 lanes of a warp walk the same row and entry, so the
+// eid test and the butterfly are warp-uniform.  q with four accumulators (eight gathers in flight with
+// interleaved butterflies need 64 registers and ran slower: 1260 against 1231 ms per ER 1M step).
+__global__ void __launch_bounds__(CH_THREADS) k_spmm_diff(int64_t n, const int32_t* __restrict__ cstart,
+                                                          int32_t nchunks, const int64_t* __restrict__ ptr,
+                                                          const int32_t* __restrict__ idx,
+                                                          const double* __restrict__ val,
+                                                          const int32_t* __restrict__ eid, const double* xt,
+                                                          double* qt, int32_t kcols, double* __restrict__ d2,
+                                                          int first) {
+    __shared__ int32_t s_idx[CH_WARPS][CHUNK_CAP];
+    __shared__ double s_val[CH_WARPS][CHUNK_CAP];
+    __shared__ int32_t s_eid[CH_WARPS][CHUNK_CAP];
+    __shared__ int32_t s_ptr[CH_WARPS][CHUNK_ROWS + 1];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const bool live = lane < kcols;
+    int32_t* si = s_idx[w];
+    double* sv = s_val[w];
+    int32_t* se = s_eid[w];
+    int32_t* sp = s_ptr[w];
+    // one entry: its gathered value g, and the squared difference into d2 when the entry names an edge
+    auto edge = [&](int32_t e, double xo, double g) {
+        if (e < 0) return;  // warp-uniform
+        const double dx = live ? __dsub_rn(xo, g) : 0.0;
+        double sq = __dmul_rn(dx, dx);
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) sq = __dadd_rn(sq, __shfl_xor_sync(0xffffffffu, sq, o));
+        if (lane == 0) d2[e] = first ? sq : __dadd_rn(d2[e], sq);
+    };
+    for (int32_t c = blockIdx.x * CH_WARPS + w; c < nchunks; c += gridDim.x * CH_WARPS) {
+        const int32_t r0 = cstart[c], r1 = cstart[c + 1];
+        const int64_t e0 = ptr[r0], e1 = ptr[r1];
+        const int64_t ne = e1 - e0;
+        if (ne <= CHUNK_CAP) {
+            for (int64_t i = lane; i < ne; i += 32) {
+                si[i] = __ldcs(idx + e0 + i);
+                sv[i] = __ldcs(val + e0 + i);
+                se[i] = __ldcs(eid + e0 + i);
+            }
+            for (int32_t i = lane; i <= r1 - r0; i += 32) sp[i] = (int32_t)(ptr[r0 + i] - e0);
+            __syncwarp();
+            for (int32_t rr = 0; rr < r1 - r0; rr++) {
+                const int64_t row = r0 + rr;
+                const double xo = live ? xt[row * TILE + lane] : 0.0;
+                const int32_t q0 = sp[rr], q1 = sp[rr + 1];
+                double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+                int32_t q = q0;
+                for (; q + 3 < q1; q += 4) {
+                    const double g0 = live ? xt[(int64_t)si[q] * TILE + lane] : 0.0;
+                    const double g1 = live ? xt[(int64_t)si[q + 1] * TILE + lane] : 0.0;
+                    const double g2 = live ? xt[(int64_t)si[q + 2] * TILE + lane] : 0.0;
+                    const double g3 = live ? xt[(int64_t)si[q + 3] * TILE + lane] : 0.0;
+                    a0 += sv[q] * g0;
+                    a1 += sv[q + 1] * g1;
+                    a2 += sv[q + 2] * g2;
+                    a3 += sv[q + 3] * g3;
+                    edge(se[q], xo, g0);
+                    edge(se[q + 1], xo, g1);
+                    edge(se[q + 2], xo, g2);
+                    edge(se[q + 3], xo, g3);
+                }
+                for (; q < q1; q++) {
+                    const double g = live ? xt[(int64_t)si[q] * TILE + lane] : 0.0;
+                    a0 += sv[q] * g;
+                    edge(se[q], xo, g);
+                }
+                __stcs(qt + row * TILE + lane, (a0 + a1) + (a2 + a3));
+            }
+            __syncwarp();
+        } else {
+            // one long row, lane = column
+            const double xo = live ? xt[(int64_t)r0 * TILE + lane] : 0.0;
+            double a0 = 0, a1 = 0;
+            int64_t q = e0;
+            for (; q + 1 < e1; q += 2) {
+                const int32_t i0 = __ldcs(idx + q), i1 = __ldcs(idx + q + 1);
+                const double g0 = live ? xt[(int64_t)i0 * TILE + lane] : 0.0;
+                const double g1 = live ? xt[(int64_t)i1 * TILE + lane] : 0.0;
+                a0 += __ldcs(val + q) * g0;
+                a1 += __ldcs(val + q + 1) * g1;
+                edge(__ldcs(eid + q), xo, g0);
+                edge(__ldcs(eid + q + 1), xo, g1);
+            }
+            if (q < e1) {
+                const double g = live ? xt[(int64_t)__ldcs(idx + q) * TILE + lane] : 0.0;
+                a0 += __ldcs(val + q) * g;
+                edge(__ldcs(eid + q), xo, g);
+            }
+            __stcs(qt + (int64_t)r0 * TILE + lane, a0 + a1);
+        }
+    }
+}
+
 // blocks per tile: about one wave of resident blocks, so the gathered slab of the tile being worked
 // on is the only one live in L2
 static int chunk_blocks(int32_t nchunks) {
@@ -1139,7 +1235,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
 // "pcg_x" (tile-major); *x_out points at it.
 void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx, const double* lap_val,
                 const DevFactor& F, const double* Y, int32_t k, const double** x_out, const PcgOptions& opt,
-                PcgReport& rep, int32_t* h_iters, double* h_relres) {
+                PcgReport& rep, int32_t* h_iters, double* h_relres, const int32_t* lap_eid, double* d2) {
     SSP_REQUIRE(k > 0, SSP_ERR_INVALID, "pcg: k must be positive");
     const bool mixed = opt.precision == SSP_PRECISION_MIXED;
     SSP_REQUIRE(mixed || opt.precision == SSP_PRECISION_FP64, SSP_ERR_INVALID, "pcg: unknown precision");
@@ -1291,10 +1387,20 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
             if (active > 0 && !use64 && (hw > MIXED_MIN_CONTRACTION || its == 0 || hit_cap)) use64 = true;
         }
     }
-    // true relative residual ||(Y - mean) - A x|| / ||Y - mean||
-    launch_spmm<double>(C, n, A, A.val, x, q, ld, false, k);
-    SSP_CHECK_LAUNCH();
-    C.kernels_launched += A.nslabs;
+    // true relative residual ||(Y - mean) - A x|| / ||Y - mean|| (with the edges' squared diff norms when asked)
+    if (lap_eid && d2 && A.nslabs == 1) {
+        for (int64_t t = 0; t < ntiles; t++)
+            k_spmm_diff<<<dim3(A.grid.x, 1), CH_THREADS, 0, C.stream>>>(
+                n, A.chunks[0], A.nchunks[0], A.ptr, A.idx, A.val, lap_eid, x + t * n * TILE, q + t * n * TILE,
+                (int32_t)(k - t * TILE), d2, t == 0 ? 1 : 0);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched += ntiles;
+        rep.diff_fused = true;
+    } else {
+        launch_spmm<double>(C, n, A, A.val, x, q, ld, false, k);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched += A.nslabs;
+    }
     R.run<OP_SQDIFF_CENTERED, double>(Y, q, relres, mean);
     std::vector<double> hb(ld), hr(ld);
     std::vector<int32_t> hi(ld);

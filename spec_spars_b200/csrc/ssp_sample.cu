@@ -5,8 +5,10 @@
 // keep iff coin_e < p_e              sample_and_reweight  (sparsifier.rs:635-680)
 // L_H = L_G + dL, exact zeros drop   apply_reweightings   (sparsifier.rs:682-691)
 //
-// The diff-norm reduction order is fixed (lane l sums columns l, l+32, ... with fma, then an xor
-// butterfly) and mirrored by the CPU oracle, so given the same Z the norms are bit-identical.
+// The diff-norm reduction order is fixed and mirrored by the CPU oracle, so given the same Z the norms are
+// bit-identical: per 32-column tile, lane l squares the difference in its column (0 past k), an xor
+// butterfly sums the 32 squares, and the tile sums are added in tile order.  The PCG's final product can
+// form the same sums tile by tile while it gathers the same rows (pcg_device with an edge map).
 #include "ssp_internal.cuh"
 
 namespace ssp {
@@ -20,16 +22,21 @@ __global__ void __launch_bounds__(256) k_diff_norms(int64_t m, const int32_t* __
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < m; e += nw) {
         const int64_t a = v1[e], b = v2[e];
-        double s = 0.0;
-        for (int32_t j = lane; j < k; j += 32) {
-            const int64_t oa = TM ? tile_off(n, a, j) : a * ldz + j;
-            const int64_t ob = TM ? tile_off(n, b, j) : b * ldz + j;
-            const double x = __dsub_rn(Z[oa], Z[ob]);
-            s = __fma_rn(x, x, s);
-        }
+        double acc = 0.0;
+        for (int32_t j0 = 0; j0 < k; j0 += 32) {
+            const int32_t j = j0 + lane;
+            double x = 0.0;
+            if (j < k) {
+                const int64_t oa = TM ? tile_off(n, a, j) : a * ldz + j;
+                const int64_t ob = TM ? tile_off(n, b, j) : b * ldz + j;
+                x = __dsub_rn(Z[oa], Z[ob]);
+            }
+            double s = __dmul_rn(x, x);
 #pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
-        if (lane == 0) d[e] = ROOT ? sqrt(s) : s;
+            for (int o = 16; o >= 1; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+            acc = __dadd_rn(acc, s);
+        }
+        if (lane == 0) d[e] = ROOT ? sqrt(acc) : acc;
     }
 }
 

@@ -120,6 +120,7 @@ __global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, const int64_t* _
 
 void sketch_device(Context& C, const DevGraph& G, int32_t k, double scale, uint64_t seed, int uniform, double* Y,
                    int64_t ldy, int tile_major, int32_t col_lo) {
+    const cudaStream_t stream = C.stream;
     SSP_REQUIRE(k > 0 && (tile_major || ldy >= k), SSP_ERR_INVALID, "sketch: need 0 < k <= ld");
     SSP_REQUIRE(col_lo >= 0 && (int64_t)col_lo + k <= INT32_MAX, SSP_ERR_INVALID, "sketch: bad column range");
     const int32_t col_hi = col_lo + k;
@@ -129,10 +130,10 @@ void sketch_device(Context& C, const DevGraph& G, int32_t k, double scale, uint6
     const int threads = 256;
     const int blocks = grid_for(items * 32, threads, 148 * 16);
     if (uniform)
-        k_sketch_unif<<<blocks, threads, 0, C.stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, col_lo, col_hi,
+        k_sketch_unif<<<blocks, threads, 0, stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, col_lo, col_hi,
                                                         tile_lo, ntiles, scale, seed, Y, ldy, tile_major);
     else
-        k_sketch_sign<<<blocks, threads, 0, C.stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, col_lo, col_hi,
+        k_sketch_sign<<<blocks, threads, 0, stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, col_lo, col_hi,
                                                         tile_lo, ntiles, scale, seed, Y, ldy, tile_major);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;

@@ -397,3 +397,20 @@ def test_device_scan_every_depth(ssp, ctx, n):
     ref = np.zeros(n + 1, np.int64)
     np.cumsum(a, dtype=np.int64, out=ref[1:])
     assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("name", ["er5k", "grid3d", "rand2k_disconnected"])
+def test_fused_diff_norms_equal_separate_pass(ssp, ctx, monkeypatch, name):
+    """The solve's final product forms the edges' squared diff norms while it gathers x (per 32-column tile
+    a butterfly, tiles added in order); the separate pass over the edges forms the same sums: the two
+    sparsifiers must be identical bit for bit, for k in one tile (k = 13) and across several (baseline k)."""
+    G = GRAPHS[name](ssp)
+    for prm in (ssp.SparsifierParameters.cli(0.5), ssp.SparsifierParameters.baseline(1.0, pcg_tol=1e-8)):
+        monkeypatch.setenv("SSP_DIFF_FUSED", "1")
+        H1, s1 = ctx.sparsify(G, prm)
+        monkeypatch.setenv("SSP_DIFF_FUSED", "0")
+        H0, s0 = ctx.sparsify(G, prm)
+        # (the residual products sum in different orders: relres agrees to rounding only)
+        assert s1["m_out"] == s0["m_out"] and abs(s1["pcg_max_relres"] - s0["pcg_max_relres"]) <= 1e-6 * s0["pcg_max_relres"]
+        assert np.array_equal(H1.colptr, H0.colptr) and np.array_equal(H1.rowidx, H0.rowidx)
+        assert np.array_equal(H1.values.view(np.uint64), H0.values.view(np.uint64))
