@@ -448,6 +448,7 @@ def main():
         e1 = torch.cuda.Event(enable_timing=True)
         h2d = G.colptr.nbytes + G.rowidx.nbytes + G.values.nbytes
         d2h = 0
+        ctx.sparsify(G, prm)  # untimed: the host path's one-time set-up (its pinned staging ring)
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(args.e2e_steps):

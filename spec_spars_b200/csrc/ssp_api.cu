@@ -64,6 +64,7 @@ static void destroy_context(Context& C) {
     cudaSetDevice(C.device);
     if (C.stream) cudaStreamSynchronize(C.stream);
     C.ws.release();
+    release_staging(C);
     if (C.h_pinned) cudaFreeHost(C.h_pinned);
     if (C.own_stream && C.stream) cudaStreamDestroy(C.stream);
     C.h_pinned = nullptr;
@@ -114,10 +115,10 @@ static DevCsc to_device(Context& C, const ssp_csc* m, const char* tag) {
     int64_t* cp = C.ws.get_t<int64_t>(t + "_cp", m->n + 1);
     int32_t* ri = C.ws.get_t<int32_t>(t + "_ri", m->nnz + 1);
     double* va = C.ws.get_t<double>(t + "_va", m->nnz + 1);
-    SSP_CUDA(cudaMemcpyAsync(cp, m->colptr, sizeof(int64_t) * (m->n + 1), cudaMemcpyHostToDevice, C.stream));
+    copy_h2d(C, cp, m->colptr, sizeof(int64_t) * (m->n + 1));
     if (m->nnz) {
-        SSP_CUDA(cudaMemcpyAsync(ri, m->rowidx, sizeof(int32_t) * m->nnz, cudaMemcpyHostToDevice, C.stream));
-        SSP_CUDA(cudaMemcpyAsync(va, m->values, sizeof(double) * m->nnz, cudaMemcpyHostToDevice, C.stream));
+        copy_h2d(C, ri, m->rowidx, sizeof(int32_t) * m->nnz);
+        copy_h2d(C, va, m->values, sizeof(double) * m->nnz);
     }
     d.colptr = cp;
     d.rowidx = ri;
@@ -382,10 +383,9 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
                 memset(out, 0, sizeof(*out));
                 throw Error(SSP_ERR_NOMEM, "host allocation of the output failed");
             }
-            SSP_CUDA(cudaMemcpyAsync(out->colptr, lh_ptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, C.stream));
-            SSP_CUDA(cudaMemcpyAsync(out->rowidx, lh_idx, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, C.stream));
-            SSP_CUDA(cudaMemcpyAsync(out->values, lh_val, sizeof(double) * nnz, cudaMemcpyDeviceToHost, C.stream));
-            SSP_CUDA(cudaStreamSynchronize(C.stream));
+            copy_d2h(C, out->colptr, lh_ptr, sizeof(int64_t) * (n + 1));
+            copy_d2h(C, out->rowidx, lh_idx, sizeof(int32_t) * nnz);
+            copy_d2h(C, out->values, lh_val, sizeof(double) * nnz);
             out->mem = SSP_MEM_HOST;
         }
     }

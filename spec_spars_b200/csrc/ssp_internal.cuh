@@ -153,6 +153,9 @@ struct Context {
     bool own_stream = false;
     Workspace ws;
     int64_t* h_pinned = nullptr;  // small pinned scratch for scalar readbacks
+    // pinned staging ring for large copies between pageable host memory and the device (copy_*_large)
+    char* h_stage = nullptr;
+    cudaEvent_t stage_ev[3] = {nullptr, nullptr, nullptr};
     int verbose = 0;
     int64_t kernels_launched = 0;  // count of library kernel launches (for bench accounting)
 };
@@ -206,6 +209,13 @@ constexpr int CHUNK_CAP = SSP_CHUNK_CAP;
 constexpr int CHUNK_ROWS = 32;
 void make_chunks(const std::vector<int64_t>& ptr, int32_t r0, int32_t r1, std::vector<int32_t>& starts);
 void make_chunks(const int64_t* ptr, int32_t r0, int32_t r1, std::vector<int32_t>& starts);
+// Copies between pageable host memory and the device on C.stream, returning once the host side is done
+// (host to device: the source may be reused; device to host: the data is in dst).  Large copies go through
+// a pinned staging ring with the host-side memcpy split over a few threads and overlapped with the DMA;
+// small ones are plain cudaMemcpyAsync.
+void copy_h2d(Context& C, void* dst, const void* src, size_t bytes);
+void copy_d2h(Context& C, void* dst, const void* src, size_t bytes);
+void release_staging(Context& C);
 // Matrix Market on the device (ssp_mtxio.cu).  read_mtx_device leaves the CSC in workspace buffers named
 // after tag and returns false when the file needs the host reader; write_mtx_device takes device arrays.
 bool read_mtx_device(Context& C, const char* path, int64_t* n, int64_t* nnz, int64_t** colptr, int32_t** rowidx,

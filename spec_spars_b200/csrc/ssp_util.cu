@@ -1,5 +1,9 @@
 // ssp_util.cu -- deterministic device-wide scans and segmented sorts used by the
 // graph assembly and factorization stages.
+#include <algorithm>
+#include <cstring>
+#include <thread>
+
 #include "ssp_internal.cuh"
 #include "ssp_sort.cuh"
 
@@ -365,6 +369,97 @@ void radix_sort_u64(Context& C, uint64_t* keys, int32_t* vals, int64_t n, int ke
         SSP_CUDA(cudaMemcpyAsync(keys, ka, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, C.stream));
         SSP_CUDA(cudaMemcpyAsync(vals, va, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, C.stream));
     }
+}
+
+// ---------------------------------------------------------------- large host <-> device copies
+// CUDA copies pageable memory through its own staging at one host memcpy's speed (11 GB/s measured on the
+// B200 host, against 37-40 GB/s from pinned memory).  Here a 3 x 32 MB pinned ring takes the chunks: the
+// host side of each chunk is copied by up to four threads while the previous chunk's DMA runs.
+namespace {
+constexpr size_t STAGE_CHUNK = 32u << 20;
+constexpr int STAGE_SLOTS = 3;
+constexpr size_t LARGE_COPY = 64u << 20;  // smaller copies stay plain cudaMemcpyAsync
+
+void ensure_staging(Context& C) {
+    if (C.h_stage) return;
+    SSP_CUDA(cudaHostAlloc((void**)&C.h_stage, STAGE_CHUNK * STAGE_SLOTS, cudaHostAllocDefault));
+    for (auto& e : C.stage_ev) SSP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+
+void parallel_memcpy(char* dst, const char* src, size_t n) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int T = (int)std::min<unsigned>(4, hw);
+    if (T <= 1 || n < (4u << 20)) {
+        memcpy(dst, src, n);
+        return;
+    }
+    const size_t part = (n / T + 4095) & ~(size_t)4095;
+    std::thread th[4];
+    for (int t = 1; t < T; t++) {
+        const size_t a = std::min(n, part * t), b = std::min(n, part * (t + 1));
+        if (a < b) th[t] = std::thread([=] { memcpy(dst + a, src + a, b - a); });
+    }
+    memcpy(dst, src, std::min(n, part));
+    for (int t = 1; t < T; t++)
+        if (th[t].joinable()) th[t].join();
+}
+}  // namespace
+
+void copy_h2d(Context& C, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return;
+    if (bytes < LARGE_COPY) {
+        SSP_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, C.stream));
+        return;
+    }
+    ensure_staging(C);
+    size_t off = 0;
+    for (int i = 0; off < bytes; i++) {
+        const int slot = i % STAGE_SLOTS;
+        const size_t n = std::min(STAGE_CHUNK, bytes - off);
+        if (i >= STAGE_SLOTS) SSP_CUDA(cudaEventSynchronize(C.stage_ev[slot]));
+        char* st = C.h_stage + (size_t)slot * STAGE_CHUNK;
+        parallel_memcpy(st, (const char*)src + off, n);
+        SSP_CUDA(cudaMemcpyAsync((char*)dst + off, st, n, cudaMemcpyHostToDevice, C.stream));
+        SSP_CUDA(cudaEventRecord(C.stage_ev[slot], C.stream));
+        off += n;
+    }
+    // the ring is reused by the next call; the caller's source is already free
+    for (auto& e : C.stage_ev) SSP_CUDA(cudaEventSynchronize(e));
+}
+
+void copy_d2h(Context& C, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return;
+    if (bytes < LARGE_COPY) {
+        SSP_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+        return;
+    }
+    ensure_staging(C);
+    const size_t nch = (bytes + STAGE_CHUNK - 1) / STAGE_CHUNK;
+    auto issue = [&](size_t i) {
+        const int slot = (int)(i % STAGE_SLOTS);
+        const size_t off = i * STAGE_CHUNK, n = std::min(STAGE_CHUNK, bytes - off);
+        SSP_CUDA(cudaMemcpyAsync(C.h_stage + (size_t)slot * STAGE_CHUNK, (const char*)src + off, n,
+                                 cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaEventRecord(C.stage_ev[slot], C.stream));
+    };
+    for (size_t i = 0; i < nch && i < (size_t)STAGE_SLOTS; i++) issue(i);
+    for (size_t i = 0; i < nch; i++) {
+        const int slot = (int)(i % STAGE_SLOTS);
+        const size_t off = i * STAGE_CHUNK, n = std::min(STAGE_CHUNK, bytes - off);
+        SSP_CUDA(cudaEventSynchronize(C.stage_ev[slot]));
+        parallel_memcpy((char*)dst + off, C.h_stage + (size_t)slot * STAGE_CHUNK, n);
+        if (i + STAGE_SLOTS < nch) issue(i + STAGE_SLOTS);
+    }
+}
+
+void release_staging(Context& C) {
+    for (auto& e : C.stage_ev) {
+        if (e) cudaEventDestroy(e);
+        e = nullptr;
+    }
+    if (C.h_stage) cudaFreeHost(C.h_stage);
+    C.h_stage = nullptr;
 }
 
 }  // namespace ssp

@@ -414,3 +414,27 @@ def test_fused_diff_norms_equal_separate_pass(ssp, ctx, monkeypatch, name):
         assert s1["m_out"] == s0["m_out"] and abs(s1["pcg_max_relres"] - s0["pcg_max_relres"]) <= 1e-6 * s0["pcg_max_relres"]
         assert np.array_equal(H1.colptr, H0.colptr) and np.array_equal(H1.rowidx, H0.rowidx)
         assert np.array_equal(H1.values.view(np.uint64), H0.values.view(np.uint64))
+
+
+def test_large_host_buffers_match_device_buffers(ssp, ctx, tmp_path):
+    """A graph whose value arrays exceed the staged-copy threshold (64 MB): host in / host out goes through the
+    pinned ring and the pre-faulted result buffers, and must return exactly the device path's L_H (both
+    written with the device writer, whose %.17g text round-trips every value)."""
+    import ctypes
+    import torch
+    from spec_spars_b200 import _lib as L
+    G = ssp.gen_er(1_000_000, 10.0, 0.5, 2.0, 4)
+    assert G.values.nbytes > 64 << 20
+    prm = ssp.SparsifierParameters.baseline(1.5, pcg_tol=1e-6)
+    H, st = ctx.sparsify(G, prm)
+    assert H.values.nbytes > 64 << 20
+    dev = torch.device("cuda", 0)
+    cp, ri, va = (torch.from_numpy(a).to(dev) for a in (G.colptr, G.rowidx, G.values))
+    (nnz, dcp, dri, dva), st2 = ctx.sparsify_device(G.n, G.nnz, cp.data_ptr(), ri.data_ptr(), va.data_ptr(), prm)
+    torch.cuda.synchronize()
+    assert nnz == H.nnz and st["m_out"] == st2["m_out"]
+    pd, ph = tmp_path / "dev.mtx", tmp_path / "host.mtx"
+    s = L._Csc(G.n, nnz, dcp, dri, dva, L.SSP_MEM_DEVICE)
+    L._check(L.lib().ssp_write_mtx_device(ctx._h, str(pd).encode(), ctypes.byref(s)))
+    ctx.write_mtx(str(ph), H)
+    assert ph.read_bytes() == pd.read_bytes()
