@@ -30,6 +30,10 @@ WORKLOADS = {
     # 3-D 7-point grids with log-uniform weights in [1e-3, 1e3] (the ill-conditioned mesh configuration)
     "grid3d_64": ("grid3d", dict(nx=64, ny=64, nz=64, lo=-3.0, hi=3.0, seed=2), 0.5),
     "grid3d_128": ("grid3d", dict(nx=128, ny=128, nz=128, lo=-3.0, hi=3.0, seed=2), 0.5),
+    # the R-MAT configuration: scale 22, edge factor 16, (a, b, c) = (0.57, 0.19, 0.19), largest connected
+    # component, LogNormal(0, 1) weights, eps 0.3 (k ~ 4000: the columns are solved in memory-sized batches)
+    "rmat_s22": ("rmat", dict(scale=22, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=3), 0.3),
+    "rmat_s18": ("rmat", dict(scale=18, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=3), 0.3),
 }
 PCG_TOL = 1e-8
 
@@ -42,6 +46,8 @@ def make_graph(S, name, rank=0):
         return S.gen_er(kw["n"], kw["avg_degree"], kw["wlo"], kw["whi"], kw["seed"]), eps
     if kind == "grid3d":
         return S.gen_grid3d(kw["nx"], kw["ny"], kw["nz"], kw["lo"], kw["hi"], kw["seed"]), eps
+    if kind == "rmat":
+        return S.gen_rmat(kw["scale"], kw["edge_factor"], kw["a"], kw["b"], kw["c"], kw["seed"] + rank), eps
     return S.gen_grid2d(kw["nx"], kw["ny"]), eps
 
 

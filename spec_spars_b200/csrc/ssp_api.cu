@@ -213,6 +213,59 @@ struct HostOutBuffers {
 };
 constexpr int64_t HOST_OUT_PREFAULT_MIN = 1 << 20;  // entries; smaller outputs allocate at the end
 
+// Columns solved per pass.  The PCG holds six n x ld FP64 blocks (sketch, x, r, z, p, q; the mixed mode adds
+// five FP32 blocks and an FP64 increment), which for the R-MAT configuration (scale 22, eps 0.3: k = 3917)
+// need 450 GB.  The columns are independent once the factor exists, so they are solved in batches of whole
+// 32-column tiles.  Whether to batch is decided before the factorization with room set aside for it (70 % of
+// the free memory, less 40 B per Laplacian entry and 48 B per edge); the batch size after it, from the memory
+// then free (80 %, less the per-edge arrays).  SSP_COLUMN_BATCH=<columns> sets the batch.
+static double column_bytes(int64_t n, int32_t precision) {
+    return (double)n * (8.0 * 6 + (precision == SSP_PRECISION_MIXED ? 4.0 * 5 + 8.0 : 0.0));
+}
+static int32_t forced_batch(int32_t k) {
+    if (const char* e = getenv("SSP_COLUMN_BATCH")) {
+        const int b = atoi(e);
+        if (b > 0) return std::min<int32_t>(k, std::max<int32_t>(SSP_TILE, b / SSP_TILE * SSP_TILE));
+    }
+    return 0;
+}
+static double free_for_solve(Context& C) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        return 1e300;
+    }
+    // the solve's own buffers from an earlier call are reused
+    return (double)fr + (double)(C.ws.bytes_with_prefix("sp_Y") + C.ws.bytes_with_prefix("pcg"));
+}
+static bool columns_fit(Context& C, const DevGraph& G, int32_t k, int32_t precision) {
+    const double need = column_bytes(G.n, precision) * (double)tile_ld(k);
+    return need <= 0.7 * free_for_solve(C) - 40.0 * (double)G.lap_nnz - 48.0 * (double)G.m;
+}
+static int32_t batch_after_factor(Context& C, const DevGraph& G, int32_t k, int32_t precision) {
+    const double avail = 0.8 * free_for_solve(C) - 48.0 * (double)G.m - (1.0 * (1 << 30));
+    const int64_t cols = (int64_t)(avail / column_bytes(G.n, precision)) / SSP_TILE * SSP_TILE;
+    return (int32_t)std::max<int64_t>(SSP_TILE, std::min<int64_t>(cols, k));
+}
+
+static void merge_report(PcgReport& a, const PcgReport& b, int32_t ka, int32_t kb) {
+    a.mean_iters = (a.mean_iters * ka + b.mean_iters * kb) / (double)(ka + kb);
+    a.max_iters_used = std::max(a.max_iters_used, b.max_iters_used);
+    a.max_relres = std::max(a.max_relres, b.max_relres);
+    a.not_converged += b.not_converged;
+    a.ms_spmm += b.ms_spmm;
+    a.n_spmm += b.n_spmm;
+    a.ms_precond += b.ms_precond;
+    a.n_precond += b.n_precond;
+    a.ms_loop += b.ms_loop;
+    a.iters_run = std::max(a.iters_run, b.iters_run);
+    a.refinements += b.refinements;
+    a.fp64_rounds += b.fp64_rounds;
+    a.ms_resid += b.ms_resid;
+    a.n_resid += b.n_resid;
+    a.diff_fused = a.diff_fused && b.diff_fused;
+}
+
 static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* prm, int32_t out_mem, ssp_csc_out* out,
                           ssp_stats* st, const ShardArgs* sh = nullptr) {
     SSP_REQUIRE(prm, SSP_ERR_INVALID, "params is NULL");
@@ -238,11 +291,15 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
         col_lo = sh->col_lo;
         kl = sh->col_hi - sh->col_lo;
     }
-    const int64_t ld = tile_ld(kl);
+    // one shard of columns per call; otherwise all columns at once, or batches sized after the factorization
+    const bool can_batch = !finish_only && !(sh && sh->sq_out);
+    const int32_t forced = can_batch ? forced_batch(kl) : 0;
+    const bool batched = can_batch && ((forced > 0 && forced < kl) || !columns_fit(C, G, kl, prm->precision));
+    int32_t kb = kl;
     double* Y = nullptr;
-    if (!finish_only) {
-        Y = C.ws.get_t<double>("sp_Y", (size_t)n * ld);
-        sketch_device(C, SG, kl, scale, prm->sketch_seed, prm->sketch_uniform, Y, ld, 1, col_lo);
+    if (!finish_only && !batched) {
+        Y = C.ws.get_t<double>("sp_Y", (size_t)n * tile_ld(kl));
+        sketch_device(C, SG, kl, scale, prm->sketch_seed, prm->sketch_uniform, Y, tile_ld(kl), 1, col_lo);
     }
     T.mark();  // 2
     DevFactor F;
@@ -265,7 +322,7 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
         // the same factor
         const double* probe = Y;
         const int32_t kp = std::min<int32_t>(k, SSP_PROBE_COLS);
-        if (col_lo != 0 || kl < kp) {
+        if (col_lo != 0 || kl < kp || batched) {
             double* Yp = C.ws.get_t<double>("sp_Yprobe", (size_t)n * tile_ld(kp));
             sketch_device(C, SG, kp, scale, prm->sketch_seed, prm->sketch_uniform, Yp, tile_ld(kp), 1, 0);
             probe = Yp;
@@ -283,8 +340,32 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     const bool fuse = !(fe && fe[0] == '0');
     double* d2 = (finish_only || !fuse) ? nullptr
                  : (sh && sh->sq_out) ? sh->sq_out : C.ws.get_t<double>("sp_d2", G.m + 1);
+    double* d2sum = batched ? C.ws.get_t<double>("sp_d2", G.m + 1) : nullptr;  // batches: their squared sums
+    if (batched) {
+        kb = forced > 0 ? forced : batch_after_factor(C, G, kl, prm->precision);
+        Y = C.ws.get_t<double>("sp_Y", (size_t)n * tile_ld(kb));
+        sketch_device(C, SG, kb, scale, prm->sketch_seed, prm->sketch_uniform, Y, tile_ld(kb), 1, 0);
+    }
     if (!finish_only)
-        pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, kl, &Zt, po, rep, nullptr, nullptr, G.lap_eid, d2);
+        pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, kb, &Zt, po, rep, nullptr, nullptr, G.lap_eid, d2);
+    if (batched) {
+        // the batches' squared diff norms accumulate tile by tile into d2sum: fused, they continue the single
+        // pass's order exactly; from the separate pass, each batch's partial sum is added
+        double* part = C.ws.get_t<double>("sp_d2part", G.m + 1);
+        if (!rep.diff_fused) diff_sq_device(C, G.m, G.v1, G.v2, Zt, kb, n, d2sum);
+        for (int32_t c0 = kb; c0 < kl; c0 += kb) {
+            const int32_t kc = std::min(kb, kl - c0);
+            sketch_device(C, SG, kc, scale, prm->sketch_seed, prm->sketch_uniform, Y, tile_ld(kc), 1, c0);
+            PcgReport rb;
+            pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, kc, &Zt, po, rb, nullptr, nullptr, G.lap_eid,
+                       fuse ? d2sum : nullptr, true);
+            if (!rb.diff_fused) {
+                diff_sq_device(C, G.m, G.v1, G.v2, Zt, kc, n, part);
+                add_device(C, G.m, part, d2sum);
+            }
+            merge_report(rep, rb, c0, kc);
+        }
+    }
     T.mark();  // 4
     if (sh && sh->sq_out) {
         if (!rep.diff_fused) diff_sq_device(C, G.m, G.v1, G.v2, Zt, kl, n, sh->sq_out);
@@ -326,10 +407,12 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     double* coins = C.ws.get_t<double>("sp_coins", G.m + 1);
     if (finish_only)
         sqrt_device(C, G.m, sh->sq_in, d);
+    else if (batched)
+        sqrt_device(C, G.m, d2sum, d);
     else if (rep.diff_fused)
         sqrt_device(C, G.m, d2, d);
     else
-        diff_norms_device(C, G.m, G.v1, G.v2, Zt, k, ld, d, n);
+        diff_norms_device(C, G.m, G.v1, G.v2, Zt, k, tile_ld(kl), d, n);
     const double beta = beta_of(prm, n);
     const double denom = prm->prob_variance_correction ? (double)k * scale * scale : (double)k;
     probs_device(C, G.m, G.w, d, beta, denom, p);

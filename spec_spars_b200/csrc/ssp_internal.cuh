@@ -142,6 +142,12 @@ public:
         for (auto& kv : bufs_) s += kv.second.bytes;
         return s;
     }
+    size_t bytes_with_prefix(const std::string& p) const {
+        size_t s = 0;
+        for (auto& kv : bufs_)
+            if (kv.first.compare(0, p.size(), p) == 0) s += kv.second.bytes;
+        return s;
+    }
 private:
     struct Buf { void* ptr; size_t bytes; };
     std::map<std::string, Buf> bufs_;
@@ -372,7 +378,7 @@ int64_t autotune_factor(Context& C, int64_t n, const int64_t* lap_ptr, const int
 void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx, const double* lap_val,
                 const DevFactor& F, const double* Y, int32_t k, const double** x_out, const PcgOptions& opt,
                 PcgReport& rep, int32_t* h_iters = nullptr, double* h_relres = nullptr,
-                const int32_t* lap_eid = nullptr, double* d2 = nullptr);
+                const int32_t* lap_eid = nullptr, double* d2 = nullptr, bool d2_accumulate = false);
 void rowmajor_to_tiles(Context& C, int64_t n, int32_t k, int64_t ldr, const double* src, double* dst);
 void tiles_to_rowmajor(Context& C, int64_t n, int32_t k, const double* src, double* dst, int64_t ldr);
 void precond_apply_device(Context& C, const DevFactor& F, const double* R, double* Z, int64_t ld);
@@ -385,6 +391,8 @@ void diff_norms_device(Context& C, int64_t m, const int32_t* v1, const int32_t* 
 void diff_sq_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z, int32_t k,
                     int64_t n_tile_major, double* sq);
 void sqrt_device(Context& C, int64_t m, const double* sq, double* d);
+// dst[i] += src[i]
+void add_device(Context& C, int64_t m, const double* src, double* dst);
 void probs_device(Context& C, int64_t m, const double* w, const double* d, double beta, double denom, double* p);
 void coins_device(Context& C, int64_t m, uint64_t seed, double* coins);
 

@@ -1235,7 +1235,8 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
 // "pcg_x" (tile-major); *x_out points at it.
 void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx, const double* lap_val,
                 const DevFactor& F, const double* Y, int32_t k, const double** x_out, const PcgOptions& opt,
-                PcgReport& rep, int32_t* h_iters, double* h_relres, const int32_t* lap_eid, double* d2) {
+                PcgReport& rep, int32_t* h_iters, double* h_relres, const int32_t* lap_eid, double* d2,
+                bool d2_accumulate) {
     SSP_REQUIRE(k > 0, SSP_ERR_INVALID, "pcg: k must be positive");
     const bool mixed = opt.precision == SSP_PRECISION_MIXED;
     SSP_REQUIRE(mixed || opt.precision == SSP_PRECISION_FP64, SSP_ERR_INVALID, "pcg: unknown precision");
@@ -1392,7 +1393,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         for (int64_t t = 0; t < ntiles; t++)
             k_spmm_diff<<<dim3(A.grid.x, 1), CH_THREADS, 0, C.stream>>>(
                 n, A.chunks[0], A.nchunks[0], A.ptr, A.idx, A.val, lap_eid, x + t * n * TILE, q + t * n * TILE,
-                (int32_t)(k - t * TILE), d2, t == 0 ? 1 : 0);
+                (int32_t)(k - t * TILE), d2, (t == 0 && !d2_accumulate) ? 1 : 0);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += ntiles;
         rep.diff_fused = true;

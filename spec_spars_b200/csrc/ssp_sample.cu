@@ -150,6 +150,18 @@ void diff_sq_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2,
     C.kernels_launched++;
 }
 
+__global__ void k_add_vec(int64_t m, const double* __restrict__ src, double* __restrict__ dst) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x)
+        dst[e] = __dadd_rn(dst[e], src[e]);
+}
+
+void add_device(Context& C, int64_t m, const double* src, double* dst) {
+    if (m == 0) return;
+    k_add_vec<<<grid_for(m, 256), 256, 0, C.stream>>>(m, src, dst);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+}
+
 void sqrt_device(Context& C, int64_t m, const double* sq, double* d) {
     if (m == 0) return;
     k_sqrt_vec<<<grid_for(m, 256), 256, 0, C.stream>>>(m, sq, d);

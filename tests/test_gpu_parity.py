@@ -438,3 +438,22 @@ def test_large_host_buffers_match_device_buffers(ssp, ctx, tmp_path):
     L._check(L.lib().ssp_write_mtx_device(ctx._h, str(pd).encode(), ctypes.byref(s)))
     ctx.write_mtx(str(ph), H)
     assert ph.read_bytes() == pd.read_bytes()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_column_batches_match_single_pass(ssp, ctx, monkeypatch, precision):
+    """Columns solved in memory-sized batches (forced here to 64 columns: k = 205 in four batches, the last
+    partial): the factor is built once and the squared diff norms accumulate tile by tile, so the sparsifier
+    equals the single pass up to the solves' rounding (FP64: the same keep set, weights within 1e-9)."""
+    G = GRAPHS["er5k"](ssp)
+    prm = ssp.SparsifierParameters.baseline(1.0, pcg_tol=1e-9)
+    prm.precision = precision
+    monkeypatch.delenv("SSP_COLUMN_BATCH", raising=False)
+    H1, s1 = ctx.sparsify(G, prm)
+    monkeypatch.setenv("SSP_COLUMN_BATCH", "64")
+    H4, s4 = ctx.sparsify(G, prm)
+    assert s1["k"] == s4["k"] == 205 and s4["pcg_max_relres"] <= 1e-9 * 1.0001
+    assert abs(s1["m_out"] - s4["m_out"]) <= (0 if precision == 0 else 3)
+    if precision == 0:
+        assert np.array_equal(H1.colptr, H4.colptr) and np.array_equal(H1.rowidx, H4.rowidx)
+        np.testing.assert_allclose(H4.values, H1.values, rtol=1e-9, atol=0)
