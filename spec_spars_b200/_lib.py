@@ -155,6 +155,9 @@ def lib():
                                ctypes.POINTER(_SolveReport)], ctypes.c_int),
             "ssp_sparsify": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(_Params), I32, ctypes.POINTER(_CscOut),
                               ctypes.POINTER(_Stats)], ctypes.c_int),
+            "ssp_sparsify_laplacian": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(_Params), I32,
+                                        ctypes.POINTER(_CscOut), ctypes.POINTER(_Stats)], ctypes.c_int),
+            "ssp_laplacian_to_graph": ([ctypes.POINTER(_Csc), ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_csc_free": ([ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_sparsify_mtx": ([ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_Params),
                                   ctypes.POINTER(_Stats)], ctypes.c_int),
@@ -313,6 +316,15 @@ def _take_out(out):
 def read_mtx(path):
     out = _CscOut()
     _check(lib().ssp_read_mtx(path.encode(), ctypes.byref(out)))
+    return _take_out(out)
+
+
+def laplacian_to_graph(lap):
+    """The graph whose Laplacian is lap: entry (i, j) = -lap[i, j] off the diagonal, the diagonal dropped
+    (host only, no GPU needed)."""
+    s = lap._struct()
+    out = _CscOut()
+    _check(lib().ssp_laplacian_to_graph(ctypes.byref(s), ctypes.byref(out)))
     return _take_out(out)
 
 
@@ -515,6 +527,16 @@ class Context:
         st = _Stats()
         _check(lib().ssp_sparsify(self._h, ctypes.byref(g), ctypes.byref(params._s), SSP_MEM_HOST,
                                   ctypes.byref(out), ctypes.byref(st)))
+        return _take_out(out), _stats_dict(st)
+
+    def sparsify_laplacian(self, lap, params):
+        """Host Laplacian L_G in (as Sparsifier::from_matrix reads one, sparsifier.rs:299-300), host L_H out;
+        the same result as sparsify on laplacian_to_graph(lap)."""
+        g = lap._struct()
+        out = _CscOut()
+        st = _Stats()
+        _check(lib().ssp_sparsify_laplacian(self._h, ctypes.byref(g), ctypes.byref(params._s), SSP_MEM_HOST,
+                                            ctypes.byref(out), ctypes.byref(st)))
         return _take_out(out), _stats_dict(st)
 
     def sparsify_device(self, n, nnz, colptr_ptr, rowidx_ptr, values_ptr, params):

@@ -742,6 +742,76 @@ int ssp_sparsify(ssp_context* c, const ssp_csc* graph, const ssp_params* params,
     });
 }
 
+static void host_out(const HostCsc& h, ssp_csc_out* out);
+
+// the Laplacian's off-diagonal entries, negated, in their stored order (host arrays)
+static void laplacian_to_graph_host(int64_t n, int64_t nnz, const int64_t* cp, const int32_t* ri, const double* va,
+                                    HostCsc& g) {
+    g.n = n;
+    g.colptr.assign(n + 1, 0);
+    g.rowidx.clear();
+    g.val.clear();
+    for (int64_t j = 0; j < n; j++) {
+        SSP_REQUIRE(cp[j] <= cp[j + 1] && cp[j + 1] <= nnz, SSP_ERR_INVALID, "CSC colptr must be non-decreasing");
+        for (int64_t p = cp[j]; p < cp[j + 1]; p++) {
+            if (ri[p] == j) continue;
+            g.rowidx.push_back(ri[p]);
+            g.val.push_back(-va[p]);
+        }
+        g.colptr[j + 1] = (int64_t)g.rowidx.size();
+    }
+}
+
+static void laplacian_to_host_graph(Context& C, const ssp_csc* lap, HostCsc& g) {
+    SSP_REQUIRE(lap && lap->n > 0 && lap->nnz >= 0 && lap->colptr && (lap->nnz == 0 || (lap->rowidx && lap->values)),
+                SSP_ERR_INVALID, "invalid CSC descriptor");
+    if (lap->mem == SSP_MEM_DEVICE) {
+        std::vector<int64_t> cp(lap->n + 1);
+        std::vector<int32_t> ri(lap->nnz + 1);
+        std::vector<double> va(lap->nnz + 1);
+        SSP_CUDA(cudaMemcpyAsync(cp.data(), lap->colptr, sizeof(int64_t) * (lap->n + 1), cudaMemcpyDeviceToHost,
+                                 C.stream));
+        if (lap->nnz) {
+            SSP_CUDA(cudaMemcpyAsync(ri.data(), lap->rowidx, sizeof(int32_t) * lap->nnz, cudaMemcpyDeviceToHost,
+                                     C.stream));
+            SSP_CUDA(cudaMemcpyAsync(va.data(), lap->values, sizeof(double) * lap->nnz, cudaMemcpyDeviceToHost,
+                                     C.stream));
+        }
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+        SSP_REQUIRE(cp[0] == 0 && cp[lap->n] == lap->nnz, SSP_ERR_INVALID, "CSC colptr must start at 0 and end at nnz");
+        laplacian_to_graph_host(lap->n, lap->nnz, cp.data(), ri.data(), va.data(), g);
+        return;
+    }
+    SSP_REQUIRE(lap->colptr[0] == 0 && lap->colptr[lap->n] == lap->nnz, SSP_ERR_INVALID,
+                "CSC colptr must start at 0 and end at nnz");
+    laplacian_to_graph_host(lap->n, lap->nnz, lap->colptr, lap->rowidx, lap->values, g);
+}
+
+int ssp_laplacian_to_graph(const ssp_csc* lap, ssp_csc_out* graph) {
+    return guarded([&] {
+        SSP_REQUIRE(lap && graph && lap->mem == SSP_MEM_HOST, SSP_ERR_INVALID, "laplacian_to_graph needs a host CSC");
+        SSP_REQUIRE(lap->n > 0 && lap->nnz >= 0 && lap->colptr && (lap->nnz == 0 || (lap->rowidx && lap->values)),
+                    SSP_ERR_INVALID, "invalid CSC descriptor");
+        SSP_REQUIRE(lap->colptr[0] == 0 && lap->colptr[lap->n] == lap->nnz, SSP_ERR_INVALID,
+                    "CSC colptr must start at 0 and end at nnz");
+        HostCsc g;
+        laplacian_to_graph_host(lap->n, lap->nnz, lap->colptr, lap->rowidx, lap->values, g);
+        host_out(g, graph);
+    });
+}
+
+int ssp_sparsify_laplacian(ssp_context* c, const ssp_csc* lap, const ssp_params* params, int32_t out_mem,
+                           ssp_csc_out* out, ssp_stats* stats) {
+    return guarded([&] {
+        SSP_REQUIRE(c, SSP_ERR_INVALID, "ctx is NULL");
+        SSP_CUDA(cudaSetDevice(c->ctx.device));
+        HostCsc g;
+        laplacian_to_host_graph(c->ctx, lap, g);
+        const ssp_csc gc{g.n, g.colptr[g.n], g.colptr.data(), g.rowidx.data(), g.val.data(), SSP_MEM_HOST};
+        sparsify_impl(c->ctx, &gc, params, out_mem, out, stats);
+    });
+}
+
 int ssp_shard_leverage(ssp_context* c, const ssp_csc* graph, const ssp_params* params, int32_t col_begin,
                        int32_t col_end, double* sq, int64_t* m, ssp_stats* stats) {
     return guarded([&] {
