@@ -23,6 +23,11 @@ GRAPHS = {
     "rmat": lambda ssp: ssp.gen_rmat(11, 16, 0.57, 0.19, 0.19, 4),  # hubs and isolated vertices
     "grid3d": lambda ssp: ssp.gen_grid3d(12, 10, 9, -3, 3, 5),
 }
+# the graphs the other GPU tests already sparsify with the CLI parameters
+SPARSIFY = {
+    "er5k": lambda ssp: ssp.gen_er(5000, 20.0, 0.5, 2.0, 1),
+    "grid3d": lambda ssp: ssp.gen_grid3d(10, 9, 8, -3, 3, 2),
+}
 
 
 @pytest.mark.parametrize("name", list(GRAPHS))
@@ -59,9 +64,9 @@ def test_laplacian_to_graph_rejects_bad_descriptors(ssp):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["er", "rmat"])
+@pytest.mark.parametrize("name", list(SPARSIFY))
 def test_sparsify_laplacian_equals_sparsify(ssp, ora, ctx, name):
-    G = GRAPHS[name](ssp)
+    G = SPARSIFY[name](ssp)
     L = _laplacian_of(ssp, ora, G)
     prm = ssp.SparsifierParameters.cli(0.5)
     H, st = ctx.sparsify(G, prm)
@@ -73,7 +78,7 @@ def test_sparsify_laplacian_equals_sparsify(ssp, ora, ctx, name):
 def test_sparsify_laplacian_from_device_memory(ssp, ora, ctx):
     import torch
     import spec_spars_b200._lib as Lb
-    G = GRAPHS["er"](ssp)
+    G = SPARSIFY["er5k"](ssp)
     L = _laplacian_of(ssp, ora, G)
     prm = ssp.SparsifierParameters.cli(0.5)
     H, _ = ctx.sparsify(G, prm)
