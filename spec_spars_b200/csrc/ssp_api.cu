@@ -988,20 +988,34 @@ int ssp_csc_free(ssp_csc_out* out) {
     return SSP_OK;
 }
 
-static void host_out(const HostCsc& h, ssp_csc_out* out) {
+// a library-owned host CSC of n columns and nnz entries (freed with ssp_csc_free); nothing is left allocated
+// when one of the three arrays cannot be
+static void alloc_host_csc(ssp_csc_out* out, int64_t n, int64_t nnz) {
     memset(out, 0, sizeof(*out));
-    out->n = h.n;
-    out->nnz = h.colptr.empty() ? 0 : h.colptr[h.n];
-    out->colptr = (int64_t*)malloc(sizeof(int64_t) * (h.n + 1));
-    out->rowidx = (int32_t*)malloc(sizeof(int32_t) * (out->nnz + 1));
-    out->values = (double*)malloc(sizeof(double) * (out->nnz + 1));
-    if (!out->colptr || !out->rowidx || !out->values) throw std::bad_alloc();
+    int64_t* cp = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+    int32_t* ri = (int32_t*)malloc(sizeof(int32_t) * (nnz + 1));
+    double* va = (double*)malloc(sizeof(double) * (nnz + 1));
+    if (!cp || !ri || !va) {
+        free(cp);
+        free(ri);
+        free(va);
+        throw Error(SSP_ERR_NOMEM, "host allocation of the output failed");
+    }
+    out->n = n;
+    out->nnz = nnz;
+    out->colptr = cp;
+    out->rowidx = ri;
+    out->values = va;
+    out->mem = SSP_MEM_HOST;
+}
+
+static void host_out(const HostCsc& h, ssp_csc_out* out) {
+    alloc_host_csc(out, h.n, h.colptr.empty() ? 0 : h.colptr[h.n]);
     memcpy(out->colptr, h.colptr.data(), sizeof(int64_t) * (h.n + 1));
     if (out->nnz) {
         memcpy(out->rowidx, h.rowidx.data(), sizeof(int32_t) * out->nnz);
         memcpy(out->values, h.val.data(), sizeof(double) * out->nnz);
     }
-    out->mem = SSP_MEM_HOST;
 }
 
 int ssp_read_mtx(const char* path, ssp_csc_out* out) {
@@ -1065,10 +1079,7 @@ int ssp_read_mtx_device(ssp_context* ctx, const char* path, int32_t out_mem, ssp
         out->n = g.n;
         out->nnz = g.nnz;
         if (out_mem == SSP_MEM_HOST) {
-            out->colptr = (int64_t*)malloc(sizeof(int64_t) * (g.n + 1));
-            out->rowidx = (int32_t*)malloc(sizeof(int32_t) * (g.nnz + 1));
-            out->values = (double*)malloc(sizeof(double) * (g.nnz + 1));
-            if (!out->colptr || !out->rowidx || !out->values) throw std::bad_alloc();
+            alloc_host_csc(out, g.n, g.nnz);
             SSP_CUDA(cudaMemcpyAsync(out->colptr, g.colptr, sizeof(int64_t) * (g.n + 1), cudaMemcpyDeviceToHost,
                                      C.stream));
             SSP_CUDA(cudaMemcpyAsync(out->rowidx, g.rowidx, sizeof(int32_t) * g.nnz, cudaMemcpyDeviceToHost, C.stream));
@@ -1369,13 +1380,7 @@ int ssp_stage_sample_apply(ssp_context* c, const ssp_csc* graph, const double* p
         int32_t* li;
         double* lv;
         int64_t nnz = sample_apply_device(C, G, dp, dc, reweight, &lp, &li, &lv, dkeep);
-        memset(out, 0, sizeof(*out));
-        out->n = G.n;
-        out->nnz = nnz;
-        out->mem = SSP_MEM_HOST;
-        out->colptr = (int64_t*)malloc(sizeof(int64_t) * (G.n + 1));
-        out->rowidx = (int32_t*)malloc(sizeof(int32_t) * (nnz + 1));
-        out->values = (double*)malloc(sizeof(double) * (nnz + 1));
+        alloc_host_csc(out, G.n, nnz);
         SSP_CUDA(cudaMemcpyAsync(out->colptr, lp, sizeof(int64_t) * (G.n + 1), cudaMemcpyDeviceToHost, C.stream));
         SSP_CUDA(cudaMemcpyAsync(out->rowidx, li, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, C.stream));
         SSP_CUDA(cudaMemcpyAsync(out->values, lv, sizeof(double) * nnz, cudaMemcpyDeviceToHost, C.stream));
