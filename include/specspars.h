@@ -295,6 +295,7 @@ typedef struct {
 typedef struct {
     int64_t submitted, completed, failed, rejected, pending;
     int32_t inflight, peak_inflight, slots;
+    int32_t waiters;          /* threads inside ssp_wait / ssp_poll */
     int64_t peak_inflight_bytes, budget_bytes;
 } ssp_server_info;
 void ssp_server_opts_default(ssp_server_opts* opts);

@@ -112,7 +112,7 @@ class _Result(ctypes.Structure):
 class _ServerInfo(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
                 ("rejected", ctypes.c_int64), ("pending", ctypes.c_int64), ("inflight", ctypes.c_int32),
-                ("peak_inflight", ctypes.c_int32), ("slots", ctypes.c_int32),
+                ("peak_inflight", ctypes.c_int32), ("slots", ctypes.c_int32), ("waiters", ctypes.c_int32),
                 ("peak_inflight_bytes", ctypes.c_int64), ("budget_bytes", ctypes.c_int64)]
 
 

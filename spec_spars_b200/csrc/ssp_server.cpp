@@ -103,6 +103,7 @@ struct ssp_server {
     int32_t inflight = 0, peak_inflight = 0;
     int64_t inflight_bytes = 0, peak_inflight_bytes = 0;
     int64_t submitted = 0, completed = 0, failed = 0, rejected = 0;
+    int32_t waiters = 0;  // threads inside ssp_wait; destroy lets them leave before the server goes
     bool stopping = false;
     std::vector<ssp_context*> ctxs;
     std::vector<std::thread> workers;
@@ -299,18 +300,33 @@ int ssp_submit(ssp_server* s, const ssp_request* req, uint64_t* ticket) {
 }
 
 // On completion the result (including ownership of res->out) moves to the caller and the ticket is retired.
+// Several threads may wait on one ticket: the first to see it done collects it, the others get
+// SSP_ERR_INVALID (the job is looked up again after every wake-up, never through a pointer kept across one).
 int ssp_wait(ssp_server* s, uint64_t ticket, int64_t timeout_ms, ssp_result* res) {
     if (!s || !res) return fail(SSP_ERR_INVALID, "ssp_wait: bad arguments");
     std::unique_lock<std::mutex> lk(s->mu);
-    auto it = s->jobs.find(ticket);
-    if (it == s->jobs.end()) return fail(SSP_ERR_INVALID, "ssp_wait: unknown or already collected ticket");
-    Job* j = it->second.get();
-    auto ready = [&] { return j->done; };
+    struct Waiting {  // counted while inside; the last to leave wakes a destroy that waits for it
+        ssp_server* s;
+        explicit Waiting(ssp_server* sv) : s(sv) { s->waiters++; }
+        ~Waiting() {
+            s->waiters--;
+            s->cv_done.notify_all();
+        }
+    } waiting(s);
+    if (s->jobs.find(ticket) == s->jobs.end())
+        return fail(SSP_ERR_INVALID, "ssp_wait: unknown or already collected ticket");
+    auto ready = [&] {
+        auto f = s->jobs.find(ticket);
+        return f == s->jobs.end() || f->second->done;
+    };
     if (timeout_ms < 0) s->cv_done.wait(lk, ready);
     else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
         return SSP_ERR_PENDING;
-    s->fill(j, res);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end()) return fail(SSP_ERR_INVALID, "ssp_wait: the ticket was collected by another caller");
+    s->fill(it->second.get(), res);
     s->jobs.erase(it);
+    s->cv_done.notify_all();  // other waiters of this ticket re-check and leave
     return SSP_OK;
 }
 
@@ -330,16 +346,28 @@ int ssp_server_info_get(ssp_server* s, ssp_server_info* info) {
     info->peak_inflight_bytes = s->peak_inflight_bytes;
     info->budget_bytes = s->opts.hbm_budget_bytes;
     info->slots = s->opts.slots;
+    info->waiters = s->waiters;
     return SSP_OK;
 }
 
-// Requests still pending are dropped; admitted ones finish first.  Uncollected results are freed.
+// Requests still pending are dropped: they complete with SSP_ERR_INVALID, so threads waiting on them return.
+// Admitted ones finish first, and threads inside ssp_wait leave before the server is freed.  Uncollected
+// results are freed.
 int ssp_server_destroy(ssp_server* s) {
     if (!s) return SSP_OK;
     {
         std::unique_lock<std::mutex> lk(s->mu);
+        const Clock::time_point now = Clock::now();
+        for (Job* j : s->pending) {
+            j->status = SSP_ERR_INVALID;
+            j->error = "dropped: the server was destroyed before the request was admitted";
+            j->t_admit = j->t_done = now;
+            j->done = true;
+            s->failed++;
+        }
         s->pending.clear();
-        s->cv_done.wait(lk, [&] { return s->inflight == 0; });
+        s->cv_done.notify_all();
+        s->cv_done.wait(lk, [&] { return s->inflight == 0 && s->waiters == 0; });
         s->stopping = true;
         s->cv_work.notify_all();
     }

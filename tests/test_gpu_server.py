@@ -2,6 +2,7 @@
 comes back identical to each request run alone, requests overlap on the device, and admission respects the
 HBM budget."""
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -104,3 +105,60 @@ def test_inline_check_matches_direct_probe(ssp, ora, ctx):
     assert chk["mean_relative_error"] == direct["mean_relative_error"]
     assert chk["ccs_equal"] and chk["components_graph"] == ctx.connected_components(G)[0]
     assert chk["max_relative_error"] < 0.5 and chk["check_ms"] > 0
+
+
+@pytest.mark.gpu
+def test_two_waiters_on_one_ticket(ssp):
+    """Each result is collected once: of two threads waiting on the same ticket one gets it, the other an
+    error (the server looks the ticket up again after every wake-up)."""
+    G = ssp.gen_grid2d(60, 60)
+    prm = ssp.SparsifierParameters.cli(0.5)
+    got, errs = [], []
+    with ssp.Server(0, slots=1) as srv:
+        t = srv.submit(G, prm)
+
+        def waiter():
+            try:
+                got.append(srv.wait(t, timeout_ms=120_000))
+            except ssp.SspError as e:
+                errs.append(e.code)
+        th = [threading.Thread(target=waiter) for _ in range(2)]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        assert srv.info()["completed"] == 1
+    assert len(got) == 1 and got[0] is not None and got[0][1]["m_in"] == 2 * 60 * 59
+    assert errs == [-1]
+
+
+@pytest.mark.gpu
+def test_destroy_releases_waiters_of_dropped_requests(ssp):
+    """Destroying the server drops the requests not yet admitted: a thread waiting on one returns with an
+    error instead of waiting for good, and the destroy itself returns once the admitted request is done."""
+    big = ssp.gen_er(200_000, 20.0, 0.5, 2.0, 5)
+    small = ssp.gen_grid2d(40, 40)
+    prm = ssp.SparsifierParameters.cli(0.5)
+    out = []
+    srv = ssp.Server(0, slots=1)
+    t_big = srv.submit(big, prm)
+    t_small = srv.submit(small, prm)  # behind the big one on the only slot
+
+    def waiter():
+        try:
+            out.append(("result", srv.wait(t_small)))
+        except ssp.SspError as e:
+            out.append(("error", e.code, str(e)))
+    th = threading.Thread(target=waiter)
+    th.start()
+    for _ in range(3000):  # close only once the waiter is inside ssp_wait
+        if srv.info()["waiters"] == 1:
+            break
+        time.sleep(0.01)
+    assert srv.info()["waiters"] == 1
+    srv.close()
+    th.join(timeout=300)
+    assert not th.is_alive() and len(out) == 1
+    if out[0][0] == "error":  # dropped before admission (the usual case)
+        assert out[0][1] == -1 and "dropped" in out[0][2]
+    assert t_big != t_small
