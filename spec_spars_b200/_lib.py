@@ -676,7 +676,8 @@ def run_solve_lap(shared_jl_cols, col_ptrs, row_indices, values, solver_output_f
 
 class Sparsifier:
     """Sparsifier (sparsifier.rs:244-297, 357-376, 735-790): a current Laplacian plus the edges inserted since
-    the last sparsification.  Built from a graph (all its edges pending) or from a vertex count (empty).
+    the last sparsification.  Built from a graph (all its edges pending), from a vertex count (empty), or with
+    from_matrix from a Laplacian file (the current Laplacian, nothing pending).
 
     insert() skips zero values and checks the reference's streaming trigger: with params.streaming set, it
     sparsifies when the current Laplacian has more than threshold = n * round(beta) * row_constant edges
@@ -685,7 +686,7 @@ class Sparsifier:
 
     def __init__(self, graph, parameters, ctx=None):
         self.params = parameters
-        self.ctx = ctx or _ctx()
+        self._ctx = ctx  # the device context is taken on first use, so building one needs no GPU
         self.stats = None
         if isinstance(graph, (int, np.integer)):
             self.num_nodes = int(graph)
@@ -700,9 +701,46 @@ class Sparsifier:
         self.threshold = self.num_nodes * int(math.floor(beta + 0.5)) * parameters.row_constant
         self.current_laplacian = None
 
+    @classmethod
+    def from_matrix(cls, filename, parameters, ctx=None):
+        """Sparsifier::from_matrix (sparsifier.rs:299-335): the current Laplacian read from a .mtx file, no
+        edges pending, the same threshold."""
+        lap = read_mtx(filename)
+        sp = cls(lap.n, parameters, ctx)
+        sp.current_laplacian = lap
+        return sp
+
+    @property
+    def ctx(self):
+        if self._ctx is None:
+            self._ctx = _ctx()
+        return self._ctx
+
     @property
     def graph(self):
         return self._pending_csc()
+
+    def laplacian_edges(self):
+        """(row, col, value) of the current Laplacian's entries with row < col in CSC order: the edges, in the
+        order compute_diff_norms and compute_probs walk them (sparsifier.rs:546-547,571-572)."""
+        L = self.current_laplacian
+        cols = np.repeat(np.arange(L.n, dtype=np.int32), np.diff(L.colptr))
+        up = L.rowidx < cols
+        return np.ascontiguousarray(L.rowidx[up], np.int32), np.ascontiguousarray(cols[up]), L.values[up]
+
+    def compute_diff_norms(self, solution):
+        """Per edge of the current Laplacian, ||X[row] - X[col]|| over the columns of the n x k solution
+        (compute_diff_norms, sparsifier.rs:565-583).  On the GPU; the squares are summed per 32-column tile
+        and the tiles in order, where the reference adds the columns one by one."""
+        v1, v2, _ = self.laplacian_edges()
+        return stage_diff_norms(self.ctx, v1, v2, solution)
+
+    def compute_probs(self, diff_norms):
+        """Per edge, min(1, beta * (-value) * d^2 / jl_dim) (compute_probs, sparsifier.rs:542-562), with
+        beta and jl_dim of this Sparsifier's vertex count.  On the GPU."""
+        _, _, val = self.laplacian_edges()
+        n = self.num_nodes
+        return stage_probs(self.ctx, -val, diff_norms, self.params.beta(n), float(self.params.jl_dim(n)))
 
     def insert(self, v1, v2, value):
         if not (0 <= v1 < self.num_nodes and 0 <= v2 < self.num_nodes):

@@ -3,6 +3,7 @@ laplacian_to_graph must invert the oracle's Laplacian bit for bit (the off-diago
 dropped, the stored order kept), and sparsify_laplacian must return exactly what sparsify returns on the
 graph itself."""
 import ctypes
+import math
 
 import numpy as np
 import pytest
@@ -90,3 +91,41 @@ def test_sparsify_laplacian_from_device_memory(ssp, ora, ctx):
     Lb._check(Lb.lib().ssp_sparsify_laplacian(ctx._h, ctypes.byref(s), ctypes.byref(prm._s), Lb.SSP_MEM_HOST,
                                               ctypes.byref(out), ctypes.byref(st)))
     assert _same(H, Lb._take_out(out))
+
+
+def test_sparsifier_from_matrix(ssp, ora, tmp_path):
+    """Sparsifier.from_matrix (sparsifier.rs:299-335): the Laplacian file becomes the current Laplacian as
+    read_mtx gives it, nothing is pending, and its edges are the row < col entries in CSC order with values
+    -w, the same edges in the same order as the graph's."""
+    G = GRAPHS["er"](ssp)
+    L = _laplacian_of(ssp, ora, G)
+    path = tmp_path / "lap.mtx"
+    ssp.write_mtx(str(path), L)
+    prm = ssp.SparsifierParameters.new_default()
+    sp = ssp.Sparsifier.from_matrix(str(path), prm)
+    assert sp.num_nodes == G.n and _same(sp.current_laplacian, ssp.read_mtx(str(path)))
+    v1, v2, w = ora.extract_edges(G.n, G.colptr, G.rowidx, G.values)
+    r, c, val = sp.laplacian_edges()
+    assert np.array_equal(r, v1) and np.array_equal(c, v2) and np.array_equal(-val, w)
+    assert sp.num_edges() == len(w) and sp.graph.nnz == 0
+    beta = prm.beta(G.n)
+    assert sp.threshold == G.n * int(math.floor(beta + 0.5)) * prm.row_constant  # sparsifier.rs:264-266
+
+
+@pytest.mark.gpu
+def test_sparsifier_from_matrix_probabilities(ssp, ora, ctx, tmp_path):
+    """compute_diff_norms / compute_probs on a loaded Laplacian (as tests.rs:747-764 uses them) equal the
+    oracle's stages on the same edges, bit for bit."""
+    G = GRAPHS["er"](ssp)
+    L = _laplacian_of(ssp, ora, G)
+    path = tmp_path / "lap.mtx"
+    ssp.write_mtx(str(path), L)
+    prm = ssp.SparsifierParameters.new_default()
+    sp = ssp.Sparsifier.from_matrix(str(path), prm, ctx=ctx)
+    X = np.random.default_rng(5).standard_normal((G.n, 21))
+    d = sp.compute_diff_norms(X)
+    v1, v2, w = ora.extract_edges(G.n, G.colptr, G.rowidx, G.values)
+    assert np.array_equal(d, ora.diff_norms(v1, v2, X))
+    p = sp.compute_probs(d)
+    assert np.array_equal(p, ora.probs(w, d, prm.beta(G.n), float(prm.jl_dim(G.n))))
+    assert np.all((p >= 0) & (p <= 1))
