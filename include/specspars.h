@@ -216,9 +216,9 @@ int ssp_solve_lap(ssp_context* ctx, const ssp_csc* lap, const double* Y, int32_t
 /* ---- sparsify one graph (input: symmetric matrix whose upper triangle holds the edges) ---- */
 int ssp_sparsify(ssp_context* ctx, const ssp_csc* graph, const ssp_params* params, int32_t out_mem,
                  ssp_csc_out* out, ssp_stats* stats);
-/* The same with a graph Laplacian as input, as Sparsifier::from_matrix reads one (sparsifier.rs:299-300) and
- * sparsify then works on it: the graph is the negated off-diagonal (ssp_laplacian_to_graph), so edge (i, j) has
- * weight -L[i][j], and the result equals ssp_sparsify on that graph.  lap in host or device memory. */
+/* The same with a graph Laplacian as input (Sparsifier::from_matrix loads one, sparsifier.rs:299-300): the
+ * graph is the negated off-diagonal (ssp_laplacian_to_graph), so edge (i, j) has weight -L[i][j], every edge is
+ * sketched, and the result equals ssp_sparsify on that graph.  lap in host or device memory. */
 int ssp_sparsify_laplacian(ssp_context* ctx, const ssp_csc* lap, const ssp_params* params, int32_t out_mem,
                            ssp_csc_out* out, ssp_stats* stats);
 /* host only: the adjacency of a Laplacian, entry (i, j) = -L[i][j] for i != j, diagonal dropped, order kept
