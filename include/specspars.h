@@ -13,6 +13,7 @@
  *   ssp_sparsify        <- Sparsifier::sparsify         src/sparsifier.rs:722-770, driven like
  *                          InputStream::run_stream      src/stream.rs:40-64
  *   ssp_sparsify_mtx    <- sparsify_dataset             src/lib.rs:145-166 (read .mtx, sparsify, write .mtx)
+ *   ssp_sparsify_laplacian <- a Laplacian input, as Sparsifier::from_matrix loads one  src/sparsifier.rs:299-300
  *   ssp_params_default  <- SparsifierParameters::new_default  src/sparsifier.rs:182-209
  *   ssp_params_new      <- SparsifierParameters::new          src/sparsifier.rs:163-179
  *   ssp_params_cli      <- the knobs sparsify_dataset hard-codes, src/lib.rs:149-156
