@@ -35,6 +35,8 @@ CASES = {
     "er800": lambda: S.gen_er(800, 8.0, 0.5, 2.0, 1),
     "grid3d_8x7x6": lambda: S.gen_grid3d(8, 7, 6, -3, 3, 2),  # weights over six decades
     "er400_isolated_vertex": lambda: S.gen_er(400, 5.0, 0.5, 2.0, 3),
+    "rmat_s9": lambda: S.gen_rmat(9, 8, 0.57, 0.19, 0.19, 4),  # power law: hubs, LogNormal weights
+    "rgg500": lambda: S.gen_rgg(500, 10.0, 0.1, 10.0, 6),  # random geometric: mesh-like, local
 }
 
 

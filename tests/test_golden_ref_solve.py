@@ -40,8 +40,8 @@ def _check_against_reference(f, X, ora):
 
 def test_fixtures_present():
     names = {_name(f) for f in FIXTURES}
-    assert {"grid20", "er800", "grid3d_8x7x6", "er400_isolated_vertex"} <= names
-    assert len(CONVERGED) == 3
+    assert {"grid20", "er800", "grid3d_8x7x6", "er400_isolated_vertex", "rmat_s9", "rgg500"} <= names
+    assert len(CONVERGED) == 5
 
 
 @pytest.mark.parametrize("path", FIXTURES, ids=_name)
