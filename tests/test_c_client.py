@@ -41,8 +41,20 @@ def test_c_client_without_device(ssp, client, tmp_path):
     assert f"n {G.n} nnz {G.nnz} jl_dim {k}" in r.stdout and "no CUDA device" in r.stdout
 
 
+def _shared_compute_mode():
+    """The client runs in its own process beside this one's context: only in the default compute mode."""
+    try:
+        r = subprocess.run(["nvidia-smi", "--id=0", "--query-gpu=compute_mode", "--format=csv,noheader"],
+                           capture_output=True, text=True, timeout=30)
+    except (OSError, subprocess.TimeoutExpired):
+        return False
+    return r.returncode == 0 and r.stdout.strip().lower() == "default"
+
+
 @pytest.mark.gpu
 def test_c_client_output_equals_python_host(ssp, ctx, client, tmp_path):
+    if not _shared_compute_mode():
+        pytest.skip("the GPU is not in the default (shared) compute mode")
     G, path = _graph_file(ssp, tmp_path)
     out = tmp_path / "out.mtx"
     r = subprocess.run([client, str(path), str(out)], capture_output=True, text=True, timeout=300)
