@@ -18,7 +18,7 @@ SSP_REWEIGHT_INV_SQRT_P, SSP_REWEIGHT_INV_P = 0, 1
 SSP_PRECISION_FP64, SSP_PRECISION_MIXED = 0, 1
 
 ERROR_NAMES = {-1: "SSP_ERR_INVALID", -2: "SSP_ERR_CUDA", -3: "SSP_ERR_NOMEM", -4: "SSP_ERR_NOT_CONVERGED",
-               -5: "SSP_ERR_CAPACITY", -6: "SSP_ERR_IO", -7: "SSP_ERR_NO_DEVICE"}
+               -5: "SSP_ERR_CAPACITY", -6: "SSP_ERR_IO", -7: "SSP_ERR_NO_DEVICE", -8: "SSP_ERR_PENDING"}
 
 
 def _header_symbols():

@@ -38,3 +38,14 @@ def test_ctypes_structs_match_the_header(tmp_path):
     assert len(got) == len(expect)
     bad = [(what, want, int(g)) for (what, want), g in zip(expect, got) if int(g) != want]
     assert bad == []
+
+
+def test_status_codes_match_the_header():
+    """Every SSP_ERR_* the header defines has the same value and name in the Python host's table."""
+    import re
+
+    import spec_spars_b200._lib as L
+    txt = open(os.path.join(ROOT, "include", "specspars.h")).read()
+    codes = {int(v): name for name, v in re.findall(r"#define (SSP_ERR_\w+) \((-\d+)\)", txt)}
+    assert len(codes) >= 8 and codes == L.ERROR_NAMES
+    assert re.search(r"#define SSP_OK 0\b", txt) and L.SSP_OK == 0
