@@ -413,8 +413,12 @@ int ssp_stage_sample_apply(ssp_context* ctx, const ssp_csc* graph, const double*
  * d lives in a static device array of SSP_STATIC_SCRATCH_EDGES doubles: m above that returns
  * SSP_ERR_CAPACITY before anything is launched; nothing in it must start at zero.  The array is shared by
  * all calls on a device, so overlapping calls (two streams or threads in flight at once) race: serialise
- * them.  The first call with each device current looks the array up with cudaGetSymbolAddress; make that
- * first call before any stream capture.  An edge with an endpoint outside [0, n) gets p = 1 (d = NaN). */
+ * them.  The first call with each device current loads the library's device code there (with CUDA's lazy
+ * module loading, that is when the static array is created: a device allocation) and looks the array up
+ * with cudaGetSymbolAddress, so make that first call at start-up, before any stream capture.  The address
+ * is kept per device for the life of the process: after cudaDeviceReset on a device, do not call this entry
+ * point on it again.  An edge with an endpoint outside [0, n) gets p = 1 (d = NaN), as ssp_stage_diff_norms
+ * gives NaN for device input and rejects host input. */
 #define SSP_STATIC_SCRATCH_EDGES (1 << 20)
 int ssp_stage_leverage_probs_static(void* stream, int64_t n, int64_t m, const int32_t* v1, const int32_t* v2,
                                     const double* Z, int32_t k, const double* w, double beta, double denom,

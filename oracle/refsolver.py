@@ -19,9 +19,11 @@ def available():
     return os.path.exists(BIN) and os.access(BIN, os.X_OK)
 
 
-def build(ref_root="/root/reference"):
-    """Compile ref_solve from the reference sources when they are present (never on a machine without them)."""
-    if not os.path.exists(os.path.join(ref_root, "src", "example.cc")):
+def build(ref_root=None):
+    """Compile ref_solve from the reference sources at ref_root (default: $SSP_REFERENCE_DIR) when they are
+    present; without them (a machine that only has the prebuilt binary) nothing is compiled."""
+    ref_root = ref_root or os.environ.get("SSP_REFERENCE_DIR")
+    if not ref_root or not os.path.exists(os.path.join(ref_root, "src", "example.cc")):
         return available()
     r = subprocess.run(["make", "-s", f"REF={ref_root}"], cwd=os.path.join(HERE, "ref"), capture_output=True,
                        text=True)

@@ -412,7 +412,7 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
     else if (rep.diff_fused)
         sqrt_device(C, G.m, d2, d);
     else
-        diff_norms_device(C, G.m, G.v1, G.v2, Zt, k, tile_ld(kl), d, n);
+        diff_norms_device(C, G.m, G.v1, G.v2, Zt, k, tile_ld(kl), d, n, true);
     const double beta = beta_of(prm, n);
     const double denom = prm->prob_variance_correction ? (double)k * scale * scale : (double)k;
     probs_device(C, G.m, G.w, d, beta, denom, p);
@@ -1307,14 +1307,21 @@ int ssp_stage_precond(ssp_context* c, const ssp_csc* lap, uint64_t seed, int64_t
 int ssp_stage_diff_norms(ssp_context* c, int64_t n, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z,
                          int32_t k, int32_t mem, double* d) {
     return guarded([&] {
-        SSP_REQUIRE(c && k > 0 && d, SSP_ERR_INVALID, "bad arguments");
+        SSP_REQUIRE(c && k > 0 && n >= 0 && m >= 0 && (m == 0 || (v1 && v2 && Z && d)), SSP_ERR_INVALID,
+                    "ssp_stage_diff_norms: need n >= 0, m >= 0, k > 0 and non-null arrays");
+        if (mem == SSP_MEM_HOST)
+            for (int64_t e = 0; e < m; e++)
+                SSP_REQUIRE(v1[e] >= 0 && v1[e] < n && v2[e] >= 0 && v2[e] < n, SSP_ERR_INVALID,
+                            "ssp_stage_diff_norms: edge " + std::to_string(e) + " has an endpoint outside [0, n)");
         Context& C = c->ctx;
         SSP_CUDA(cudaSetDevice(C.device));
+        if (m == 0) return;
         const int32_t* dv1 = stage_in(C, v1, m, mem, "dn_v1");
         const int32_t* dv2 = stage_in(C, v2, m, mem, "dn_v2");
         const double* dZ = stage_in(C, Z, n * (int64_t)k, mem, "dn_Z");
         double* dd = mem == SSP_MEM_DEVICE ? d : C.ws.get_t<double>("dn_d", m + 1);
-        diff_norms_device(C, m, dv1, dv2, dZ, k, k, dd);
+        // device input is not checked on the host: an edge with an endpoint outside [0, n) gets d = NaN
+        diff_norms_device(C, m, dv1, dv2, dZ, k, k, dd, n, false);
         if (mem == SSP_MEM_HOST && m)
             SSP_CUDA(cudaMemcpyAsync(d, dd, sizeof(double) * m, cudaMemcpyDeviceToHost, C.stream));
         SSP_CUDA(cudaStreamSynchronize(C.stream));

@@ -187,6 +187,40 @@ constexpr int SSP_PROBE_COLS = 8;
 // ---------------------------------------------------------------- small device helpers
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
+// One warp's sum over columns [0, k) of (Z[a, j] - Z[b, j])^2 (compute_diff_norms, sparsifier.rs:565-583),
+// Z row-major with leading dimension ldz or (TM) tile-major with n rows.  Per 32-column group lane l squares
+// the difference in column j0 + l (0 past k), a fixed xor butterfly sums the 32 squares and the groups are
+// added in order; every lane returns the same value.  Every step is an explicit round-to-nearest operation,
+// so the CPU oracle and every kernel that calls this form the same bits.
+template <bool TM>
+__device__ __forceinline__ double warp_edge_sq(int64_t a, int64_t b, const double* __restrict__ Z, int32_t k,
+                                               int64_t ldz, int64_t n, int lane) {
+    double acc = 0.0;
+    for (int32_t j0 = 0; j0 < k; j0 += 32) {
+        const int32_t j = j0 + lane;
+        double x = 0.0;
+        if (j < k) {
+            const int64_t oa = TM ? tile_off(n, a, j) : a * ldz + j;
+            const int64_t ob = TM ? tile_off(n, b, j) : b * ldz + j;
+            x = __dsub_rn(Z[oa], Z[ob]);
+        }
+        double s = __dmul_rn(x, x);
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+        acc = __dadd_rn(acc, s);
+    }
+    return acc;
+}
+
+// p_e = min(((beta * w_e) * d_e^2) / denom, 1) (compute_probs, sparsifier.rs:542-562); a NaN ratio (an edge
+// whose norm could not be formed) maps to 1, so such an edge is always kept.
+__device__ __forceinline__ double leverage_prob(double w, double d, double beta, double denom) {
+    const double d2 = __dmul_rn(d, d);
+    const double x = __ddiv_rn(__dmul_rn(__dmul_rn(beta, w), d2), denom);
+    if (x != x) return 1.0;
+    return (x < 1.0) ? x : 1.0;
+}
+
 template <class T>
 inline T ceil_div(T a, T b) { return (a + b - 1) / b; }
 
@@ -384,9 +418,10 @@ void tiles_to_rowmajor(Context& C, int64_t n, int32_t k, const double* src, doub
 void precond_apply_device(Context& C, const DevFactor& F, const double* R, double* Z, int64_t ld);
 
 // a9-a12
-// Z row-major (leading dimension ldz) or, when n_tile_major > 0, tile-major with that many rows
+// Z has n rows, row-major (leading dimension ldz) or tile-major; an edge with an endpoint outside [0, n) is
+// not read and gets d = NaN
 void diff_norms_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z, int32_t k,
-                       int64_t ldz, double* d, int64_t n_tile_major = 0);
+                       int64_t ldz, double* d, int64_t n, bool tile_major);
 // per-edge sum over the k columns of (Z[v1,j] - Z[v2,j])^2, Z tile-major with n_tile_major rows
 void diff_sq_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z, int32_t k,
                     int64_t n_tile_major, double* sq);

@@ -15,8 +15,13 @@
 //   * nothing in the scratch has to start at zero: entries [0, m) are written before they are read;
 //   * the scratch is shared by every call on a device, so two calls in flight at the same time on one
 //     device (different streams or host threads) race -- callers serialise them (one stream, or events);
-//   * the scratch address is looked up with cudaGetSymbolAddress on the first call made with each device
-//     current; that first call should come before any stream capture.
+//   * the first call made with each device current loads this library's device code on that device (under
+//     CUDA's lazy module loading that is when the scratch array itself is created, a device allocation) and
+//     looks the scratch address up with cudaGetSymbolAddress; make that first call at start-up, before any
+//     stream capture, so that no later call allocates;
+//   * the address is kept per device index for the life of the process: after cudaDeviceReset (or anything
+//     else that destroys the device's primary context) it is stale, so a process that resets a device must
+//     not call this entry point on that device again.
 #include <atomic>
 #include <cstdio>
 
@@ -29,10 +34,9 @@ static __device__ __align__(256) double g_ssp_static_scratch[SSP_STATIC_SCRATCH_
 constexpr int kMaxDevices = 64;
 std::atomic<double*> g_scratch_addr[kMaxDevices];
 
-// d_e into the scratch: one warp per edge over row-major Z (leading dimension k), 32 columns at a time: each
-// lane squares its column's difference, a fixed xor-butterfly sums the 32 squares, and the groups' sums are
-// added in order -- the order of k_diff_norms.
-// An edge with an endpoint outside [0, n) is not read and gets d_e = NaN.
+// d_e into the scratch: one warp per edge over row-major Z (leading dimension k), with the per-edge sum of
+// k_diff_norms (warp_edge_sq: 32 columns at a time, a fixed xor butterfly, groups added in order).
+// An edge with an endpoint outside [0, n) is not read and gets d_e = NaN, as in k_diff_norms.
 __global__ void __launch_bounds__(256) k_norms_static(int64_t n, int64_t m, const int32_t* __restrict__ v1,
                                                       const int32_t* __restrict__ v2, const double* __restrict__ Z,
                                                       int32_t k, double* __restrict__ d) {
@@ -44,28 +48,16 @@ __global__ void __launch_bounds__(256) k_norms_static(int64_t n, int64_t m, cons
             if (lane == 0) d[e] = __longlong_as_double(0x7ff8000000000000LL);
             continue;
         }
-        double acc = 0.0;
-        for (int32_t j0 = 0; j0 < k; j0 += 32) {
-            const int32_t j = j0 + lane;
-            const double x = j < k ? __dsub_rn(Z[a * k + j], Z[b * k + j]) : 0.0;
-            double s = __dmul_rn(x, x);
-#pragma unroll
-            for (int o = 16; o >= 1; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
-            acc = __dadd_rn(acc, s);
-        }
+        const double acc = ssp::warp_edge_sq<false>(a, b, Z, k, k, n, lane);
         if (lane == 0) d[e] = sqrt(acc);
     }
 }
 
-// p_e from the scratch d_e, as k_probs: a NaN ratio maps to probability 1.
+// p_e from the scratch d_e with the body of k_probs (leverage_prob): a NaN ratio maps to probability 1.
 __global__ void k_probs_static(int64_t m, const double* __restrict__ w, const double* __restrict__ d, double beta,
                                double denom, double* __restrict__ p) {
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
-        const double d2 = __dmul_rn(d[e], d[e]);
-        const double x = __ddiv_rn(__dmul_rn(__dmul_rn(beta, w[e]), d2), denom);
-        p[e] = (x < 1.0) ? x : 1.0;
-        if (x != x) p[e] = 1.0;
-    }
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x)
+        p[e] = ssp::leverage_prob(w[e], d[e], beta, denom);
 }
 
 int fail(int code, const char* msg) {

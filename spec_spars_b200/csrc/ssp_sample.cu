@@ -13,7 +13,8 @@
 
 namespace ssp {
 
-// ROOT = false leaves the sum of squares (one rank's share of the columns, summed across ranks later)
+// ROOT = false leaves the sum of squares (one rank's share of the columns, summed across ranks later).
+// An edge with an endpoint outside [0, n) is not read and gets NaN.
 template <bool TM, bool ROOT = true>
 __global__ void __launch_bounds__(256) k_diff_norms(int64_t m, const int32_t* __restrict__ v1,
                                                     const int32_t* __restrict__ v2, const double* __restrict__ Z,
@@ -22,20 +23,11 @@ __global__ void __launch_bounds__(256) k_diff_norms(int64_t m, const int32_t* __
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < m; e += nw) {
         const int64_t a = v1[e], b = v2[e];
-        double acc = 0.0;
-        for (int32_t j0 = 0; j0 < k; j0 += 32) {
-            const int32_t j = j0 + lane;
-            double x = 0.0;
-            if (j < k) {
-                const int64_t oa = TM ? tile_off(n, a, j) : a * ldz + j;
-                const int64_t ob = TM ? tile_off(n, b, j) : b * ldz + j;
-                x = __dsub_rn(Z[oa], Z[ob]);
-            }
-            double s = __dmul_rn(x, x);
-#pragma unroll
-            for (int o = 16; o >= 1; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
-            acc = __dadd_rn(acc, s);
+        if (a < 0 || a >= n || b < 0 || b >= n) {
+            if (lane == 0) d[e] = __longlong_as_double(0x7ff8000000000000LL);
+            continue;
         }
+        const double acc = warp_edge_sq<TM>(a, b, Z, k, ldz, n, lane);
         if (lane == 0) d[e] = ROOT ? sqrt(acc) : acc;
     }
 }
@@ -47,12 +39,8 @@ __global__ void k_sqrt_vec(int64_t m, const double* __restrict__ sq, double* __r
 
 __global__ void k_probs(int64_t m, const double* __restrict__ w, const double* __restrict__ d, double beta,
                         double denom, double* __restrict__ p) {
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
-        const double d2 = __dmul_rn(d[e], d[e]);
-        const double x = __ddiv_rn(__dmul_rn(__dmul_rn(beta, w[e]), d2), denom);
-        p[e] = (x < 1.0) ? x : 1.0;
-        if (x != x) p[e] = 1.0;
-    }
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x)
+        p[e] = leverage_prob(w[e], d[e], beta, denom);
 }
 
 __global__ void k_coins(int64_t m, uint64_t seed, double* __restrict__ coins) {
@@ -131,12 +119,12 @@ __global__ void k_lh_fill(int64_t n, const int64_t* __restrict__ adj_ptr, const 
 }
 
 void diff_norms_device(Context& C, int64_t m, const int32_t* v1, const int32_t* v2, const double* Z, int32_t k,
-                       int64_t ldz, double* d, int64_t n_tile_major) {
+                       int64_t ldz, double* d, int64_t n, bool tile_major) {
     if (m == 0) return;
-    if (n_tile_major > 0)
-        k_diff_norms<true><<<grid_for(m * 32, 256, 148 * 16), 256, 0, C.stream>>>(m, v1, v2, Z, k, ldz, n_tile_major, d);
+    if (tile_major)
+        k_diff_norms<true><<<grid_for(m * 32, 256, 148 * 16), 256, 0, C.stream>>>(m, v1, v2, Z, k, ldz, n, d);
     else
-        k_diff_norms<false><<<grid_for(m * 32, 256, 148 * 16), 256, 0, C.stream>>>(m, v1, v2, Z, k, ldz, 0, d);
+        k_diff_norms<false><<<grid_for(m * 32, 256, 148 * 16), 256, 0, C.stream>>>(m, v1, v2, Z, k, ldz, n, d);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
 }

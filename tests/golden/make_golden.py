@@ -64,7 +64,9 @@ def make(name, G):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SSP_REFERENCE_DIR")
+    if not ref:
+        raise SystemExit("usage: make_golden.py <reference source tree>  (or set SSP_REFERENCE_DIR)")
     if not refsolver.build(ref):
         raise SystemExit("oracle/_ref/ref_solve could not be built: the reference's sources are needed")
     for name, gen in CASES.items():
