@@ -135,97 +135,171 @@ def precond_bytes(n, nnz_l, k, s=8):
     return 2 * (8 * (n + 1) + nnz_l * (4 + s) + 2 * n * k * s) + s * n
 
 
-def cpu_baseline(eps, k_full, impl="port", budget_cols=16):
-    """The CPU path timed on a bounded sample: ER n=50K (avg degree 20) with the full pipeline on
-    `budget_cols` of the k_full RHS columns; per-column costs extrapolated to k_full."""
-    import numpy as np
+# ER sample sizes of the CPU legs (average degree 20, weights U[0.5, 2], the workload's generator and seed).
+# The reference's factorization keeps its fill in a fixed edge pool of 5 nnz(L) entries (example.cc:336-337)
+# and stops with "need more edge map capacity" (auxilliary.hpp:114-117) when it runs out: on ER with average
+# degree 20 that happens from n = 650K on (the 1M workload always aborts), so the reference arm runs the
+# largest size that completes, 600K, and steps down if a run there still aborts (the reference's fill
+# sampler is seeded from random_device, example.cc:99-101).
+REF_SAMPLE_LADDER = (600_000, 500_000, 400_000)
+PORT_SAMPLE_N = 200_000
+REF_UNAVAILABLE_AT_CONFIG = ("ER n=1M (the workload itself) aborts in the reference's factorization: assertion "
+                             "'need more edge map capacity' (auxilliary.hpp:114-117; edge pool 5*nnz, "
+                             "example.cc:336-337), log in profiles/reference_cpu_er_n1M_abort.md")
+
+
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import spec_spars_b200 as S
     import pyoracle as ora
-    G = S.gen_er(50_000, 20.0, 0.5, 2.0, 11)
-    n = G.n
+    return ora
+
+
+def cpu_baseline(eps, k_full, n_sample=PORT_SAMPLE_N, budget_cols=16):
+    """The C port of every stage (the oracle) on one core over a bounded sample: ER n_sample, average degree
+    20, the full pipeline with budget_cols of the k_full right-hand sides; the per-column cost (sketch, PCG
+    solve, diff norms) is extrapolated to k_full.  Builds its input with the oracle's generator, so nothing
+    of the library is involved."""
+    ora = _oracle()
+    v1, v2, w = ora.gen_er(n_sample, 20.0, 0.5, 2.0, 1)
+    n = n_sample
     t0 = time.perf_counter()
-    v1, v2, w = ora.extract_edges(n, G.colptr, G.rowidx, G.values)
     cp, ri, va = ora.laplacian(n, v1, v2, w)
     t_graph = time.perf_counter() - t0
     kc = budget_cols
-    scale = 1.0 / math.sqrt(k_full)
     t0 = time.perf_counter()
-    Y = ora.sketch(n, v1, v2, w, kc, scale, 0)
+    Y = ora.sketch(n, v1, v2, w, kc, 1.0 / math.sqrt(k_full), 0)
     t_sketch = time.perf_counter() - t0
     t0 = time.perf_counter()
-    if impl == "reference":
-        # the reference factors once and solves column by column (example.cc:520-569): time set-up +
-        # factorization alone, then with the sampled columns, and take the difference as their solves
-        import refsolver
-        threads = os.cpu_count()
-        st0, t_fact, _ = refsolver.solve(n, cp, ri, va, np.zeros((n, 0)), threads=threads)
-        st1, t_all, Z = refsolver.solve(n, cp, ri, va, Y, threads=threads)
-        if st0 != 0 or st1 != 0:
-            raise RuntimeError(f"reference solver failed on the sample (status {st0}, {st1})")
-        t_solve = max(t_all - t_fact, 0.0)
-    else:
-        F = ora.Factor(n, cp, ri, va, 0, 4096, 64)
-        t_fact = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        Z, it, rel, rc = ora.pcg(n, cp, ri, va, F, Y, PCG_TOL, 0.0, 400)
-        t_solve = time.perf_counter() - t0
+    F = ora.Factor(n, cp, ri, va, 0, 4096, 64)
+    t_fact = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    Z, it, rel, rc = ora.pcg(n, cp, ri, va, F, Y, PCG_TOL, 0.0, 400)
+    t_solve = time.perf_counter() - t0
     t0 = time.perf_counter()
     d = ora.diff_norms(v1, v2, Z)
     t_norms = time.perf_counter() - t0
     t0 = time.perf_counter()
     p = ora.probs(w, d, math.pow(eps, -2) * 4 * math.log(n), 1.0)
-    coins = ora.coins(0, len(w))
-    ora.sample_apply(n, v1, v2, w, p, coins, 0, (cp, ri, va))
+    ora.sample_apply(n, v1, v2, w, p, ora.coins(0, len(w)), 0, (cp, ri, va))
     t_tail = time.perf_counter() - t0
     per_col = (t_sketch + t_solve + t_norms) / kc
     total = t_graph + t_fact + per_col * k_full + t_tail
     measured = t_graph + t_fact + t_sketch + t_solve + t_norms + t_tail
-    cores = os.cpu_count() if impl == "reference" else 1
-    who = ("factorization + PCG by the reference's C++ solver (oracle/_ref), graph assembly, sketch and "
-           "sampling by the C port of its Rust stages" if impl == "reference" else "C port of every stage")
-    return {"value": len(w) / total, "unit": "edges/s", "cores": cores,
-            "kind": "reference" if impl == "reference" else "port",
-            "sample": f"ER n={n} avg deg 20 (m={len(w)}), full pipeline with {kc} of k={k_full} RHS columns, "
-                      f"per-column cost extrapolated to k; {who}; measured {measured:.1f}s"}
+    return {"value": len(w) / total, "unit": "edges/s", "cores": 1, "kind": "port",
+            "sample": f"ER n={n} avg deg 20 (m={len(w)}), C port of every stage (the oracle), full pipeline with "
+                      f"{kc} of k={k_full} right-hand sides, per-column cost extrapolated to k; measured "
+                      f"{measured:.1f}s"}
 
 
 def run_reference(args):
-    """--impl reference: the reference CPU implementation of the path on this host's cores."""
+    """--impl reference: the reference's own CPU solver on this host's cores.
+
+    The sample is the workload's graph family at the largest size the reference completes (ER n =
+    REF_SAMPLE_N, average degree 20, k = the workload's 1327 columns).  One run of the reference solver
+    (oracle/_ref/ref_solve: src/example.cc factorization_driver + include/custom_cg.hpp, all host threads)
+    factors the Laplacian once and solves 2 (W + K) right-hand sides one after another, as the reference does
+    (example.cc:551-568); the MKL shim records when each solve starts.  Warm-up step i covers right-hand sides
+    2i and 2i + 1 and is discarded; timed step i covers the next pair.  A step's value is the input edges per
+    second of the whole sparsification at k columns, extrapolated from that step's two solves:
+        m / (assembly + set-up and factorization + k (solve + sketch + diff norms per column) + sampling)
+    The Rust stages (Laplacian assembly, sketch, diff norms, probabilities, sampling) are the oracle's C port
+    on one core.  Only oracle/ code runs here; nothing of the library is imported."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     _, kw, eps = WORKLOADS[args.workload]
-    n = kw.get("n", 10_000)
-    k = math.ceil(24 * math.log(n) / eps ** 2)
-    impl = "reference" if _ref_available() else "port"
-    vals = []
-    for _ in range(max(args.warmup, 0)):
-        pass  # the CPU path has no warm-up state worth timing; samples are independent
-    walls = []
-    for _ in range(args.steps):
+    n_cfg = kw.get("n", 10_000)
+    k = math.ceil(24 * math.log(n_cfg) / eps ** 2) if args.jl_cols <= 0 else args.jl_cols
+    base = {"impl": "reference", "metric": "input edges sparsified/sec", "unit": "edges/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
+    ora = _oracle()
+    import refsolver
+    if args.workload != "er_n1M_deg20" and args.reference_n <= 0:
+        print(json.dumps({**base, "unavailable": f"the reference arm samples the ER workload only "
+                                                 f"(asked for {args.workload})"}), flush=True)
+        return
+    if not refsolver.available():
+        # the reference's sources were not at hand where this tree was built: time the oracle port instead
+        walls, vals = [], []
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            cb = cpu_baseline(eps, k, n_sample=100_000, budget_cols=4)
+            if i >= args.warmup:
+                walls.append((time.perf_counter() - t0) * 1e3)
+                vals.append(cb["value"])
+        v = statistics.median(vals)
+        print(json.dumps({**base, "value": v, "ms_per_step": statistics.median(walls),
+                          "config": {"workload": args.workload, "eps": eps, "k": k, "pcg_tol": PCG_TOL},
+                          "unavailable_at_config": REF_UNAVAILABLE_AT_CONFIG,
+                          "cpu_baseline": {**cb, "value": v},
+                          "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    sizes = [args.reference_n] if args.reference_n > 0 else list(REF_SAMPLE_LADDER)
+    threads = os.cpu_count()
+    ncols = 2 * (args.warmup + args.steps)
+    t_run0 = time.perf_counter()
+    aborted = []
+    for n in sizes:
+        v1, v2, w = ora.gen_er(n, 20.0, 0.5, 2.0, 1)
+        m = len(w)
         t0 = time.perf_counter()
-        cb = cpu_baseline(eps, k, impl=impl, budget_cols=4)
-        walls.append((time.perf_counter() - t0) * 1e3)
-        vals.append(cb["value"])
+        cp, ri, va = ora.laplacian(n, v1, v2, w)
+        t_graph = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        Y = ora.sketch(n, v1, v2, w, ncols, 1.0 / math.sqrt(k), 0)
+        t_sketch_col = (time.perf_counter() - t0) / ncols
+        try:
+            status, secs, Z, starts = refsolver.solve(n, cp, ri, va, Y, threads=threads, timeout=3000,
+                                                      timings=True)
+            break
+        except RuntimeError as e:
+            msg = str(e).strip().splitlines()
+            aborted.append(f"ER n={n}: {msg[-1][-240:] if msg else 'failed'}")
+            sys.stderr.write(f"reference solver failed on ER n={n} avg deg 20:\n{e}\n")
+    else:
+        print(json.dumps({**base, "unavailable": "the reference solver failed on every sample size: " +
+                                                 "; ".join(aborted)}), flush=True)
+        return
+    if status != 0 or len(starts) != ncols:
+        print(json.dumps({**base, "unavailable": f"the reference solver did not converge on ER n={n} (status "
+                                                 f"{status}, {len(starts)} of {ncols} solves started)"}),
+              flush=True)
+        return
+    t_fact = float(starts[0])
+    col_s = [float(b - a) for a, b in zip(starts[:-1], starts[1:])] + [float(secs - starts[-1])]
+    t0 = time.perf_counter()
+    d = ora.diff_norms(v1, v2, Z)
+    t_norm_col = (time.perf_counter() - t0) / ncols
+    t0 = time.perf_counter()
+    p = ora.probs(w, d, math.pow(eps, -2) * 4 * math.log(n), 1.0)
+    ora.sample_apply(n, v1, v2, w, p, ora.coins(0, m), 0, (cp, ri, va))
+    t_tail = time.perf_counter() - t0
+    wall = time.perf_counter() - t_run0
+    vals, step_ms = [], []
+    for i in range(args.warmup, args.warmup + args.steps):
+        solve = 0.5 * (col_s[2 * i] + col_s[2 * i + 1])
+        per_col = solve + t_sketch_col + t_norm_col
+        vals.append(m / (t_graph + t_fact + k * per_col + t_tail))
+        step_ms.append(2 * per_col * 1e3)
     v = statistics.median(vals)
-    line = {"impl": "reference", "metric": "input edges sparsified/sec", "value": v, "unit": "edges/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": statistics.median(walls), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "eps": eps, "k": k, "pcg_tol": PCG_TOL},
-            "cpu_baseline": {**cb, "value": v},
+    sample = (f"ER n={n} avg deg 20 (m={m}), the largest ER size the reference completes here; one run of the "
+              f"reference's own solver (oracle/_ref: factorization_driver + example_pcg_solver, {threads} threads, "
+              f"the reference's stopping rule) factoring once ({t_fact:.1f}s) and solving {ncols} right-hand sides "
+              f"one after another (2 per step; the first {2 * args.warmup} are warm-up), per-column cost "
+              f"extrapolated to k={k}; assembly, sketch, diff norms and sampling by the C port of the Rust stages "
+              f"on 1 core; whole run {wall:.1f}s")
+    line = {**base, "value": v, "ms_per_step": statistics.median(step_ms),
+            "ms_per_sparsification_extrapolated": m / v * 1e3,
+            "config": {"workload": args.workload, "eps": eps, "k": k, "pcg_tol": PCG_TOL,
+                       "sample_n": n, "sample_m": m},
+            "unavailable_at_config": REF_UNAVAILABLE_AT_CONFIG, "aborted_samples": aborted,
+            "reference_solve_s_per_column_median": statistics.median(col_s), "reference_factor_s": t_fact,
+            "cpu_baseline": {"value": v, "unit": "edges/s", "cores": threads, "kind": "reference",
+                             "sample": sample},
             "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-def _ref_available():
-    try:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import refsolver
-        return refsolver.available()
-    except Exception:
-        return False
 
 
 def serving_mix(S, count, max_n, seed=4):
@@ -374,6 +448,8 @@ def main():
     ap.add_argument("--serve-max-n", type=int, default=100_000)
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--mtx", action="store_true", help="time the GPU Matrix Market reader/writer and sparsify_dataset")
+    ap.add_argument("--reference-n", type=int, default=0,
+                    help="--impl reference: ER sample size (default: the largest size the reference completes)")
     args = ap.parse_args()
     if args.serve:
         run_serve(args)

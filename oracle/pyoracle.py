@@ -72,6 +72,9 @@ def lib():
                                        ctypes.c_int, i64p, i32p, f64p,
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.ora_sample_apply.restype = ctypes.c_int64
+        L.ora_gen_er.argtypes = [ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
+                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
+        L.ora_gen_er.restype = ctypes.c_int64
         _LIB = L
     return _LIB
 
@@ -109,6 +112,15 @@ def extract_edges(n, colptr, rowidx, val):
         raise ValueError(f"oracle edge extraction failed ({m})")
     v1 = np.zeros(m, np.int32); v2 = np.zeros(m, np.int32); w = np.zeros(m, np.float64)
     lib().ora_extract_edges(n, colptr, rowidx, val, v1.ctypes.data, v2.ctypes.data, w.ctypes.data)
+    return v1, v2, w
+
+
+def gen_er(n, avg_degree, wlo, whi, seed):
+    """Edges (v1 < v2, CSC-upper order) and weights of the synthetic ER graph the library's gen_er builds."""
+    m = lib().ora_gen_er(n, avg_degree, wlo, whi, seed, None, None, None, 0)
+    v1 = np.zeros(m, np.int32); v2 = np.zeros(m, np.int32); w = np.zeros(m, np.float64)
+    if lib().ora_gen_er(n, avg_degree, wlo, whi, seed, v1.ctypes.data, v2.ctypes.data, w.ctypes.data, m) != m:
+        raise RuntimeError("oracle ER generator: edge count changed between passes")
     return v1, v2, w
 
 

@@ -12,11 +12,21 @@
 //   dpar[3] = dpar[0] * dpar[2] + dpar[1], dpar[4] current ||r||^2, dpar[5] previous ||r||^2,
 //   dpar[6] alpha, dpar[7] beta.  The iteration is textbook preconditioned CG from x0.
 // MKL's own summation orders are not reproduced, so iterates agree with MKL's to rounding only.
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "mkl.h"
+
+// When each PCG solve began (steady-clock seconds at every dcg_init; the reference starts one solve per
+// right-hand side, example.cc:551-568), so that the harness can split the reference's own run into set-up +
+// factorization and per-column solve times without touching the reference's code.
+static std::vector<double> g_solve_starts;
+extern "C" int ssp_shim_solve_starts(const double** t) {
+    *t = g_solve_starts.data();
+    return (int)g_solve_starts.size();
+}
 
 struct sparse_matrix {
     MKL_INT rows, cols;
@@ -42,6 +52,8 @@ double dot(MKL_INT n, const double* a, const double* b) {
 
 void dcg_init(const MKL_INT* n, const double*, const double*, MKL_INT* rci, MKL_INT* ipar, double* dpar,
               double*) {
+    g_solve_starts.push_back(
+        std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count());
     for (int i = 0; i < 128; ++i) ipar[i] = 0, dpar[i] = 0.0;
     ipar[0] = *n;
     ipar[1] = 6;

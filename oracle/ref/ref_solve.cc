@@ -8,12 +8,15 @@
 //   i32 colptr[n+1], i32 rowidx[nnz], f64 values[nnz]   -- the Laplacian, CSC, all entries
 //   f64 rhs[k][n]                                          -- one right-hand side after another
 // Output file: i32 status (0 = every column converged, 1 = the driver returned false, 2 = it threw),
-//   f64 seconds (processor set-up + factorization + solves), f64 x[k][n], then the exception text if any.
+//   f64 seconds (processor set-up + factorization + solves), i32 s, f64 starts[s] (seconds from the start to
+//   the beginning of each PCG solve, recorded by the MKL shim), f64 x[k][n], then the exception text if any.
 #include "spec_spars/src/example.cc"
 
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+
+extern "C" int ssp_shim_solve_starts(const double** t);
 
 namespace {
 template <class T>
@@ -61,6 +64,14 @@ int main(int argc, char** argv) {
     if (!o) return 67;
     std::fwrite(&status, sizeof status, 1, o);
     std::fwrite(&secs, sizeof secs, 1, o);
+    const double* st = nullptr;
+    const int32_t ns = ssp_shim_solve_starts(&st);
+    const double base = std::chrono::duration<double>(t0.time_since_epoch()).count();
+    std::fwrite(&ns, sizeof ns, 1, o);
+    for (int32_t i = 0; i < ns; ++i) {
+        const double rel = st[i] - base;
+        std::fwrite(&rel, sizeof rel, 1, o);
+    }
     for (int j = 0; j < k; ++j) std::fwrite(sol[j].data(), sizeof(double), n, o);
     std::fwrite(err.data(), 1, err.size(), o);
     std::fclose(o);

@@ -32,12 +32,14 @@ def build(ref_root=None):
     return available()
 
 
-def solve(n, colptr, rowidx, values, rhs, threads=1, verbose=False, timeout=600):
+def solve(n, colptr, rowidx, values, rhs, threads=1, verbose=False, timeout=600, timings=False):
     """Solve L x_j = b_j for the columns of rhs (n x k) with the reference solver.
 
     Returns (status, seconds, X): status 0 = every column converged (relative residual < 0.01,
     custom_cg.hpp:256), 1 = the driver returned false, 2 = it threw (example.cc:566); seconds covers the
-    solver's set-up (elimination tree), factorization and all solves.
+    solver's set-up (elimination tree), factorization and all solves.  With timings=True a fourth item
+    holds, per right-hand side, the seconds from the start to the beginning of its PCG solve: the first one
+    is the set-up + factorization time, the differences are the per-column solve times.
     """
     rhs = np.asarray(rhs, np.float64)
     if rhs.ndim == 1:
@@ -59,7 +61,10 @@ def solve(n, colptr, rowidx, values, rhs, threads=1, verbose=False, timeout=600)
         if r.returncode != 0:
             raise RuntimeError(f"ref_solve exited {r.returncode}: {r.stderr[-2000:]}")
         raw = open(fout, "rb").read()
-    status, secs = struct.unpack_from("<id", raw, 0)
-    off = 12
+    status, secs, ns = struct.unpack_from("<idi", raw, 0)
+    starts = np.frombuffer(raw, np.float64, count=ns, offset=16).copy()
+    off = 16 + 8 * ns
     X = np.frombuffer(raw, np.float64, count=k * n, offset=off).reshape(k, n).T.copy()
+    if timings:
+        return status, secs, X, starts
     return status, secs, X

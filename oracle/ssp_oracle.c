@@ -691,3 +691,42 @@ int64_t ora_sample_apply(int64_t n, int64_t m, const int32_t* v1, const int32_t*
     free(ptr); free(nbr); free(eid); free(dchange); free(offchange);
     return q;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Synthetic ER workload (the same graph as the library's generator; see the header). */
+#define ORA_STREAM_GEN 0x47454e31ULL
+static double gen_u53(uint64_t seed, uint64_t a, uint64_t b) {
+    uint64_t ctr[4] = {a, b, 0, 0}, out[4];
+    ora_philox4x64(ctr, seed, ORA_STREAM_GEN, out);
+    return u53(out[0]);
+}
+
+int64_t ora_gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, int32_t* v1, int32_t* v2,
+                   double* w, int64_t cap) {
+    if (n < 2) return 0;
+    double p = avg_degree / (double)(n - 1);
+    if (p > 1.0) p = 1.0;
+    const double lp = log1p(-p);
+    int64_t v = 1, u = -1, m = 0;
+    uint64_t draw = 0;
+    while (v < n) {
+        const double x = gen_u53(seed, draw++, 0);
+        const int64_t skip = (p >= 1.0) ? 0 : (int64_t)floor(log1p(-x) / lp);
+        u += 1 + skip;
+        while (u >= v && v < n) {
+            u -= v;
+            v++;
+        }
+        if (v < n) {
+            const double uw = gen_u53(seed, draw++, 1);
+            if (v1) {
+                if (m >= cap) return -1;
+                v1[m] = (int32_t)u;
+                v2[m] = (int32_t)v;
+                w[m] = (double)(float)(wlo + (whi - wlo) * uw);
+            }
+            m++;
+        }
+    }
+    return m;
+}

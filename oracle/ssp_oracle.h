@@ -104,6 +104,15 @@ int64_t ora_sample_apply(int64_t n, int64_t m, const int32_t* v1, const int32_t*
                          const int64_t* lg_colptr, const int32_t* lg_rowidx, const double* lg_val,
                          int64_t* lh_colptr, int32_t* lh_rowidx, double* lh_val, uint8_t* keep);
 
+/* Synthetic Erdos-Renyi G(n, p = avg_degree / (n - 1)) edge list, generated exactly as the library's
+ * ssp_gen_er (Batagelj-Brandes geometric skipping over pairs (w < v) in order of v then w, uniforms from
+ * Philox(seed, draw, 0|1) of the generator stream, weights U[wlo, whi] rounded to FP32), so that the CPU
+ * baselines build their samples without loading the library.  Edges come in CSC-upper order (v1 < v2,
+ * ascending v2, then v1), the order edge extraction produces.  With v1 == NULL only the count is returned;
+ * otherwise at most cap edges are written and -1 is returned when more exist. */
+int64_t ora_gen_er(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed, int32_t* v1, int32_t* v2,
+                   double* w, int64_t cap);
+
 #ifdef __cplusplus
 }
 #endif
