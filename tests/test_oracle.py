@@ -412,3 +412,14 @@ def test_reweight_inv_p_unbiased(ora, ssp):
         H = sp.csc_matrix((hva, hri, hcp), shape=(n, n))
         tot += H.diagonal().sum()
     assert abs(tot / 20 / (2 * w.sum()) - 1.0) < 0.02
+
+
+def test_oracle_er_generator_is_the_library_generator(ora, ssp):
+    # the CPU baselines build their ER samples with the oracle's generator (no library in the reference
+    # process); it must give the library's graph edge for edge
+    for n, deg, seed in [(2, 20.0, 3), (50, 9.0, 9), (5000, 20.0, 1), (60_000, 20.0, 11)]:
+        G = ssp.gen_er(n, deg, 0.5, 2.0, seed)
+        a = ora.extract_edges(G.n, G.colptr, G.rowidx, G.values)
+        b = ora.gen_er(n, deg, 0.5, 2.0, seed)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)

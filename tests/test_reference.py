@@ -62,3 +62,15 @@ def test_reference_and_oracle_both_reject_inconsistent_rhs(ssp, ora):
     F = ora.Factor(G.n, cp, ri, va, 0, 4096, 0)
     _, iters, rel, rc = ora.pcg(G.n, cp, ri, va, F, B, 0.0, ABS_TOL, 400)
     assert rc != 0 and iters.max() == 400 and rel.max() >= 0.01
+
+
+def test_reference_solve_start_times(ora):
+    # the MKL shim records when each of the reference's sequential PCG solves starts (example.cc:551-568):
+    # one start per right-hand side, after the set-up and factorization, in increasing order, within the run
+    n = 3000
+    v1, v2, w = ora.gen_er(n, 12.0, 0.5, 2.0, 4)
+    cp, ri, va = ora.laplacian(n, v1, v2, w)
+    Y = ora.sketch(n, v1, v2, w, 5, 1 / math.sqrt(5), 0)
+    status, secs, X, starts = refsolver.solve(n, cp, ri, va, Y, threads=2, timings=True)
+    assert status == 0 and X.shape == (n, 5)
+    assert len(starts) == 5 and starts[0] > 0 and np.all(np.diff(starts) > 0) and starts[-1] < secs
