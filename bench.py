@@ -428,6 +428,62 @@ def run_mtx(args):
     os.rmdir(d)
 
 
+def spectral_check(S, ctx, LG, H, eps, st, probes=100):
+    """probe_quadratic_form (experiments.rs:88-122) on the device: x^T L_H x against x^T L_G x for 100
+    seeded uniform(-1, 1) probes, with the (1 +- eps) violation counts."""
+    r = ctx.probe_quadratic_form(LG, H, eps, probes=probes, seed=11)
+    return {"probes": r["probes"], "eps": eps, "upper_violations": r["upper_bound_violations"],
+            "lower_violations": r["lower_bound_violations"], "max_rel_err": r["max_relative_error"],
+            "mean_rel_err": r["mean_relative_error"], "kept_fraction": st["m_out"] / st["m_in"],
+            "passed": r["upper_bound_violations"] == 0 and r["lower_bound_violations"] == 0}
+
+
+def mesh_step(S, ctx, stream, name="grid3d_128"):
+    """The ill-conditioned mesh configuration (3-D 7-point grid 128^3, weights log-uniform over six decades,
+    eps 0.5, k = ceil(24 ln n / eps^2) = 1398, PCG tol 1e-8, FP64): one untimed step, one timed step (CUDA
+    events on the library's stream), with the preconditioner's roofline (it dominates there) and the
+    spectral check of the output."""
+    import torch
+    G, eps = make_graph(S, name)
+    prm = S.SparsifierParameters.baseline(eps, pcg_tol=PCG_TOL)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    cp = torch.from_numpy(G.colptr).to(dev)
+    ri = torch.from_numpy(G.rowidx).to(dev)
+    va = torch.from_numpy(G.values).to(dev)
+    _, LG = S.stage_graph(ctx, G)
+    torch.cuda.synchronize()
+    ctx.sparsify_device(G.n, G.nnz, cp.data_ptr(), ri.data_ptr(), va.data_ptr(), prm)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    H_dev, st = ctx.sparsify_device(G.n, G.nnz, cp.data_ptr(), ri.data_ptr(), va.data_ptr(), prm)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    spec = spectral_check(S, ctx, LG, S.DeviceCSC(G.n, *H_dev), eps, st)
+    peak, src = peaks()
+    n, k = st["n"], st["k"]
+    pc_ms = st["ms_precond"] / max(1, st["n_precond"])
+    sp_ms = st["ms_spmm"] / max(1, st["n_spmm"])
+    pb = precond_bytes(n, st["nnz_factor"], k)
+    out = {"workload": name, "n": n, "m": st["m_in"], "eps": eps, "k": k, "pcg_tol": PCG_TOL, "dtype": "f64",
+           "ms_per_step": ms, "value": st["m_in"] / (ms / 1000.0), "unit": "edges/s", "steps": 1, "warmup": 1,
+           "kept_fraction": st["m_out"] / st["m_in"], "pcg_iters_max": st["pcg_max_iters_used"],
+           "factor_nnz": st["nnz_factor"], "factor_levels": st["factor_levels"],
+           "factor_max_degree_used": st["factor_max_degree_used"],
+           "stages_ms": {x: st[x] for x in ("ms_assembly", "ms_sketch", "ms_factor", "ms_solve", "ms_leverage",
+                                            "ms_sample", "ms_total")},
+           "roofline": {"kernel": "precond (fwd+bwd level-set triangular solves, all k columns)", "bound": "hbm",
+                        "achieved": pb / (pc_ms / 1000.0) / 1e9 if pc_ms > 0 else None, "peak": peak,
+                        "unit": "GB/s", "peak_source": src, "avg_launch_ms": pc_ms, "algorithmic_bytes_per_launch": pb,
+                        "frac": pb / (pc_ms / 1000.0) / 1e9 / peak if pc_ms > 0 else None,
+                        "spmm_avg_ms": sp_ms},
+           "spectral": spec}
+    del cp, ri, va
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -448,6 +504,8 @@ def main():
     ap.add_argument("--serve-max-n", type=int, default=100_000)
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--mtx", action="store_true", help="time the GPU Matrix Market reader/writer and sparsify_dataset")
+    ap.add_argument("--no-mesh", dest="mesh", action="store_false",
+                    help="skip the one-step grid3d_128 measurement reported beside the ER headline")
     ap.add_argument("--reference-n", type=int, default=0,
                     help="--impl reference: ER sample size (default: the largest size the reference completes)")
     args = ap.parse_args()
@@ -491,6 +549,8 @@ def main():
     def step():
         return ctx.sparsify_device(G.n, G.nnz, cp.data_ptr(), ri.data_ptr(), va.data_ptr(), prm)
 
+    # L_G as the library forms it, for the spectral check of the timed steps' output (untimed)
+    _, LG = S.stage_graph(ctx, G)
     for _ in range(args.warmup):
         _, st = step()
     torch.cuda.synchronize()
@@ -507,13 +567,15 @@ def main():
     t_start.record(stream)
     stats = []
     for _ in range(args.steps):
-        _, st = step()
+        H_dev, st = step()
         stats.append(st)
     t_end.record(stream)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     clocks.stop()
+    # "at verified eps": the last timed step's L_H, still in the context, against L_G on seeded probes
+    spectral = spectral_check(S, ctx, LG, S.DeviceCSC(G.n, *H_dev), eps, stats[-1])
     launches = ctx.kernels_launched - k0
     ms = t_start.elapsed_time(t_end) / args.steps
     if world > 1:
@@ -589,7 +651,7 @@ def main():
             "pcg_iters_mean": st["pcg_mean_iters"], "pcg_max_relres": st["pcg_max_relres"],
             "pcg_refinements": st["pcg_refinements"], "pcg_fp64_rounds": st["pcg_fp64_rounds"],
             "spmm_slabs": st["spmm_slabs"], "factor_nnz": st["nnz_factor"], "factor_levels": st["factor_levels"],
-            "roofline": roof, "clocks": clocks.summary(), "e2e": e2e}
+            "roofline": roof, "spectral": spectral, "clocks": clocks.summary(), "e2e": e2e}
     if args.precision == "fp64" and not args.no_mixed:
         # the same workload with FP32 inner solves inside FP64 refinement (same PCG tolerance), beside the
         # plain FP64 headline; one untimed step, then two timed ones, on the same stream and clock rules
@@ -614,6 +676,13 @@ def main():
                                    "pcg_refinements": stm["pcg_refinements"], "spmm_slabs": stm["spmm_slabs"],
                                    "spmm_avg_ms": stm["ms_spmm"] / max(1, stm["n_spmm"])}
         prm.precision = S.SSP_PRECISION_FP64
+    if args.mesh and world == 1 and args.workload == "er_n1M_deg20":
+        # the mesh configuration beside the headline, on a released workspace (its n x k blocks are 141 GB)
+        ctx.release_workspace()
+        try:
+            line["mesh_grid3d_128"] = mesh_step(S, ctx, stream)
+        except Exception as e:  # reported, never fatal to the headline
+            line["mesh_grid3d_128"] = {"error": f"{type(e).__name__}: {e}"[:400]}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(eps, k)
     if rank == 0:

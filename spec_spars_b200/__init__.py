@@ -11,7 +11,7 @@ All numerical work happens in libspecspars.so on the GPU; importing works withou
 first call that needs one raises SspError if no device is visible.
 """
 from ._lib import (  # noqa: F401
-    SspError, lib, Context, CSC, SparsifierParameters, Sparsifier, InputStream, SparsificationStats,
+    SspError, lib, Context, CSC, DeviceCSC, SparsifierParameters, Sparsifier, InputStream, SparsificationStats,
     sparsify_dataset, run_solve_lap, solve_lap, read_mtx, write_mtx, laplacian_to_graph, parse_decimal, format_g17, gen_grid2d, gen_grid3d, gen_er, gen_rgg, gen_rmat,
     Server, request_footprint, edge_list_to_matrix_market,
     stage_graph, stage_sketch, stage_factor, stage_precond, stage_diff_norms, stage_probs, stage_coins, stage_scan,

@@ -281,6 +281,18 @@ class CSC:
         return (self.nnz - diag) // 2
 
 
+class DeviceCSC:
+    """A CSC whose arrays live on the device, given as raw pointers (for example the L_H that
+    Context.sparsify_device returns, or torch tensors' data_ptr()); usable wherever the API takes a CSC."""
+
+    def __init__(self, n, nnz, colptr_ptr, rowidx_ptr, values_ptr):
+        self.n, self.nnz = int(n), int(nnz)
+        self._p = (colptr_ptr, rowidx_ptr, values_ptr)
+
+    def _struct(self):
+        return _Csc(self.n, self.nnz, self._p[0], self._p[1], self._p[2], SSP_MEM_DEVICE)
+
+
 class _HostOut:
     """Owns a library-allocated host CSC; frees it once no array views it any more."""
 
@@ -423,11 +435,15 @@ class SparsifierParameters:
 
     @classmethod
     def baseline(cls, epsilon=0.5, pcg_tol=1e-8, sketch_seed=0, sampling_seed=0):
-        """k = ceil(24 ln n / eps^2) columns of +-1/sqrt(k) signs, variance-corrected probabilities."""
+        """k = ceil(24 ln n / eps^2) columns of +-1/sqrt(k) signs, variance-corrected probabilities, kept
+        edges reweighted by w/p.  These are the benchmark configurations, whose outputs are checked against
+        (1 +- eps) on probes and extremal eigenvalues: w/p keeps E[L_H] = L_G, while the reference's w/sqrt(p)
+        (sparsifier.rs:657) leaves L_H biased low wherever p < 1."""
         p = cls.cli(epsilon=epsilon, sketch_seed=sketch_seed, sampling_seed=sampling_seed)
         p.jl_dim_rule = SSP_JL_DIM_24
         p.jl_scale_rule = SSP_JL_SCALE_INV_SQRT_K
         p.prob_variance_correction = 1
+        p.reweight = SSP_REWEIGHT_INV_P
         p.pcg_tol = pcg_tol
         p.pcg_abs_tol = 0.0
         return p
@@ -517,6 +533,10 @@ class Context:
         return lib().ssp_context_kernels_launched(self._h)
 
     @property
+    def release_workspace(self):
+        """Free the context's cached device workspace (it grows again on the next call)."""
+        _check(lib().ssp_context_release_workspace(self._h))
+
     def workspace_bytes(self):
         return lib().ssp_context_workspace_bytes(self._h)
 
