@@ -1382,6 +1382,9 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
             std::vector<int64_t> hp(n + 1);
             SSP_CUDA(cudaMemcpyAsync(hp.data(), *pptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, C.stream));
             SSP_CUDA(cudaStreamSynchronize(C.stream));
+            const int64_t last_nnz = NL > 0 ? hp[lp[NL]] - hp[lp[NL - 1]] : 0;
+            if (pptr == &out.prow_ptr) out.last_fwd_nnz = last_nnz;
+            else out.last_bwd_nnz = last_nnz;
             std::vector<int32_t> starts;
             chunk_lvl.assign(NL + 1, 0);
             for (int32_t l = 0; l < NL; l++) {

@@ -345,6 +345,12 @@ struct DevFactor {
     std::vector<int64_t> frontier_sizes;  // rows of each sparse level
     int32_t compactions = 0;
     int64_t truncated_rows = 0;           // vertices left to the diagonal final level
+    // entries of the last level's rows in the row form (forward solve) and the column form (backward
+    // solve); -1 until the storage-order forms are built.  The column count is 0 for every factor (nothing is
+    // eliminated after the last level, and a level's rows never reference each other), which lets the
+    // forward solve of that level finish its rows (z = y / D) and the backward solve skip it.
+    int64_t last_fwd_nnz = -1;
+    int64_t last_bwd_nnz = -1;
     // Solve schedule.  Maximal runs of consecutive thin levels (at most THIN_ROWS rows each, two or more
     // levels) are solved by one launch that walks "steps": the run's rows grouped by their dependency depth
     // inside the run (a row's depth is one more than the deepest row of the same run it reads), which is

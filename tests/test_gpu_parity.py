@@ -98,6 +98,27 @@ def test_precond_matches_oracle(ssp, ora, ctx, dense, maxdeg):
     assert np.abs(Z - Zo).max() <= 1e-12 * np.abs(Zo).max()
 
 
+@pytest.mark.parametrize("name,k,maxdeg", [("er5k", 70, 23), ("er5k", 5, 23), ("grid3d", 33, 8),
+                                            ("rand2k_disconnected", 40, 6), ("er5k", 40, 0)])
+def test_precond_last_level_finished_by_forward_solve(ssp, ora, ctx, monkeypatch, name, k, maxdeg):
+    """The last level's rows are finished (z = y / D) by the forward solve and the backward launch of that
+    level is skipped (k_fwd_last): the result equals the two separate launches bit for bit, and the oracle.
+    Truncated factors end in a wide diagonal level of short rows (the case the kernel is for); complete
+    elimination ends in a one-vertex level."""
+    G = GRAPHS[name](ssp)
+    (_, _, _), (cp, ri, va) = _oracle_graph(ora, G)
+    lap = ssp.CSC(G.n, cp, ri, va)
+    R = np.random.default_rng(k).standard_normal((G.n, k))
+    monkeypatch.setenv("SSP_PRECOND_FUSE_LAST", "1")
+    Zf = ssp.stage_precond(ctx, lap, 7, R, 4096, maxdeg)
+    monkeypatch.setenv("SSP_PRECOND_FUSE_LAST", "0")
+    Zs = ssp.stage_precond(ctx, lap, 7, R, 4096, maxdeg)
+    np.testing.assert_array_equal(Zf.view(np.uint64), Zs.view(np.uint64))
+    o = ora.Factor(G.n, cp, ri, va, 7, 4096, maxdeg)
+    Zo = np.column_stack([o.precond(R[:, j].copy()) for j in range(k)])
+    assert np.abs(Zf - Zo).max() <= 1e-12 * np.abs(Zo).max()
+
+
 @pytest.mark.parametrize("k", [5, 40])
 @pytest.mark.parametrize("dense", [0, 1024])
 def test_precond_step_schedule_matches_oracle(ssp, ora, ctx, k, dense):
