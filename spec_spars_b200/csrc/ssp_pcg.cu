@@ -189,12 +189,13 @@ __global__ void k_center(int64_t n, int32_t k, const double* __restrict__ Y, con
     }
 }
 
-// x += alpha p ; r -= alpha q ; partial ||r||^2 per column (FP64 accumulation)
+// r -= alpha q ; partial ||r||^2 per column (FP64 accumulation).  The matching x += alpha p is deferred to
+// the next p update (k_update_xp), which reads p anyway, or to k_axpy_x after the last iteration: x gets
+// the same additions in the same order, one n x k stream fewer per iteration.
 template <class T>
-__global__ void __launch_bounds__(RED_THREADS) k_axpy_xr_rr(int64_t n, const double* __restrict__ alpha,
-                                                            const T* __restrict__ p, const T* __restrict__ q,
-                                                            T* __restrict__ x, T* __restrict__ r,
-                                                            int64_t rows_per_blk, int64_t ld, double* __restrict__ part) {
+__global__ void __launch_bounds__(RED_THREADS) k_axpy_r_rr(int64_t n, const double* __restrict__ alpha,
+                                                           const T* __restrict__ q, T* __restrict__ r,
+                                                           int64_t rows_per_blk, int64_t ld, double* __restrict__ part) {
     __shared__ double s[RED_THREADS];
     const int64_t t = blockIdx.y;
     const int c = threadIdx.x % TILE, rl = threadIdx.x / TILE;
@@ -207,7 +208,6 @@ __global__ void __launch_bounds__(RED_THREADS) k_axpy_xr_rr(int64_t n, const dou
         const int64_t o = base + row * TILE + c;
         T rv = r[o];
         if (a64 != 0.0) {
-            x[o] += a * p[o];
             rv -= a * q[o];
             r[o] = rv;
         }
@@ -222,13 +222,31 @@ __global__ void __launch_bounds__(RED_THREADS) k_axpy_xr_rr(int64_t n, const dou
     }
 }
 
+// x += alpha p (the previous step's alpha and p), then p = z + beta p
 template <class T>
-__global__ void k_update_p(int64_t n, const double* __restrict__ beta, const T* __restrict__ z, T* __restrict__ p) {
+__global__ void k_update_xp(int64_t n, const double* __restrict__ alpha, const double* __restrict__ beta,
+                            const T* __restrict__ z, T* __restrict__ p, T* __restrict__ x) {
     const int64_t t = blockIdx.y;
     const int64_t cnt = n * TILE;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t o = t * cnt + i;
-        p[o] = z[o] + (T)beta[t * TILE + (i % TILE)] * p[o];
+        const int64_t c = t * TILE + (i % TILE);
+        const double a64 = alpha[c];
+        const T pv = p[o];
+        if (a64 != 0.0) x[o] += (T)a64 * pv;
+        p[o] = z[o] + (T)beta[c] * pv;
+    }
+}
+
+// the last step's x += alpha p
+template <class T>
+__global__ void k_axpy_x(int64_t n, const double* __restrict__ alpha, const T* __restrict__ p, T* __restrict__ x) {
+    const int64_t t = blockIdx.y;
+    const int64_t cnt = n * TILE;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = t * cnt + i;
+        const double a64 = alpha[t * TILE + (i % TILE)];
+        if (a64 != 0.0) x[o] += (T)a64 * p[o];
     }
 }
 
@@ -1253,8 +1271,8 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         tm.spmm.end(C.stream);
         colred_final(C, ld, (int)A.grid.x, A.part, S.pq);
         k_cols_alpha<<<cg, 256, 0, C.stream>>>(ld, S);
-        k_axpy_xr_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
-            n, S.alpha, B.p, B.q, B.e, B.r, R.rows_per_blk, ld, R.part);
+        k_axpy_r_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
+            n, S.alpha, B.q, B.r, R.rows_per_blk, ld, R.part);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += 3 + A.nslabs;
         R.finish(S.rr);
@@ -1285,7 +1303,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         C.kernels_launched += pc_launches;
         R.run<OP_DOT, T>(B.r, B.z, S.rz_new);
         k_cols_beta<<<cg, 256, 0, C.stream>>>(ld, S);
-        k_update_p<T><<<egrid, 256, 0, C.stream>>>(n, S.beta, B.z, B.p);
+        k_update_xp<T><<<egrid, 256, 0, C.stream>>>(n, S.alpha, S.beta, B.z, B.p, B.e);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += 2;
     }
@@ -1330,12 +1348,12 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
             body_kernels += launch_precond<T>(C, F, V, n, B.r, B.z, ld, k);
             R.run<OP_DOT, T>(B.r, B.z, S.rz_new);
             k_cols_beta<<<cg, 256, 0, C.stream>>>(ld, S);
-            k_update_p<T><<<egrid, 256, 0, C.stream>>>(n, S.beta, B.z, B.p);
+            k_update_xp<T><<<egrid, 256, 0, C.stream>>>(n, S.alpha, S.beta, B.z, B.p, B.e);
             launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, true, k);
             colred_final(C, ld, (int)A.grid.x, A.part, S.pq);
             k_cols_alpha<<<cg, 256, 0, C.stream>>>(ld, S);
-            k_axpy_xr_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
-                n, S.alpha, B.p, B.q, B.e, B.r, R.rows_per_blk, ld, R.part);
+            k_axpy_r_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
+                n, S.alpha, B.q, B.r, R.rows_per_blk, ld, R.part);
             R.finish(S.rr);
             k_it_next<<<1, 1, 0, C.stream>>>(d_it);
             SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
@@ -1353,6 +1371,10 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         C.kernels_launched += 1 + body_kernels * (int64_t)(it_end - it);
         it = it_end;
     }
+    // the last step's x += alpha p (alpha is 0 for columns that stopped earlier)
+    k_axpy_x<T><<<egrid, 256, 0, C.stream>>>(n, S.alpha, B.p, B.e);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
     tm.loop.end(C.stream);
     return it;
 }
