@@ -302,9 +302,11 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def serving_mix(S, count, max_n, seed=4):
+def serving_mix(S, count, max_n, seed=4, precision="fp64"):
     """The serving mix of seeded requests: random-geometric or ER graphs (equiprobable), n log-uniform in
-    [1e3, max_n], average degree uniform in 8..32, weights uniform [0.1, 10] rounded to FP32, eps 0.3 or 0.5."""
+    [1e3, max_n], average degree uniform in 8..32, weights uniform [0.1, 10] rounded to FP32, eps 0.3 or 0.5.
+    Every request asks for complete elimination in the sparse phase (dense_threshold = factor_max_degree = 0),
+    so the server may batch it; the plain path runs the same parameters one request at a time."""
     import numpy as np
     rng = np.random.default_rng(seed)
     reqs = []
@@ -314,21 +316,19 @@ def serving_mix(S, count, max_n, seed=4):
         eps = float(rng.choice([0.3, 0.5]))
         G = S.gen_rgg(n, d, 0.1, 10.0, 1000 + i) if rng.random() < 0.5 else S.gen_er(n, d, 0.1, 10.0, 1000 + i)
         prm = S.SparsifierParameters.baseline(eps, pcg_tol=PCG_TOL, sampling_seed=i)
+        prm.dense_threshold = 0
+        prm.factor_max_degree = 0
+        if precision == "mixed":
+            prm.precision = S.SSP_PRECISION_MIXED
         reqs.append((G, prm))
     return reqs
 
 
-def run_serve(args):
-    """--serve: the serving mix through the persistent request loop (ssp_server_*).  A closed-loop pass
-    (everything submitted at once) measures the capacity; the timed pass submits at Poisson arrivals at 80% of
-    that rate and reports throughput and per-request latency (submit -> done) percentiles."""
+def serve_measure(S, reqs, slots, max_batch, rate_frac=0.8, seed=5):
+    """Closed loop (everything submitted at once) for the capacity, then Poisson arrivals at rate_frac of it;
+    returns throughput, latency percentiles and the batching the server did."""
     import numpy as np
-    import spec_spars_b200 as S
-    reqs = serving_mix(S, args.serve_requests, args.serve_max_n)
     m_total = sum(G.nnz // 2 for G, _ in reqs)
-    if args.precision == "mixed":
-        for _, prm in reqs:
-            prm.precision = S.SSP_PRECISION_MIXED
 
     def run_pass(srv, arrivals):
         t0 = time.perf_counter()
@@ -344,30 +344,70 @@ def run_serve(args):
         th = threading.Thread(target=submitter)
         th.start()
         th.join()
-        lat = []
+        lat, batch = [], []
         for t in tickets:
             _, st, tm = srv.wait(t)
             lat.append(tm["latency_ms"])
-        return time.perf_counter() - t0, lat
+            batch.append(tm["batch"])
+        return time.perf_counter() - t0, lat, batch
 
-    with S.Server(0, slots=args.serve_slots) as srv:
+    with S.Server(0, slots=slots, max_batch=max_batch) as srv:
         run_pass(srv, [0.0] * len(reqs))  # warm-up: workspaces grow, modules load
-        cap_s, _ = run_pass(srv, [0.0] * len(reqs))
-        rate = 0.8 * len(reqs) / cap_s
-        rng = np.random.default_rng(5)
+        cap_s, _, _ = run_pass(srv, [0.0] * len(reqs))
+        rate = rate_frac * len(reqs) / cap_s
+        rng = np.random.default_rng(seed)
         arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs))).tolist()
-        wall, lat = run_pass(srv, arrivals)
+        wall, lat, batch = run_pass(srv, arrivals)
         info = srv.info()
-    line = {"metric": "serving mix: input edges sparsified/sec", "value": m_total / wall, "unit": "edges/s",
-            "n_gpus": 1, "higher_is_better": True, "dtype": "f64" if args.precision == "fp64" else "mixed",
-            "data": "synthetic",
-            "config": {"workload": "serving mix", "requests": len(reqs), "n_range": [1000, args.serve_max_n],
-                       "degree_range": [8, 32], "eps": [0.3, 0.5], "slots": args.serve_slots,
-                       "arrivals": f"Poisson at {rate:.2f} req/s (0.8 x closed-loop capacity)",
-                       "precision": args.precision},
-            "closed_loop_edges_per_s": m_total / cap_s, "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(np.mean(lat)), "edges": m_total,
+    return {"value": m_total / wall, "unit": "edges/s", "closed_loop_edges_per_s": m_total / cap_s,
+            "arrivals": f"Poisson at {rate:.2f} req/s ({rate_frac} x closed-loop capacity)",
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(np.mean(lat)), "slots": slots, "max_batch": max_batch,
+            "mean_batch": float(np.mean(batch)), "peak_batch": info["peak_batch"], "runs": info["batches"],
             "peak_inflight": info["peak_inflight"], "peak_inflight_bytes": info["peak_inflight_bytes"]}
+
+
+def plain_measure(S, reqs):
+    """The plain single-graph path: each request alone through ssp_sparsify on one context, back to back."""
+    ctx = S.Context(0)
+    try:
+        ctx.sparsify(*reqs[0])  # warm-up
+        t0 = time.perf_counter()
+        for G, prm in reqs:
+            ctx.sparsify(G, prm)
+        wall = time.perf_counter() - t0
+    finally:
+        ctx.close()
+    return sum(G.nnz // 2 for G, _ in reqs) / wall
+
+
+def serving_section(S, count, max_n, slots=2, max_batch=64):
+    """The serving mix on the plain path, through the server without batching (slots only) and with
+    continuous batching, in FP64 and in mixed precision."""
+    reqs = serving_mix(S, count, max_n)
+    m_total = sum(G.nnz // 2 for G, _ in reqs)
+    plain = plain_measure(S, reqs)
+    slots_only = serve_measure(S, reqs, 4, 1)
+    batched = serve_measure(S, reqs, slots, max_batch)
+    batched_mixed = serve_measure(S, serving_mix(S, count, max_n, precision="mixed"), slots, max_batch)
+    return {"workload": "serving mix", "requests": count, "n_range": [1000, max_n], "degree_range": [8, 32],
+            "eps": [0.3, 0.5], "edges": m_total,
+            "plain_fp64_edges_per_s": plain, "served_slots_only_fp64": slots_only,
+            "served_batched_fp64": batched, "served_batched_mixed": batched_mixed,
+            "batched_mixed_over_plain": batched_mixed["value"] / plain,
+            "batched_fp64_over_plain": batched["value"] / plain}
+
+
+def run_serve(args):
+    """--serve: the serving mix through the persistent request loop (ssp_server_*), beside the plain path."""
+    import spec_spars_b200 as S
+    sec = serving_section(S, args.serve_requests, args.serve_max_n, args.serve_slots, args.serve_batch)
+    best = sec["served_batched_mixed"] if args.precision == "mixed" else sec["served_batched_fp64"]
+    line = {"metric": "serving mix: input edges sparsified/sec", "value": best["value"], "unit": "edges/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f64" if args.precision == "fp64" else "mixed",
+            "data": "synthetic", "config": {k: sec[k] for k in ("workload", "requests", "n_range", "degree_range",
+                                                              "eps", "edges")},
+            "p50_ms": best["p50_ms"], "p99_ms": best["p99_ms"], "serving": sec}
     print(json.dumps(line), flush=True)
 
 
@@ -502,7 +542,8 @@ def main():
     ap.add_argument("--serve", action="store_true", help="run the serving mix through the request loop")
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--serve-max-n", type=int, default=100_000)
-    ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--serve-slots", type=int, default=2)
+    ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--mtx", action="store_true", help="time the GPU Matrix Market reader/writer and sparsify_dataset")
     ap.add_argument("--no-mesh", dest="mesh", action="store_false",
                     help="skip the one-step grid3d_128 measurement reported beside the ER headline")

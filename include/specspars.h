@@ -227,6 +227,21 @@ int ssp_sparsify_laplacian(ssp_context* ctx, const ssp_csc* lap, const ssp_param
 int ssp_laplacian_to_graph(const ssp_csc* lap, ssp_csc_out* graph);
 int ssp_csc_free(ssp_csc_out* out);
 
+/* ---- several graphs in one launch sequence (batched serving) ----
+ * No counterpart in the reference, which sparsifies one graph per process and solves its right-hand sides one
+ * after another (example.cc:551-568).  The count graphs (host CSCs, as for ssp_sparsify) are sparsified as
+ * the disjoint union of their Laplacians: one assembly, one factorization and one all-columns PCG for the
+ * batch.  Graph b keeps its own parameters where they shape its result (epsilon, beta and row constants, JL
+ * rule, scale and seeds, variance correction, output_file), and every PCG scalar is kept per (graph,
+ * column), so outs[b] equals ssp_sparsify of graph b alone to the solve's rounding (the kept edges match
+ * unless a coin falls within that rounding of its probability).  The batch must agree on factor_seed,
+ * precision, pcg_tol, pcg_abs_tol, pcg_max_iters, reweight, and use dense_threshold = 0 and
+ * factor_max_degree = 0 (complete elimination in the sparse phase: the dense tail and truncation look at the
+ * whole Schur complement and would couple the graphs).  outs[b] is host memory (free with ssp_csc_free);
+ * stats[b] has graph b's sizes and PCG figures, and the batch's stage times. */
+int ssp_sparsify_batch(ssp_context* ctx, int32_t count, const ssp_csc* graphs, const ssp_params* params,
+                       ssp_csc_out* outs, ssp_stats* stats);
+
 /* ---- streaming: sparsify again after inserting edges (Sparsifier::insert + sparsify, sparsifier.rs:357-376,
  * 735-790) ----
  * laplacian: the current L_H (n x n, nnz may be 0); new_edges: the edges inserted since (a symmetric CSC
@@ -255,12 +270,15 @@ int ssp_shard_finish(ssp_context* ctx, const ssp_csc* graph, const ssp_params* p
 /* ---- serving: a persistent request loop on one device ----
  * No counterpart in the reference, which sparsifies one graph per process (sparsify_dataset, lib.rs:158-168).
  * Requests of uneven size are submitted from any host thread and served by `slots` workers, each with its
- * own stream and workspace, so admitted requests overlap on the device.  The oldest pending request is
- * admitted as soon as a slot is free and its estimated device footprint (ssp_request_footprint) fits beside
- * those in flight within hbm_budget_bytes; a request whose footprint alone exceeds the budget is refused
- * at submit (SSP_ERR_CAPACITY).  Each request runs exactly ssp_sparsify, so its result is the same as a
- * lone call's.  Results are collected once with ssp_wait / ssp_poll (which then own res->out: free it
- * with ssp_csc_free). */
+ * own stream and workspace, so admitted requests overlap on the device.  A free slot admits the oldest pending
+ * request whose estimated device footprint (ssp_request_footprint) fits beside those in flight within
+ * hbm_budget_bytes (a younger one may go first while the oldest has waited less than 500 ms; after that the
+ * oldest is admitted first); a request whose footprint alone exceeds the budget is refused at submit
+ * (SSP_ERR_CAPACITY).  The slot then adds pending requests that can share its run (same epsilon, factor
+ * seed, precision, PCG options and reweighting, and dense_threshold = factor_max_degree = 0), up to max_batch
+ * and its share of the budget, and runs them with ssp_sparsify_batch; other requests run exactly
+ * ssp_sparsify, so their result is the same as a lone call's.  Results are collected once with ssp_wait /
+ * ssp_poll (which then own res->out: free it with ssp_csc_free). */
 #define SSP_REQ_SPARSIFY 0
 typedef struct ssp_server ssp_server;
 typedef struct {
@@ -268,6 +286,7 @@ typedef struct {
     int32_t slots;            /* requests on the device at once */
     int64_t hbm_budget_bytes; /* admission limit on in-flight footprints; <= 0: 85% of free memory at creation */
     int32_t max_pending;      /* queue length beyond which ssp_submit refuses (0: unbounded) */
+    int32_t max_batch;        /* requests that may share one run (ssp_sparsify_batch); <= 1: each runs alone */
 } ssp_server_opts;
 typedef struct {
     int32_t kind;             /* SSP_REQ_SPARSIFY */
@@ -292,12 +311,15 @@ typedef struct {
     double probe_mean_relative_error, probe_max_relative_error;
     int64_t components_graph, components_sparsifier;
     double check_ms;
+    int32_t batch;            /* requests in the run that served this one (1: it ran alone) */
 } ssp_result;
 typedef struct {
     int64_t submitted, completed, failed, rejected, pending;
     int32_t inflight, peak_inflight, slots;
     int32_t waiters;          /* threads inside ssp_wait / ssp_poll */
     int64_t peak_inflight_bytes, budget_bytes;
+    int64_t batches;          /* runs started (a lone request or a batch) */
+    int32_t peak_batch;       /* largest batch so far */
 } ssp_server_info;
 void ssp_server_opts_default(ssp_server_opts* opts);
 int64_t ssp_request_footprint(const ssp_csc* graph, const ssp_params* params);

@@ -159,6 +159,7 @@ pub struct SspServerOpts {
     pub slots: i32,
     pub hbm_budget_bytes: i64,
     pub max_pending: i32,
+    pub max_batch: i32,
 }
 
 /// ssp_request: one sparsification request (graph and parameters are copied by ssp_submit).
@@ -191,6 +192,7 @@ pub struct SspResult {
     pub components_graph: i64,
     pub components_sparsifier: i64,
     pub check_ms: f64,
+    pub batch: i32,
 }
 
 /// ssp_server_info: counters of the request loop.
@@ -208,6 +210,8 @@ pub struct SspServerInfo {
     pub waiters: i32,
     pub peak_inflight_bytes: i64,
     pub budget_bytes: i64,
+    pub batches: i64,
+    pub peak_batch: i32,
 }
 
 /// ssp_probe_result: probe_quadratic_form's counts (experiments.rs:88-122).
@@ -257,6 +261,8 @@ extern "C" {
 
     pub fn ssp_sparsify(ctx: *mut SspContext, graph: *const SspCsc, params: *const SspParams, out_mem: i32,
                         out: *mut SspCscOut, stats: *mut SspStats) -> c_int;
+    pub fn ssp_sparsify_batch(ctx: *mut SspContext, count: i32, graphs: *const SspCsc, params: *const SspParams,
+                              outs: *mut SspCscOut, stats: *mut SspStats) -> c_int;
     pub fn ssp_sparsify_laplacian(ctx: *mut SspContext, lap: *const SspCsc, params: *const SspParams, out_mem: i32,
                                   out: *mut SspCscOut, stats: *mut SspStats) -> c_int;
     pub fn ssp_laplacian_to_graph(lap: *const SspCsc, graph: *mut SspCscOut) -> c_int;

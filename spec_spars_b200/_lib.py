@@ -92,7 +92,7 @@ class _SolveReport(ctypes.Structure):
 
 class _ServerOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("slots", ctypes.c_int32), ("hbm_budget_bytes", ctypes.c_int64),
-                ("max_pending", ctypes.c_int32)]
+                ("max_pending", ctypes.c_int32), ("max_batch", ctypes.c_int32)]
 
 
 class _Request(ctypes.Structure):
@@ -106,14 +106,15 @@ class _Result(ctypes.Structure):
                 ("probe_upper_violations", ctypes.c_int64), ("probe_lower_violations", ctypes.c_int64),
                 ("probe_mean_relative_error", ctypes.c_double), ("probe_max_relative_error", ctypes.c_double),
                 ("components_graph", ctypes.c_int64), ("components_sparsifier", ctypes.c_int64),
-                ("check_ms", ctypes.c_double)]
+                ("check_ms", ctypes.c_double), ("batch", ctypes.c_int32)]
 
 
 class _ServerInfo(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
                 ("rejected", ctypes.c_int64), ("pending", ctypes.c_int64), ("inflight", ctypes.c_int32),
                 ("peak_inflight", ctypes.c_int32), ("slots", ctypes.c_int32), ("waiters", ctypes.c_int32),
-                ("peak_inflight_bytes", ctypes.c_int64), ("budget_bytes", ctypes.c_int64)]
+                ("peak_inflight_bytes", ctypes.c_int64), ("budget_bytes", ctypes.c_int64),
+                ("batches", ctypes.c_int64), ("peak_batch", ctypes.c_int32)]
 
 
 class _ProbeResult(ctypes.Structure):
@@ -153,6 +154,8 @@ def lib():
             "ssp_solve_opts_default": ([ctypes.POINTER(_SolveOpts)], None),
             "ssp_solve_lap": ([P, ctypes.POINTER(_Csc), P, I32, P, I32, ctypes.POINTER(_SolveOpts),
                                ctypes.POINTER(_SolveReport)], ctypes.c_int),
+            "ssp_sparsify_batch": ([P, I32, ctypes.POINTER(_Csc), ctypes.POINTER(_Params), ctypes.POINTER(_CscOut),
+                                    ctypes.POINTER(_Stats)], ctypes.c_int),
             "ssp_sparsify": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(_Params), I32, ctypes.POINTER(_CscOut),
                               ctypes.POINTER(_Stats)], ctypes.c_int),
             "ssp_sparsify_laplacian": ([P, ctypes.POINTER(_Csc), ctypes.POINTER(_Params), I32,
@@ -532,11 +535,11 @@ class Context:
     def kernels_launched(self):
         return lib().ssp_context_kernels_launched(self._h)
 
-    @property
     def release_workspace(self):
         """Free the context's cached device workspace (it grows again on the next call)."""
         _check(lib().ssp_context_release_workspace(self._h))
 
+    @property
     def workspace_bytes(self):
         return lib().ssp_context_workspace_bytes(self._h)
 
@@ -548,6 +551,30 @@ class Context:
         _check(lib().ssp_sparsify(self._h, ctypes.byref(g), ctypes.byref(params._s), SSP_MEM_HOST,
                                   ctypes.byref(out), ctypes.byref(st)))
         return _take_out(out), _stats_dict(st)
+
+    def sparsify_batch(self, graphs, params):
+        """Several host graphs sparsified as one disjoint union (ssp_sparsify_batch): one factorization and one
+        all-columns PCG for the batch, every PCG scalar per (graph, column).  params: one SparsifierParameters
+        per graph, or one for all; they must agree on the factor seed, precision, PCG options and reweighting and
+        ask for complete elimination (dense_threshold = 0, factor_max_degree = 0).  Returns [(L_H, stats)]."""
+        graphs = list(graphs)
+        if isinstance(params, SparsifierParameters):
+            params = [params] * len(graphs)
+        params = list(params)
+        if len(params) != len(graphs) or not graphs:
+            raise ValueError("sparsify_batch: need one SparsifierParameters per graph")
+        cnt = len(graphs)
+        gs = (_Csc * cnt)(*[g._struct() for g in graphs])
+        ps = (_Params * cnt)(*[p._s for p in params])
+        outs = (_CscOut * cnt)()
+        sts = (_Stats * cnt)()
+        _check(lib().ssp_sparsify_batch(self._h, cnt, gs, ps, outs, sts))
+        res = []
+        for i in range(cnt):
+            out = _CscOut()
+            ctypes.memmove(ctypes.byref(out), ctypes.byref(outs[i]), ctypes.sizeof(_CscOut))
+            res.append((_take_out(out), _stats_dict(sts[i])))
+        return res
 
     def sparsify_laplacian(self, lap, params):
         """Host Laplacian L_G in (as Sparsifier::from_matrix reads one, sparsifier.rs:299-300), host L_H out;
@@ -925,8 +952,9 @@ def request_footprint(graph, params):
 class Server:
     """Persistent request loop on one device (ssp_server_*): submit from any thread, collect with wait/poll."""
 
-    def __init__(self, device=0, slots=4, hbm_budget_bytes=0, max_pending=0):
-        o = _ServerOpts(device, slots, hbm_budget_bytes, max_pending)
+    def __init__(self, device=0, slots=4, hbm_budget_bytes=0, max_pending=0, max_batch=32):
+        """max_batch: requests that may share one run (ssp_sparsify_batch); 1 runs every request alone."""
+        o = _ServerOpts(device, slots, hbm_budget_bytes, max_pending, max_batch)
         h = P()
         _check(lib().ssp_server_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h
@@ -940,7 +968,7 @@ class Server:
 
     def _collect(self, res):
         info = {"queue_ms": res.queue_ms, "run_ms": res.run_ms, "latency_ms": res.latency_ms, "slot": res.slot,
-                "est_bytes": res.est_bytes}
+                "est_bytes": res.est_bytes, "batch": res.batch}
         if res.checked:
             info["check"] = {"upper_bound_violations": res.probe_upper_violations,
                              "lower_bound_violations": res.probe_lower_violations,

@@ -599,6 +599,250 @@ static const T* stage_in(Context& C, const T* p, int64_t cnt, int32_t mem, const
     return d;
 }
 
+// ---------------------------------------------------------------- several graphs at once
+// The reference sparsifies one graph per process and solves its right-hand sides one after another
+// (example.cc:551-568).  For many small graphs that leaves the GPU mostly idle, so a batch is run as the
+// disjoint union of its graphs: one assembly, one factorization and one PCG for all of them.
+//   * Graph b's vertices are [V_b, V_b + n_b) of the union and its edges [E_b, E_b + m_b) (the union's CSC
+//     keeps each graph's columns together, and edges are extracted in CSC order).
+//   * Its sketch uses its own seed, scale, k_b and edge ids counted from E_b; its factor draws are keyed by
+//     in-graph vertex ids, so both equal the lone run's.  Elimination is complete in the sparse phase (no
+//     dense tail, no truncation: those look at the whole Schur complement and would couple the graphs).
+//   * The PCG keeps every scalar per (graph, column) (PcgSegments), so each graph's iterates are its own;
+//     its reductions are blocked differently from a lone run's, so a served result equals the lone result
+//     to the solve's rounding, not bit for bit.
+//   * Probabilities and coins use each graph's beta, k, seeds and edge ids; L_H is assembled once and split.
+__global__ void k_add_i64(int64_t count, int64_t* a, int64_t add) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+        a[i] += add;
+}
+__global__ void k_add_i32(int64_t count, int32_t* a, int32_t add) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+        a[i] += add;
+}
+// graph of every union vertex and the first vertex of that graph (V: nseg + 1 starts)
+__global__ void k_vertex_graph(int64_t n, const int64_t* __restrict__ V, int32_t nseg, int32_t* __restrict__ rowseg,
+                               int32_t* __restrict__ vbase) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        int32_t lo = 0, hi = nseg - 1;  // last s with V[s] <= v
+        while (lo < hi) {
+            const int32_t mid = (lo + hi + 1) >> 1;
+            if (V[mid] <= v) lo = mid;
+            else hi = mid - 1;
+        }
+        rowseg[v] = lo;
+        vbase[v] = (int32_t)V[lo];
+    }
+}
+
+static bool same_batch_options(const ssp_params& a, const ssp_params& b) {
+    return a.factor_seed == b.factor_seed && a.precision == b.precision && a.pcg_tol == b.pcg_tol &&
+           a.pcg_abs_tol == b.pcg_abs_tol && a.pcg_max_iters == b.pcg_max_iters && a.reweight == b.reweight &&
+           a.dense_threshold == b.dense_threshold && a.factor_max_degree == b.factor_max_degree;
+}
+
+static void sparsify_batch_impl(Context& C, int32_t count, const ssp_csc* graphs, const ssp_params* prms,
+                                ssp_csc_out* outs, ssp_stats* stats) {
+    SSP_REQUIRE(count >= 1 && graphs && prms && outs, SSP_ERR_INVALID, "batch: need count >= 1, graphs, params, outs");
+    for (int32_t b = 0; b < count; b++) memset(&outs[b], 0, sizeof(outs[b]));
+    const ssp_params& p0 = prms[0];
+    int64_t n = 0, nnz = 0;
+    std::vector<int64_t> V(count + 1, 0), NZ(count + 1, 0), E(count + 1, 0);
+    for (int32_t b = 0; b < count; b++) {
+        const ssp_csc& g = graphs[b];
+        const ssp_params& p = prms[b];
+        SSP_REQUIRE(g.mem == SSP_MEM_HOST && g.n > 0 && g.nnz >= 0 && g.colptr && (g.nnz == 0 || (g.rowidx && g.values)),
+                    SSP_ERR_INVALID, "batch: every graph must be a host CSC with n > 0");
+        SSP_REQUIRE(g.colptr[0] == 0 && g.colptr[g.n] == g.nnz, SSP_ERR_INVALID, "batch: colptr must run 0 .. nnz");
+        SSP_REQUIRE(p.epsilon > 0 && std::isfinite(p.epsilon), SSP_ERR_INVALID, "batch: epsilon must be positive");
+        SSP_REQUIRE(same_batch_options(p, p0), SSP_ERR_INVALID,
+                    "batch: factor seed, precision, PCG options, reweighting and factor options must agree");
+        SSP_REQUIRE(p.dense_threshold == 0 && p.factor_max_degree == 0, SSP_ERR_INVALID,
+                    "batch: the graphs must ask for complete sparse elimination (dense_threshold = 0, "
+                    "factor_max_degree = 0)");
+        // edges: upper entries with a non-zero value (sparsifier.rs:365), in CSC order
+        int64_t m = 0;
+        for (int64_t j = 0; j < g.n; j++)
+            for (int64_t q = g.colptr[j]; q < g.colptr[j + 1]; q++) {
+                SSP_REQUIRE(g.rowidx[q] >= 0 && g.rowidx[q] < g.n, SSP_ERR_INVALID, "batch: row index out of range");
+                m += (g.rowidx[q] < j && g.values[q] != 0.0) ? 1 : 0;
+            }
+        V[b + 1] = V[b] + g.n;
+        NZ[b + 1] = NZ[b] + g.nnz;
+        E[b + 1] = E[b] + m;
+    }
+    n = V[count];
+    nnz = NZ[count];
+    SSP_REQUIRE(n < (int64_t)INT32_MAX, SSP_ERR_INVALID, "batch: the union must have fewer than 2^31 vertices");
+    SSP_CUDA(cudaSetDevice(C.device));
+    StageTimer T(C);
+    T.mark();  // 0
+    // the union CSC: each graph's arrays copied into place, then shifted by its vertex and entry offsets
+    Workspace& W = C.ws;
+    int64_t* ucp = W.get_t<int64_t>("bt_cp", n + 1);
+    int32_t* uri = W.get_t<int32_t>("bt_ri", nnz + 1);
+    double* uva = W.get_t<double>("bt_va", nnz + 1);
+    for (int32_t b = 0; b < count; b++) {
+        const ssp_csc& g = graphs[b];
+        copy_h2d(C, ucp + V[b], g.colptr, sizeof(int64_t) * g.n);
+        if (g.nnz) {
+            copy_h2d(C, uri + NZ[b], g.rowidx, sizeof(int32_t) * g.nnz);
+            copy_h2d(C, uva + NZ[b], g.values, sizeof(double) * g.nnz);
+        }
+        if (NZ[b]) k_add_i64<<<grid_for(g.n, 256), 256, 0, C.stream>>>(g.n, ucp + V[b], NZ[b]);
+        if (V[b] && g.nnz) k_add_i32<<<grid_for(g.nnz, 256), 256, 0, C.stream>>>(g.nnz, uri + NZ[b], (int32_t)V[b]);
+        SSP_CHECK_LAUNCH();
+    }
+    SSP_CUDA(cudaMemcpyAsync(ucp + n, &nnz, sizeof(int64_t), cudaMemcpyHostToDevice, C.stream));
+    SSP_CUDA(cudaStreamSynchronize(C.stream));  // &nnz is a stack value
+    DevGraph G;
+    build_graph_from_csc(C, n, ucp, uri, uva, nnz, G, "bt_g");
+    SSP_REQUIRE(G.m == E[count], SSP_ERR_INVALID, "batch: edge count of the union differs from its graphs'");
+    int64_t* dV = W.get_t<int64_t>("bt_V", count + 1);
+    int32_t* rowseg = W.get_t<int32_t>("bt_rowseg", n);
+    int32_t* vbase = W.get_t<int32_t>("bt_vbase", n);
+    SSP_CUDA(cudaMemcpyAsync(dV, V.data(), sizeof(int64_t) * (count + 1), cudaMemcpyHostToDevice, C.stream));
+    k_vertex_graph<<<grid_for(n, 256), 256, 0, C.stream>>>(n, dV, count, rowseg, vbase);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched += 1 + 2 * count;
+    T.mark();  // 1
+    // sketch: graph b fills its rows' first k_b columns; the other columns of its rows stay zero
+    std::vector<int32_t> k(count);
+    int32_t kmax = 1;
+    for (int32_t b = 0; b < count; b++) {
+        k[b] = jl_dim(&prms[b], V[b + 1] - V[b]);
+        kmax = std::max(kmax, k[b]);
+    }
+    const int64_t ld = tile_ld(kmax);
+    double* Y = W.get_t<double>("bt_Y", (size_t)n * ld);
+    SSP_CUDA(cudaMemsetAsync(Y, 0, sizeof(double) * (size_t)n * ld, C.stream));
+    for (int32_t b = 0; b < count; b++)
+        sketch_device_part(C, G, V[b], V[b + 1] - V[b], E[b], k[b], jl_scale(&prms[b], k[b]), prms[b].sketch_seed,
+                           prms[b].sketch_uniform, Y, ld, 1, 0);
+    T.mark();  // 2
+    DevFactor F;
+    FactorOptions fo;
+    fo.seed = p0.factor_seed;
+    fo.dense_threshold = 0;
+    fo.max_degree = 0;
+    fo.vbase = vbase;
+    factor_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, fo, F, "bt_f");
+    T.mark();  // 3
+    PcgOptions po;
+    po.tol = p0.pcg_tol;
+    po.abs_tol = p0.pcg_abs_tol;
+    po.max_iters = p0.pcg_max_iters;
+    po.verbose = p0.verbose;
+    po.precision = p0.precision;
+    PcgSegments segs;
+    segs.row0 = V;
+    segs.k = k;
+    segs.rowseg = rowseg;
+    po.segs = &segs;
+    PcgReport rep;
+    const double* Zt = nullptr;
+    double* d2 = W.get_t<double>("bt_d2", G.m + 1);
+    pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, kmax, &Zt, po, rep, nullptr, nullptr, G.lap_eid, d2);
+    T.mark();  // 4
+    double* d = W.get_t<double>("bt_d", G.m + 1);
+    double* pr = W.get_t<double>("bt_p", G.m + 1);
+    double* coins = W.get_t<double>("bt_coins", G.m + 1);
+    // columns past a graph's k_b are zero in its rows, so they add nothing to its norms
+    if (rep.diff_fused) sqrt_device(C, G.m, d2, d);
+    else diff_norms_device(C, G.m, G.v1, G.v2, Zt, kmax, ld, d, n, true);
+    for (int32_t b = 0; b < count; b++) {
+        const int64_t mb = E[b + 1] - E[b], nb = V[b + 1] - V[b];
+        const double scale = jl_scale(&prms[b], k[b]);
+        const double denom = prms[b].prob_variance_correction ? (double)k[b] * scale * scale : (double)k[b];
+        probs_device(C, mb, G.w + E[b], d + E[b], beta_of(&prms[b], nb), denom, pr + E[b]);
+    }
+    T.mark();  // 5
+    for (int32_t b = 0; b < count; b++) coins_device(C, E[b + 1] - E[b], prms[b].sampling_seed, coins + E[b]);
+    int64_t* lh_ptr;
+    int32_t* lh_idx;
+    double* lh_val;
+    sample_apply_device(C, G, pr, coins, p0.reweight, &lh_ptr, &lh_idx, &lh_val, nullptr);
+    T.mark();  // 6
+    // split L_H: graph b's columns, its row ids shifted back
+    std::vector<int64_t> hptr(n + 1);
+    copy_d2h(C, hptr.data(), lh_ptr, sizeof(int64_t) * (n + 1));
+    for (int32_t b = 0; b < count; b++) {
+        const int64_t nb = V[b + 1] - V[b];
+        const int64_t e0 = hptr[V[b]], e1 = hptr[V[b + 1]], cnt = e1 - e0;
+        ssp_csc_out& o = outs[b];
+        o.n = nb;
+        o.nnz = cnt;
+        o.mem = SSP_MEM_HOST;
+        o.colptr = (int64_t*)malloc(sizeof(int64_t) * (nb + 1));
+        o.rowidx = (int32_t*)malloc(sizeof(int32_t) * (cnt + 1));
+        o.values = (double*)malloc(sizeof(double) * (cnt + 1));
+        if (!o.colptr || !o.rowidx || !o.values) {
+            for (int32_t a = 0; a <= b; a++) {
+                free(outs[a].colptr); free(outs[a].rowidx); free(outs[a].values);
+                memset(&outs[a], 0, sizeof(outs[a]));
+            }
+            throw Error(SSP_ERR_NOMEM, "host allocation of a batch output failed");
+        }
+        for (int64_t j = 0; j <= nb; j++) o.colptr[j] = hptr[V[b] + j] - e0;
+        if (cnt) {
+            copy_d2h(C, o.rowidx, lh_idx + e0, sizeof(int32_t) * cnt);
+            copy_d2h(C, o.values, lh_val + e0, sizeof(double) * cnt);
+        }
+        for (int64_t q = 0; q < cnt; q++) o.rowidx[q] -= (int32_t)V[b];
+    }
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    for (int32_t b = 0; b < count; b++) {
+        const ssp_csc_out& o = outs[b];
+        int64_t diag = 0;
+        for (int64_t j = 0; j < o.n; j++)
+            for (int64_t q = o.colptr[j]; q < o.colptr[j + 1]; q++) diag += o.rowidx[q] == j;
+        int32_t it_max = 0;
+        double it_sum = 0.0, rel_max = 0.0;
+        for (int32_t j = 0; j < k[b]; j++) {
+            const int64_t s = (int64_t)b * ld + j;
+            it_max = std::max(it_max, segs.iters[s]);
+            it_sum += segs.iters[s];
+            rel_max = std::max(rel_max, segs.relres[s]);
+        }
+        if (stats) {
+            ssp_stats& st = stats[b];
+            memset(&st, 0, sizeof(st));
+            st.n = o.n;
+            st.m_in = E[b + 1] - E[b];
+            st.m_out = (o.nnz - diag) / 2;
+            st.k = k[b];
+            st.beta = beta_of(&prms[b], o.n);
+            st.pcg_max_iters_used = it_max;
+            st.pcg_mean_iters = it_sum / k[b];
+            st.pcg_max_relres = rel_max;
+            // the batch's shared figures: every graph of the batch reports the same stage times and factor
+            st.nnz_factor = F.nnz;
+            st.factor_levels = F.num_levels;
+            st.ms_assembly = T.ms(0, 1);
+            st.ms_sketch = T.ms(1, 2);
+            st.ms_factor = T.ms(2, 3);
+            st.ms_solve = T.ms(3, 4);
+            st.ms_leverage = T.ms(4, 5);
+            st.ms_sample = T.ms(5, 6);
+            st.ms_total = T.ms(0, 6);
+            st.kernels_launched = C.kernels_launched;
+            st.ms_spmm = rep.ms_spmm;
+            st.n_spmm = rep.n_spmm;
+            st.ms_precond = rep.ms_precond;
+            st.n_precond = rep.n_precond;
+            st.nnz_laplacian = G.lap_nnz;
+            st.pcg_refinements = rep.refinements;
+            st.pcg_fp64_rounds = rep.fp64_rounds;
+            st.spmm_slabs = rep.spmm_slabs;
+        }
+        if (prms[b].output_file && prms[b].output_file[0]) {
+            std::string err;
+            if (write_mtx(prms[b].output_file, o.n, o.colptr, o.rowidx, o.values, err) != SSP_OK)
+                throw Error(SSP_ERR_IO, err);
+        }
+    }
+}
+
 }  // namespace ssp
 
 using namespace ssp;
@@ -739,6 +983,14 @@ int ssp_sparsify(ssp_context* c, const ssp_csc* graph, const ssp_params* params,
     return guarded([&] {
         SSP_REQUIRE(c, SSP_ERR_INVALID, "ctx is NULL");
         sparsify_impl(c->ctx, graph, params, out_mem, out, stats);
+    });
+}
+
+int ssp_sparsify_batch(ssp_context* c, int32_t count, const ssp_csc* graphs, const ssp_params* params,
+                       ssp_csc_out* outs, ssp_stats* stats) {
+    return guarded([&] {
+        SSP_REQUIRE(c, SSP_ERR_INVALID, "ctx is NULL");
+        sparsify_batch_impl(c->ctx, count, graphs, params, outs, stats);
     });
 }
 

@@ -32,6 +32,9 @@ constexpr int DENSE_FRONTIER_MAX = 8;   // dense tail once the frontier has coll
 struct FDev {
     int64_t n;
     uint64_t seed;
+    // several graphs factored at once: vbase[v] is the first vertex of v's graph, and every random draw is keyed
+    // by the vertex's id inside its graph, so each graph's factor is the one it gets alone (null: one graph)
+    const int32_t* vbase;
     const uint64_t* prio;
     int32_t* count;
     int32_t* level;
@@ -61,9 +64,11 @@ __device__ __forceinline__ bool key_less(const uint64_t* prio, int32_t a, int32_
 }
 
 // ---------------------------------------------------------------- init
-__global__ void k_prio(int64_t n, uint64_t seed, uint64_t* prio) {
+__device__ __forceinline__ int64_t local_vertex(const int32_t* vbase, int64_t v) { return vbase ? v - vbase[v] : v; }
+
+__global__ void k_prio(int64_t n, uint64_t seed, uint64_t* prio, const int32_t* vbase) {
     for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
-        prio[v] = vertex_priority(seed, v);
+        prio[v] = vertex_priority(seed, local_vertex(vbase, v));
 }
 
 // lower entries (r > c, |val| != 0) counted for both endpoints
@@ -158,7 +163,7 @@ __device__ __forceinline__ void emit_slot(const FDev& F, int32_t v, int64_t fidx
     if (i + 1 < cnt) {
         const double ci = sc[i];
         const double rem = S - ci;
-        const double tgt = factor_uniform(F.seed, v, i) * rem;
+        const double tgt = factor_uniform(F.seed, local_vertex(F.vbase, v), i) * rem;
         int32_t lo = i + 1, hi = cnt;
         while (lo < hi) {
             int32_t mid = lo + ((hi - lo) >> 1);
@@ -815,7 +820,7 @@ __global__ void __launch_bounds__(1024) k_dense_elim(FDev F, const int32_t* rem,
             if (q + 1 < cnt) {
                 const double ci = sc[q];
                 const double rem_ = S - ci;
-                const double tgt = factor_uniform(F.seed, v, q) * rem_;
+                const double tgt = factor_uniform(F.seed, local_vertex(F.vbase, v), q) * rem_;
                 int32_t lo = q + 1, hi = cnt;
                 while (lo < hi) {
                     int32_t mid = lo + ((hi - lo) >> 1);
@@ -1028,6 +1033,11 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
     FDev F;
     F.n = n;
     F.seed = opt.seed;
+    F.vbase = opt.vbase;
+    // the dense tail and the truncation test look at the whole Schur complement: with several graphs they
+    // would couple them, so a union is eliminated completely in the sparse phase
+    SSP_REQUIRE(!opt.vbase || (opt.dense_threshold == 0 && opt.max_degree == 0), SSP_ERR_INVALID,
+                "factor: several graphs at once need dense_threshold = 0 and max_degree = 0");
     uint64_t* prio = W.get_t<uint64_t>(nm("prio"), n);
     F.prio = prio;
     F.count = W.get_t<int32_t>(nm("count"), n);
@@ -1045,7 +1055,7 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
     SSP_CUDA(cudaMemsetAsync(F.bag_len, 0, sizeof(int32_t) * n, C.stream));
     SSP_CUDA(cudaMemsetAsync(F.Lcnt, 0, sizeof(int32_t) * (n + 1), C.stream));
     const int T256 = 256;
-    k_prio<<<grid_for(n, T256), T256, 0, C.stream>>>(n, opt.seed, prio);
+    k_prio<<<grid_for(n, T256), T256, 0, C.stream>>>(n, opt.seed, prio, opt.vbase);
     k_lower_deg<<<grid_for(n, T256), T256, 0, C.stream>>>(n, colptr, rowidx, val, deg);
     k_bag_caps<<<grid_for(n, T256), T256, 0, C.stream>>>(n, deg, F.bag_cap);
     SSP_CHECK_LAUNCH();

@@ -309,6 +309,9 @@ int64_t laplacian_plus_graph_device(Context& C, int64_t n, const int64_t* lptr, 
 // a4: Y = B^T Q, columns [0,k): row-major with leading dimension ldy, or tile-major (SSP_TILE-column slabs)
 void sketch_device(Context& C, const DevGraph& G, int32_t k, double scale, uint64_t seed, int uniform,
                    double* Y, int64_t ldy, int tile_major, int32_t col_lo = 0);
+// the same for vertices [v0, v0 + nv) only, edge ids counted from e0 (one graph of a union of graphs)
+void sketch_device_part(Context& C, const DevGraph& G, int64_t v0, int64_t nv, int64_t e0, int32_t k, double scale,
+                        uint64_t seed, int uniform, double* Y, int64_t ldy, int tile_major, int32_t col_lo = 0);
 
 // a7: factor
 struct DevFactor {
@@ -372,6 +375,7 @@ struct FactorOptions {
     uint64_t seed = 0;
     int64_t dense_threshold = 4096;
     int64_t max_degree = 0;  // stop once the live Schur complement's average degree exceeds this (0: never)
+    const int32_t* vbase = nullptr;  // device [n]: first vertex of each vertex's graph (several graphs at once)
 };
 // Input: Laplacian CSC on device (rows > col used, |value| as weight).
 void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,
@@ -379,6 +383,16 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
 
 // a8: PCG on all k columns.  Y: tile-major n x round8(k) device block; the solution is left in the
 // workspace (tile-major) and returned through *x_out.
+// Several graphs solved at once as the disjoint union of their Laplacians (rows [row0[s], row0[s + 1]) are
+// graph s, which uses the first k[s] columns).  Every per-column scalar of the PCG is then per (graph,
+// column), so each graph's iterates are its own.  iters / relres come back per (graph, column), at s * ld + c.
+struct PcgSegments {
+    std::vector<int64_t> row0;        // nseg + 1 row starts
+    std::vector<int32_t> k;           // columns of each graph
+    const int32_t* rowseg = nullptr;  // device [n]: graph of each row
+    std::vector<int32_t> iters;       // out
+    std::vector<double> relres;       // out
+};
 struct PcgOptions {
     double tol = 1e-8;
     double abs_tol = 0.0;
@@ -386,6 +400,7 @@ struct PcgOptions {
     int verbose = 0;
     std::vector<double>* history = nullptr;  // per iteration: max over columns of ||r|| / ||b||
     int precision = SSP_PRECISION_FP64;      // SSP_PRECISION_MIXED: FP32 inner solves, FP64 refinement
+    PcgSegments* segs = nullptr;             // several graphs at once (see PcgSegments)
 };
 struct PcgReport {
     int32_t max_iters_used = 0;

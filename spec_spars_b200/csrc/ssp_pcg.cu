@@ -77,6 +77,36 @@ void tiles_to_rowmajor(Context& C, int64_t n, int32_t k, const double* src, doub
     C.kernels_launched++;
 }
 
+// ---------------------------------------------------------------- segments (several graphs in one solve)
+// A batch of graphs is solved as the disjoint union of their Laplacians: rows [row0_s, row0_{s+1}) belong to
+// segment s, which owns columns [0, k_s) of the n x k block (the rest of its columns stay zero and inactive).
+// Every per-column scalar (norms, thresholds, alpha, beta, activity) is per (segment, column), at index
+// s * ld + c, so each graph's iterates are its own; reductions use blocks that never straddle two segments.
+// A single graph is one segment with null tables, and every kernel then does exactly what it did before.
+struct SegDev {
+    int32_t nseg = 1;
+    const int32_t* rowseg = nullptr;    // [n] segment of each row
+    const int32_t* kseg = nullptr;      // [nseg] columns of each segment
+    const int64_t* segrows = nullptr;   // [nseg] rows of each segment
+    const int64_t* blk_row = nullptr;   // [nparts + 1] row boundaries of the reduction blocks
+    const int32_t* blk_seg = nullptr;   // [nparts] segment of each reduction block
+    const int32_t* part_start = nullptr;  // [nseg + 1] first reduction block of each segment
+};
+__device__ __forceinline__ int64_t seg_of_row(const SegDev& G, int64_t row) { return G.rowseg ? G.rowseg[row] : 0; }
+// rows of reduction block blockIdx.x and the state offset (segment * ld) of its segment
+__device__ __forceinline__ void red_block(const SegDev& G, int64_t n, int64_t rows_per_blk, int64_t ld, int64_t& r0,
+                                          int64_t& r1, int64_t& sbase) {
+    if (G.blk_row) {
+        r0 = G.blk_row[blockIdx.x];
+        r1 = G.blk_row[blockIdx.x + 1];
+        sbase = (int64_t)G.blk_seg[blockIdx.x] * ld;
+    } else {
+        r0 = (int64_t)blockIdx.x * rows_per_blk;
+        r1 = min(n, r0 + rows_per_blk);
+        sbase = 0;
+    }
+}
+
 // ---------------------------------------------------------------- column reductions
 enum ColOp { OP_SUM = 0, OP_DOT = 1, OP_SQ = 2, OP_SQDIFF_CENTERED = 3 };
 
@@ -85,14 +115,15 @@ template <int OP, class T>
 __global__ void __launch_bounds__(RED_THREADS) k_colred_partial(int64_t n, const T* __restrict__ a,
                                                                 const T* __restrict__ b,
                                                                 const double* __restrict__ mean, int64_t rows_per_blk,
-                                                                int64_t ld, double* __restrict__ part) {
+                                                                int64_t ld, double* __restrict__ part, SegDev G) {
     __shared__ double s[RED_THREADS];
     const int64_t t = blockIdx.y;
     const int c = threadIdx.x % TILE, rl = threadIdx.x / TILE;
-    const int64_t r0 = (int64_t)blockIdx.x * rows_per_blk, r1 = min(n, r0 + rows_per_blk);
+    int64_t r0, r1, sb;
+    red_block(G, n, rows_per_blk, ld, r0, r1, sb);
     const T* at = a + t * n * TILE;
     const T* bt = b ? b + t * n * TILE : nullptr;
-    const double mu = (OP == OP_SQDIFF_CENTERED) ? mean[t * TILE + c] : 0.0;
+    const double mu = (OP == OP_SQDIFF_CENTERED) ? mean[sb + t * TILE + c] : 0.0;
     double acc = 0.0;
     for (int64_t r = r0 + rl; r < r1; r += RED_THREADS / TILE) {
         const double x = (double)at[r * TILE + c];
@@ -117,30 +148,37 @@ __global__ void __launch_bounds__(RED_THREADS) k_colred_partial(int64_t n, const
 // at a time, then the warps' sums are added in warp order (fixed order: deterministic).  Hundreds of parts per
 // column (the SpMM's p.q partials) are then 16-way parallel instead of one thread's dependent chain.
 constexpr int FIN_WARPS = 16;
+// With segments, out[s * ld + c] sums the parts of segment s's blocks, in the same order.
 __global__ void __launch_bounds__(FIN_WARPS * 32) k_colred_final(int64_t ld, int nparts, const double* __restrict__ part,
-                                                                  double* __restrict__ out) {
+                                                                  double* __restrict__ out, SegDev G) {
     __shared__ double s[FIN_WARPS][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t c = (int64_t)blockIdx.x * 32 + lane;
+    const int64_t o = (int64_t)blockIdx.x * 32 + lane;
+    const int64_t seg = o / ld, c = o - seg * ld;
+    const bool in = o < (int64_t)G.nseg * ld;
+    const int p0 = G.part_start && in ? G.part_start[seg] : 0;
+    const int np = G.part_start && in ? G.part_start[seg + 1] - p0 : nparts;
     double a0 = 0.0, a1 = 0.0;
-    if (c < ld) {
+    if (in) {
         int i = w;
-        for (; i + FIN_WARPS < nparts; i += 2 * FIN_WARPS) {
-            a0 += part[(int64_t)i * ld + c];
-            a1 += part[(int64_t)(i + FIN_WARPS) * ld + c];
+        for (; i + FIN_WARPS < np; i += 2 * FIN_WARPS) {
+            a0 += part[(int64_t)(p0 + i) * ld + c];
+            a1 += part[(int64_t)(p0 + i + FIN_WARPS) * ld + c];
         }
-        if (i < nparts) a0 += part[(int64_t)i * ld + c];
+        if (i < np) a0 += part[(int64_t)(p0 + i) * ld + c];
     }
     s[w][lane] = a0 + a1;
     __syncthreads();
-    if (w == 0 && c < ld) {
+    if (w == 0 && in) {
         double t = 0.0;
         for (int j = 0; j < FIN_WARPS; j++) t += s[j][lane];
-        out[c] = t;
+        out[o] = t;
     }
 }
-static void colred_final(Context& C, int64_t ld, int nparts, const double* part, double* out) {
-    k_colred_final<<<(unsigned)ceil_div<int64_t>(ld, 32), FIN_WARPS * 32, 0, C.stream>>>(ld, nparts, part, out);
+static void colred_final(Context& C, int64_t ld, int nparts, const double* part, double* out,
+                         const SegDev& G = SegDev()) {
+    k_colred_final<<<(unsigned)ceil_div<int64_t>((int64_t)G.nseg * ld, 32), FIN_WARPS * 32, 0, C.stream>>>(
+        ld, nparts, part, out, G);
 }
 
 struct Reducer {
@@ -149,42 +187,87 @@ struct Reducer {
     int nparts;
     int64_t rows_per_blk;
     double* part;
-    void init(Context& c, int64_t n_, int64_t ld_, const char* tag = "pcg_red_part") {
+    SegDev G;  // segment tables (the block tables are filled in by init when there are several segments)
+    // row0: nseg + 1 segment row starts on the host (empty: one segment); G's rowseg/kseg/segrows are the
+    // caller's
+    void init(Context& c, int64_t n_, int64_t ld_, const char* tag = "pcg_red_part", const SegDev& segs = SegDev(),
+              const std::vector<int64_t>* row0 = nullptr) {
         C = &c;
         n = n_;
         ld = ld_;
+        G = segs;
         const int64_t ntiles = ld / TILE;
         int64_t target = std::max<int64_t>(8, std::min<int64_t>(1184 / std::max<int64_t>(1, ntiles) + 1, 1024));
         rows_per_blk = std::max<int64_t>(RED_THREADS / TILE, ceil_div<int64_t>(n, target));
-        nparts = (int)ceil_div<int64_t>(n, rows_per_blk);
+        if (G.nseg <= 1 || !row0) {
+            nparts = (int)ceil_div<int64_t>(n, rows_per_blk);
+        } else {
+            // blocks of at most rows_per_blk rows inside each segment
+            std::vector<int64_t> brow;
+            std::vector<int32_t> bseg, pstart;
+            for (int32_t sg = 0; sg < G.nseg; sg++) {
+                pstart.push_back((int32_t)bseg.size());
+                for (int64_t r = (*row0)[sg]; r < (*row0)[sg + 1]; r += rows_per_blk) {
+                    brow.push_back(r);
+                    bseg.push_back(sg);
+                }
+            }
+            pstart.push_back((int32_t)bseg.size());
+            brow.push_back(n);
+            nparts = (int)bseg.size();
+            int64_t* d_brow = c.ws.get_t<int64_t>(std::string(tag) + "_brow", brow.size());
+            int32_t* d_bseg = c.ws.get_t<int32_t>(std::string(tag) + "_bseg", bseg.size() + 1);
+            int32_t* d_pst = c.ws.get_t<int32_t>(std::string(tag) + "_pstart", pstart.size());
+            SSP_CUDA(cudaMemcpyAsync(d_brow, brow.data(), sizeof(int64_t) * brow.size(), cudaMemcpyHostToDevice,
+                                     c.stream));
+            SSP_CUDA(cudaMemcpyAsync(d_bseg, bseg.data(), sizeof(int32_t) * bseg.size(), cudaMemcpyHostToDevice,
+                                     c.stream));
+            SSP_CUDA(cudaMemcpyAsync(d_pst, pstart.data(), sizeof(int32_t) * pstart.size(), cudaMemcpyHostToDevice,
+                                     c.stream));
+            SSP_CUDA(cudaStreamSynchronize(c.stream));
+            G.blk_row = d_brow;
+            G.blk_seg = d_bseg;
+            G.part_start = d_pst;
+        }
         part = c.ws.get_t<double>(tag, (size_t)nparts * ld);
     }
     template <int OP, class T>
     void run(const T* a, const T* b, double* out, const double* mean = nullptr) {
         dim3 grid((unsigned)nparts, (unsigned)(ld / TILE));
-        k_colred_partial<OP, T><<<grid, RED_THREADS, 0, C->stream>>>(n, a, b, mean, rows_per_blk, ld, part);
-        colred_final(*C, ld, nparts, part, out);
+        k_colred_partial<OP, T><<<grid, RED_THREADS, 0, C->stream>>>(n, a, b, mean, rows_per_blk, ld, part, G);
+        colred_final(*C, ld, nparts, part, out, G);
         SSP_CHECK_LAUNCH();
         C->kernels_launched += 2;
     }
     void finish(double* out) {
-        colred_final(*C, ld, nparts, part, out);
+        colred_final(*C, ld, nparts, part, out, G);
         SSP_CHECK_LAUNCH();
         C->kernels_launched++;
     }
 };
 
 // ---------------------------------------------------------------- elementwise (grid.y = tile)
-__global__ void k_center(int64_t n, int32_t k, const double* __restrict__ Y, const double* __restrict__ colsum,
-                         double* __restrict__ r, double* __restrict__ x, double* __restrict__ mean) {
+// r = Y - mean(Y) over each segment's rows for its columns (0 elsewhere), x = 0, mean per (segment, column)
+__global__ void k_center(int64_t n, int32_t k, int64_t ld, const double* __restrict__ Y,
+                         const double* __restrict__ colsum, double* __restrict__ r, double* __restrict__ x,
+                         double* __restrict__ mean, SegDev G) {
     const int64_t t = blockIdx.y;
     const int64_t cnt = n * TILE;
+    if (blockIdx.x == 0 && threadIdx.x < TILE)
+        for (int32_t sg = 0; sg < G.nseg; sg++) {
+            const int64_t c = t * TILE + threadIdx.x;
+            const int32_t kk = G.kseg ? G.kseg[sg] : k;
+            const int64_t nr = G.segrows ? G.segrows[sg] : n;
+            mean[sg * ld + c] = c < kk ? colsum[sg * ld + c] / (double)nr : 0.0;
+        }
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t c = t * TILE + (i % TILE);
         const int64_t o = t * cnt + i;
-        const double mu = c < k ? colsum[c] / (double)n : 0.0;
-        if (i < TILE && blockIdx.x == 0) mean[c] = mu;
-        r[o] = c < k ? Y[o] - mu : 0.0;
+        const int64_t sg = seg_of_row(G, i / TILE);
+        const int32_t kk = G.kseg ? G.kseg[sg] : k;
+        const int64_t nr = G.segrows ? G.segrows[sg] : n;
+        const double mu = c < kk ? colsum[sg * ld + c] / (double)nr : 0.0;
+        r[o] = c < kk ? Y[o] - mu : 0.0;
         x[o] = 0.0;
     }
 }
@@ -195,12 +278,14 @@ __global__ void k_center(int64_t n, int32_t k, const double* __restrict__ Y, con
 template <class T>
 __global__ void __launch_bounds__(RED_THREADS) k_axpy_r_rr(int64_t n, const double* __restrict__ alpha,
                                                            const T* __restrict__ q, T* __restrict__ r,
-                                                           int64_t rows_per_blk, int64_t ld, double* __restrict__ part) {
+                                                           int64_t rows_per_blk, int64_t ld, double* __restrict__ part,
+                                                           SegDev G) {
     __shared__ double s[RED_THREADS];
     const int64_t t = blockIdx.y;
     const int c = threadIdx.x % TILE, rl = threadIdx.x / TILE;
-    const int64_t r0 = (int64_t)blockIdx.x * rows_per_blk, r1 = min(n, r0 + rows_per_blk);
-    const double a64 = alpha[t * TILE + c];
+    int64_t r0, r1, sb;
+    red_block(G, n, rows_per_blk, ld, r0, r1, sb);
+    const double a64 = alpha[sb + t * TILE + c];
     const T a = (T)a64;
     const int64_t base = t * n * TILE;
     double acc = 0.0;
@@ -224,13 +309,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_axpy_r_rr(int64_t n, const doub
 
 // x += alpha p (the previous step's alpha and p), then p = z + beta p
 template <class T>
-__global__ void k_update_xp(int64_t n, const double* __restrict__ alpha, const double* __restrict__ beta,
-                            const T* __restrict__ z, T* __restrict__ p, T* __restrict__ x) {
+__global__ void k_update_xp(int64_t n, int64_t ld, const double* __restrict__ alpha, const double* __restrict__ beta,
+                            const T* __restrict__ z, T* __restrict__ p, T* __restrict__ x, SegDev G) {
     const int64_t t = blockIdx.y;
     const int64_t cnt = n * TILE;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t o = t * cnt + i;
-        const int64_t c = t * TILE + (i % TILE);
+        const int64_t c = seg_of_row(G, i / TILE) * ld + t * TILE + (i % TILE);
         const double a64 = alpha[c];
         const T pv = p[o];
         if (a64 != 0.0) x[o] += (T)a64 * pv;
@@ -240,12 +325,13 @@ __global__ void k_update_xp(int64_t n, const double* __restrict__ alpha, const d
 
 // the last step's x += alpha p
 template <class T>
-__global__ void k_axpy_x(int64_t n, const double* __restrict__ alpha, const T* __restrict__ p, T* __restrict__ x) {
+__global__ void k_axpy_x(int64_t n, int64_t ld, const double* __restrict__ alpha, const T* __restrict__ p,
+                         T* __restrict__ x, SegDev G) {
     const int64_t t = blockIdx.y;
     const int64_t cnt = n * TILE;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t o = t * cnt + i;
-        const double a64 = alpha[t * TILE + (i % TILE)];
+        const double a64 = alpha[seg_of_row(G, i / TILE) * ld + t * TILE + (i % TILE)];
         if (a64 != 0.0) x[o] += (T)a64 * p[o];
     }
 }
@@ -259,12 +345,13 @@ __global__ void k_d2f(int64_t count, const double* __restrict__ src, float* __re
 // inner right-hand side: the FP64 residual of the columns still active, rounded to T; zero elsewhere
 // (runs in place when T is double)
 template <class T>
-__global__ void k_rhs_masked(int64_t n, const double* r64, const int32_t* __restrict__ active, T* rin) {
+__global__ void k_rhs_masked(int64_t n, int64_t ld, const double* r64, const int32_t* __restrict__ active, T* rin,
+                             SegDev G) {
     const int64_t t = blockIdx.y;
     const int64_t cnt = n * TILE;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t o = t * cnt + i;
-        rin[o] = active[t * TILE + (i % TILE)] ? (T)r64[o] : (T)0;
+        rin[o] = active[seg_of_row(G, i / TILE) * ld + t * TILE + (i % TILE)] ? (T)r64[o] : (T)0;
     }
 }
 
@@ -278,13 +365,16 @@ __global__ void k_add_into(int64_t count, const T* __restrict__ e, double* __res
 __global__ void __launch_bounds__(RED_THREADS) k_true_resid(int64_t n, int32_t k, const double* __restrict__ Y,
                                                             const double* __restrict__ mean,
                                                             const double* __restrict__ q, double* __restrict__ r,
-                                                            int64_t rows_per_blk, int64_t ld, double* __restrict__ part) {
+                                                            int64_t rows_per_blk, int64_t ld, double* __restrict__ part,
+                                                            SegDev G) {
     __shared__ double s[RED_THREADS];
     const int64_t t = blockIdx.y;
     const int c = threadIdx.x % TILE, rl = threadIdx.x / TILE;
-    const int64_t r0 = (int64_t)blockIdx.x * rows_per_blk, r1 = min(n, r0 + rows_per_blk);
+    int64_t r0, r1, sb;
+    red_block(G, n, rows_per_blk, ld, r0, r1, sb);
     const int64_t col = t * TILE + c;
-    const double mu = mean[col];
+    if (G.kseg) k = G.kseg[sb / ld];
+    const double mu = mean[sb + col];
     const int64_t base = t * n * TILE;
     double acc = 0.0;
     for (int64_t row = r0 + rl; row < r1; row += RED_THREADS / TILE) {
@@ -324,14 +414,17 @@ static ColState make_colstate(Context& C, int64_t ld, const std::string& tag) {
     return ColState{v, v + ld, v + 2 * ld, v + 3 * ld, v + 4 * ld, v + 5 * ld, v + 6 * ld, v + 7 * ld, iv, iv + ld, na};
 }
 
-__global__ void k_cols_init(int64_t ld, int32_t k, double tol, double abs_tol, ColState S) {
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x) {
+// state entries c = segment * ld + column; a column past its segment's k_s is inactive
+__global__ void k_cols_init(int64_t ld, int32_t k, double tol, double abs_tol, ColState S, SegDev G) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < (int64_t)G.nseg * ld;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t kk = G.kseg ? G.kseg[c / ld] : k;
         double bn = sqrt(S.bnorm2[c]);
         double thr = tol * bn;
         if (abs_tol > thr) thr = abs_tol;
         S.thr[c] = thr;
         S.rr[c] = S.bnorm2[c];
-        int act = (c < k) && (bn > thr);
+        int act = (c % ld < kk) && (bn > thr);
         S.active[c] = act;
         S.iters[c] = 0;
         S.alpha[c] = 0.0;
@@ -343,15 +436,17 @@ __global__ void k_cols_init(int64_t ld, int32_t k, double tol, double abs_tol, C
 // inner solve of a refinement round: stop at a relative reduction `reduction` of its right-hand side, or
 // once below half the outer threshold of the column (no point solving past what the outer test needs)
 __global__ void k_cols_init_inner(int64_t ld, int32_t k, double reduction, const double* __restrict__ thr_out,
-                                  ColState S) {
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x) {
+                                  ColState S, SegDev G) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < (int64_t)G.nseg * ld;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t kk = G.kseg ? G.kseg[c / ld] : k;
         const double bn = sqrt(S.bnorm2[c]);
         double thr = reduction * bn;
         const double half_out = 0.5 * thr_out[c];
         if (half_out > thr) thr = half_out;
         S.thr[c] = thr;
         S.rr[c] = S.bnorm2[c];
-        const int act = (c < k) && (bn > thr);
+        const int act = (c % ld < kk) && (bn > thr);
         S.active[c] = act;
         S.iters[c] = 0;
         S.alpha[c] = 0.0;
@@ -360,13 +455,13 @@ __global__ void k_cols_init_inner(int64_t ld, int32_t k, double reduction, const
     }
 }
 
-__global__ void k_cols_alpha(int64_t ld, ColState S) {
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x)
+__global__ void k_cols_alpha(int64_t cnt, ColState S) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < cnt; c += (int64_t)gridDim.x * blockDim.x)
         S.alpha[c] = S.active[c] ? S.rz[c] / S.pq[c] : 0.0;
 }
 
-__global__ void k_cols_check(int64_t ld, int32_t it, ColState S) {
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x) {
+__global__ void k_cols_check(int64_t cnt, int32_t it, ColState S) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < cnt; c += (int64_t)gridDim.x * blockDim.x) {
         if (!S.active[c]) continue;
         S.iters[c] = it;
         if (sqrt(S.rr[c]) <= S.thr[c]) S.active[c] = 0;
@@ -374,8 +469,8 @@ __global__ void k_cols_check(int64_t ld, int32_t it, ColState S) {
     }
 }
 
-__global__ void k_cols_beta(int64_t ld, ColState S) {
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x) {
+__global__ void k_cols_beta(int64_t cnt, ColState S) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < cnt; c += (int64_t)gridDim.x * blockDim.x) {
         double b = 0.0;
         if (S.active[c]) b = S.rz_new[c] / S.rz[c];
         S.beta[c] = b;
@@ -385,9 +480,9 @@ __global__ void k_cols_beta(int64_t ld, ColState S) {
 
 // outer test of a refinement round on the true residual: adds the round's inner iterations to the
 // column's count, deactivates converged columns, and records the largest residual ratio new/old
-__global__ void k_cols_outer(int64_t ld, const int32_t* __restrict__ inner_iters, const double* __restrict__ rr_new,
+__global__ void k_cols_outer(int64_t cnt, const int32_t* __restrict__ inner_iters, const double* __restrict__ rr_new,
                              ColState S, double* __restrict__ worst_ratio) {
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < cnt; c += (int64_t)gridDim.x * blockDim.x) {
         if (!S.active[c]) continue;
         S.iters[c] += inner_iters[c];
         const double before = S.rr[c], after = rr_new[c];
@@ -411,9 +506,9 @@ __global__ void k_cols_outer(int64_t ld, const int32_t* __restrict__ inner_iters
 __global__ void k_it_set(int32_t* it, int32_t v) { *it = v; }
 __global__ void k_it_next(int32_t* it) { *it += 1; }
 
-__global__ void k_cols_check_at(int64_t ld, const int32_t* __restrict__ it, ColState S) {
+__global__ void k_cols_check_at(int64_t cnt, const int32_t* __restrict__ it, ColState S) {
     const int32_t i = *it;
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ld; c += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < cnt; c += (int64_t)gridDim.x * blockDim.x) {
         if (!S.active[c]) continue;
         S.iters[c] = i;
         if (sqrt(S.rr[c]) <= S.thr[c]) S.active[c] = 0;
@@ -1254,7 +1349,14 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
     const dim3 egrid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div<int64_t>(n * TILE, 256),
                                                                       2048 / std::max<int64_t>(1, ntiles) + 4)),
                      (unsigned)ntiles);
-    const int cg = grid_for(ld, 256);
+    const SegDev& G = R.G;
+    const int64_t ns = (int64_t)G.nseg * ld;  // per-(graph, column) state entries
+    const int cg = grid_for(ns, 256);
+    // with several graphs the SpMM's blocks straddle graphs, so p.q is a segmented reduction of its own
+    auto pq_dot = [&]() {
+        if (G.nseg > 1) R.run<OP_DOT, T>(B.p, B.q, S.pq);
+        else colred_final(C, ld, (int)A.grid.x, A.part, S.pq);
+    };
     int64_t active = read_i64(C, S.nactive);
     int32_t it = 0;
     if (active == 0) return 0;
@@ -1267,28 +1369,28 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
     tm.loop.begin(C.stream);
     while (it < max_iters) {
         tm.spmm.begin(C.stream);
-        launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, true, k);
+        launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, G.nseg == 1, k);
         tm.spmm.end(C.stream);
-        colred_final(C, ld, (int)A.grid.x, A.part, S.pq);
-        k_cols_alpha<<<cg, 256, 0, C.stream>>>(ld, S);
+        pq_dot();
+        k_cols_alpha<<<cg, 256, 0, C.stream>>>(ns, S);
         k_axpy_r_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
-            n, S.alpha, B.q, B.r, R.rows_per_blk, ld, R.part);
+            n, S.alpha, B.q, B.r, R.rows_per_blk, ld, R.part, G);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += 3 + A.nslabs;
         R.finish(S.rr);
         it++;
         SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
-        k_cols_check<<<cg, 256, 0, C.stream>>>(ld, it, S);
+        k_cols_check<<<cg, 256, 0, C.stream>>>(ns, it, S);
         SSP_CHECK_LAUNCH();
         C.kernels_launched++;
         active = read_i64(C, S.nactive);
         if (opt.history) {
-            std::vector<double> hrr(k), hbb(k);
-            SSP_CUDA(cudaMemcpyAsync(hrr.data(), S.rr, sizeof(double) * k, cudaMemcpyDeviceToHost, C.stream));
-            SSP_CUDA(cudaMemcpyAsync(hbb.data(), S.bnorm2, sizeof(double) * k, cudaMemcpyDeviceToHost, C.stream));
+            std::vector<double> hrr(ns), hbb(ns);
+            SSP_CUDA(cudaMemcpyAsync(hrr.data(), S.rr, sizeof(double) * ns, cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(hbb.data(), S.bnorm2, sizeof(double) * ns, cudaMemcpyDeviceToHost, C.stream));
             SSP_CUDA(cudaStreamSynchronize(C.stream));
             double mx = 0.0;
-            for (int32_t j = 0; j < k; j++)
+            for (int64_t j = 0; j < ns; j++)
                 if (hbb[j] > 0) mx = std::max(mx, std::sqrt(hrr[j] / hbb[j]));
             opt.history->push_back(mx);
         }
@@ -1302,8 +1404,8 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         tm.pc.end(C.stream);
         C.kernels_launched += pc_launches;
         R.run<OP_DOT, T>(B.r, B.z, S.rz_new);
-        k_cols_beta<<<cg, 256, 0, C.stream>>>(ld, S);
-        k_update_xp<T><<<egrid, 256, 0, C.stream>>>(n, S.alpha, S.beta, B.z, B.p, B.e);
+        k_cols_beta<<<cg, 256, 0, C.stream>>>(ns, S);
+        k_update_xp<T><<<egrid, 256, 0, C.stream>>>(n, ld, S.alpha, S.beta, B.z, B.p, B.e, G);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += 2;
     }
@@ -1347,21 +1449,22 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         capture(cp.conditional.phGraph_out[0], [&] {
             body_kernels += launch_precond<T>(C, F, V, n, B.r, B.z, ld, k);
             R.run<OP_DOT, T>(B.r, B.z, S.rz_new);
-            k_cols_beta<<<cg, 256, 0, C.stream>>>(ld, S);
-            k_update_xp<T><<<egrid, 256, 0, C.stream>>>(n, S.alpha, S.beta, B.z, B.p, B.e);
-            launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, true, k);
-            colred_final(C, ld, (int)A.grid.x, A.part, S.pq);
-            k_cols_alpha<<<cg, 256, 0, C.stream>>>(ld, S);
+            k_cols_beta<<<cg, 256, 0, C.stream>>>(ns, S);
+            k_update_xp<T><<<egrid, 256, 0, C.stream>>>(n, ld, S.alpha, S.beta, B.z, B.p, B.e, G);
+            launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, G.nseg == 1, k);
+            pq_dot();
+            k_cols_alpha<<<cg, 256, 0, C.stream>>>(ns, S);
             k_axpy_r_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
-                n, S.alpha, B.q, B.r, R.rows_per_blk, ld, R.part);
+                n, S.alpha, B.q, B.r, R.rows_per_blk, ld, R.part, G);
             R.finish(S.rr);
             k_it_next<<<1, 1, 0, C.stream>>>(d_it);
             SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
-            k_cols_check_at<<<cg, 256, 0, C.stream>>>(ld, d_it, S);
+            k_cols_check_at<<<cg, 256, 0, C.stream>>>(ns, d_it, S);
             k_loop_ctl<<<1, 1, 0, C.stream>>>(h, S.nactive, d_it, max_iters);
             SSP_CHECK_LAUNCH();
         });
-        body_kernels += (C.kernels_launched - k_before) + 9 + A.nslabs;  // the helpers count theirs
+        // the helpers count theirs; with several graphs p.q is a reduction (counted) instead of a final pass
+        body_kernels += (C.kernels_launched - k_before) + 9 + A.nslabs - (G.nseg > 1 ? 1 : 0);
         C.kernels_launched = k_before;
         SSP_CUDA(cudaGraphInstantiate(&L.exec, L.graph, 0));
         SSP_CUDA(cudaGraphLaunch(L.exec, C.stream));
@@ -1372,7 +1475,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         it = it_end;
     }
     // the last step's x += alpha p (alpha is 0 for columns that stopped earlier)
-    k_axpy_x<T><<<egrid, 256, 0, C.stream>>>(n, S.alpha, B.p, B.e);
+    k_axpy_x<T><<<egrid, 256, 0, C.stream>>>(n, ld, S.alpha, B.p, B.e, G);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
     tm.loop.end(C.stream);
@@ -1398,13 +1501,37 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
     double* z = W.get_t<double>("pcg_z", total);
     double* p = W.get_t<double>("pcg_p", total);
     double* q = W.get_t<double>("pcg_q", total);
-    ColState S = make_colstate(C, ld, "pcg");
-    double* colv = W.get_t<double>("pcg_aux", 3 * ld);
+    // graphs solved at once (one segment: a single graph)
+    SegDev G;
+    PcgSegments* segs = opt.segs;
+    if (segs) {
+        const int32_t nseg = (int32_t)segs->k.size();
+        SSP_REQUIRE(nseg >= 1 && (int64_t)segs->row0.size() == nseg + 1 && segs->row0.front() == 0 &&
+                        segs->row0.back() == n && segs->rowseg,
+                    SSP_ERR_INVALID, "pcg: inconsistent graph segments");
+        std::vector<int64_t> rows(nseg);
+        for (int32_t i = 0; i < nseg; i++) {
+            SSP_REQUIRE(segs->k[i] >= 1 && segs->k[i] <= k && segs->row0[i + 1] > segs->row0[i], SSP_ERR_INVALID,
+                        "pcg: a graph segment needs rows and 1..k columns");
+            rows[i] = segs->row0[i + 1] - segs->row0[i];
+        }
+        int32_t* d_k = W.get_t<int32_t>("pcg_seg_k", nseg);
+        int64_t* d_rows = W.get_t<int64_t>("pcg_seg_rows", nseg);
+        SSP_CUDA(cudaMemcpyAsync(d_k, segs->k.data(), sizeof(int32_t) * nseg, cudaMemcpyHostToDevice, C.stream));
+        SSP_CUDA(cudaMemcpyAsync(d_rows, rows.data(), sizeof(int64_t) * nseg, cudaMemcpyHostToDevice, C.stream));
+        G.nseg = nseg;
+        G.rowseg = segs->rowseg;
+        G.kseg = d_k;
+        G.segrows = d_rows;
+    }
+    const int64_t ns = (int64_t)G.nseg * ld;  // per-(graph, column) state entries
+    ColState S = make_colstate(C, ns, "pcg");
+    double* colv = W.get_t<double>("pcg_aux", 3 * ns);
     double* colsum = colv;
-    double* relres = colv + ld;
-    double* mean = colv + 2 * ld;
+    double* relres = colv + ns;
+    double* mean = colv + 2 * ns;
     Reducer R;
-    R.init(C, n, ld);
+    R.init(C, n, ld, "pcg_red_part", G, segs ? &segs->row0 : nullptr);
     // SpMM: row-aligned chunks of the Laplacian (column slabs on large random graphs), about one wave of
     // blocks per tile
     const SpmmPlan A = make_spmm_plan(C, n, lap_ptr, lap_idx, lap_val, ld);
@@ -1412,16 +1539,16 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
     const dim3 egrid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div<int64_t>(n * TILE, 256),
                                                                       2048 / std::max<int64_t>(1, ntiles) + 4)),
                      (unsigned)ntiles);
-    const int cg = grid_for(ld, 256);
+    const int cg = grid_for(ns, 256);
 
     // r = Y - mean(Y); x = 0; ||b||^2
     R.run<OP_SUM, double>(Y, nullptr, colsum);
-    k_center<<<egrid, 256, 0, C.stream>>>(n, k, Y, colsum, r, x, mean);
+    k_center<<<egrid, 256, 0, C.stream>>>(n, k, ld, Y, colsum, r, x, mean, R.G);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
     R.run<OP_SQ, double>(r, nullptr, S.bnorm2);
     SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
-    k_cols_init<<<cg, 256, 0, C.stream>>>(ld, k, opt.tol, opt.abs_tol, S);
+    k_cols_init<<<cg, 256, 0, C.stream>>>(ld, k, opt.tol, opt.abs_tol, S, R.G);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;
 
@@ -1463,7 +1590,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         float* z32 = W.get_t<float>("pcgm_z", total);
         float* p32 = W.get_t<float>("pcgm_p", total);
         float* q32 = W.get_t<float>("pcgm_q", total);
-        ColState Si = make_colstate(C, ld, "pcgm_in");
+        ColState Si = make_colstate(C, ns, "pcgm_in");
         double* worst = W.get_t<double>("pcgm_worst", 1);
         double* e64 = nullptr;  // FP64 inner increment, only if a round falls back
         Precond P32, P64;
@@ -1476,10 +1603,10 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
             bool hit_cap = false;
             SSP_CUDA(cudaMemsetAsync(Si.nactive, 0, sizeof(int64_t), C.stream));
             if (!use64) {
-                k_rhs_masked<float><<<egrid, 256, 0, C.stream>>>(n, r, S.active, r32);
+                k_rhs_masked<float><<<egrid, 256, 0, C.stream>>>(n, ld, r, S.active, r32, R.G);
                 SSP_CUDA(cudaMemsetAsync(e32, 0, sizeof(float) * total, C.stream));
                 R.run<OP_SQ, float>(r32, nullptr, Si.bnorm2);
-                k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, MIXED_INNER_REDUCTION, S.thr, Si);
+                k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, MIXED_INNER_REDUCTION, S.thr, Si, R.G);
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
                 if (!P32.exec) build_precond_graph<float>(C, F, V32, n, r32, z32, ld, k, P32, pc32);
@@ -1497,10 +1624,10 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 if (!e64) e64 = W.get_t<double>("pcgm_e64", total);
                 // the FP64 inner solve runs in place on the residual of the active columns and goes straight
                 // to (half) the outer threshold
-                k_rhs_masked<double><<<egrid, 256, 0, C.stream>>>(n, r, S.active, r);
+                k_rhs_masked<double><<<egrid, 256, 0, C.stream>>>(n, ld, r, S.active, r, R.G);
                 SSP_CUDA(cudaMemsetAsync(e64, 0, sizeof(double) * total, C.stream));
                 R.run<OP_SQ, double>(r, nullptr, Si.bnorm2);
-                k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, 0.0, S.thr, Si);
+                k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, 0.0, S.thr, Si, R.G);
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
                 if (!P64.exec) build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P64, pc64);
@@ -1518,13 +1645,13 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
             launch_spmm<double>(C, n, A, A.val, x, q, ld, false, k);
             ev_resid.end(C.stream);
             k_true_resid<<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
-                n, k, Y, mean, q, r, R.rows_per_blk, ld, R.part);
+                n, k, Y, mean, q, r, R.rows_per_blk, ld, R.part, R.G);
             SSP_CHECK_LAUNCH();
             C.kernels_launched += 1 + A.nslabs;
             R.finish(relres);
             SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
             SSP_CUDA(cudaMemsetAsync(worst, 0, sizeof(double), C.stream));
-            k_cols_outer<<<cg, 256, 0, C.stream>>>(ld, Si.iters, relres, S, worst);
+            k_cols_outer<<<cg, 256, 0, C.stream>>>(ns, Si.iters, relres, S, worst);
             SSP_CHECK_LAUNCH();
             C.kernels_launched++;
             active = read_i64(C, S.nactive);
@@ -1552,23 +1679,37 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         C.kernels_launched += A.nslabs;
     }
     R.run<OP_SQDIFF_CENTERED, double>(Y, q, relres, mean);
-    std::vector<double> hb(ld), hr(ld);
-    std::vector<int32_t> hi(ld);
-    SSP_CUDA(cudaMemcpyAsync(hb.data(), S.bnorm2, sizeof(double) * ld, cudaMemcpyDeviceToHost, C.stream));
-    SSP_CUDA(cudaMemcpyAsync(hr.data(), relres, sizeof(double) * ld, cudaMemcpyDeviceToHost, C.stream));
-    SSP_CUDA(cudaMemcpyAsync(hi.data(), S.iters, sizeof(int32_t) * ld, cudaMemcpyDeviceToHost, C.stream));
+    std::vector<double> hb(ns), hr(ns);
+    std::vector<int32_t> hi(ns);
+    SSP_CUDA(cudaMemcpyAsync(hb.data(), S.bnorm2, sizeof(double) * ns, cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaMemcpyAsync(hr.data(), relres, sizeof(double) * ns, cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaMemcpyAsync(hi.data(), S.iters, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, C.stream));
     SSP_CUDA(cudaStreamSynchronize(C.stream));
     double sum_it = 0;
-    for (int32_t j = 0; j < k; j++) {
-        double rel = hb[j] > 0 ? sqrt(hr[j]) / sqrt(hb[j]) : 0.0;
-        if (h_relres) h_relres[j] = rel;
-        if (h_iters) h_iters[j] = hi[j];
-        rep.max_iters_used = std::max(rep.max_iters_used, hi[j]);
-        sum_it += hi[j];
-        rep.max_relres = std::max(rep.max_relres, rel);
-        if (!(rel < 0.01)) rep.not_converged++;
+    int64_t cols = 0;
+    if (segs) {
+        segs->iters.assign(ns, 0);
+        segs->relres.assign(ns, 0.0);
     }
-    rep.mean_iters = sum_it / k;
+    for (int32_t sg = 0; sg < G.nseg; sg++) {
+        const int32_t kk = segs ? segs->k[sg] : k;
+        for (int32_t j = 0; j < kk; j++) {
+            const int64_t o = (int64_t)sg * ld + j;
+            double rel = hb[o] > 0 ? sqrt(hr[o]) / sqrt(hb[o]) : 0.0;
+            if (h_relres && !segs) h_relres[j] = rel;
+            if (h_iters && !segs) h_iters[j] = hi[o];
+            if (segs) {
+                segs->iters[o] = hi[o];
+                segs->relres[o] = rel;
+            }
+            rep.max_iters_used = std::max(rep.max_iters_used, hi[o]);
+            sum_it += hi[o];
+            cols++;
+            rep.max_relres = std::max(rep.max_relres, rel);
+            if (!(rel < 0.01)) rep.not_converged++;
+        }
+    }
+    rep.mean_iters = sum_it / std::max<int64_t>(1, cols);
     rep.ms_spmm = tm.spmm.total_ms();
     rep.n_spmm = (int64_t)tm.spmm.used;
     rep.ms_precond = tm.pc.total_ms();

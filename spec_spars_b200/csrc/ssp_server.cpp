@@ -3,11 +3,20 @@
 // The reference runs one graph per process (sparsify_dataset, lib.rs:158-168; InputStream::run_stream,
 // stream.rs:40-64).  Here requests of uneven size arrive from any host thread (ssp_submit) and are served by
 // `slots` worker threads, each owning one ssp_context (its own stream and grow-only workspace), so the
-// admitted requests run concurrently on the device.  Admission is first come, first served: the oldest
-// pending request is admitted as soon as a slot is free and its estimated device footprint fits beside the
-// footprints of the requests in flight (the HBM budget); a request whose footprint alone exceeds the budget
-// is refused at submit.  Each request runs the same ssp_sparsify as a lone call, so its result does not
-// depend on what else is in flight.
+// admitted requests run concurrently on the device.
+// Admission: a free slot takes the oldest pending request whose estimated device footprint fits beside the
+// footprints in flight (the HBM budget).  A younger request may go ahead of an older one that does not fit
+// yet, until the older one has waited FRONT_AGE_MS; from then on admission is strictly first come, first
+// served, so a large request is not starved.  A request whose footprint alone exceeds the budget is refused
+// at submit.
+// Batching (continuous): the slot then adds the other pending requests that can share its run -- the same
+// factor seed, precision, PCG options and reweighting, the same epsilon, and complete elimination
+// (dense_threshold = 0, factor_max_degree = 0) -- up to max_batch requests and the slot's share of the
+// budget, and runs them as one ssp_sparsify_batch: one factorization and one PCG over their disjoint union.
+// Requests that arrive while batches run are picked up by the next free slot, so their work overlaps on the
+// device.  A request that cannot be batched runs the same ssp_sparsify as a lone call; a batched one equals
+// its lone result to the solve's rounding (ssp_sparsify_batch).  If a batch fails as a whole, its requests are
+// run one by one.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -42,6 +51,8 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
+constexpr double FRONT_AGE_MS = 500.0;  // after this wait the oldest request is admitted strictly first
+
 struct Job {
     uint64_t ticket = 0;
     int64_t n = 0;
@@ -59,6 +70,7 @@ struct Job {
     ssp_csc_out out;
     ssp_stats stats;
     int32_t slot = -1;
+    int32_t batch = 0;  // requests in the run that served this one
     // inline check (a15)
     bool checked = false;
     ssp_probe_result probe{};
@@ -91,6 +103,28 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
+bool batchable(const ssp_params& p) { return p.dense_threshold == 0 && p.factor_max_degree == 0; }
+
+bool same_batch(const ssp_params& a, const ssp_params& b) {
+    return a.epsilon == b.epsilon && a.factor_seed == b.factor_seed && a.precision == b.precision &&
+           a.pcg_tol == b.pcg_tol && a.pcg_abs_tol == b.pcg_abs_tol && a.pcg_max_iters == b.pcg_max_iters &&
+           a.reweight == b.reweight && batchable(a) && batchable(b);
+}
+
+// device footprint of a batch: its union's n x ld blocks use the largest k of the batch for every row
+int64_t batch_footprint(const std::vector<Job*>& js) {
+    if (js.size() == 1) return js[0]->est_bytes;
+    int64_t ld = 0, n = 0, nnz = 0;
+    for (const Job* j : js) {
+        const int64_t k = ssp_params_jl_dim(&j->params, j->n);
+        ld = std::max<int64_t>(ld, (k + 31) / 32 * 32);
+        n += j->n;
+        nnz += (int64_t)j->values.size();
+    }
+    const double blocks = js[0]->params.precision == SSP_PRECISION_MIXED ? 6.0 + 2.5 + 1.0 : 6.0;
+    return (int64_t)(blocks * 8.0 * (double)n * (double)ld) + 200 * nnz + 96 * n + (16ll << 20);
+}
+
 }  // namespace
 
 struct ssp_server {
@@ -100,7 +134,8 @@ struct ssp_server {
     std::deque<Job*> pending;
     std::unordered_map<uint64_t, std::unique_ptr<Job>> jobs;
     uint64_t next_ticket = 1;
-    int32_t inflight = 0, peak_inflight = 0;
+    int32_t inflight = 0, peak_inflight = 0, peak_batch = 0;
+    int64_t batches = 0;
     int64_t inflight_bytes = 0, peak_inflight_bytes = 0;
     int64_t submitted = 0, completed = 0, failed = 0, rejected = 0;
     int32_t waiters = 0;  // threads inside ssp_wait; destroy lets them leave before the server goes
@@ -108,69 +143,139 @@ struct ssp_server {
     std::vector<ssp_context*> ctxs;
     std::vector<std::thread> workers;
 
+    // Under the lock: the requests a free slot runs next (empty: none can be admitted now).
+    std::vector<Job*> take() {
+        std::vector<Job*> run;
+        if (pending.empty()) return run;
+        const Clock::time_point now = Clock::now();
+        auto fits = [&](int64_t bytes) { return inflight == 0 || inflight_bytes + bytes <= opts.hbm_budget_bytes; };
+        size_t lead = pending.size();
+        if (fits(pending.front()->est_bytes)) {
+            lead = 0;
+        } else if (ms_between(pending.front()->t_submit, now) < FRONT_AGE_MS) {
+            for (size_t i = 1; i < pending.size(); i++)
+                if (fits(pending[i]->est_bytes)) {
+                    lead = i;
+                    break;
+                }
+        }
+        if (lead == pending.size()) return run;
+        run.push_back(pending[lead]);
+        if (opts.max_batch > 1 && batchable(run[0]->params)) {
+            const int64_t share = opts.hbm_budget_bytes / std::max(1, opts.slots);
+            for (size_t i = lead + 1; i < pending.size() && (int32_t)run.size() < opts.max_batch; i++) {
+                if (!same_batch(pending[i]->params, run[0]->params)) continue;
+                run.push_back(pending[i]);
+                const int64_t b = batch_footprint(run);
+                if (b > share || !fits(b)) run.pop_back();
+            }
+        }
+        for (Job* j : run) pending.erase(std::find(pending.begin(), pending.end(), j));
+        return run;
+    }
+
+    void run_alone(ssp_context* ctx, Job* j) {
+        ssp_csc g{j->n, (int64_t)j->values.size(), j->colptr.data(), j->rowidx.data(), j->values.data(), SSP_MEM_HOST};
+        j->params.output_file = j->output_file.c_str();
+        memset(&j->out, 0, sizeof(j->out));
+        memset(&j->stats, 0, sizeof(j->stats));
+        const int rc = ssp_sparsify(ctx, &g, &j->params, SSP_MEM_HOST, &j->out, &j->stats);
+        j->status = rc;
+        j->error = rc == SSP_OK ? std::string() : std::string(ssp_last_error());
+    }
+
+    void run_batch(ssp_context* ctx, const std::vector<Job*>& run) {
+        const size_t cnt = run.size();
+        std::vector<ssp_csc> gs(cnt);
+        std::vector<ssp_params> ps(cnt);
+        std::vector<ssp_csc_out> outs(cnt);
+        std::vector<ssp_stats> sts(cnt);
+        for (size_t i = 0; i < cnt; i++) {
+            Job* j = run[i];
+            j->params.output_file = j->output_file.c_str();
+            gs[i] = ssp_csc{j->n, (int64_t)j->values.size(), j->colptr.data(), j->rowidx.data(), j->values.data(),
+                            SSP_MEM_HOST};
+            ps[i] = j->params;
+        }
+        const int rc = ssp_sparsify_batch(ctx, (int32_t)cnt, gs.data(), ps.data(), outs.data(), sts.data());
+        if (rc != SSP_OK) {  // the batch as a whole failed: run its requests one by one
+            for (Job* j : run) run_alone(ctx, j);
+            return;
+        }
+        for (size_t i = 0; i < cnt; i++) {
+            run[i]->out = outs[i];
+            run[i]->stats = sts[i];
+            run[i]->status = SSP_OK;
+            run[i]->error.clear();
+        }
+    }
+
     void worker(int slot) {
         ssp_context* ctx = ctxs[slot];
         const int64_t keep_ws = opts.hbm_budget_bytes / std::max(1, opts.slots);
         std::unique_lock<std::mutex> lk(mu);
         for (;;) {
-            cv_work.wait(lk, [&] {
+            std::vector<Job*> run;
+            // a request that must wait for capacity is re-examined when anything finishes, or when it ages
+            cv_work.wait_for(lk, std::chrono::milliseconds((int64_t)FRONT_AGE_MS), [&] {
                 if (stopping) return true;
-                if (pending.empty()) return false;
-                const Job* j = pending.front();
-                return inflight == 0 || inflight_bytes + j->est_bytes <= opts.hbm_budget_bytes;
+                run = take();
+                return !run.empty();
             });
             if (stopping) return;
-            Job* j = pending.front();
-            pending.pop_front();
-            inflight++;
-            inflight_bytes += j->est_bytes;
+            if (run.empty()) continue;
+            const int64_t bytes = batch_footprint(run);
+            inflight += (int32_t)run.size();
+            inflight_bytes += bytes;
             peak_inflight = std::max(peak_inflight, inflight);
             peak_inflight_bytes = std::max(peak_inflight_bytes, inflight_bytes);
-            j->t_admit = Clock::now();
-            j->slot = slot;
+            peak_batch = std::max(peak_batch, (int32_t)run.size());
+            batches++;
+            const Clock::time_point t_admit = Clock::now();
+            for (Job* j : run) {
+                j->t_admit = t_admit;
+                j->slot = slot;
+                j->batch = (int32_t)run.size();
+            }
             lk.unlock();
 
-            ssp_csc g;
-            g.n = j->n;
-            g.nnz = (int64_t)j->values.size();
-            g.colptr = j->colptr.data();
-            g.rowidx = j->rowidx.data();
-            g.values = j->values.data();
-            g.mem = SSP_MEM_HOST;
-            j->params.output_file = j->output_file.c_str();
-            memset(&j->out, 0, sizeof(j->out));
-            memset(&j->stats, 0, sizeof(j->stats));
-            const int rc = ssp_sparsify(ctx, &g, &j->params, SSP_MEM_HOST, &j->out, &j->stats);
-            std::string err = rc == SSP_OK ? std::string() : std::string(ssp_last_error());
-            int status = rc;
-            if (rc == SSP_OK && j->check_probes > 0) {
-                const Clock::time_point t0 = Clock::now();
-                const int crc = check_result(ctx, g, j->params, j->check_probes, j->out, j);
-                j->check_ms = ms_between(t0, Clock::now());
-                if (crc == SSP_OK) {
-                    j->checked = true;
-                } else {
-                    status = crc;
-                    err = std::string("inline check: ") + ssp_last_error();
-                    ssp_csc_free(&j->out);
+            if (run.size() == 1) run_alone(ctx, run[0]);
+            else run_batch(ctx, run);
+            for (Job* j : run) {
+                if (j->status == SSP_OK && j->check_probes > 0) {
+                    ssp_csc g{j->n, (int64_t)j->values.size(), j->colptr.data(), j->rowidx.data(), j->values.data(),
+                              SSP_MEM_HOST};
+                    const Clock::time_point t0 = Clock::now();
+                    const int crc = check_result(ctx, g, j->params, j->check_probes, j->out, j);
+                    j->check_ms = ms_between(t0, Clock::now());
+                    if (crc == SSP_OK) {
+                        j->checked = true;
+                    } else {
+                        j->status = crc;
+                        j->error = std::string("inline check: ") + ssp_last_error();
+                        ssp_csc_free(&j->out);
+                    }
                 }
             }
-            // keep the slot's cached workspace within its share of the budget
+            // keep the slot's cached workspace within its share of the budget (batches are sized to that share,
+            // so this frees only after a request larger than the share ran alone)
             if (ssp_context_workspace_bytes(ctx) > keep_ws) ssp_context_release_workspace(ctx);
-            // the input copy is no longer needed
-            std::vector<int64_t>().swap(j->colptr);
-            std::vector<int32_t>().swap(j->rowidx);
-            std::vector<double>().swap(j->values);
+            for (Job* j : run) {  // the input copies are no longer needed
+                std::vector<int64_t>().swap(j->colptr);
+                std::vector<int32_t>().swap(j->rowidx);
+                std::vector<double>().swap(j->values);
+            }
 
             lk.lock();
-            j->status = status;
-            j->error = err;
-            j->t_done = Clock::now();
-            j->done = true;
-            inflight--;
-            inflight_bytes -= j->est_bytes;
-            if (status == SSP_OK) completed++;
-            else failed++;
+            const Clock::time_point t_done = Clock::now();
+            for (Job* j : run) {
+                j->t_done = t_done;
+                j->done = true;
+                if (j->status == SSP_OK) completed++;
+                else failed++;
+            }
+            inflight -= (int32_t)run.size();
+            inflight_bytes -= bytes;
             cv_done.notify_all();
             cv_work.notify_all();
         }
@@ -187,6 +292,7 @@ struct ssp_server {
         r->run_ms = ms_between(j->t_admit, j->t_done);
         r->latency_ms = ms_between(j->t_submit, j->t_done);
         r->slot = j->slot;
+        r->batch = j->batch;
         r->checked = j->checked ? 1 : 0;
         r->probe_upper_violations = j->probe.upper_bound_violations;
         r->probe_lower_violations = j->probe.lower_bound_violations;
@@ -206,6 +312,7 @@ void ssp_server_opts_default(ssp_server_opts* o) {
     o->slots = 4;
     o->hbm_budget_bytes = 0;  // 85% of the device memory free at creation
     o->max_pending = 0;       // unbounded
+    o->max_batch = 32;        // requests that may share one run (ssp_sparsify_batch)
 }
 
 int64_t ssp_request_footprint(const ssp_csc* graph, const ssp_params* params) {
@@ -232,6 +339,8 @@ int ssp_server_create(const ssp_server_opts* opts, ssp_server** out) {
     if (opts) o = *opts;
     else ssp_server_opts_default(&o);
     if (o.slots < 1 || o.slots > 64) return fail(SSP_ERR_INVALID, "ssp_server_create: slots must be in [1, 64]");
+    if (o.max_batch < 0 || o.max_batch > 4096)
+        return fail(SSP_ERR_INVALID, "ssp_server_create: max_batch must be in [0, 4096]");
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
         cudaGetLastError();
@@ -347,6 +456,8 @@ int ssp_server_info_get(ssp_server* s, ssp_server_info* info) {
     info->budget_bytes = s->opts.hbm_budget_bytes;
     info->slots = s->opts.slots;
     info->waiters = s->waiters;
+    info->batches = s->batches;
+    info->peak_batch = s->peak_batch;
     return SSP_OK;
 }
 

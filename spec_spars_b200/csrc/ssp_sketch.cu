@@ -16,7 +16,8 @@
 
 namespace ssp {
 
-__global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, const int64_t* __restrict__ adj_ptr,
+__global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, int64_t v0, int64_t e0, int64_t nrows,
+                                                     const int64_t* __restrict__ adj_ptr,
                                                      const int32_t* __restrict__ adj_eid,
                                                      const int32_t* __restrict__ v2, const double* __restrict__ w,
                                                      int32_t col_lo, int32_t col_hi, int32_t tile_lo,
@@ -25,8 +26,8 @@ __global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, const int64_t* _
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t item = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < n * ntiles; item += nw) {
-        const int64_t v = item / ntiles;
-        const int32_t tile = tile_lo + (int32_t)(item - v * ntiles);
+        const int64_t v = v0 + item / ntiles;
+        const int32_t tile = tile_lo + (int32_t)(item - (v - v0) * ntiles);
         double acc[8];
 #pragma unroll
         for (int t = 0; t < 8; t++) acc[t] = 0.0;
@@ -37,7 +38,7 @@ __global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, const int64_t* _
             double b = 0.0;
             if (lane < cnt) {
                 int32_t e = adj_eid[p0 + lane];
-                u64x4 r = philox((uint64_t)e, (uint64_t)tile, 0, 0, seed, STREAM_SIGN);
+                u64x4 r = philox((uint64_t)(e - e0), (uint64_t)tile, 0, 0, seed, STREAM_SIGN);
                 r0 = r.x; r1 = r.y; r2 = r.z; r3 = r.w;
                 double sw = sqrt(w[e]);
                 b = (v2[e] == (int32_t)v) ? sw : -sw;
@@ -63,14 +64,15 @@ __global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, const int64_t* _
             const int64_t col = (int64_t)tile * 256 + lane + 32 * t;
             if (col >= col_lo && col < col_hi) {
                 const int64_t lc = col - col_lo;  // column of the stored block
-                Y[tm ? tile_off(n, v, lc) : v * ldy + lc] = acc[t];
+                Y[tm ? tile_off(nrows, v, lc) : v * ldy + lc] = acc[t];
             }
         }
     }
 }
 
 // Uniform (-1,1) entries: 32 bits each, 8 per Philox call (hash_with_inputs_alt, sparsifier.rs:410-420).
-__global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, const int64_t* __restrict__ adj_ptr,
+__global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, int64_t v0, int64_t e0, int64_t nrows,
+                                                     const int64_t* __restrict__ adj_ptr,
                                                      const int32_t* __restrict__ adj_eid,
                                                      const int32_t* __restrict__ v2, const double* __restrict__ w,
                                                      int32_t col_lo, int32_t col_hi, int32_t tile_lo,
@@ -79,8 +81,8 @@ __global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, const int64_t* _
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t item = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < n * ntiles; item += nw) {
-        const int64_t v = item / ntiles;
-        const int32_t tile = tile_lo + (int32_t)(item - v * ntiles);
+        const int64_t v = v0 + item / ntiles;
+        const int32_t tile = tile_lo + (int32_t)(item - (v - v0) * ntiles);
         double acc[8];
 #pragma unroll
         for (int t = 0; t < 8; t++) acc[t] = 0.0;
@@ -89,7 +91,7 @@ __global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, const int64_t* _
             const double sw = sqrt(w[e]);
             const double b = (v2[e] == (int32_t)v) ? sw : -sw;
             // lane computes call index tile*32 + lane -> u32 entries for columns 8*(tile*32+lane) .. +7
-            u64x4 r = philox((uint64_t)e, (uint64_t)tile * 32 + lane, 0, 0, seed, STREAM_UNIF);
+            u64x4 r = philox((uint64_t)(e - e0), (uint64_t)tile * 32 + lane, 0, 0, seed, STREAM_UNIF);
 #pragma unroll
             for (int t = 0; t < 8; t++) {
                 // my column j = tile*256 + lane + 32 t ; its call = j >> 3 -> source lane (lane >> 3) + 4 t
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, const int64_t* _
             const int64_t col = (int64_t)tile * 256 + lane + 32 * t;
             if (col >= col_lo && col < col_hi) {
                 const int64_t lc = col - col_lo;  // column of the stored block
-                Y[tm ? tile_off(n, v, lc) : v * ldy + lc] = acc[t];
+                Y[tm ? tile_off(nrows, v, lc) : v * ldy + lc] = acc[t];
             }
         }
     }
@@ -120,20 +122,28 @@ __global__ void __launch_bounds__(256) k_sketch_unif(int64_t n, const int64_t* _
 
 void sketch_device(Context& C, const DevGraph& G, int32_t k, double scale, uint64_t seed, int uniform, double* Y,
                    int64_t ldy, int tile_major, int32_t col_lo) {
+    sketch_device_part(C, G, 0, G.n, 0, k, scale, seed, uniform, Y, ldy, tile_major, col_lo);
+}
+
+// vertices [v0, v0 + nv) of G only, with edge ids counted from e0 for the signs (one graph of a union: its
+// vertices and edges are contiguous, so its entries are the ones it gets alone); Y has G.n rows
+void sketch_device_part(Context& C, const DevGraph& G, int64_t v0, int64_t nv, int64_t e0, int32_t k, double scale,
+                        uint64_t seed, int uniform, double* Y, int64_t ldy, int tile_major, int32_t col_lo) {
     const cudaStream_t stream = C.stream;
     SSP_REQUIRE(k > 0 && (tile_major || ldy >= k), SSP_ERR_INVALID, "sketch: need 0 < k <= ld");
     SSP_REQUIRE(col_lo >= 0 && (int64_t)col_lo + k <= INT32_MAX, SSP_ERR_INVALID, "sketch: bad column range");
     const int32_t col_hi = col_lo + k;
     const int32_t tile_lo = col_lo >> 8;
     const int32_t ntiles = ((col_hi - 1) >> 8) - tile_lo + 1;
-    const int64_t items = G.n * ntiles;
+    const int64_t items = nv * ntiles;
+    if (items == 0) return;
     const int threads = 256;
     const int blocks = grid_for(items * 32, threads, 148 * 16);
     if (uniform)
-        k_sketch_unif<<<blocks, threads, 0, stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, col_lo, col_hi,
+        k_sketch_unif<<<blocks, threads, 0, stream>>>(nv, v0, e0, G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, col_lo, col_hi,
                                                         tile_lo, ntiles, scale, seed, Y, ldy, tile_major);
     else
-        k_sketch_sign<<<blocks, threads, 0, stream>>>(G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, col_lo, col_hi,
+        k_sketch_sign<<<blocks, threads, 0, stream>>>(nv, v0, e0, G.n, G.adj_ptr, G.adj_eid, G.v2, G.w, col_lo, col_hi,
                                                         tile_lo, ntiles, scale, seed, Y, ldy, tile_major);
     SSP_CHECK_LAUNCH();
     C.kernels_launched++;

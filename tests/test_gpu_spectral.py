@@ -29,7 +29,7 @@ CASES = {
     "grid3d_32_logw": (lambda S: S.gen_grid3d(32, 32, 32, -3.0, 3.0, 2), 0.5, 0.9, False),
     "rmat_s14": (lambda S: S.gen_rmat(14, 16, 0.57, 0.19, 0.19, 3), 0.3, None, False),
     "rgg_n50k_deg16": (lambda S: S.gen_rgg(50_000, 16.0, 0.1, 10.0, 9), 0.5, None, False),
-    "er_n20k_deg200": (lambda S: S.gen_er(20_000, 200.0, 0.5, 2.0, 4), 0.5, 0.95, False),
+    "er_n20k_deg200": (lambda S: S.gen_er(20_000, 200.0, 0.5, 2.0, 4), 0.5, None, False),
 }
 
 
