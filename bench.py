@@ -524,6 +524,112 @@ def mesh_step(S, ctx, stream, name="grid3d_128"):
     return out
 
 
+def run_sharded(args, S, torch, dist, world, rank, local):
+    """--gpus N (N > 1): ONE graph with its k JL columns split over the N ranks (spec_spars_b200.sharded's
+    scheme): every rank factors the same graph, sketches and solves its tile-aligned share of the columns
+    (ssp_shard_leverage), one NCCL all-reduce(sum) of the m per-edge partial squares, then every rank forms
+    the same probabilities, coins and L_H (ssp_shard_finish).  Total work is fixed (strong scaling); value =
+    the graph's input edges / (max over ranks of the device time per step)."""
+    from spec_spars_b200.sharded import column_range
+    G, eps = make_graph(S, args.workload)  # the same graph on every rank
+    prm = S.SparsifierParameters.baseline(eps, pcg_tol=PCG_TOL)
+    if args.jl_cols > 0:
+        prm.jl_dim_override = args.jl_cols
+    if args.precision == "mixed":
+        prm.precision = S.SSP_PRECISION_MIXED
+    ctx = S.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    dev = torch.device("cuda", local)
+    cp = torch.from_numpy(G.colptr).to(dev)
+    ri = torch.from_numpy(G.rowidx).to(dev)
+    va = torch.from_numpy(G.values).to(dev)
+    Gd = S.DeviceCSC(G.n, G.nnz, cp.data_ptr(), ri.data_ptr(), va.data_ptr())
+    m = ctx.num_edges(Gd)
+    k = prm.jl_dim(G.n)
+    c0, c1 = column_range(k, world, rank)
+    sq = torch.zeros(max(m, 1), dtype=torch.float64, device=dev)
+
+    def step():
+        part = {}
+        if c1 > c0:
+            part = ctx.shard_leverage(Gd, prm, c0, c1, sq.data_ptr())
+        else:
+            sq.zero_()
+        dist.all_reduce(sq, op=dist.ReduceOp.SUM)
+        _, st = ctx.shard_finish(Gd, prm, sq.data_ptr(), device_out=True)
+        return part, st
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    k0 = ctx.kernels_launched
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        part, st = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks.stop()
+    launches = ctx.kernels_launched - k0
+    ms = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    # end to end: host graph in, host L_H out, every step (the graph's H2D on every rank)
+    Gh = G
+
+    def step_host():
+        if c1 > c0:
+            ctx.shard_leverage(Gh, prm, c0, c1, sq.data_ptr())
+        else:
+            sq.zero_()
+        dist.all_reduce(sq, op=dist.ReduceOp.SUM)
+        return ctx.shard_finish(Gh, prm, sq.data_ptr())
+
+    step_host()
+    torch.cuda.synchronize()
+    dist.barrier()
+    h0 = torch.cuda.Event(enable_timing=True)
+    h1 = torch.cuda.Event(enable_timing=True)
+    h0.record(stream)
+    for _ in range(args.e2e_steps):
+        H, _ = step_host()
+    h1.record(stream)
+    torch.cuda.synchronize()
+    ems = h0.elapsed_time(h1) / max(1, args.e2e_steps)
+    t = torch.tensor([ems], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ems = float(t.item())
+    if rank == 0:
+        line = {"metric": "input edges sparsified/sec", "value": m / (ms / 1000.0), "unit": "edges/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32 inner PCG, f64 dots + refinement",
+                "data": "synthetic",
+                "config": {"workload": args.workload, "n": G.n, "m": m, "eps": eps, "k": k, "pcg_tol": PCG_TOL,
+                           "precision": args.precision,
+                           "parallelism": f"JL columns split over {world} ranks, one NCCL all-reduce of m doubles",
+                           "columns_rank0": [c0, c1],
+                           "l2": "inputs and n-by-k working set larger than L2; no flush"},
+                "gpu_launches": launches, "kept_fraction": st["m_out"] / st["m_in"],
+                "pcg_iters_max": part.get("pcg_max_iters_used"), "clocks": clocks.summary(),
+                "e2e": {"value": m / (ems / 1000.0), "unit": "edges/s",
+                        "h2d_bytes_per_step": G.colptr.nbytes + G.rowidx.nbytes + G.values.nbytes,
+                        "d2h_bytes_per_step": H.colptr.nbytes + H.rowidx.nbytes + H.values.nbytes,
+                        "ms_per_step": ems}}
+        print(json.dumps(line), flush=True)
+    del sq
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -545,6 +651,9 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--mtx", action="store_true", help="time the GPU Matrix Market reader/writer and sparsify_dataset")
+    ap.add_argument("--mode", default="auto", choices=["auto", "sharded", "replicas"],
+                    help="N > 1: split one graph's JL columns over the ranks (auto, sharded) or run N independent "
+                         "replicas, one graph each (replicas)")
     ap.add_argument("--no-mesh", dest="mesh", action="store_false",
                     help="skip the one-step grid3d_128 measurement reported beside the ER headline")
     ap.add_argument("--reference-n", type=int, default=0,
@@ -570,7 +679,14 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
+        # the communicator's set-up lines show the rank count
+        os.environ.setdefault("NCCL_DEBUG", "INFO")
+        os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if args.mode != "replicas":
+            run_sharded(args, S, torch, dist, world, rank, local)
+            dist.destroy_process_group()
+            return
 
     G, eps = make_graph(S, args.workload, rank)
     prm = S.SparsifierParameters.baseline(eps, pcg_tol=PCG_TOL)

@@ -669,13 +669,18 @@ class Context:
                                         sq_ptr, ctypes.byref(m), ctypes.byref(st)))
         return _stats_dict(st)
 
-    def shard_finish(self, graph, params, sq_total_ptr):
-        """Phase 2: probabilities, coins and L_H from the per-edge squares summed over all columns."""
+    def shard_finish(self, graph, params, sq_total_ptr, device_out=False):
+        """Phase 2: probabilities, coins and L_H from the per-edge squares summed over all columns.  With
+        device_out, L_H stays in the context (nnz, colptr, rowidx, values device pointers, valid until the
+        context's next call), as sparsify_device returns it."""
         g = graph._struct()
         out = _CscOut()
         st = _Stats()
         _check(lib().ssp_shard_finish(self._h, ctypes.byref(g), ctypes.byref(params._s), sq_total_ptr,
-                                      SSP_MEM_HOST, ctypes.byref(out), ctypes.byref(st)))
+                                      SSP_MEM_DEVICE if device_out else SSP_MEM_HOST, ctypes.byref(out),
+                                      ctypes.byref(st)))
+        if device_out:
+            return (out.nnz, out.colptr, out.rowidx, out.values), _stats_dict(st)
         return _take_out(out), _stats_dict(st)
 
     def solve_lap(self, lap, Y, tol=0.0, abs_tol=np.sqrt(2e-7), max_iters=400, factor_seed=0,

@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ssp_host.h"
@@ -185,25 +186,72 @@ void gen_rgg(int64_t n, double avg_degree, double wlo, double whi, uint64_t seed
 // made undirected and deduplicated, each kept pair gets a LogNormal(0, 1) weight (Box-Muller from the
 // counter (min * 2^scale + max, 6), rounded to FP32), and only the largest connected component is kept, its
 // vertices renumbered in increasing order.
+// Runs fn(t, lo, hi) over [0, count) split into contiguous ranges, one per host thread.
+template <class Fn>
+static void parallel_ranges(uint64_t count, Fn fn) {
+    const unsigned hw = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    const uint64_t T = std::max<uint64_t>(1, std::min<uint64_t>(hw, count / 65536 + 1));
+    std::vector<std::thread> th;
+    for (uint64_t t = 0; t < T; t++)
+        th.emplace_back([&, t] { fn(t, count * t / T, count * (t + 1) / T); });
+    for (auto& x : th) x.join();
+}
+
+// Sorts in parallel: contiguous chunks sorted on their own threads, then merged pairwise (the result is
+// the sorted sequence, whatever the thread count).
+static void parallel_sort(std::vector<uint64_t>& v) {
+    const unsigned hw = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    size_t parts = 1;
+    while (parts * 2 <= hw && v.size() / (parts * 2) >= (1u << 20)) parts *= 2;
+    std::vector<size_t> cut(parts + 1);
+    for (size_t i = 0; i <= parts; i++) cut[i] = v.size() * i / parts;
+    {
+        std::vector<std::thread> th;
+        for (size_t i = 0; i < parts; i++) th.emplace_back([&, i] { std::sort(v.begin() + cut[i], v.begin() + cut[i + 1]); });
+        for (auto& x : th) x.join();
+    }
+    std::vector<uint64_t> tmp(v.size());
+    for (size_t w = 1; w < parts; w *= 2) {
+        std::vector<std::thread> th;
+        for (size_t i = 0; i + w < parts; i += 2 * w) {
+            const size_t lo = cut[i], mid = cut[i + w], hi = cut[std::min(parts, i + 2 * w)];
+            th.emplace_back([&, lo, mid, hi] { std::merge(v.begin() + lo, v.begin() + mid, v.begin() + mid, v.begin() + hi,
+                                                          tmp.begin() + lo); });
+        }
+        for (auto& x : th) x.join();
+        // ranges left without a partner keep their place
+        for (size_t i = 0; i < parts; i += 2 * w)
+            if (i + w >= parts) std::copy(v.begin() + cut[i], v.begin() + cut[parts], tmp.begin() + cut[i]);
+        v.swap(tmp);
+    }
+}
+
+// R-MAT (Chakrabarti, Zhan, Faloutsos 2004): each of edge_factor * 2^scale samples picks a quadrant per bit
+// level with probabilities (a, b, c, 1 - a - b - c), from Philox(seed, sample * 64 + level).  Self-loops are
+// dropped, pairs symmetrized and deduplicated, the largest connected component kept (vertices renumbered in
+// order), weights LogNormal(0, 1) rounded to FP32 from Philox counters of the pair.  Samples and weights are
+// drawn on all host threads; every value depends only on its own counter, so the graph does not depend on
+// the thread count.
 void gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed, HostCsc& out) {
     const uint64_t nv = 1ull << scale;
     const uint64_t samples = (uint64_t)edge_factor << scale;
-    std::vector<uint64_t> keys;
-    keys.reserve(samples);
-    for (uint64_t t = 0; t < samples; t++) {
-        uint64_t u = 0, v = 0;
-        for (int32_t bit = 0; bit < scale; bit++) {
-            const double r = gen_u53(seed, t * 64 + (uint64_t)bit, 5);
-            const int q = r < a ? 0 : r < a + b ? 1 : r < a + b + c ? 2 : 3;
-            u = (u << 1) | (uint64_t)(q >> 1);
-            v = (v << 1) | (uint64_t)(q & 1);
+    const uint64_t NONE = ~0ull;
+    std::vector<uint64_t> keys(samples);
+    parallel_ranges(samples, [&](uint64_t, uint64_t lo, uint64_t hi) {
+        for (uint64_t t = lo; t < hi; t++) {
+            uint64_t u = 0, v = 0;
+            for (int32_t bit = 0; bit < scale; bit++) {
+                const double r = gen_u53(seed, t * 64 + (uint64_t)bit, 5);
+                const int q = r < a ? 0 : r < a + b ? 1 : r < a + b + c ? 2 : 3;
+                u = (u << 1) | (uint64_t)(q >> 1);
+                v = (v << 1) | (uint64_t)(q & 1);
+            }
+            keys[t] = u == v ? NONE : std::min(u, v) * nv + std::max(u, v);
         }
-        if (u == v) continue;
-        const uint64_t lo = std::min(u, v), hi = std::max(u, v);
-        keys.push_back(lo * nv + hi);
-    }
-    std::sort(keys.begin(), keys.end());
+    });
+    parallel_sort(keys);
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    if (!keys.empty() && keys.back() == NONE) keys.pop_back();
     // largest connected component by union-find (smaller root wins, so labels are deterministic)
     std::vector<uint64_t> parent(nv);
     for (uint64_t i = 0; i < nv; i++) parent[i] = i;
@@ -238,14 +286,16 @@ void gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, 
     std::sort(order.begin(), order.end(), [&](size_t x, size_t y) { return e[x] < e[y]; });
     std::vector<int32_t> va(e.size()), vb(e.size());
     std::vector<double> w(e.size());
-    for (size_t t = 0; t < order.size(); t++) {
-        const size_t i = order[t];
-        vb[t] = (int32_t)e[i].first;
-        va[t] = (int32_t)e[i].second;
-        const double u1 = gen_u53(seed, ek[i], 6), u2 = gen_u53(seed ^ 0x9e3779b97f4a7c15ull, ek[i], 6);
-        const double z = std::sqrt(-2.0 * std::log(1.0 - u1)) * std::cos(2.0 * M_PI * u2);
-        w[t] = (double)(float)std::exp(z);
-    }
+    parallel_ranges(order.size(), [&](uint64_t, uint64_t lo, uint64_t hi) {
+        for (uint64_t t = lo; t < hi; t++) {
+            const size_t i = order[t];
+            vb[t] = (int32_t)e[i].first;
+            va[t] = (int32_t)e[i].second;
+            const double u1 = gen_u53(seed, ek[i], 6), u2 = gen_u53(seed ^ 0x9e3779b97f4a7c15ull, ek[i], 6);
+            const double z = std::sqrt(-2.0 * std::log(1.0 - u1)) * std::cos(2.0 * M_PI * u2);
+            w[t] = (double)(float)std::exp(z);
+        }
+    });
     out.from_upper_edges(n, va, vb, w);
 }
 
