@@ -302,11 +302,16 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# the truncation of the serving mix's factors (the autotuner picks 26 to 31 on its ER and RGG graphs)
+SERVE_MAX_DEGREE = 28
+
+
 def serving_mix(S, count, max_n, seed=4, precision="fp64"):
     """The serving mix of seeded requests: random-geometric or ER graphs (equiprobable), n log-uniform in
     [1e3, max_n], average degree uniform in 8..32, weights uniform [0.1, 10] rounded to FP32, eps 0.3 or 0.5.
-    Every request asks for complete elimination in the sparse phase (dense_threshold = factor_max_degree = 0),
-    so the server may batch it; the plain path runs the same parameters one request at a time."""
+    Every request asks for sparse-phase elimination truncated at average live degree SERVE_MAX_DEGREE
+    (dense_threshold = 0, a fixed factor_max_degree), so the server may batch it; the plain path runs the same
+    parameters one request at a time."""
     import numpy as np
     rng = np.random.default_rng(seed)
     reqs = []
@@ -317,7 +322,7 @@ def serving_mix(S, count, max_n, seed=4, precision="fp64"):
         G = S.gen_rgg(n, d, 0.1, 10.0, 1000 + i) if rng.random() < 0.5 else S.gen_er(n, d, 0.1, 10.0, 1000 + i)
         prm = S.SparsifierParameters.baseline(eps, pcg_tol=PCG_TOL, sampling_seed=i)
         prm.dense_threshold = 0
-        prm.factor_max_degree = 0
+        prm.factor_max_degree = SERVE_MAX_DEGREE
         if precision == "mixed":
             prm.precision = S.SSP_PRECISION_MIXED
         reqs.append((G, prm))

@@ -235,9 +235,10 @@ int ssp_csc_free(ssp_csc_out* out);
  * rule, scale and seeds, variance correction, output_file), and every PCG scalar is kept per (graph,
  * column), so outs[b] equals ssp_sparsify of graph b alone to the solve's rounding (the kept edges match
  * unless a coin falls within that rounding of its probability).  The batch must agree on factor_seed,
- * precision, pcg_tol, pcg_abs_tol, pcg_max_iters, reweight, and use dense_threshold = 0 and
- * factor_max_degree = 0 (complete elimination in the sparse phase: the dense tail and truncation look at the
- * whole Schur complement and would couple the graphs).  outs[b] is host memory (free with ssp_csc_free);
+ * precision, pcg_tol, pcg_abs_tol, pcg_max_iters, reweight and factor_max_degree, which must be a fixed value
+ * (>= 0: each graph is truncated by its own test, as alone; the autotuner's -1 is refused), and use
+ * dense_threshold = 0 (the dense tail looks at the whole Schur complement and would couple the graphs).
+ * outs[b] is host memory (free with ssp_csc_free);
  * stats[b] has graph b's sizes and PCG figures, and the batch's stage times. */
 int ssp_sparsify_batch(ssp_context* ctx, int32_t count, const ssp_csc* graphs, const ssp_params* params,
                        ssp_csc_out* outs, ssp_stats* stats);
@@ -275,7 +276,8 @@ int ssp_shard_finish(ssp_context* ctx, const ssp_csc* graph, const ssp_params* p
  * hbm_budget_bytes (a younger one may go first while the oldest has waited less than 500 ms; after that the
  * oldest is admitted first); a request whose footprint alone exceeds the budget is refused at submit
  * (SSP_ERR_CAPACITY).  The slot then adds pending requests that can share its run (same epsilon, factor
- * seed, precision, PCG options and reweighting, and dense_threshold = factor_max_degree = 0), up to max_batch
+ * seed, precision, PCG options, reweighting and fixed factor_max_degree >= 0, and dense_threshold = 0), up to
+ * max_batch
  * and its share of the budget, and runs them with ssp_sparsify_batch; other requests run exactly
  * ssp_sparsify, so their result is the same as a lone call's.  Results are collected once with ssp_wait /
  * ssp_poll (which then own res->out: free it with ssp_csc_free). */

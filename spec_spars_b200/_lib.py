@@ -555,8 +555,8 @@ class Context:
     def sparsify_batch(self, graphs, params):
         """Several host graphs sparsified as one disjoint union (ssp_sparsify_batch): one factorization and one
         all-columns PCG for the batch, every PCG scalar per (graph, column).  params: one SparsifierParameters
-        per graph, or one for all; they must agree on the factor seed, precision, PCG options and reweighting and
-        ask for complete elimination (dense_threshold = 0, factor_max_degree = 0).  Returns [(L_H, stats)]."""
+        per graph, or one for all; they must agree on the factor seed, precision, PCG options, reweighting and a
+        fixed truncation (factor_max_degree >= 0), with dense_threshold = 0.  Returns [(L_H, stats)]."""
         graphs = list(graphs)
         if isinstance(params, SparsifierParameters):
             params = [params] * len(graphs)

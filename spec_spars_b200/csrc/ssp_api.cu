@@ -606,8 +606,8 @@ static const T* stage_in(Context& C, const T* p, int64_t cnt, int32_t mem, const
 //   * Graph b's vertices are [V_b, V_b + n_b) of the union and its edges [E_b, E_b + m_b) (the union's CSC
 //     keeps each graph's columns together, and edges are extracted in CSC order).
 //   * Its sketch uses its own seed, scale, k_b and edge ids counted from E_b; its factor draws are keyed by
-//     in-graph vertex ids, so both equal the lone run's.  Elimination is complete in the sparse phase (no
-//     dense tail, no truncation: those look at the whole Schur complement and would couple the graphs).
+//     in-graph vertex ids, and each graph is truncated by its own live-entry test, so both equal the lone
+//     run's.  There is no dense tail (it looks at the whole Schur complement and would couple the graphs).
 //   * The PCG keeps every scalar per (graph, column) (PcgSegments), so each graph's iterates are its own;
 //     its reductions are blocked differently from a lone run's, so a served result equals the lone result
 //     to the solve's rounding, not bit for bit.
@@ -657,9 +657,9 @@ static void sparsify_batch_impl(Context& C, int32_t count, const ssp_csc* graphs
         SSP_REQUIRE(p.epsilon > 0 && std::isfinite(p.epsilon), SSP_ERR_INVALID, "batch: epsilon must be positive");
         SSP_REQUIRE(same_batch_options(p, p0), SSP_ERR_INVALID,
                     "batch: factor seed, precision, PCG options, reweighting and factor options must agree");
-        SSP_REQUIRE(p.dense_threshold == 0 && p.factor_max_degree == 0, SSP_ERR_INVALID,
-                    "batch: the graphs must ask for complete sparse elimination (dense_threshold = 0, "
-                    "factor_max_degree = 0)");
+        SSP_REQUIRE(p.dense_threshold == 0 && p.factor_max_degree >= 0, SSP_ERR_INVALID,
+                    "batch: the graphs must ask for sparse-phase elimination with a fixed truncation "
+                    "(dense_threshold = 0, factor_max_degree >= 0)");
         // edges: upper entries with a non-zero value (sparsifier.rs:365), in CSC order
         int64_t m = 0;
         for (int64_t j = 0; j < g.n; j++)
@@ -724,8 +724,10 @@ static void sparsify_batch_impl(Context& C, int32_t count, const ssp_csc* graphs
     FactorOptions fo;
     fo.seed = p0.factor_seed;
     fo.dense_threshold = 0;
-    fo.max_degree = 0;
+    fo.max_degree = p0.factor_max_degree;
     fo.vbase = vbase;
+    fo.vseg = rowseg;
+    fo.seg_row0 = V;
     factor_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, fo, F, "bt_f");
     T.mark();  // 3
     PcgOptions po;
@@ -818,6 +820,7 @@ static void sparsify_batch_impl(Context& C, int32_t count, const ssp_csc* graphs
             // the batch's shared figures: every graph of the batch reports the same stage times and factor
             st.nnz_factor = F.nnz;
             st.factor_levels = F.num_levels;
+            st.factor_max_degree_used = p0.factor_max_degree;
             st.ms_assembly = T.ms(0, 1);
             st.ms_sketch = T.ms(1, 2);
             st.ms_factor = T.ms(2, 3);

@@ -25,6 +25,7 @@ namespace ssp {
 
 enum { C_NEXT = 0, C_LCUR, C_FCUR, C_ERR, C_NB, C_NG, C_MAXLIVE, C_POOL, C_OWNERS, C_REM, C_NFILL, C_NCTR };
 enum { FERR_POOL = 1, FERR_OVERFLOW = 2 };
+enum { GC_FCUR = 0, GC_NFRONT = 1, GC_NFILL = 2 };
 
 constexpr int BLOCK_TIER_MAX = 4096;    // live entries handled in shared memory
 constexpr int DENSE_FRONTIER_MAX = 8;   // dense tail once the frontier has collapsed to this size
@@ -35,6 +36,11 @@ struct FDev {
     // several graphs factored at once: vbase[v] is the first vertex of v's graph, and every random draw is keyed
     // by the vertex's id inside its graph, so each graph's factor is the one it gets alone (null: one graph)
     const int32_t* vbase;
+    // ... and vseg[v] its graph: per graph, gctr[3 g + GC_*] count the upcoming frontier's live entries and
+    // vertices and the fill of the level just eliminated, for the truncation test of each graph
+    const int32_t* vseg;
+    int64_t* gctr;
+    int32_t nseg;
     const uint64_t* prio;
     int32_t* count;
     int32_t* level;
@@ -142,6 +148,10 @@ __global__ void k_live_count(FDev F, const int32_t* frontier, int32_t* live_cnt,
         for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
         if (lane == 0) {
             live_cnt[i] = cnt;
+            if (F.vseg) {
+                atomicAdd((unsigned long long*)&F.gctr[3 * F.vseg[v] + GC_FCUR], (unsigned long long)cnt);
+                atomicAdd((unsigned long long*)&F.gctr[3 * F.vseg[v] + GC_NFRONT], 1ull);
+            }
             F.Lstart[v] = (int64_t)atomicAdd((unsigned long long*)&F.ctr[C_LCUR], (unsigned long long)cnt);
             F.fstart[i] = (int64_t)atomicAdd((unsigned long long*)&F.ctr[C_FCUR], (unsigned long long)cnt);
             atomicMax((unsigned long long*)&F.ctr[C_MAXLIVE], (unsigned long long)cnt);
@@ -279,6 +289,8 @@ __global__ void __launch_bounds__(128) k_elim_warp(FDev F, const int32_t* fronti
             F.Lcnt[v] = cnt;
             F.fcnt[fi] = cnt > 0 ? cnt - 1 : 0;
             if (cnt > 1) atomicAdd((unsigned long long*)&F.ctr[C_NFILL], (unsigned long long)(cnt - 1));
+            if (cnt > 1 && F.vseg)
+                atomicAdd((unsigned long long*)&F.gctr[3 * F.vseg[v] + GC_NFILL], (unsigned long long)(cnt - 1));
         }
         __syncwarp();
     }
@@ -420,6 +432,8 @@ __device__ void block_finish_column(const FDev& F, int32_t v, int64_t fidx, int3
         if (fidx >= 0) {
             F.fcnt[fidx] = cnt - 1;
             if (cnt > 1) atomicAdd((unsigned long long*)&F.ctr[C_NFILL], (unsigned long long)(cnt - 1));
+            if (cnt > 1 && F.vseg)
+                atomicAdd((unsigned long long*)&F.gctr[3 * F.vseg[v] + GC_NFILL], (unsigned long long)(cnt - 1));
         }
     }
     __syncthreads();
@@ -577,18 +591,51 @@ __global__ void k_fill_scatter(FDev F) {
 }
 
 // frontier swap bookkeeping: REM <- NEXT, reset per-level cursors
-__global__ void k_level_begin(int64_t* ctr) {
+__global__ void k_level_begin(int64_t* ctr, int64_t* gctr, int32_t nseg) {
     ctr[C_REM] = ctr[C_NEXT];
     ctr[C_NEXT] = 0;
     ctr[C_OWNERS] = 0;
     ctr[C_NFILL] = 0;
+    for (int32_t g = 0; g < nseg; g++) gctr[3 * g + GC_NFILL] = 0;
 }
-__global__ void k_level_prep(int64_t* ctr) {
+__global__ void k_level_prep(int64_t* ctr, int64_t* gctr, int32_t nseg) {
     // the upcoming frontier's counts become the live-count kernel's domain
     ctr[C_FCUR] = 0;
     ctr[C_NB] = 0;
     ctr[C_NG] = 0;
     ctr[C_MAXLIVE] = 0;
+    for (int32_t g = 0; g < nseg; g++) gctr[3 * g + GC_FCUR] = gctr[3 * g + GC_NFRONT] = 0;
+}
+__global__ void k_set_ctr(int64_t* ctr, int idx, int64_t v) { ctr[idx] = v; }
+// the frontier without the vertices of stopped graphs (order kept)
+__global__ void k_drop_stopped(const int32_t* __restrict__ in, int64_t nin, const int32_t* __restrict__ vseg,
+                               const int32_t* __restrict__ stopped, int32_t* __restrict__ out, int64_t* cnt) {
+    // one block: order-preserving compaction
+    __shared__ int32_t s_base;
+    if (threadIdx.x == 0) s_base = 0;
+    __syncthreads();
+    for (int64_t b0 = 0; b0 < nin; b0 += blockDim.x) {
+        const int64_t i = b0 + threadIdx.x;
+        const int keep = i < nin && !stopped[vseg[in[i]]];
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        __shared__ int32_t s_warp[32];
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if (lane == 0) s_warp[w] = __popc(bal);
+        __syncthreads();
+        int32_t before = 0;
+        for (int j = 0; j < w; j++) before += s_warp[j];
+        int32_t tot = 0;
+        for (int j = 0; j < (int)(blockDim.x >> 5); j++) tot += s_warp[j];
+        if (keep) out[s_base + before + __popc(bal & ((1u << lane) - 1u))] = in[i];
+        __syncthreads();
+        if (threadIdx.x == 0) s_base += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *cnt = s_base;
+}
+__global__ void k_collect_live_range(int64_t v0, int64_t v1, const int32_t* level, int32_t* rem, int64_t* cnt) {
+    for (int64_t v = v0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < v1; v += (int64_t)gridDim.x * blockDim.x)
+        if (level[v] < 0) rem[atomicAdd((unsigned long long*)cnt, 1ull)] = (int32_t)v;
 }
 
 // ---------------------------------------------------------------- solve schedule
@@ -1034,10 +1081,19 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
     F.n = n;
     F.seed = opt.seed;
     F.vbase = opt.vbase;
-    // the dense tail and the truncation test look at the whole Schur complement: with several graphs they
-    // would couple them, so a union is eliminated completely in the sparse phase
-    SSP_REQUIRE(!opt.vbase || (opt.dense_threshold == 0 && opt.max_degree == 0), SSP_ERR_INVALID,
-                "factor: several graphs at once need dense_threshold = 0 and max_degree = 0");
+    // the dense tail looks at the whole Schur complement and would couple several graphs: a union is
+    // eliminated in the sparse phase, and truncated graph by graph (vseg)
+    SSP_REQUIRE(!opt.vbase || (opt.dense_threshold == 0 && opt.max_degree >= 0 && (opt.max_degree == 0 || opt.vseg)),
+                SSP_ERR_INVALID, "factor: several graphs at once need dense_threshold = 0 and max_degree >= 0 "
+                                 "(with the graph of every vertex when truncating)");
+    const bool seg_mode = opt.vseg != nullptr;
+    const int32_t nseg = seg_mode ? (int32_t)opt.seg_row0.size() - 1 : 0;
+    SSP_REQUIRE(!seg_mode || (nseg >= 1 && opt.seg_row0.front() == 0 && opt.seg_row0.back() == n), SSP_ERR_INVALID,
+                "factor: inconsistent graph ranges");
+    F.vseg = opt.vseg;
+    F.nseg = nseg;
+    F.gctr = seg_mode ? W.get_t<int64_t>(nm("gctr"), 3 * (size_t)nseg) : nullptr;
+    if (seg_mode) SSP_CUDA(cudaMemsetAsync(F.gctr, 0, sizeof(int64_t) * 3 * nseg, C.stream));
     uint64_t* prio = W.get_t<uint64_t>(nm("prio"), n);
     F.prio = prio;
     F.count = W.get_t<int32_t>(nm("count"), n);
@@ -1103,7 +1159,7 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
 
     // live counts of the first frontier
     auto live_count = [&](int32_t* fr) {
-        k_level_prep<<<1, 1, 0, C.stream>>>(F.ctr);
+        k_level_prep<<<1, 1, 0, C.stream>>>(F.ctr, F.gctr, F.nseg);
         k_live_count<<<grid_for(n * 32, T256, 148 * 64), T256, 0, C.stream>>>(F, fr, live_cnt, list_b, list_g);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += 2;
@@ -1125,14 +1181,98 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
     int64_t Lused_prev = 0;
     const size_t blk_smem = (size_t)BLOCK_TIER_MAX * (3 * sizeof(double) + 2 * sizeof(int32_t));
     SSP_CUDA(cudaFuncSetAttribute(k_elim_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem));
+    // several graphs: each graph's own truncation test, with its own live-entry count (the same accounting
+    // as the single-graph test below, restricted to its vertices)
+    std::vector<int64_t> g_live(nseg, 0), g_elim(nseg, 0), g_prev(nseg, -1), g_cnt(3 * (size_t)nseg + 1, 0);
+    std::vector<int32_t> g_stopped(nseg, 0);
+    int32_t* d_stopped = seg_mode ? W.get_t<int32_t>(nm("gstop"), nseg) : nullptr;
+    int32_t last_trunc_level = -1;
+    if (seg_mode) {
+        std::vector<int32_t> hdeg(n);
+        SSP_CUDA(cudaMemcpyAsync(hdeg.data(), deg, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+        for (int32_t g = 0; g < nseg; g++)
+            for (int64_t v = opt.seg_row0[g]; v < opt.seg_row0[g + 1]; v++) g_live[g] += hdeg[v];
+    }
+    // graph g's live vertices become its final, diagonal level `at` (k_trunc_diag), as a lone truncation does
+    auto truncate_graph = [&](int32_t g, int32_t at) -> int64_t {
+        const int64_t v0 = opt.seg_row0[g], v1 = opt.seg_row0[g + 1];
+        int32_t* rem = W.get_t<int32_t>(nm("rem"), n + 1);
+        SSP_CUDA(cudaMemsetAsync(F.ctr + C_REM, 0, sizeof(int64_t), C.stream));
+        k_collect_live_range<<<grid_for(v1 - v0, T256), T256, 0, C.stream>>>(v0, v1, F.level, rem, F.ctr + C_REM);
+        SSP_CHECK_LAUNCH();
+        const int64_t R = read_i64(C, F.ctr + C_REM);
+        if (R == 0) return 0;
+        std::vector<int32_t> lens(v1 - v0);
+        SSP_CUDA(cudaMemcpyAsync(lens.data(), F.bag_len + v0, sizeof(int32_t) * (v1 - v0), cudaMemcpyDeviceToHost,
+                                 C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+        int32_t maxlen = 0;
+        for (auto x : lens) maxlen = std::max(maxlen, x);
+        int32_t cap = 64;
+        while (cap < maxlen) cap <<= 1;
+        if (cap <= BLOCK_TIER_MAX) {
+            size_t smem = (size_t)cap * (2 * sizeof(double) + 2 * sizeof(int32_t));
+            SSP_CUDA(cudaFuncSetAttribute(k_trunc_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_trunc_diag<<<(int)std::min<int64_t>(R, 148 * 8), 256, smem, C.stream>>>(F, rem, (int32_t)R, at, cap,
+                                                                                      nullptr, nullptr, 0);
+        } else {
+            int blocks = 32;
+            int32_t* gu = W.get_t<int32_t>(nm("gscr_u"), (size_t)2 * cap * blocks);
+            double* gw = W.get_t<double>(nm("gscr_w"), (size_t)4 * cap * blocks);
+            k_trunc_diag<<<blocks, 1024, 0, C.stream>>>(F, rem, (int32_t)R, at, cap, gu, gw, 1);
+        }
+        k_set_level<<<grid_for(R, T256), T256, 0, C.stream>>>(rem, (int32_t)R, at, F.level);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched += 3;
+        int64_t hh[C_NCTR];
+        read_i64s(C, F.ctr, hh, C_NCTR);
+        if (hh[C_ERR]) throw Error(SSP_ERR_CAPACITY, "factor: truncation overflow");
+        return R;
+    };
     while (true) {
         read_i64s(C, F.ctr, h, C_NCTR);
         if (h[C_ERR] & FERR_POOL) throw Error(SSP_ERR_CAPACITY, "factor: bag pool exhausted");
         if (h[C_ERR] & FERR_OVERFLOW) throw Error(SSP_ERR_CAPACITY, "factor: bag overflow");
         if (prev_fcur >= 0) live_entries += 2 * h[C_NFILL] - 2 * prev_fcur;
-        const int64_t nf = h[C_NEXT];
+        int64_t nf = h[C_NEXT];
+        if (seg_mode) {
+            read_i64s(C, F.gctr, g_cnt.data(), 3 * nseg);
+            for (int32_t g = 0; g < nseg; g++)
+                if (g_prev[g] >= 0) g_live[g] += 2 * g_cnt[3 * g + GC_NFILL] - 2 * g_prev[g];
+        }
         if (nf == 0) break;
-        if (opt.max_degree > 0 && live_entries > opt.max_degree * (n - eliminated)) {
+        if (seg_mode && opt.max_degree > 0) {
+            std::vector<int32_t> stop;
+            for (int32_t g = 0; g < nseg; g++) {
+                const int64_t ng = opt.seg_row0[g + 1] - opt.seg_row0[g];
+                if (!g_stopped[g] && g_cnt[3 * g + GC_NFRONT] > 0 && g_live[g] > opt.max_degree * (ng - g_elim[g]))
+                    stop.push_back(g);
+            }
+            if (!stop.empty()) {
+                for (int32_t g : stop) {
+                    const int64_t R = truncate_graph(g, lvl);
+                    g_stopped[g] = 1;
+                    eliminated += R;
+                    out.truncated_rows += R;
+                    last_trunc_level = lvl;
+                }
+                // the frontier without the stopped graphs, and its reservations made again
+                SSP_CUDA(cudaMemcpyAsync(d_stopped, g_stopped.data(), sizeof(int32_t) * nseg, cudaMemcpyHostToDevice,
+                                         C.stream));
+                k_drop_stopped<<<1, 1024, 0, C.stream>>>(next, nf, F.vseg, d_stopped, frontier, F.ctr + C_NEXT);
+                k_set_ctr<<<1, 1, 0, C.stream>>>(F.ctr, C_LCUR, Lused_prev);
+                SSP_CHECK_LAUNCH();
+                C.kernels_launched += 2;
+                std::swap(frontier, next);
+                live_count(next);
+                read_i64s(C, F.ctr, h, C_NCTR);
+                read_i64s(C, F.gctr, g_cnt.data(), 3 * nseg);
+                nf = h[C_NEXT];
+                if (nf == 0) break;
+            }
+        }
+        if (!seg_mode && opt.max_degree > 0 && live_entries > opt.max_degree * (n - eliminated)) {
             truncated = true;
             break;
         }
@@ -1180,8 +1320,12 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
         }
         Lused_prev = h[C_LCUR];
         prev_fcur = h[C_FCUR];
+        for (int32_t g = 0; g < nseg; g++) {
+            g_prev[g] = g_cnt[3 * g + GC_FCUR];
+            g_elim[g] += g_cnt[3 * g + GC_NFRONT];
+        }
         std::swap(frontier, next);
-        k_level_begin<<<1, 1, 0, C.stream>>>(F.ctr);  // REM <- NEXT (frontier size), NEXT <- 0
+        k_level_begin<<<1, 1, 0, C.stream>>>(F.ctr, F.gctr, F.nseg);  // REM <- NEXT (frontier size), NEXT <- 0
         k_elim_warp<<<grid_for(nf * 32, 128, 148 * 64), 128, 0, C.stream>>>(F, frontier, live_cnt);
         SSP_CHECK_LAUNCH();
         C.kernels_launched += 2;
@@ -1215,6 +1359,7 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
         lvl++;
         live_count(next);
     }
+    if (seg_mode && last_trunc_level >= lvl) lvl = last_trunc_level + 1;  // a graph truncated after the last level
     const int32_t sparse_levels = lvl;
     const int64_t T = truncated ? 0 : n - eliminated;
     if (truncated) {

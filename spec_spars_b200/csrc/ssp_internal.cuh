@@ -376,6 +376,9 @@ struct FactorOptions {
     int64_t dense_threshold = 4096;
     int64_t max_degree = 0;  // stop once the live Schur complement's average degree exceeds this (0: never)
     const int32_t* vbase = nullptr;  // device [n]: first vertex of each vertex's graph (several graphs at once)
+    const int32_t* vseg = nullptr;   // device [n]: graph of each vertex; with max_degree > 0 each graph is
+                                     // truncated by its own test, at the level where it would stop alone
+    std::vector<int64_t> seg_row0;   // host: nseg + 1 first vertices of the graphs (with vseg)
 };
 // Input: Laplacian CSC on device (rows > col used, |value| as weight).
 void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,

@@ -539,7 +539,7 @@ struct LoopGraph {
 // evict the gathered slab from L2), then every (row, column) lane pair sums its row with independent
 // gathers from the tile slab.  Warps never wait for each other.  Modes: SpMM (+ p.q partials), SpMM
 // adding into its output (the second and later column slabs of the matrix), forward solve, backward solve.
-enum { M_SPMM = 0, M_FWD = 1, M_BWD = 2, M_SPMM_ACC = 3 };
+enum { M_SPMM = 0, M_FWD = 1, M_BWD = 2, M_SPMM_ACC = 3, M_FWD_LAST = 4 };
 constexpr int CH_THREADS = 256;
 // independent gathers in flight per lane in the chunk kernels (powers of two).  Measured on B200 at ER n = 1M,
 // k = 1327: 8 for the SpMM takes it from 48 to 38 ms; the level solves are faster with 4 (19 against 22 ms).
@@ -554,7 +554,7 @@ constexpr int MINB_SPMM = 6, MINB_FWD = 6, MINB_BWD = 5;
 
 template <int MODE, class T>
 __device__ __forceinline__ void chunk_epilogue(T* out, const T* aux, const T* xt, int64_t toff, int64_t v, int col,
-                                               T acc, double& dot, bool want_dot) {
+                                               T acc, double& dot, bool want_dot, const T* dlast) {
     const int64_t o = toff + v * TILE + col;
     if (MODE == M_SPMM || MODE == M_SPMM_ACC) {
         // q streams out (evict-first), so it does not push the gathered slab out of L2
@@ -563,6 +563,11 @@ __device__ __forceinline__ void chunk_epilogue(T* out, const T* aux, const T* xt
         if (want_dot) dot += (double)acc * (double)xt[v * TILE + col];
     } else if (MODE == M_FWD) {
         out[o] = aux[o] - acc;
+    } else if (MODE == M_FWD_LAST) {
+        // the forward value, then the backward solve's step for a row with an empty column
+        const T yu = aux[o] - acc;
+        const T d = dlast[v];
+        out[o] = (d != (T)0 ? yu / d : yu) - (T)0;
     } else {
         const T d = aux[v];
         const T yu = out[o];
@@ -582,7 +587,7 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
     k_chunked(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks, const int64_t* __restrict__ ptr,
               const int32_t* __restrict__ idx, const T* __restrict__ val, const int32_t* __restrict__ rowmap,
               const T* xsrc, T* out, const T* __restrict__ aux, int64_t ld, double* __restrict__ part,
-              int32_t kcols, int nsub) {
+              int32_t kcols, int nsub, const T* __restrict__ dlast = nullptr) {
     __shared__ int32_t s_idx[CH_WARPS][CHUNK_CAP];
     __shared__ T s_val[CH_WARPS][CHUNK_CAP];
     __shared__ int32_t s_ptr[CH_WARPS][CHUNK_ROWS + 1];
@@ -636,7 +641,8 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
 #pragma unroll
                     for (int u = 0; u < GATHER_UNROLL; u += 2 * h) a[u] += a[u + h];
                 const int64_t row = r0 + rr;
-                chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[row] : row, col, a[0], dot, want_dot);
+                chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[row] : row, col, a[0], dot, want_dot,
+                                        dlast);
             }
             __syncwarp();
         } else {
@@ -654,7 +660,8 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
 #pragma unroll
             for (int o = W; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
             if (lane < W)
-                chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[r0] : r0, col, acc, dot, want_dot);
+                chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[r0] : r0, col, acc, dot, want_dot,
+                                        dlast);
         }
     }
     if (want_dot) {
@@ -865,110 +872,11 @@ __global__ void __launch_bounds__(RUN_THREADS) k_trsv_run(int64_t n, const int32
 // The rows of a factor's last level are read by no later forward level, and their columns of L are empty
 // (nothing is eliminated after them; a level's rows never reference each other), so the backward solve's
 // whole work on them is z_u = y_u / D_u - 0.  When the last level is a level of its own (not part of a
-// thin-level run) the forward solve of that level does this too and the backward launch of the level is
-// skipped; each value is formed by the same operations in the same order as in the two launches.
-// The truncated factor's remainder level is the case that matters: at ER n = 1M it holds 855K of the 1M
-// rows, 3.3 entries each, all pointing at eliminated rows (L2-resident).  The chunk walk there does one
-// row after another -- a gather batch, then the row's r load -- and stays latency-bound.  Here a warp takes
-// several rows at once (LastRows): one coalesced load brings their entry lists, then every row's r value and
-// first four gathers are issued before any is used, several times the loads in flight.  Each row's sum is
-// the chunk walk's own (four accumulators, entries round-robin while four remain, the rest into the first,
-// summed pairwise), so the result is bit-identical.  Lane = column of the tile (TILE columns).
-// rows per warp: 3 in FP64 (4 spill at the 80 registers three resident blocks allow), 4 in FP32
-template <class T>
-struct LastRows { static constexpr int value = sizeof(T) == 8 ? 3 : 4; };
-constexpr int LAST_THREADS = 256;
-constexpr int LAST_MAX_AVG_ENTRIES = 16;  // longer rows keep the chunk walk (and the separate backward launch)
-
-template <class T>
-__global__ void __launch_bounds__(LAST_THREADS, 3)
-    k_fwd_last(int64_t n, int32_t s0, int32_t s1, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-               const T* __restrict__ val, const int32_t* __restrict__ rowmap, const T* __restrict__ rsrc, T* y,
-               const T* __restrict__ D, int32_t kcols) {
-    constexpr unsigned FULL = 0xffffffffu;
-    constexpr int LAST_ROWS = LastRows<T>::value;
-    const int lane = threadIdx.x & 31;
-    const int64_t t = blockIdx.y;
-    const int64_t toff = t * n * TILE;
-    const T* yt = y + toff;
-    const bool live = t * TILE + lane < kcols;
-    const int64_t step = (int64_t)gridDim.x * (LAST_THREADS / 32) * LAST_ROWS;
-    for (int64_t g = s0 + ((int64_t)blockIdx.x * (LAST_THREADS / 32) + (threadIdx.x >> 5)) * LAST_ROWS; g < s1;
-         g += step) {
-        const int nr = (int)min((int64_t)LAST_ROWS, (int64_t)s1 - g);
-        const int64_t pb = lane <= nr ? ptr[g + lane] : 0;
-        const int32_t ub = lane < nr ? rowmap[g + lane] : 0;
-        const int64_t e_lo = __shfl_sync(FULL, pb, 0);
-        const int64_t ne = __shfl_sync(FULL, pb, nr) - e_lo;
-        int32_t my_i = 0;
-        T my_v = 0;
-        if (lane < ne) {
-            my_i = __ldcs(idx + e_lo + lane);
-            my_v = __ldcs(val + e_lo + lane);
-        }
-        // entry q of the group (warp-uniform q): from the coalesced load, past the first 32 from memory
-        auto col_of = [&](int32_t q) -> int32_t {
-            int32_t c = __shfl_sync(FULL, my_i, q & 31);
-            if (q >= 32) c = __ldcs(idx + e_lo + q);
-            return c;
-        };
-        auto val_of = [&](int32_t q) -> T {
-            T v = __shfl_sync(FULL, my_v, q & 31);
-            if (q >= 32) v = __ldcs(val + e_lo + q);
-            return v;
-        };
-        int32_t b[LAST_ROWS + 1];
-#pragma unroll
-        for (int rr = 0; rr <= LAST_ROWS; rr++) b[rr] = (int32_t)(__shfl_sync(FULL, pb, min(rr, nr)) - e_lo);
-        int32_t u[LAST_ROWS];
-        T rv[LAST_ROWS], gv[LAST_ROWS][4];
-#pragma unroll
-        for (int rr = 0; rr < LAST_ROWS; rr++) {
-            u[rr] = __shfl_sync(FULL, ub, rr);
-            rv[rr] = rr < nr ? rsrc[toff + (int64_t)u[rr] * TILE + lane] : (T)0;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int32_t q = b[rr] + j;
-                const bool has = q < b[rr + 1];
-                const int32_t c = has ? col_of(q) : 0;
-                gv[rr][j] = has && live ? yt[(int64_t)c * TILE + lane] : (T)0;
-            }
-        }
-#pragma unroll
-        for (int rr = 0; rr < LAST_ROWS; rr++) {
-            if (rr >= nr) break;
-            const int32_t q0 = b[rr], q1 = b[rr + 1];
-            T a[4] = {0, 0, 0, 0};
-            if (q1 - q0 >= 4) {
-#pragma unroll
-                for (int j = 0; j < 4; j++) a[j] += val_of(q0 + j) * gv[rr][j];
-                int32_t q = q0 + 4;
-                for (; q + 3 < q1; q += 4) {
-                    T g4[4];
-#pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const int32_t c = col_of(q + j);
-                        g4[j] = live ? yt[(int64_t)c * TILE + lane] : (T)0;
-                    }
-#pragma unroll
-                    for (int j = 0; j < 4; j++) a[j] += val_of(q + j) * g4[j];
-                }
-                for (; q < q1; q++) {
-                    const int32_t c = col_of(q);
-                    a[0] += val_of(q) * (live ? yt[(int64_t)c * TILE + lane] : (T)0);
-                }
-            } else {
-#pragma unroll
-                for (int j = 0; j < 3; j++)
-                    if (q0 + j < q1) a[0] += val_of(q0 + j) * gv[rr][j];
-            }
-            const T acc = live ? (a[0] + a[1]) + (a[2] + a[3]) : (T)0;
-            const T yu = rv[rr] - acc;  // the forward solve's value
-            const T d = D[u[rr]];
-            y[toff + (int64_t)u[rr] * TILE + lane] = (d != (T)0 ? yu / d : yu) - (T)0;  // the backward solve's, empty column
-        }
-    }
-}
+// thin-level run), its forward launch (M_FWD_LAST) does this too and its backward launch is skipped; each
+// value is formed by the same operations in the same order as in the two launches.  At ER n = 1M the
+// truncated factor's last level holds 855K of the 1M rows, and its backward launch took 5.5 ms of a 21 ms
+// application.  (A kernel that gave each warp several of these short rows at once, with all their loads
+// issued first, ran slower than this chunk walk: 28.8 against 20.8 ms per application.)
 
 // ---------------------------------------------------------------- preconditioner as a CUDA graph
 // values of the factor in the precision of the solve (the structure is shared)
@@ -1013,14 +921,12 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
             seg.push_back({l++, -1});
         }
     }
-    // the last level finished by the forward solve (k_fwd_last) when it is a level of its own with short rows
-    const int32_t L_last = F.num_levels - 1;
-    const int64_t last_rows = L_last >= 0 ? F.level_ptr[L_last + 1] - F.level_ptr[L_last] : 0;
+    // the last level finished by its forward launch (M_FWD_LAST) when it is a level of its own;
     // SSP_PRECOND_FUSE_LAST=0 keeps the level's two launches (the same values, bit for bit; for comparisons)
+    const int32_t L_last = F.num_levels - 1;
     const char* fuse_env = getenv("SSP_PRECOND_FUSE_LAST");
     const bool fuse_last = !(fuse_env && fuse_env[0] == '0') && !seg.empty() && seg.back().second < 0 &&
-                           F.last_bwd_nnz == 0 && last_rows > 0 && F.last_fwd_nnz >= 0 &&
-                           F.last_fwd_nnz <= LAST_MAX_AVG_ENTRIES * last_rows;
+                           F.last_bwd_nnz == 0 && L_last >= 0;
     auto level = [&](bool fwd, int32_t l) {
         const auto& lvl = fwd ? F.fchunk_lvl : F.bchunk_lvl;
         const int32_t c0 = lvl[l], nc = lvl[l + 1] - c0;
@@ -1028,7 +934,14 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
         const bool split = narrow || F.level_ptr[l + 1] - F.level_ptr[l] <= SPLIT_LEVEL_ROWS;
         const dim3 grid((unsigned)chunk_blocks(nc), (unsigned)(split ? ntiles * nsub : ntiles));
         const int32_t* ch = (fwd ? F.fchunk : F.bchunk) + c0;
-        if (fwd && split)
+        const bool last = fwd && fuse_last && l == L_last;
+        if (last && split)
+            k_chunked<M_FWD_LAST, T, NARROW_W, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
+                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, nsub, V.D);
+        else if (last)
+            k_chunked<M_FWD_LAST, T, TILE, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
+                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, 1, V.D);
+        else if (fwd && split)
             k_chunked<M_FWD, T, NARROW_W, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
                 n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, nsub);
         else if (fwd)
@@ -1044,15 +957,6 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
     };
     const unsigned rgrid = (unsigned)(ntiles * nsub);
     for (size_t i = 0; i < seg.size(); i++) {
-        if (fuse_last && i + 1 == seg.size()) {
-            const int64_t groups = ceil_div<int64_t>(last_rows, (int64_t)(LAST_THREADS / 32) * LastRows<T>::value);
-            const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(groups, 148 * 4)), (unsigned)ntiles);
-            k_fwd_last<T><<<grid, LAST_THREADS, 0, C.stream>>>(n, F.level_ptr[L_last], F.level_ptr[L_last + 1],
-                                                               F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, r,
-                                                               y, V.D, kcols);
-            launches++;
-            continue;
-        }
         if (seg[i].second < 0) {
             level(true, seg[i].first);
             continue;
@@ -1064,7 +968,7 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
         launches++;
     }
     for (size_t i = seg.size(); i-- > 0;) {
-        if (fuse_last && i + 1 == seg.size()) continue;  // finished by k_fwd_last
+        if (fuse_last && i + 1 == seg.size()) continue;  // finished by its forward launch (M_FWD_LAST)
         if (seg[i].second < 0) {
             level(false, seg[i].first);
             continue;

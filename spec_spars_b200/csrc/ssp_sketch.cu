@@ -49,13 +49,14 @@ __global__ void __launch_bounds__(256) k_sketch_sign(int64_t n, int64_t v0, int6
                 const uint64_t q2 = __shfl_sync(0xffffffffu, r2, i);
                 const uint64_t q3 = __shfl_sync(0xffffffffu, r3, i);
                 const double bi = __shfl_sync(0xffffffffu, b, i);
+                // (+-scale) * b_ev is +-(scale * b_ev) exactly (negation is exact): one product per edge
+                const double sb = __dmul_rn(scale, bi);
                 const uint64_t words[4] = {q0, q1, q2, q3};
 #pragma unroll
                 for (int t = 0; t < 8; t++) {
                     // column c = lane + 32 t inside the tile: word t>>1, bit lane + 32 (t & 1)
                     const uint64_t bit = (words[t >> 1] >> (lane + 32 * (t & 1))) & 1ull;
-                    const double hs = bit ? -scale : scale;
-                    acc[t] = __dadd_rn(acc[t], __dmul_rn(hs, bi));
+                    acc[t] = __dadd_rn(acc[t], bit ? -sb : sb);
                 }
             }
         }

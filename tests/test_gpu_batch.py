@@ -15,10 +15,10 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-8
 
 
-def _prm(ssp, eps, seed, mixed=False):
+def _prm(ssp, eps, seed, mixed=False, max_degree=24):
     p = ssp.SparsifierParameters.baseline(eps, pcg_tol=1e-8, sampling_seed=seed, sketch_seed=seed + 7)
-    p.dense_threshold = 0      # complete elimination in the sparse phase: what a batch runs
-    p.factor_max_degree = 0
+    p.dense_threshold = 0           # no dense tail: a batch eliminates in the sparse phase
+    p.factor_max_degree = max_degree  # a fixed truncation, applied graph by graph (0: complete elimination)
     if mixed:
         p.precision = ssp.SSP_PRECISION_MIXED
     return p
@@ -36,9 +36,12 @@ def _close(H, H0):
     np.testing.assert_allclose(H.values, H0.values, rtol=RTOL, atol=0)
 
 
-def test_batch_equals_each_graph_alone(ssp, ctx):
+@pytest.mark.parametrize("max_degree", [24, 0, 6])
+def test_batch_equals_each_graph_alone(ssp, ctx, max_degree):
+    """Truncated at average live degree 24 (graphs stop at different levels), 6 (early), or eliminated
+    completely (0)."""
     graphs = _graphs(ssp)
-    params = [_prm(ssp, [0.5, 0.3][i % 2], i) for i in range(len(graphs))]
+    params = [_prm(ssp, [0.5, 0.3][i % 2], i, max_degree=max_degree) for i in range(len(graphs))]
     got = ctx.sparsify_batch(graphs, params)
     assert len(got) == len(graphs)
     for G, prm, (H, st) in zip(graphs, params, got):
@@ -47,6 +50,7 @@ def test_batch_equals_each_graph_alone(ssp, ctx):
         assert st["n"] == G.n and st["m_in"] == st0["m_in"] and st["m_out"] == st0["m_out"]
         assert st["k"] == st0["k"]
         assert abs(st["pcg_max_iters_used"] - st0["pcg_max_iters_used"]) <= 1
+        assert st["factor_max_degree_used"] == st0["factor_max_degree_used"] == max_degree
         assert st["pcg_max_relres"] < 1e-7
 
 
@@ -67,7 +71,7 @@ def test_mixed_precision_batch_meets_the_tolerance(ssp, ctx):
 
 
 def test_batch_of_one_and_a_dense_graph_really_sparsifies(ssp, ctx):
-    G = ssp.gen_er(800, 200.0, 0.5, 2.0, 9)
+    G = ssp.gen_er(2000, 400.0, 0.5, 2.0, 7)
     prm = _prm(ssp, 0.5, 4)
     (H, st), = ctx.sparsify_batch([G], prm)
     H0, st0 = ctx.sparsify(G, prm)
@@ -83,7 +87,11 @@ def test_batch_rejects_mixed_options(ssp, ctx):
         ctx.sparsify_batch([a, b], [p, q])
     r = _prm(ssp, 0.5, 3)
     r.factor_max_degree = -1
-    with pytest.raises(ssp.SspError, match="complete sparse elimination"):
+    with pytest.raises(ssp.SspError, match="fixed truncation"):
+        ctx.sparsify_batch([a], [r])
+    r = _prm(ssp, 0.5, 3)
+    r.dense_threshold = 4096
+    with pytest.raises(ssp.SspError, match="fixed truncation"):
         ctx.sparsify_batch([a], [r])
 
 
