@@ -302,16 +302,12 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-# the truncation of the serving mix's factors (the autotuner picks 26 to 31 on its ER and RGG graphs)
-SERVE_MAX_DEGREE = 28
-
-
 def serving_mix(S, count, max_n, seed=4, precision="fp64"):
     """The serving mix of seeded requests: random-geometric or ER graphs (equiprobable), n log-uniform in
     [1e3, max_n], average degree uniform in 8..32, weights uniform [0.1, 10] rounded to FP32, eps 0.3 or 0.5.
-    Every request asks for sparse-phase elimination truncated at average live degree SERVE_MAX_DEGREE
-    (dense_threshold = 0, a fixed factor_max_degree), so the server may batch it; the plain path runs the same
-    parameters one request at a time."""
+    Every request asks for the autotuned factor without the dense tail (factor_max_degree = -1,
+    dense_threshold = 0), so the server may batch it; the plain path runs the same parameters one request at a
+    time."""
     import numpy as np
     rng = np.random.default_rng(seed)
     reqs = []
@@ -322,7 +318,7 @@ def serving_mix(S, count, max_n, seed=4, precision="fp64"):
         G = S.gen_rgg(n, d, 0.1, 10.0, 1000 + i) if rng.random() < 0.5 else S.gen_er(n, d, 0.1, 10.0, 1000 + i)
         prm = S.SparsifierParameters.baseline(eps, pcg_tol=PCG_TOL, sampling_seed=i)
         prm.dense_threshold = 0
-        prm.factor_max_degree = SERVE_MAX_DEGREE
+        prm.factor_max_degree = -1
         if precision == "mixed":
             prm.precision = S.SSP_PRECISION_MIXED
         reqs.append((G, prm))
@@ -373,7 +369,8 @@ def serve_measure(S, reqs, slots, max_batch, rate_frac=0.8, seed=5):
 
 
 def plain_measure(S, reqs):
-    """The plain single-graph path: each request alone through ssp_sparsify on one context, back to back."""
+    """The plain single-graph path: each request alone through ssp_sparsify on one context, back to back (the
+    same parameters; with the default dense tail as well, reported beside)."""
     ctx = S.Context(0)
     try:
         ctx.sparsify(*reqs[0])  # warm-up
@@ -392,15 +389,21 @@ def serving_section(S, count, max_n, slots=2, max_batch=64):
     reqs = serving_mix(S, count, max_n)
     m_total = sum(G.nnz // 2 for G, _ in reqs)
     plain = plain_measure(S, reqs)
+    # the library's default single-graph parameters (autotuned factor with the dense tail)
+    plain_default = plain_measure(S, [(G, S.SparsifierParameters.baseline(p.epsilon, pcg_tol=PCG_TOL,
+                                                                          sampling_seed=p.sampling_seed))
+                                      for G, p in reqs])
     slots_only = serve_measure(S, reqs, 4, 1)
     batched = serve_measure(S, reqs, slots, max_batch)
     batched_mixed = serve_measure(S, serving_mix(S, count, max_n, precision="mixed"), slots, max_batch)
     return {"workload": "serving mix", "requests": count, "n_range": [1000, max_n], "degree_range": [8, 32],
             "eps": [0.3, 0.5], "edges": m_total,
-            "plain_fp64_edges_per_s": plain, "served_slots_only_fp64": slots_only,
+            "plain_fp64_edges_per_s": plain, "plain_fp64_default_params_edges_per_s": plain_default,
+            "served_slots_only_fp64": slots_only,
             "served_batched_fp64": batched, "served_batched_mixed": batched_mixed,
             "batched_mixed_over_plain": batched_mixed["value"] / plain,
-            "batched_fp64_over_plain": batched["value"] / plain}
+            "batched_fp64_over_plain": batched["value"] / plain,
+            "batched_mixed_over_plain_default": batched_mixed["value"] / plain_default}
 
 
 def run_serve(args):

@@ -235,9 +235,10 @@ int ssp_csc_free(ssp_csc_out* out);
  * rule, scale and seeds, variance correction, output_file), and every PCG scalar is kept per (graph,
  * column), so outs[b] equals ssp_sparsify of graph b alone to the solve's rounding (the kept edges match
  * unless a coin falls within that rounding of its probability).  The batch must agree on factor_seed,
- * precision, pcg_tol, pcg_abs_tol, pcg_max_iters, reweight and factor_max_degree, which must be a fixed value
- * (>= 0: each graph is truncated by its own test, as alone; the autotuner's -1 is refused), and use
- * dense_threshold = 0 (the dense tail looks at the whole Schur complement and would couple the graphs).
+ * precision, pcg_tol, pcg_abs_tol, pcg_max_iters and reweight, and use dense_threshold = 0 (the dense tail
+ * looks at the whole Schur complement and would couple the graphs).  factor_max_degree is per graph: each is
+ * truncated by its own test, and -1 applies the autotuner's rule to it alone (light truncation unless its
+ * probe predicts more than 30 iterations), as a lone call with the same parameters does.
  * outs[b] is host memory (free with ssp_csc_free);
  * stats[b] has graph b's sizes and PCG figures, and the batch's stage times. */
 int ssp_sparsify_batch(ssp_context* ctx, int32_t count, const ssp_csc* graphs, const ssp_params* params,
@@ -276,8 +277,7 @@ int ssp_shard_finish(ssp_context* ctx, const ssp_csc* graph, const ssp_params* p
  * hbm_budget_bytes (a younger one may go first while the oldest has waited less than 500 ms; after that the
  * oldest is admitted first); a request whose footprint alone exceeds the budget is refused at submit
  * (SSP_ERR_CAPACITY).  The slot then adds pending requests that can share its run (same epsilon, factor
- * seed, precision, PCG options, reweighting and fixed factor_max_degree >= 0, and dense_threshold = 0), up to
- * max_batch
+ * seed, precision, PCG options and reweighting, and dense_threshold = 0), up to max_batch
  * and its share of the budget, and runs them with ssp_sparsify_batch; other requests run exactly
  * ssp_sparsify, so their result is the same as a lone call's.  Results are collected once with ssp_wait /
  * ssp_poll (which then own res->out: free it with ssp_csc_free). */

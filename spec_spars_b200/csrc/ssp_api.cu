@@ -606,8 +606,12 @@ static const T* stage_in(Context& C, const T* p, int64_t cnt, int32_t mem, const
 //   * Graph b's vertices are [V_b, V_b + n_b) of the union and its edges [E_b, E_b + m_b) (the union's CSC
 //     keeps each graph's columns together, and edges are extracted in CSC order).
 //   * Its sketch uses its own seed, scale, k_b and edge ids counted from E_b; its factor draws are keyed by
-//     in-graph vertex ids, and each graph is truncated by its own live-entry test, so both equal the lone
-//     run's.  There is no dense tail (it looks at the whole Schur complement and would couple the graphs).
+//     in-graph vertex ids, and each graph is truncated by its own live-entry test at its own degree, so both
+//     equal the lone run's.  A graph that asks for the autotuner (factor_max_degree = -1) gets the lone rule
+//     graph by graph: the union is factored with every such graph at its light truncation, one 20-iteration
+//     probe runs on the first columns with a residual history per graph, and the graphs predicted to need more
+//     than 30 iterations are factored completely (the union is factored again).  There is no dense tail (it
+//     looks at the whole Schur complement and would couple the graphs).
 //   * The PCG keeps every scalar per (graph, column) (PcgSegments), so each graph's iterates are its own;
 //     its reductions are blocked differently from a lone run's, so a served result equals the lone result
 //     to the solve's rounding, not bit for bit.
@@ -638,7 +642,7 @@ __global__ void k_vertex_graph(int64_t n, const int64_t* __restrict__ V, int32_t
 static bool same_batch_options(const ssp_params& a, const ssp_params& b) {
     return a.factor_seed == b.factor_seed && a.precision == b.precision && a.pcg_tol == b.pcg_tol &&
            a.pcg_abs_tol == b.pcg_abs_tol && a.pcg_max_iters == b.pcg_max_iters && a.reweight == b.reweight &&
-           a.dense_threshold == b.dense_threshold && a.factor_max_degree == b.factor_max_degree;
+           a.dense_threshold == b.dense_threshold;
 }
 
 static void sparsify_batch_impl(Context& C, int32_t count, const ssp_csc* graphs, const ssp_params* prms,
@@ -656,10 +660,10 @@ static void sparsify_batch_impl(Context& C, int32_t count, const ssp_csc* graphs
         SSP_REQUIRE(g.colptr[0] == 0 && g.colptr[g.n] == g.nnz, SSP_ERR_INVALID, "batch: colptr must run 0 .. nnz");
         SSP_REQUIRE(p.epsilon > 0 && std::isfinite(p.epsilon), SSP_ERR_INVALID, "batch: epsilon must be positive");
         SSP_REQUIRE(same_batch_options(p, p0), SSP_ERR_INVALID,
-                    "batch: factor seed, precision, PCG options, reweighting and factor options must agree");
-        SSP_REQUIRE(p.dense_threshold == 0 && p.factor_max_degree >= 0, SSP_ERR_INVALID,
-                    "batch: the graphs must ask for sparse-phase elimination with a fixed truncation "
-                    "(dense_threshold = 0, factor_max_degree >= 0)");
+                    "batch: factor seed, precision, PCG options and reweighting must agree");
+        SSP_REQUIRE(p.dense_threshold == 0 && p.factor_max_degree >= -1, SSP_ERR_INVALID,
+                    "batch: the graphs must ask for sparse-phase elimination (dense_threshold = 0, "
+                    "factor_max_degree >= 0, or -1 for the autotuner)");
         // edges: upper entries with a non-zero value (sparsifier.rs:365), in CSC order
         int64_t m = 0;
         for (int64_t j = 0; j < g.n; j++)
@@ -724,18 +728,63 @@ static void sparsify_batch_impl(Context& C, int32_t count, const ssp_csc* graphs
     FactorOptions fo;
     fo.seed = p0.factor_seed;
     fo.dense_threshold = 0;
-    fo.max_degree = p0.factor_max_degree;
+    fo.max_degree = 0;
     fo.vbase = vbase;
     fo.vseg = rowseg;
     fo.seg_row0 = V;
-    factor_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, fo, F, "bt_f");
-    T.mark();  // 3
     PcgOptions po;
     po.tol = p0.pcg_tol;
     po.abs_tol = p0.pcg_abs_tol;
     po.max_iters = p0.pcg_max_iters;
     po.verbose = p0.verbose;
     po.precision = p0.precision;
+    // each graph's truncation: its own, or the autotuner's light degree to be probed
+    std::vector<int64_t> maxdeg(count);
+    bool tune = false;
+    for (int32_t b = 0; b < count; b++) {
+        tune = tune || prms[b].factor_max_degree < 0;
+        maxdeg[b] = prms[b].factor_max_degree >= 0 ? prms[b].factor_max_degree
+                                                    : autotune_light_degree(V[b + 1] - V[b], 2 * (E[b + 1] - E[b]));
+    }
+    fo.seg_max_degree = maxdeg;
+    factor_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, fo, F, "bt_f");
+    if (tune) {
+        // the autotuner's probe, graph by graph (autotune_factor): 20 FP64 iterations on the first columns
+        PcgOptions pp = po;
+        pp.tol = 0.0;
+        pp.abs_tol = 0.0;
+        pp.max_iters = SSP_TUNE_PROBE_ITERS;
+        pp.verbose = 0;
+        pp.precision = SSP_PRECISION_FP64;
+        PcgSegments ps;
+        ps.row0 = V;
+        ps.rowseg = rowseg;
+        ps.record_history = true;
+        int32_t kp = 1;
+        for (int32_t b = 0; b < count; b++) {
+            ps.k.push_back(std::min<int32_t>(k[b], SSP_PROBE_COLS));
+            kp = std::max(kp, ps.k.back());
+        }
+        pp.segs = &ps;
+        PcgReport pr;
+        pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, kp, nullptr, pp, pr);
+        bool again = false;
+        for (int32_t b = 0; b < count; b++) {
+            if (prms[b].factor_max_degree >= 0) continue;
+            const std::vector<double> none;
+            const double iters = autotune_predicted_iters(b < (int32_t)ps.history.size() ? ps.history[b] : none,
+                                                          po.tol);
+            if (!(iters <= SSP_TUNE_MAX_ITERS)) {
+                maxdeg[b] = 0;
+                again = true;
+            }
+        }
+        if (again) {
+            fo.seg_max_degree = maxdeg;
+            factor_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, fo, F, "bt_f");
+        }
+    }
+    T.mark();  // 3
     PcgSegments segs;
     segs.row0 = V;
     segs.k = k;
@@ -820,7 +869,7 @@ static void sparsify_batch_impl(Context& C, int32_t count, const ssp_csc* graphs
             // the batch's shared figures: every graph of the batch reports the same stage times and factor
             st.nnz_factor = F.nnz;
             st.factor_levels = F.num_levels;
-            st.factor_max_degree_used = p0.factor_max_degree;
+            st.factor_max_degree_used = maxdeg[b];
             st.ms_assembly = T.ms(0, 1);
             st.ms_sketch = T.ms(1, 2);
             st.ms_factor = T.ms(2, 3);

@@ -18,14 +18,35 @@
 
 namespace ssp {
 
-constexpr int TUNE_PROBE_ITERS = 20;
-constexpr double TUNE_MAX_ITERS = 30.0;
+constexpr int TUNE_PROBE_ITERS = SSP_TUNE_PROBE_ITERS;
+constexpr double TUNE_MAX_ITERS = SSP_TUNE_MAX_ITERS;
+
+int64_t autotune_light_degree(int64_t n, int64_t lap_offdiag_nnz) {
+    const double d0 = n > 0 ? (double)lap_offdiag_nnz / (double)n : 0.0;
+    return (int64_t)std::ceil(1.05 * d0) + 1;
+}
+
+double autotune_predicted_iters(const std::vector<double>& hist, double tol) {
+    const double tol_rel = tol > 0 ? tol : 1e-6;
+    double iters = 1e9;
+    const size_t h = hist.size();
+    if (h >= 2 && hist.back() <= tol_rel) {
+        iters = (double)h;  // converged within the probe
+    } else if (h >= 4) {
+        const size_t a = h / 2;
+        const double r0 = hist[a - 1], r1 = hist[h - 1];
+        if (r0 > 0 && r1 > 0 && r1 < r0) {
+            const double rho = std::pow(r1 / r0, 1.0 / (double)(h - a));
+            iters = (double)h + std::log(tol_rel / r1) / std::log(rho);
+        }
+    }
+    return iters;
+}
 
 int64_t autotune_factor(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx, const double* lap_val,
                         int64_t lap_offdiag_nnz, const double* Ytiles, int32_t k, const FactorOptions& base,
                         const PcgOptions& popt, DevFactor& F, double* ms_tuning) {
-    const double d0 = n > 0 ? (double)lap_offdiag_nnz / (double)n : 0.0;
-    const int64_t light = (int64_t)std::ceil(1.05 * d0) + 1;
+    const int64_t light = autotune_light_degree(n, lap_offdiag_nnz);
     cudaEvent_t e0, e1;
     SSP_CUDA(cudaEventCreate(&e0));
     SSP_CUDA(cudaEventCreate(&e1));
@@ -44,19 +65,7 @@ int64_t autotune_factor(Context& C, int64_t n, const int64_t* lap_ptr, const int
     PcgReport rep;
     const int32_t kp = std::min<int32_t>(k, SSP_PROBE_COLS);
     pcg_device(C, n, lap_ptr, lap_idx, lap_val, F, Ytiles, kp, nullptr, po, rep);
-    const double tol_rel = popt.tol > 0 ? popt.tol : 1e-6;
-    double iters = 1e9;
-    const size_t h = hist.size();
-    if (h >= 2 && hist.back() <= tol_rel) {
-        iters = (double)h;  // converged within the probe
-    } else if (h >= 4) {
-        const size_t a = h / 2;
-        const double r0 = hist[a - 1], r1 = hist[h - 1];
-        if (r0 > 0 && r1 > 0 && r1 < r0) {
-            const double rho = std::pow(r1 / r0, 1.0 / (double)(h - a));
-            iters = (double)h + std::log(tol_rel / r1) / std::log(rho);
-        }
-    }
+    const double iters = autotune_predicted_iters(hist, popt.tol);
     int64_t chosen = light;
     if (!(iters <= TUNE_MAX_ITERS)) {
         chosen = 0;

@@ -1083,13 +1083,19 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
     F.vbase = opt.vbase;
     // the dense tail looks at the whole Schur complement and would couple several graphs: a union is
     // eliminated in the sparse phase, and truncated graph by graph (vseg)
-    SSP_REQUIRE(!opt.vbase || (opt.dense_threshold == 0 && opt.max_degree >= 0 && (opt.max_degree == 0 || opt.vseg)),
-                SSP_ERR_INVALID, "factor: several graphs at once need dense_threshold = 0 and max_degree >= 0 "
-                                 "(with the graph of every vertex when truncating)");
     const bool seg_mode = opt.vseg != nullptr;
     const int32_t nseg = seg_mode ? (int32_t)opt.seg_row0.size() - 1 : 0;
-    SSP_REQUIRE(!seg_mode || (nseg >= 1 && opt.seg_row0.front() == 0 && opt.seg_row0.back() == n), SSP_ERR_INVALID,
-                "factor: inconsistent graph ranges");
+    SSP_REQUIRE(!opt.vbase || (opt.dense_threshold == 0 && (opt.max_degree == 0 || seg_mode)), SSP_ERR_INVALID,
+                "factor: several graphs at once need dense_threshold = 0 (and the graph of every vertex when "
+                "truncating)");
+    SSP_REQUIRE(!seg_mode || (nseg >= 1 && opt.seg_row0.front() == 0 && opt.seg_row0.back() == n &&
+                              (opt.seg_max_degree.empty() || (int32_t)opt.seg_max_degree.size() == nseg)),
+                SSP_ERR_INVALID, "factor: inconsistent graph ranges");
+    std::vector<int64_t> g_maxdeg(nseg);
+    for (int32_t g = 0; g < nseg; g++) {
+        g_maxdeg[g] = opt.seg_max_degree.empty() ? opt.max_degree : opt.seg_max_degree[g];
+        SSP_REQUIRE(g_maxdeg[g] >= 0, SSP_ERR_INVALID, "factor: a graph's truncation must be >= 0");
+    }
     F.vseg = opt.vseg;
     F.nseg = nseg;
     F.gctr = seg_mode ? W.get_t<int64_t>(nm("gctr"), 3 * (size_t)nseg) : nullptr;
@@ -1242,11 +1248,12 @@ void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* 
                 if (g_prev[g] >= 0) g_live[g] += 2 * g_cnt[3 * g + GC_NFILL] - 2 * g_prev[g];
         }
         if (nf == 0) break;
-        if (seg_mode && opt.max_degree > 0) {
+        if (seg_mode) {
             std::vector<int32_t> stop;
             for (int32_t g = 0; g < nseg; g++) {
                 const int64_t ng = opt.seg_row0[g + 1] - opt.seg_row0[g];
-                if (!g_stopped[g] && g_cnt[3 * g + GC_NFRONT] > 0 && g_live[g] > opt.max_degree * (ng - g_elim[g]))
+                if (!g_stopped[g] && g_maxdeg[g] > 0 && g_cnt[3 * g + GC_NFRONT] > 0 &&
+                    g_live[g] > g_maxdeg[g] * (ng - g_elim[g]))
                     stop.push_back(g);
             }
             if (!stop.empty()) {

@@ -379,6 +379,7 @@ struct FactorOptions {
     const int32_t* vseg = nullptr;   // device [n]: graph of each vertex; with max_degree > 0 each graph is
                                      // truncated by its own test, at the level where it would stop alone
     std::vector<int64_t> seg_row0;   // host: nseg + 1 first vertices of the graphs (with vseg)
+    std::vector<int64_t> seg_max_degree;  // host: each graph's own truncation (with vseg; empty: max_degree)
 };
 // Input: Laplacian CSC on device (rows > col used, |value| as weight).
 void factor_device(Context& C, int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,
@@ -395,6 +396,10 @@ struct PcgSegments {
     const int32_t* rowseg = nullptr;  // device [n]: graph of each row
     std::vector<int32_t> iters;       // out
     std::vector<double> relres;       // out
+    // with record_history: per graph, per iteration, the largest ||r|| / ||b|| over its columns (the autotuner's
+    // probe, graph by graph)
+    bool record_history = false;
+    std::vector<std::vector<double>> history;
 };
 struct PcgOptions {
     double tol = 1e-8;
@@ -429,6 +434,13 @@ struct PcgReport {
 int64_t autotune_factor(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx,
                         const double* lap_val, int64_t lap_offdiag_nnz, const double* Ytiles, int32_t k,
                         const FactorOptions& base, const PcgOptions& popt, DevFactor& F, double* ms_tuning);
+// The autotuner's rule, its pieces shared by the single-graph and the batched autotuning: the lightest
+// truncation for a graph of n vertices and lap_offdiag_nnz off-diagonal Laplacian entries, and the
+// iterations to the tolerance predicted from a probe's residual history (1e9: no prediction).
+int64_t autotune_light_degree(int64_t n, int64_t lap_offdiag_nnz);
+double autotune_predicted_iters(const std::vector<double>& hist, double tol);
+constexpr int32_t SSP_TUNE_PROBE_ITERS = 20;
+constexpr double SSP_TUNE_MAX_ITERS = 30.0;
 // With lap_eid (the graph's per-entry edge map) and d2 (m doubles), the final product A x also forms
 // d2[e] = sum over columns of (x[v1_e] - x[v2_e])^2 in the order of diff_norms_device (per 32-column tile a
 // butterfly over the tile's columns, tiles added in order) from the rows it gathers anyway, and sets

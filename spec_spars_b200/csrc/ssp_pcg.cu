@@ -1247,7 +1247,8 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         const char* e = getenv("SSP_PCG_HOST_LOOP");
         return e && e[0] == '1';
     }();
-    const bool device_loop = !opt.history && !opt.verbose && !host_loop;
+    const bool seg_history = opt.segs && opt.segs->record_history;
+    const bool device_loop = !opt.history && !seg_history && !opt.verbose && !host_loop;
     const int64_t ntiles = ld / TILE;
     const int64_t total = n * ld;
     const dim3 egrid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div<int64_t>(n * TILE, 256),
@@ -1288,7 +1289,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         SSP_CHECK_LAUNCH();
         C.kernels_launched++;
         active = read_i64(C, S.nactive);
-        if (opt.history) {
+        if (opt.history || seg_history) {
             std::vector<double> hrr(ns), hbb(ns);
             SSP_CUDA(cudaMemcpyAsync(hrr.data(), S.rr, sizeof(double) * ns, cudaMemcpyDeviceToHost, C.stream));
             SSP_CUDA(cudaMemcpyAsync(hbb.data(), S.bnorm2, sizeof(double) * ns, cudaMemcpyDeviceToHost, C.stream));
@@ -1296,7 +1297,19 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
             double mx = 0.0;
             for (int64_t j = 0; j < ns; j++)
                 if (hbb[j] > 0) mx = std::max(mx, std::sqrt(hrr[j] / hbb[j]));
-            opt.history->push_back(mx);
+            if (opt.history) opt.history->push_back(mx);
+            if (seg_history) {
+                auto& H = opt.segs->history;
+                H.resize(G.nseg);
+                for (int32_t sg = 0; sg < G.nseg; sg++) {
+                    double m2 = 0.0;
+                    for (int64_t j = 0; j < ld; j++) {
+                        const int64_t o = (int64_t)sg * ld + j;
+                        if (hbb[o] > 0) m2 = std::max(m2, std::sqrt(hrr[o] / hbb[o]));
+                    }
+                    H[sg].push_back(m2);
+                }
+            }
         }
         if (opt.verbose && (it % 10 == 0 || active == 0))
             fprintf(stderr, "[ssp] pcg%s iter %d: %lld columns active\n", sizeof(T) == 4 ? " (fp32 inner)" : "", it,

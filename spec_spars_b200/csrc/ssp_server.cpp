@@ -10,8 +10,8 @@
 // served, so a large request is not starved.  A request whose footprint alone exceeds the budget is refused
 // at submit.
 // Batching (continuous): the slot then adds the other pending requests that can share its run -- the same
-// factor seed, precision, PCG options, reweighting and fixed truncation (factor_max_degree >= 0), the same
-// epsilon, and dense_threshold = 0 -- up to max_batch requests and the slot's share of the
+// factor seed, precision, PCG options and reweighting, the same epsilon, and dense_threshold = 0 (each keeps
+// its own truncation, fixed or autotuned) -- up to max_batch requests and the slot's share of the
 // budget, and runs them as one ssp_sparsify_batch: one factorization and one PCG over their disjoint union.
 // Requests that arrive while batches run are picked up by the next free slot, so their work overlaps on the
 // device.  A request that cannot be batched runs the same ssp_sparsify as a lone call; a batched one equals
@@ -103,12 +103,12 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
-bool batchable(const ssp_params& p) { return p.dense_threshold == 0 && p.factor_max_degree >= 0; }
+bool batchable(const ssp_params& p) { return p.dense_threshold == 0 && p.factor_max_degree >= -1; }
 
 bool same_batch(const ssp_params& a, const ssp_params& b) {
     return a.epsilon == b.epsilon && a.factor_seed == b.factor_seed && a.precision == b.precision &&
            a.pcg_tol == b.pcg_tol && a.pcg_abs_tol == b.pcg_abs_tol && a.pcg_max_iters == b.pcg_max_iters &&
-           a.reweight == b.reweight && a.factor_max_degree == b.factor_max_degree && batchable(a) && batchable(b);
+           a.reweight == b.reweight && batchable(a) && batchable(b);
 }
 
 // device footprint of a batch: its union's n x ld blocks use the largest k of the batch for every row

@@ -141,9 +141,13 @@ int64_t read_i64(Context& C, const int64_t* d_ptr) {
     return C.h_pinned[0];
 }
 void read_i64s(Context& C, const int64_t* d_ptr, int64_t* host, int cnt) {
-    SSP_CUDA(cudaMemcpyAsync(C.h_pinned, d_ptr, sizeof(int64_t) * cnt, cudaMemcpyDeviceToHost, C.stream));
-    SSP_CUDA(cudaStreamSynchronize(C.stream));
-    for (int i = 0; i < cnt; i++) host[i] = C.h_pinned[i];
+    constexpr int PINNED = 64;  // entries of the context's pinned scratch
+    for (int i0 = 0; i0 < cnt; i0 += PINNED) {
+        const int c = std::min(PINNED, cnt - i0);
+        SSP_CUDA(cudaMemcpyAsync(C.h_pinned, d_ptr + i0, sizeof(int64_t) * c, cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+        for (int i = 0; i < c; i++) host[i0 + i] = C.h_pinned[i];
+    }
 }
 
 // ---------------------------------------------------------------- segmented sort
