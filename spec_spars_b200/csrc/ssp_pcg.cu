@@ -107,6 +107,28 @@ __device__ __forceinline__ void red_block(const SegDev& G, int64_t n, int64_t ro
     }
 }
 
+// Rows of converged graphs (several graphs at once): act[s * ntiles + t] says whether graph s still has an
+// active column in tile t; the SpMM and the triangular solves skip the rows of inactive (graph, tile) pairs,
+// whose values no active column reads (alpha is 0 there).  A null act (one graph) skips nothing.
+struct RowAct {
+    const int32_t* act = nullptr;
+    const int32_t* rowseg = nullptr;  // graph of each vertex
+    int32_t ntiles = 0;
+};
+__device__ __forceinline__ bool row_on(const RowAct& A, int64_t vertex, int64_t tile) {
+    return !A.act || A.act[(int64_t)A.rowseg[vertex] * A.ntiles + tile];
+}
+__global__ void k_seg_tile_active(int32_t nseg, int32_t ntiles, int64_t ld, const int32_t* __restrict__ active,
+                                  int32_t* __restrict__ act) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)nseg * ntiles;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t sg = i / ntiles, t = i - sg * ntiles;
+        int32_t a = 0;
+        for (int c = 0; c < TILE; c++) a |= active[sg * ld + t * TILE + c];
+        act[i] = a;
+    }
+}
+
 // ---------------------------------------------------------------- column reductions
 enum ColOp { OP_SUM = 0, OP_DOT = 1, OP_SQ = 2, OP_SQDIFF_CENTERED = 3 };
 
@@ -587,7 +609,7 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
     k_chunked(int64_t n, const int32_t* __restrict__ cstart, int32_t nchunks, const int64_t* __restrict__ ptr,
               const int32_t* __restrict__ idx, const T* __restrict__ val, const int32_t* __restrict__ rowmap,
               const T* xsrc, T* out, const T* __restrict__ aux, int64_t ld, double* __restrict__ part,
-              int32_t kcols, int nsub, const T* __restrict__ dlast = nullptr) {
+              int32_t kcols, int nsub, const T* __restrict__ dlast = nullptr, RowAct ra = RowAct()) {
     __shared__ int32_t s_idx[CH_WARPS][CHUNK_CAP];
     __shared__ T s_val[CH_WARPS][CHUNK_CAP];
     __shared__ int32_t s_ptr[CH_WARPS][CHUNK_ROWS + 1];
@@ -618,7 +640,9 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
             const int32_t pairs = (r1 - r0) * W;
             for (int32_t pr = lane; pr < pairs; pr += 32) {
                 const int32_t rr = pr / W, col = c0 + pr % W;
-                const bool live = t * TILE + col < kcols;
+                const int64_t vrow = rowmap ? rowmap[r0 + rr] : r0 + rr;
+                const bool on = row_on(ra, vrow, t);
+                const bool live = on && t * TILE + col < kcols;
                 const int32_t q0 = sp[rr], q1 = live ? sp[rr + 1] : q0;
                 // GATHER_UNROLL independent accumulators, summed as a pairwise tree
                 constexpr int GATHER_UNROLL = SPMM ? SSP_GATHER_UNROLL_SPMM : SSP_GATHER_UNROLL_SOLVE;
@@ -640,15 +664,15 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
                 for (int h = 1; h < GATHER_UNROLL; h <<= 1)
 #pragma unroll
                     for (int u = 0; u < GATHER_UNROLL; u += 2 * h) a[u] += a[u + h];
-                const int64_t row = r0 + rr;
-                chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[row] : row, col, a[0], dot, want_dot,
-                                        dlast);
+                if (on) chunk_epilogue<MODE, T>(out, aux, xt, toff, vrow, col, a[0], dot, want_dot, dlast);
             }
             __syncwarp();
         } else {
             // one long row: (32 / W) entry slots x W columns per step, then a reduction over the slots
             const int slot = lane / W, col = c0 + lane % W;
-            const int64_t qe = t * TILE + col < kcols ? e1 : e0;
+            const int64_t vr0 = rowmap ? rowmap[r0] : r0;
+            const bool on = row_on(ra, vr0, t);
+            const int64_t qe = on && t * TILE + col < kcols ? e1 : e0;
             T a0 = 0, a1 = 0;
             int64_t q = e0 + slot;
             for (; q + SLOTS_W < qe; q += 2 * SLOTS_W) {
@@ -659,9 +683,7 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
             T acc = a0 + a1;
 #pragma unroll
             for (int o = W; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane < W)
-                chunk_epilogue<MODE, T>(out, aux, xt, toff, rowmap ? rowmap[r0] : r0, col, acc, dot, want_dot,
-                                        dlast);
+            if (lane < W && on) chunk_epilogue<MODE, T>(out, aux, xt, toff, vr0, col, acc, dot, want_dot, dlast);
         }
     }
     if (want_dot) {
@@ -835,7 +857,7 @@ __global__ void __launch_bounds__(RUN_THREADS) k_trsv_run(int64_t n, const int32
                                                           const int64_t* __restrict__ ptr,
                                                           const int32_t* __restrict__ idx,
                                                           const T* __restrict__ val, const T* __restrict__ aux, T* y,
-                                                          int32_t kcols, int nsub) {
+                                                          int32_t kcols, int nsub, RowAct ra) {
     __shared__ T s_part[RUN_WARPS][W];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t t = blockIdx.x / nsub;
@@ -848,12 +870,13 @@ __global__ void __launch_bounds__(RUN_THREADS) k_trsv_run(int64_t n, const int32
         if (g <= 1) {
             for (int32_t q = a + warp; q < b; q += RUN_WARPS) {
                 const int32_t i = sched[q];
-                const T acc = warp_row_share<T, W>(ptr, idx, val, i, y + toff + c0, lane, live, 0, 1);
-                if (lane < W) run_finish<T, FWD>(rows, aux, y, toff, c0 + lane, i, acc);
+                const bool on = row_on(ra, rows[i], t);
+                const T acc = warp_row_share<T, W>(ptr, idx, val, i, y + toff + c0, lane, live && on, 0, 1);
+                if (lane < W && on) run_finish<T, FWD>(rows, aux, y, toff, c0 + lane, i, acc);
             }
         } else {
             const int q = warp / g, sub = warp % g;
-            const bool mine = a + q < b;
+            const bool mine = a + q < b && row_on(ra, rows[sched[a + q]], t);
             const T acc = mine ? warp_row_share<T, W>(ptr, idx, val, sched[a + q], y + toff + c0, lane, live, sub, g)
                                : (T)0;
             if (lane < W) s_part[warp][lane] = acc;
@@ -906,7 +929,7 @@ constexpr int SPLIT_LEVEL_ROWS = 1024;
 
 template <class T>
 static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
-                              int64_t ld, int32_t kcols) {
+                              int64_t ld, int32_t kcols, const RowAct& ra = RowAct()) {
     const int ntiles = (int)(ld / TILE);
     const bool narrow = TILE > NARROW_W && kcols <= NARROW_W;
     const int nsub = narrow ? 1 : TILE / NARROW_W;  // sub-tiles of the 8-column layout
@@ -937,22 +960,27 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
         const bool last = fwd && fuse_last && l == L_last;
         if (last && split)
             k_chunked<M_FWD_LAST, T, NARROW_W, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, nsub, V.D);
+                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, nsub, V.D,
+                ra);
         else if (last)
             k_chunked<M_FWD_LAST, T, TILE, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, 1, V.D);
+                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, 1, V.D, ra);
         else if (fwd && split)
             k_chunked<M_FWD, T, NARROW_W, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, nsub);
+                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, nsub,
+                nullptr, ra);
         else if (fwd)
             k_chunked<M_FWD, T, TILE, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, 1);
+                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, 1, nullptr,
+                ra);
         else if (split)
             k_chunked<M_BWD, T, NARROW_W, MINB_BWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr, kcols, nsub);
+                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr, kcols, nsub,
+                nullptr, ra);
         else
             k_chunked<M_BWD, T, TILE, MINB_BWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr, kcols, 1);
+                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr, kcols, 1,
+                nullptr, ra);
         launches++;
     };
     const unsigned rgrid = (unsigned)(ntiles * nsub);
@@ -964,7 +992,7 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
         const auto& run = F.runs[seg[i].second];
         k_trsv_run<T, NARROW_W, true><<<rgrid, RUN_THREADS, 0, C.stream>>>(
             n, F.level_rows, F.fsched, F.fstep, run.fs0, run.fs1, F.prow_ptr, F.prow_idx, V.prow_val, r, y, kcols,
-            nsub);
+            nsub, ra);
         launches++;
     }
     for (size_t i = seg.size(); i-- > 0;) {
@@ -976,7 +1004,7 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
         const auto& run = F.runs[seg[i].second];
         k_trsv_run<T, NARROW_W, false><<<rgrid, RUN_THREADS, 0, C.stream>>>(
             n, F.level_rows, F.bsched, F.bstep, run.bs0, run.bs1, F.pcol_ptr, F.pcol_idx, V.pcol_val, V.D, y, kcols,
-            nsub);
+            nsub, ra);
         launches++;
     }
     SSP_CHECK_LAUNCH();
@@ -1145,7 +1173,7 @@ static SpmmPlan make_spmm_plan(Context& C, int64_t n, const int64_t* lap_ptr, co
 // SpMM q = A p over the plan's slabs (+ p.q partials into A.part when dot)
 template <class T>
 static void launch_spmm(Context& C, int64_t n, const SpmmPlan& A, const T* aval, const T* p, T* q, int64_t ld,
-                        bool dot, int32_t kcols) {
+                        bool dot, int32_t kcols, const RowAct& ra = RowAct()) {
     const bool narrow = TILE > NARROW_W && kcols <= NARROW_W;
     for (int32_t b = 0; b < A.nslabs; b++) {
         const int64_t* ptr = A.ptr + (int64_t)b * n;
@@ -1153,7 +1181,7 @@ static void launch_spmm(Context& C, int64_t n, const SpmmPlan& A, const T* aval,
 #define SSP_SPMM_LAUNCH(MODE, W_)                                                                                  \
     k_chunked<MODE, T, W_, MINB_SPMM><<<A.grid, CH_THREADS, 0, C.stream>>>(n, A.chunks[b], A.nchunks[b], ptr, A.idx,  \
                                                                             aval, nullptr, p, q, nullptr, ld, part,    \
-                                                                            kcols, 1)
+                                                                            kcols, 1, nullptr, ra)
         if (b == 0) {
             if (narrow) SSP_SPMM_LAUNCH(M_SPMM, NARROW_W);
             else SSP_SPMM_LAUNCH(M_SPMM, TILE);
@@ -1167,10 +1195,11 @@ static void launch_spmm(Context& C, int64_t n, const SpmmPlan& A, const T* aval,
 
 template <class T>
 static void build_precond_graph(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
-                                int64_t ld, int32_t kcols, Precond& P, int64_t& launches) {
+                                int64_t ld, int32_t kcols, Precond& P, int64_t& launches,
+                                const RowAct& ra = RowAct()) {
     SSP_CUDA(cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeThreadLocal));
     try {
-        launches = launch_precond<T>(C, F, V, n, r, y, ld, kcols);
+        launches = launch_precond<T>(C, F, V, n, r, y, ld, kcols, ra);
     } catch (...) {
         cudaGraph_t g;
         cudaStreamEndCapture(C.stream, &g);
@@ -1239,7 +1268,7 @@ template <class T>
 static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const SpmmPlan& A, const T* aval,
                          const DevFactor& F, const FactorVals<T>& V,
                          const Precond& P, int64_t pc_launches, PcgBufs<T> B, ColState& S, Reducer& R,
-                         int32_t max_iters, const PcgOptions& opt, PcgTimers& tm) {
+                         int32_t max_iters, const PcgOptions& opt, PcgTimers& tm, const RowAct& ra = RowAct()) {
     // without a residual history or progress output the iterations after the first run on the device
     // SSP_PCG_HOST_LOOP=1 keeps every iteration on the host loop (the same kernels, launched one by one), for
     // profilers that do not look inside conditional graph nodes
@@ -1262,9 +1291,17 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         if (G.nseg > 1) R.run<OP_DOT, T>(B.p, B.q, S.pq);
         else colred_final(C, ld, (int)A.grid.x, A.part, S.pq);
     };
+    // which (graph, tile) pairs still have an active column: the row kernels skip the others
+    auto update_act = [&]() {
+        if (!ra.act) return;
+        k_seg_tile_active<<<grid_for((int64_t)G.nseg * ntiles, 256), 256, 0, C.stream>>>(G.nseg, (int32_t)ntiles, ld,
+                                                                                        S.active, (int32_t*)ra.act);
+        C.kernels_launched++;
+    };
     int64_t active = read_i64(C, S.nactive);
     int32_t it = 0;
     if (active == 0) return 0;
+    update_act();
     tm.pc.begin(C.stream);
     SSP_CUDA(cudaGraphLaunch(P.exec, C.stream));
     tm.pc.end(C.stream);
@@ -1274,7 +1311,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
     tm.loop.begin(C.stream);
     while (it < max_iters) {
         tm.spmm.begin(C.stream);
-        launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, G.nseg == 1, k);
+        launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, G.nseg == 1, k, ra);
         tm.spmm.end(C.stream);
         pq_dot();
         k_cols_alpha<<<cg, 256, 0, C.stream>>>(ns, S);
@@ -1288,6 +1325,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         k_cols_check<<<cg, 256, 0, C.stream>>>(ns, it, S);
         SSP_CHECK_LAUNCH();
         C.kernels_launched++;
+        update_act();
         active = read_i64(C, S.nactive);
         if (opt.history || seg_history) {
             std::vector<double> hrr(ns), hbb(ns);
@@ -1364,11 +1402,11 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         cudaGraphNode_t wnode;
         SSP_CUDA(cudaGraphAddNode(&wnode, L.graph, roots.data(), nn, &cp));
         capture(cp.conditional.phGraph_out[0], [&] {
-            body_kernels += launch_precond<T>(C, F, V, n, B.r, B.z, ld, k);
+            body_kernels += launch_precond<T>(C, F, V, n, B.r, B.z, ld, k, ra);
             R.run<OP_DOT, T>(B.r, B.z, S.rz_new);
             k_cols_beta<<<cg, 256, 0, C.stream>>>(ns, S);
             k_update_xp<T><<<egrid, 256, 0, C.stream>>>(n, ld, S.alpha, S.beta, B.z, B.p, B.e, G);
-            launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, G.nseg == 1, k);
+            launch_spmm<T>(C, n, A, aval, B.p, B.q, ld, G.nseg == 1, k, ra);
             pq_dot();
             k_cols_alpha<<<cg, 256, 0, C.stream>>>(ns, S);
             k_axpy_r_rr<T><<<dim3((unsigned)R.nparts, (unsigned)ntiles), RED_THREADS, 0, C.stream>>>(
@@ -1377,6 +1415,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
             k_it_next<<<1, 1, 0, C.stream>>>(d_it);
             SSP_CUDA(cudaMemsetAsync(S.nactive, 0, sizeof(int64_t), C.stream));
             k_cols_check_at<<<cg, 256, 0, C.stream>>>(ns, d_it, S);
+            update_act();
             k_loop_ctl<<<1, 1, 0, C.stream>>>(h, S.nactive, d_it, max_iters);
             SSP_CHECK_LAUNCH();
         });
@@ -1457,6 +1496,12 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                                                                       2048 / std::max<int64_t>(1, ntiles) + 4)),
                      (unsigned)ntiles);
     const int cg = grid_for(ns, 256);
+    RowAct ra;
+    if (G.nseg > 1) {
+        ra.act = W.get_t<int32_t>("pcg_act", (size_t)G.nseg * ntiles);
+        ra.rowseg = G.rowseg;
+        ra.ntiles = (int32_t)ntiles;
+    }
 
     // r = Y - mean(Y); x = 0; ||b||^2
     R.run<OP_SUM, double>(Y, nullptr, colsum);
@@ -1483,9 +1528,9 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         Precond P;
         int64_t pc_launches = 0;
         if (read_i64(C, S.nactive) > 0) {
-            build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P, pc_launches);
+            build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P, pc_launches, ra);
             it = pcg_solve<double>(C, n, k, ld, A, A.val, F, fp64_vals(F), P, pc_launches,
-                                   PcgBufs<double>{x, r, z, p, q}, S, R, opt.max_iters, opt, tm);
+                                   PcgBufs<double>{x, r, z, p, q}, S, R, opt.max_iters, opt, tm, ra);
         }
     } else {
         // FP32 copies of the Laplacian and factor values, and the FP32 inner vectors
@@ -1526,14 +1571,14 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, MIXED_INNER_REDUCTION, S.thr, Si, R.G);
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
-                if (!P32.exec) build_precond_graph<float>(C, F, V32, n, r32, z32, ld, k, P32, pc32);
+                if (!P32.exec) build_precond_graph<float>(C, F, V32, n, r32, z32, ld, k, P32, pc32, ra);
                 int32_t cap = opt.max_iters - it;
                 if (first_its >= 0)
                     cap = std::min(cap, std::max(MIXED_MIN_ROUND_ITERS, MIXED_ROUND_ITER_FACTOR * first_its));
                 else
                     cap = std::min(cap, std::max(MIXED_MIN_ROUND_ITERS, opt.max_iters / MIXED_FIRST_ROUND_DIV));
                 its = pcg_solve<float>(C, n, k, ld, A, aval32, F, V32, P32, pc32,
-                                       PcgBufs<float>{e32, r32, z32, p32, q32}, Si, R, cap, opt, tm);
+                                       PcgBufs<float>{e32, r32, z32, p32, q32}, Si, R, cap, opt, tm, ra);
                 if (first_its < 0) first_its = its;
                 hit_cap = its >= cap;
                 k_add_into<float><<<grid_for(total, 256, 148 * 16), 256, 0, C.stream>>>(total, e32, x);
@@ -1547,9 +1592,9 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, 0.0, S.thr, Si, R.G);
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
-                if (!P64.exec) build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P64, pc64);
+                if (!P64.exec) build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P64, pc64, ra);
                 its = pcg_solve<double>(C, n, k, ld, A, A.val, F, fp64_vals(F), P64, pc64,
-                                        PcgBufs<double>{e64, r, z, p, q}, Si, R, opt.max_iters - it, opt, tm);
+                                        PcgBufs<double>{e64, r, z, p, q}, Si, R, opt.max_iters - it, opt, tm, ra);
                 k_add_into<double><<<grid_for(total, 256, 148 * 16), 256, 0, C.stream>>>(total, e64, x);
                 rep.fp64_rounds++;
             }
