@@ -327,7 +327,8 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
             sketch_device(C, SG, kp, scale, prm->sketch_seed, prm->sketch_uniform, Yp, tile_ld(kp), 1, 0);
             probe = Yp;
         }
-        deg_used = autotune_factor(C, n, G.lap_ptr, G.lap_idx, G.lap_val, 2 * G.m, probe, kp, fo, po, F, &ms_tune);
+        deg_used = autotune_factor(C, n, G.lap_ptr, G.lap_idx, G.lap_val, 2 * G.m, G.max_deg, probe, kp, fo, po, F,
+                                   &ms_tune);
     } else {
         factor_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, fo, F, "f");
     }
@@ -552,8 +553,8 @@ static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t 
     int64_t deg_used = fo.max_degree;
     if (fo.max_degree < 0) {
         const int64_t offdiag = L.nnz - n;  // every vertex of a connected Laplacian stores its diagonal
-        deg_used = autotune_factor(C, n, L.colptr, L.rowidx, L.val, offdiag > 0 ? offdiag : L.nnz, Yt, k, fo, po, F,
-                                   nullptr);
+        deg_used = autotune_factor(C, n, L.colptr, L.rowidx, L.val, offdiag > 0 ? offdiag : L.nnz,
+                                   max_offdiag_column(C, n, L.colptr, L.rowidx), Yt, k, fo, po, F, nullptr);
     } else {
         factor_device(C, n, L.colptr, L.rowidx, L.val, fo, F, "f");
     }
@@ -768,13 +769,18 @@ static void sparsify_batch_impl(Context& C, int32_t count, const ssp_csc* graphs
         pp.segs = &ps;
         PcgReport pr;
         pcg_device(C, n, G.lap_ptr, G.lap_idx, G.lap_val, F, Y, kp, nullptr, pp, pr);
+        // each graph's largest vertex degree, for the rule's hub test
+        std::vector<int64_t> aptr(n + 1);
+        copy_d2h(C, aptr.data(), G.adj_ptr, sizeof(int64_t) * (n + 1));
         bool again = false;
         for (int32_t b = 0; b < count; b++) {
             if (prms[b].factor_max_degree >= 0) continue;
+            int64_t dmax = 0;
+            for (int64_t v = V[b]; v < V[b + 1]; v++) dmax = std::max(dmax, aptr[v + 1] - aptr[v]);
             const std::vector<double> none;
             const double iters = autotune_predicted_iters(b < (int32_t)ps.history.size() ? ps.history[b] : none,
                                                           po.tol);
-            if (!(iters <= SSP_TUNE_MAX_ITERS)) {
+            if (!autotune_keep_light(iters, V[b + 1] - V[b], 2 * (E[b + 1] - E[b]), dmax)) {
                 maxdeg[b] = 0;
                 again = true;
             }

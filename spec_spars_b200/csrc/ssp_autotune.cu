@@ -9,8 +9,11 @@
 // 1.05 d0 + 1, d0 the graph's average degree), run a 20-iteration PCG probe on the first SSP_PROBE_COLS
 // columns of the actual right-hand sides, and estimate the iterations to reach the tolerance from the contraction
 // rate of the last ten probe iterations.  A graph whose lightly preconditioned system converges within
-// 30 iterations keeps that factor; otherwise the elimination runs to completion.  Both factorizations
-// are deterministic.
+// 30 iterations keeps that factor, and so does one with power-law hubs (largest vertex degree at least 16 times
+// the average) that converges within 150: there complete elimination builds factors with thousands of
+// latency-bound levels (R-MAT scale 18, measured on B200: 7,107 levels, 1.46 s per preconditioner application
+// and 84 s per sparsification, against 4.9 ms and 4.0 s for the light factor at 56 instead of 54 iterations).
+// Otherwise the elimination runs to completion.  Both factorizations, and so the choice, are deterministic.
 #include <cmath>
 #include <vector>
 
@@ -20,6 +23,14 @@ namespace ssp {
 
 constexpr int TUNE_PROBE_ITERS = SSP_TUNE_PROBE_ITERS;
 constexpr double TUNE_MAX_ITERS = SSP_TUNE_MAX_ITERS;
+constexpr double TUNE_MAX_ITERS_SKEWED = 150.0;
+constexpr double TUNE_SKEW = 16.0;
+
+bool autotune_keep_light(double predicted_iters, int64_t n, int64_t lap_offdiag_nnz, int64_t max_vertex_degree) {
+    if (predicted_iters <= TUNE_MAX_ITERS) return true;
+    const double d0 = n > 0 ? (double)lap_offdiag_nnz / (double)n : 0.0;
+    return predicted_iters <= TUNE_MAX_ITERS_SKEWED && d0 > 0 && (double)max_vertex_degree >= TUNE_SKEW * d0;
+}
 
 int64_t autotune_light_degree(int64_t n, int64_t lap_offdiag_nnz) {
     const double d0 = n > 0 ? (double)lap_offdiag_nnz / (double)n : 0.0;
@@ -44,8 +55,8 @@ double autotune_predicted_iters(const std::vector<double>& hist, double tol) {
 }
 
 int64_t autotune_factor(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx, const double* lap_val,
-                        int64_t lap_offdiag_nnz, const double* Ytiles, int32_t k, const FactorOptions& base,
-                        const PcgOptions& popt, DevFactor& F, double* ms_tuning) {
+                        int64_t lap_offdiag_nnz, int64_t max_vertex_degree, const double* Ytiles, int32_t k,
+                        const FactorOptions& base, const PcgOptions& popt, DevFactor& F, double* ms_tuning) {
     const int64_t light = autotune_light_degree(n, lap_offdiag_nnz);
     cudaEvent_t e0, e1;
     SSP_CUDA(cudaEventCreate(&e0));
@@ -67,7 +78,7 @@ int64_t autotune_factor(Context& C, int64_t n, const int64_t* lap_ptr, const int
     pcg_device(C, n, lap_ptr, lap_idx, lap_val, F, Ytiles, kp, nullptr, po, rep);
     const double iters = autotune_predicted_iters(hist, popt.tol);
     int64_t chosen = light;
-    if (!(iters <= TUNE_MAX_ITERS)) {
+    if (!autotune_keep_light(iters, n, lap_offdiag_nnz, max_vertex_degree)) {
         chosen = 0;
         fo.max_degree = 0;
         factor_device(C, n, lap_ptr, lap_idx, lap_val, fo, F, "f");

@@ -432,13 +432,18 @@ struct PcgReport {
 // by factoring a few candidates and timing a short PCG probe on the first column tile of Y.  Leaves
 // the chosen factor in F and returns the chosen max_degree.
 int64_t autotune_factor(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* lap_idx,
-                        const double* lap_val, int64_t lap_offdiag_nnz, const double* Ytiles, int32_t k,
-                        const FactorOptions& base, const PcgOptions& popt, DevFactor& F, double* ms_tuning);
+                        const double* lap_val, int64_t lap_offdiag_nnz, int64_t max_vertex_degree,
+                        const double* Ytiles, int32_t k, const FactorOptions& base, const PcgOptions& popt,
+                        DevFactor& F, double* ms_tuning);
 // The autotuner's rule, its pieces shared by the single-graph and the batched autotuning: the lightest
 // truncation for a graph of n vertices and lap_offdiag_nnz off-diagonal Laplacian entries, and the
 // iterations to the tolerance predicted from a probe's residual history (1e9: no prediction).
 int64_t autotune_light_degree(int64_t n, int64_t lap_offdiag_nnz);
 double autotune_predicted_iters(const std::vector<double>& hist, double tol);
+// whether the light factor is kept, given its predicted iterations and the graph's degrees
+bool autotune_keep_light(double predicted_iters, int64_t n, int64_t lap_offdiag_nnz, int64_t max_vertex_degree);
+// largest off-diagonal entry count of a column of a Laplacian (its largest vertex degree)
+int64_t max_offdiag_column(Context& C, int64_t n, const int64_t* ptr, const int32_t* idx);
 constexpr int32_t SSP_TUNE_PROBE_ITERS = 20;
 constexpr double SSP_TUNE_MAX_ITERS = 30.0;
 // With lap_eid (the graph's per-entry edge map) and d2 (m doubles), the final product A x also forms

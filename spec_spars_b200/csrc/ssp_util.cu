@@ -135,6 +135,26 @@ void make_chunks(const int64_t* ptr, int32_t r0, int32_t r1, std::vector<int32_t
     }
 }
 
+__global__ void k_max_offdiag_column(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                     unsigned long long* mx) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        unsigned long long d = 0;
+        for (int64_t p = ptr[c]; p < ptr[c + 1]; p++) d += idx[p] != c;
+        atomicMax(mx, d);
+    }
+}
+
+int64_t max_offdiag_column(Context& C, int64_t n, const int64_t* ptr, const int32_t* idx) {
+    unsigned long long* d = C.ws.get_t<unsigned long long>("u_maxcol", 1);
+    SSP_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), C.stream));
+    if (n > 0) {
+        k_max_offdiag_column<<<grid_for(n, 256), 256, 0, C.stream>>>(n, ptr, idx, d);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched++;
+    }
+    return read_i64(C, reinterpret_cast<const int64_t*>(d));
+}
+
 int64_t read_i64(Context& C, const int64_t* d_ptr) {
     SSP_CUDA(cudaMemcpyAsync(C.h_pinned, d_ptr, sizeof(int64_t), cudaMemcpyDeviceToHost, C.stream));
     SSP_CUDA(cudaStreamSynchronize(C.stream));
