@@ -419,6 +419,25 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def run_precond(args):
+    """--precond-cols N: M^-1 applied to N seeded standard-normal columns with the workload's complete factor
+    (stage entry point ssp_stage_precond, dense-tail threshold 4096), twice; prints the host-side seconds of
+    each call.  For profiling the triangular solves alone."""
+    import numpy as np
+    import spec_spars_b200 as S
+    G, _ = make_graph(S, args.workload)
+    ctx = S.Context(0)
+    _, L = S.stage_graph(ctx, G)
+    R = np.random.default_rng(0).standard_normal((G.n, args.precond_cols))
+    secs = []
+    for _ in range(2):
+        t = time.perf_counter()
+        S.stage_precond(ctx, L, 0, R, 4096, 0)
+        secs.append(time.perf_counter() - t)
+    print(json.dumps({"workload": args.workload, "n": G.n, "columns": args.precond_cols, "seconds": secs}), flush=True)
+    ctx.close()
+
+
 def run_mtx(args):
     """--mtx: the Matrix Market path of sparsify_dataset on the workload's graph.  Timed: the GPU reader and
     writer (ssp_read_mtx_device / ssp_write_mtx_device, file in the page cache) and sparsify_dataset file to
@@ -659,6 +678,8 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--mtx", action="store_true", help="time the GPU Matrix Market reader/writer and sparsify_dataset")
+    ap.add_argument("--precond-cols", type=int, default=0,
+                    help="apply the workload's complete preconditioner to this many columns, twice (profiling)")
     ap.add_argument("--mode", default="auto", choices=["auto", "sharded", "replicas"],
                     help="N > 1: split one graph's JL columns over the ranks (auto, sharded) or run N independent "
                          "replicas, one graph each (replicas)")
@@ -673,6 +694,9 @@ def main():
     if args.mtx:
         run_mtx(args)
         return
+    if args.precond_cols > 0:
+        run_precond(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -685,11 +709,14 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
+    if world > 1 or args.mode == "sharded":
         import datetime
-        # the communicator's set-up lines show the rank count
+        # the communicator's set-up lines show the rank count (--mode sharded also runs on one rank, where
+        # the all-reduce is the identity)
         os.environ.setdefault("NCCL_DEBUG", "INFO")
         os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+        for key, val in (("MASTER_ADDR", "127.0.0.1"), ("MASTER_PORT", "29511"), ("RANK", "0"), ("WORLD_SIZE", "1")):
+            os.environ.setdefault(key, val)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         if args.mode != "replicas":
             run_sharded(args, S, torch, dist, world, rank, local)
