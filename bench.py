@@ -406,6 +406,21 @@ def serving_section(S, count, max_n, slots=2, max_batch=64):
             "batched_mixed_over_plain_default": batched_mixed["value"] / plain_default}
 
 
+def serving_lite(S, count=48, max_n=20_000, slots=2, max_batch=64):
+    """The serving mix at a bounded size for the default line: the plain FP64 path one request after another,
+    then the request loop with continuous batching (closed loop for capacity, then Poisson arrivals at 0.8 of
+    it) with p50/p99 latency."""
+    reqs = serving_mix(S, count, max_n)
+    plain = plain_measure(S, reqs)
+    batched = serve_measure(S, reqs, slots, max_batch)
+    return {"workload": "serving mix", "requests": count, "n_range": [1000, max_n], "degree_range": [8, 32],
+            "eps": [0.3, 0.5], "edges": sum(G.nnz // 2 for G, _ in reqs), "dtype": "f64",
+            "plain_fp64_edges_per_s": plain, "value": batched["value"], "unit": "edges/s",
+            "p50_ms": batched["p50_ms"], "p99_ms": batched["p99_ms"], "served_batched_fp64": batched,
+            "batched_over_plain": batched["value"] / plain,
+            "batched_closed_loop_over_plain": batched["closed_loop_edges_per_s"] / plain}
+
+
 def run_serve(args):
     """--serve: the serving mix through the persistent request loop (ssp_server_*), beside the plain path."""
     import spec_spars_b200 as S
@@ -505,6 +520,16 @@ def spectral_check(S, ctx, LG, H, eps, st, probes=100):
             "passed": r["upper_bound_violations"] == 0 and r["lower_bound_violations"] == 0}
 
 
+def trsv_info(S, first, last):
+    """How the preconditioner's level-launch shapes were chosen: measured on the first step (device ms spent),
+    then taken from the context's cache; level launches at 8/16/32 columns per warp row."""
+    src = {S.SSP_TRSV_RULE: "rule", S.SSP_TRSV_TUNED: "measured", S.SSP_TRSV_CACHED: "cached",
+           S.SSP_TRSV_FORCED: "forced"}
+    return {"first_step": src.get(first["trsv_shapes"], "?"), "timed_steps": src.get(last["trsv_shapes"], "?"),
+            "ms_measuring": first["ms_trsv_tune"],
+            "level_launches_w8_w16_w32": [last["trsv_levels_w8"], last["trsv_levels_w16"], last["trsv_levels_w32"]]}
+
+
 def mesh_step(S, ctx, stream, name="grid3d_128"):
     """The ill-conditioned mesh configuration (3-D 7-point grid 128^3, weights log-uniform over six decades,
     eps 0.5, k = ceil(24 ln n / eps^2) = 1398, PCG tol 1e-8, FP64): one untimed step, one timed step (CUDA
@@ -519,7 +544,7 @@ def mesh_step(S, ctx, stream, name="grid3d_128"):
     va = torch.from_numpy(G.values).to(dev)
     _, LG = S.stage_graph(ctx, G)
     torch.cuda.synchronize()
-    ctx.sparsify_device(G.n, G.nnz, cp.data_ptr(), ri.data_ptr(), va.data_ptr(), prm)
+    _, st0 = ctx.sparsify_device(G.n, G.nnz, cp.data_ptr(), ri.data_ptr(), va.data_ptr(), prm)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -538,7 +563,7 @@ def mesh_step(S, ctx, stream, name="grid3d_128"):
            "ms_per_step": ms, "value": st["m_in"] / (ms / 1000.0), "unit": "edges/s", "steps": 1, "warmup": 1,
            "kept_fraction": st["m_out"] / st["m_in"], "pcg_iters_max": st["pcg_max_iters_used"],
            "factor_nnz": st["nnz_factor"], "factor_levels": st["factor_levels"],
-           "factor_max_degree_used": st["factor_max_degree_used"],
+           "factor_max_degree_used": st["factor_max_degree_used"], "trsv_shapes": trsv_info(S, st0, st),
            "stages_ms": {x: st[x] for x in ("ms_assembly", "ms_sketch", "ms_factor", "ms_solve", "ms_leverage",
                                             "ms_sample", "ms_total")},
            "roofline": {"kernel": "precond (fwd+bwd level-set triangular solves, all k columns)", "bound": "hbm",
@@ -683,6 +708,8 @@ def main():
     ap.add_argument("--mode", default="auto", choices=["auto", "sharded", "replicas"],
                     help="N > 1: split one graph's JL columns over the ranks (auto, sharded) or run N independent "
                          "replicas, one graph each (replicas)")
+    ap.add_argument("--no-serving", dest="serving", action="store_false",
+                    help="leave out the bounded serving-mix measurement of the default line")
     ap.add_argument("--no-mesh", dest="mesh", action="store_false",
                     help="skip the one-step grid3d_128 measurement reported beside the ER headline")
     ap.add_argument("--reference-n", type=int, default=0,
@@ -743,8 +770,10 @@ def main():
 
     # L_G as the library forms it, for the spectral check of the timed steps' output (untimed)
     _, LG = S.stage_graph(ctx, G)
+    warm = []
     for _ in range(args.warmup):
         _, st = step()
+        warm.append(st)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -843,6 +872,7 @@ def main():
             "pcg_iters_mean": st["pcg_mean_iters"], "pcg_max_relres": st["pcg_max_relres"],
             "pcg_refinements": st["pcg_refinements"], "pcg_fp64_rounds": st["pcg_fp64_rounds"],
             "spmm_slabs": st["spmm_slabs"], "factor_nnz": st["nnz_factor"], "factor_levels": st["factor_levels"],
+            "trsv_shapes": trsv_info(S, warm[0] if warm else stats[0], st),
             "roofline": roof, "spectral": spectral, "clocks": clocks.summary(), "e2e": e2e}
     if args.precision == "fp64" and not args.no_mixed:
         # the same workload with FP32 inner solves inside FP64 refinement (same PCG tolerance), beside the
@@ -875,6 +905,13 @@ def main():
             line["mesh_grid3d_128"] = mesh_step(S, ctx, stream)
         except Exception as e:  # reported, never fatal to the headline
             line["mesh_grid3d_128"] = {"error": f"{type(e).__name__}: {e}"[:400]}
+    if args.serving and world == 1 and args.workload == "er_n1M_deg20":
+        # the serving mix through the request loop, beside the headline (its own contexts; ours released)
+        ctx.release_workspace()
+        try:
+            line["serving"] = serving_lite(S)
+        except Exception as e:  # reported, never fatal to the headline
+            line["serving"] = {"error": f"{type(e).__name__}: {e}"[:400]}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(eps, k)
     if rank == 0:

@@ -59,6 +59,11 @@ extern "C" {
 #define SSP_PRECISION_FP64 0  /* every vector and matrix in FP64                                     */
 #define SSP_PRECISION_MIXED 1 /* SpMM, triangular solves and vectors in FP32 with FP64 dot products,
                                  inside FP64 iterative refinement to the same tolerance                */
+/* where the preconditioner's level-launch shapes came from (ssp_stats.trsv_shapes) */
+#define SSP_TRSV_RULE 0     /* fixed rule: levels of at most 1024 rows 8 columns per warp row, wider ones 32 */
+#define SSP_TRSV_TUNED 1    /* measured in this call: every width timed per level, the fastest kept        */
+#define SSP_TRSV_CACHED 2   /* measured by an earlier call on the same factor shape (context cache)        */
+#define SSP_TRSV_FORCED 3   /* one width for every level, from the environment (SSP_TRSV_WIDTH)            */
 /* reweighting of kept edges */
 #define SSP_REWEIGHT_INV_SQRT_P 0 /* w / sqrt(p)  (sparsifier.rs:657)           */
 #define SSP_REWEIGHT_INV_P 1      /* w / p        (stream_sparsify.jl:135)      */
@@ -143,6 +148,11 @@ typedef struct {
     int32_t pcg_refinements;        /* SSP_PRECISION_MIXED: FP64 refinement rounds (0 in FP64 mode) */
     int32_t pcg_fp64_rounds;        /* ... of which ran an FP64 inner solve after FP32 stopped contracting */
     int32_t spmm_slabs;             /* column slabs of the PCG's Laplacian product (1 = one pass) */
+    int32_t trsv_shapes;            /* SSP_TRSV_*: how the preconditioner's level-launch shapes were chosen */
+    int32_t trsv_levels_w8;         /* level launches (forward + backward) at 8 columns per warp row, */
+    int32_t trsv_levels_w16;        /* ... at 16, */
+    int32_t trsv_levels_w32;        /* ... at 32 (runs of thin levels are not counted: always 8) */
+    double ms_trsv_tune;            /* device time spent measuring them (0 when taken from the cache) */
 } ssp_stats;
 
 typedef struct {
@@ -170,6 +180,9 @@ typedef struct {
     int32_t refinements;     /* SSP_PRECISION_MIXED: FP64 refinement rounds */
     int32_t fp64_rounds;
     int32_t spmm_slabs;      /* column slabs of the Laplacian product (1 = one pass) */
+    int32_t trsv_shapes;     /* SSP_TRSV_*, as in ssp_stats */
+    int32_t trsv_levels_w8, trsv_levels_w16, trsv_levels_w32;
+    double ms_trsv_tune;
 } ssp_solve_report;
 
 /* ---- errors ---- */

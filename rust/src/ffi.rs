@@ -27,6 +27,10 @@ pub const SSP_PRECISION_FP64: i32 = 0;
 pub const SSP_PRECISION_MIXED: i32 = 1;
 pub const SSP_REWEIGHT_INV_SQRT_P: i32 = 0;
 pub const SSP_REWEIGHT_INV_P: i32 = 1;
+pub const SSP_TRSV_RULE: i32 = 0;
+pub const SSP_TRSV_TUNED: i32 = 1;
+pub const SSP_TRSV_CACHED: i32 = 2;
+pub const SSP_TRSV_FORCED: i32 = 3;
 pub const SSP_REQ_SPARSIFY: i32 = 0;
 
 /// ssp_csc: a square matrix in compressed-sparse-column form (CSC == CSR for the symmetric matrices here).
@@ -116,6 +120,11 @@ pub struct SspStats {
     pub pcg_refinements: i32,
     pub pcg_fp64_rounds: i32,
     pub spmm_slabs: i32,
+    pub trsv_shapes: i32,
+    pub trsv_levels_w8: i32,
+    pub trsv_levels_w16: i32,
+    pub trsv_levels_w32: i32,
+    pub ms_trsv_tune: f64,
 }
 
 /// ssp_solve_opts: options of ssp_solve_lap.
@@ -149,6 +158,11 @@ pub struct SspSolveReport {
     pub refinements: i32,
     pub fp64_rounds: i32,
     pub spmm_slabs: i32,
+    pub trsv_shapes: i32,
+    pub trsv_levels_w8: i32,
+    pub trsv_levels_w16: i32,
+    pub trsv_levels_w32: i32,
+    pub ms_trsv_tune: f64,
 }
 
 /// ssp_server_opts: the persistent request loop's device, slots, HBM budget and queue limit.

@@ -15,6 +15,7 @@ SSP_MEM_HOST, SSP_MEM_DEVICE = 0, 1
 SSP_JL_DIM_REF, SSP_JL_DIM_24 = 0, 1
 SSP_JL_SCALE_FIXED, SSP_JL_SCALE_INV_SQRT_K = 0, 1
 SSP_REWEIGHT_INV_SQRT_P, SSP_REWEIGHT_INV_P = 0, 1
+SSP_TRSV_RULE, SSP_TRSV_TUNED, SSP_TRSV_CACHED, SSP_TRSV_FORCED = 0, 1, 2, 3
 SSP_PRECISION_FP64, SSP_PRECISION_MIXED = 0, 1
 
 ERROR_NAMES = {-1: "SSP_ERR_INVALID", -2: "SSP_ERR_CUDA", -3: "SSP_ERR_NOMEM", -4: "SSP_ERR_NOT_CONVERGED",
@@ -73,7 +74,9 @@ class _Stats(ctypes.Structure):
                 ("ms_precond", ctypes.c_double), ("n_precond", ctypes.c_int64), ("nnz_laplacian", ctypes.c_int64),
                 ("factor_max_degree_used", ctypes.c_int64), ("ms_autotune", ctypes.c_double),
                 ("pcg_refinements", ctypes.c_int32), ("pcg_fp64_rounds", ctypes.c_int32),
-                ("spmm_slabs", ctypes.c_int32)]
+                ("spmm_slabs", ctypes.c_int32), ("trsv_shapes", ctypes.c_int32),
+                ("trsv_levels_w8", ctypes.c_int32), ("trsv_levels_w16", ctypes.c_int32),
+                ("trsv_levels_w32", ctypes.c_int32), ("ms_trsv_tune", ctypes.c_double)]
 
 
 class _SolveOpts(ctypes.Structure):
@@ -87,7 +90,10 @@ class _SolveReport(ctypes.Structure):
                 ("max_relres", ctypes.c_double), ("not_converged", ctypes.c_int32),
                 ("nnz_factor", ctypes.c_int64), ("factor_levels", ctypes.c_int32), ("ms_factor", ctypes.c_double),
                 ("ms_solve", ctypes.c_double), ("factor_max_degree_used", ctypes.c_int64),
-                ("refinements", ctypes.c_int32), ("fp64_rounds", ctypes.c_int32), ("spmm_slabs", ctypes.c_int32)]
+                ("refinements", ctypes.c_int32), ("fp64_rounds", ctypes.c_int32), ("spmm_slabs", ctypes.c_int32),
+                ("trsv_shapes", ctypes.c_int32), ("trsv_levels_w8", ctypes.c_int32),
+                ("trsv_levels_w16", ctypes.c_int32), ("trsv_levels_w32", ctypes.c_int32),
+                ("ms_trsv_tune", ctypes.c_double)]
 
 
 class _ServerOpts(ctypes.Structure):

@@ -248,6 +248,16 @@ static int32_t batch_after_factor(Context& C, const DevGraph& G, int32_t k, int3
     return (int32_t)std::max<int64_t>(SSP_TILE, std::min<int64_t>(cols, k));
 }
 
+// the preconditioner's level-launch shapes (ssp_stats / ssp_solve_report share the field names)
+template <class S>
+static void copy_trsv_stats(S& s, const PcgReport& r) {
+    s.trsv_shapes = r.trsv_shapes;
+    s.trsv_levels_w8 = r.trsv_levels[0];
+    s.trsv_levels_w16 = r.trsv_levels[1];
+    s.trsv_levels_w32 = r.trsv_levels[2];
+    s.ms_trsv_tune = r.ms_trsv_tune;
+}
+
 static void merge_report(PcgReport& a, const PcgReport& b, int32_t ka, int32_t kb) {
     a.mean_iters = (a.mean_iters * ka + b.mean_iters * kb) / (double)(ka + kb);
     a.max_iters_used = std::max(a.max_iters_used, b.max_iters_used);
@@ -264,6 +274,10 @@ static void merge_report(PcgReport& a, const PcgReport& b, int32_t ka, int32_t k
     a.ms_resid += b.ms_resid;
     a.n_resid += b.n_resid;
     a.diff_fused = a.diff_fused && b.diff_fused;
+    // the same factor in every batch: its shapes as the last batch used them, measured if any batch measured
+    a.ms_trsv_tune += b.ms_trsv_tune;
+    a.trsv_shapes = a.trsv_shapes == SSP_TRSV_TUNED ? SSP_TRSV_TUNED : b.trsv_shapes;
+    for (int i = 0; i < 3; i++) a.trsv_levels[i] = b.trsv_levels[i];
 }
 
 static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* prm, int32_t out_mem, ssp_csc_out* out,
@@ -400,6 +414,7 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
             st->pcg_refinements = rep.refinements;
             st->pcg_fp64_rounds = rep.fp64_rounds;
             st->spmm_slabs = rep.spmm_slabs;
+            copy_trsv_stats(*st, rep);
         }
         return;
     }
@@ -504,6 +519,7 @@ static void sparsify_impl(Context& C, const ssp_csc* graph, const ssp_params* pr
         st->pcg_refinements = rep.refinements;
         st->pcg_fp64_rounds = rep.fp64_rounds;
         st->spmm_slabs = rep.spmm_slabs;
+        copy_trsv_stats(*st, rep);
     }
     if (prm->verbose) {
         fprintf(stderr, "[ssp] n=%lld m=%lld k=%d nnz(L)=%lld levels=%d (sparse %zu, dense %d, truncated %lld, compactions %d) "
@@ -585,6 +601,7 @@ static void solve_impl(Context& C, const ssp_csc* lap, const double* Y, int32_t 
         rep->refinements = pr.refinements;
         rep->fp64_rounds = pr.fp64_rounds;
         rep->spmm_slabs = pr.spmm_slabs;
+        copy_trsv_stats(*rep, pr);
     }
     if (pr.not_converged > 0)
         throw Error(SSP_ERR_NOT_CONVERGED, "solver did not converge: " + std::to_string(pr.not_converged) +
@@ -892,6 +909,7 @@ static void sparsify_batch_impl(Context& C, int32_t count, const ssp_csc* graphs
             st.pcg_refinements = rep.refinements;
             st.pcg_fp64_rounds = rep.fp64_rounds;
             st.spmm_slabs = rep.spmm_slabs;
+            copy_trsv_stats(st, rep);
         }
         if (prms[b].output_file && prms[b].output_file[0]) {
             std::string err;

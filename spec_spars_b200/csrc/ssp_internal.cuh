@@ -153,6 +153,17 @@ private:
     std::map<std::string, Buf> bufs_;
 };
 
+// Launch shapes of the preconditioner's level launches (ssp_pcg.cu): per level and direction, the column width
+// of a warp's row -- code 0, 1, 2 for 8, 16, 32 columns, TILE / width blocks per column tile.  Every width gives
+// the same values bit for bit, so a shape changes only the time.  Chosen by measurement per factor and kept in
+// the context under a signature of the factor's level structure and the solve's shape.
+struct TrsvShapes {
+    std::vector<uint8_t> fw, bw;  // per level
+};
+struct TrsvShapeCache {
+    std::vector<std::pair<uint64_t, TrsvShapes>> entries;  // oldest first; a few graphs' worth
+};
+
 struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -164,6 +175,7 @@ struct Context {
     cudaEvent_t stage_ev[3] = {nullptr, nullptr, nullptr};
     int verbose = 0;
     int64_t kernels_launched = 0;  // count of library kernel launches (for bench accounting)
+    TrsvShapeCache trsv_cache;     // measured level-launch shapes of recently solved factors
 };
 
 // ---------------------------------------------------------------- n x k block layout
@@ -427,6 +439,11 @@ struct PcgReport {
     double ms_resid = 0;     // mixed precision: device time of the FP64 residual products
     int64_t n_resid = 0;
     bool diff_fused = false; // the squared diff norms were formed by the final product (d2 filled)
+    // level-launch shapes of the preconditioner (the last one built): SSP_TRSV_* source, level launches
+    // (forward + backward) at 8, 16 and 32 columns per warp row, device time spent measuring them
+    int32_t trsv_shapes = 0;
+    int32_t trsv_levels[3] = {0, 0, 0};
+    double ms_trsv_tune = 0;
 };
 // Picks the elimination truncation (FactorOptions::max_degree) for this Laplacian and right-hand sides
 // by factoring a few candidates and timing a short PCG probe on the first column tile of Y.  Leaves

@@ -613,6 +613,7 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
     __shared__ int32_t s_idx[CH_WARPS][CHUNK_CAP];
     __shared__ T s_val[CH_WARPS][CHUNK_CAP];
     __shared__ int32_t s_ptr[CH_WARPS][CHUNK_ROWS + 1];
+    __shared__ int32_t s_row[CH_WARPS][CHUNK_ROWS];
     __shared__ double s_red[CH_THREADS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t t = blockIdx.y / nsub;
@@ -622,6 +623,7 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
     int32_t* si = s_idx[w];
     T* sv = s_val[w];
     int32_t* sp = s_ptr[w];
+    int32_t* sr = s_row[w];
     constexpr int SLOTS_W = 32 / W;
     constexpr bool SPMM = MODE == M_SPMM || MODE == M_SPMM_ACC;
     const bool want_dot = SPMM && part != nullptr;
@@ -635,12 +637,16 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
                 si[i] = __ldcs(idx + e0 + i);
                 sv[i] = __ldcs(val + e0 + i);
             }
-            for (int32_t i = lane; i <= r1 - r0; i += 32) sp[i] = (int32_t)(ptr[r0 + i] - e0);
+            // the chunk's row pointers and vertex ids (level solves: storage row -> vertex) staged together
+            for (int32_t i = lane; i <= r1 - r0; i += 32) {
+                sp[i] = (int32_t)(ptr[r0 + i] - e0);
+                if (i < r1 - r0) sr[i] = rowmap ? rowmap[r0 + i] : r0 + i;
+            }
             __syncwarp();
             const int32_t pairs = (r1 - r0) * W;
             for (int32_t pr = lane; pr < pairs; pr += 32) {
                 const int32_t rr = pr / W, col = c0 + pr % W;
-                const int64_t vrow = rowmap ? rowmap[r0 + rr] : r0 + rr;
+                const int64_t vrow = sr[rr];
                 const bool on = row_on(ra, vrow, t);
                 const bool live = on && t * TILE + col < kcols;
                 const int32_t q0 = sp[rr], q1 = live ? sp[rr + 1] : q0;
@@ -668,21 +674,38 @@ __global__ void __launch_bounds__(CH_THREADS, MINB)
             }
             __syncwarp();
         } else {
-            // one long row: (32 / W) entry slots x W columns per step, then a reduction over the slots
+            // One long row: (32 / W) entry slots x W columns per step.  The sum does not depend on W: entry i
+            // of the row goes to virtual accumulator i mod LONG_ACC (each summed in entry order), and the
+            // accumulators are combined by a fixed tree, highest index bit first.  A lane of slot s holds the
+            // accumulators s + SLOTS_W j; it combines their high bits itself, the slot bits are combined
+            // across lanes afterwards (offset 16 first), so a level solved with any column width W gives
+            // the same values bit for bit -- which lets the launch shapes be chosen by measurement.
+            constexpr int LONG_ACC = 4, NA = LONG_ACC / SLOTS_W;
+            static_assert(NA >= 1 && LONG_ACC % SLOTS_W == 0, "column width below 8");
             const int slot = lane / W, col = c0 + lane % W;
             const int64_t vr0 = rowmap ? rowmap[r0] : r0;
             const bool on = row_on(ra, vr0, t);
             const int64_t qe = on && t * TILE + col < kcols ? e1 : e0;
-            T a0 = 0, a1 = 0;
-            int64_t q = e0 + slot;
-            for (; q + SLOTS_W < qe; q += 2 * SLOTS_W) {
-                a0 += __ldcs(val + q) * xt[(int64_t)__ldcs(idx + q) * TILE + col];
-                a1 += __ldcs(val + q + SLOTS_W) * xt[(int64_t)__ldcs(idx + q + SLOTS_W) * TILE + col];
-            }
-            if (q < qe) a0 += __ldcs(val + q) * xt[(int64_t)__ldcs(idx + q) * TILE + col];
-            T acc = a0 + a1;
+            T a[NA];
 #pragma unroll
-            for (int o = W; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            for (int j = 0; j < NA; j++) a[j] = 0;
+            int64_t q = e0 + slot;
+            for (; q + (NA - 1) * SLOTS_W < qe; q += NA * SLOTS_W) {
+#pragma unroll
+                for (int j = 0; j < NA; j++)
+                    a[j] += __ldcs(val + q + j * SLOTS_W) * xt[(int64_t)__ldcs(idx + q + j * SLOTS_W) * TILE + col];
+            }
+#pragma unroll
+            for (int j = 0; j < NA - 1; j++)
+                if (q + j * SLOTS_W < qe)
+                    a[j] += __ldcs(val + q + j * SLOTS_W) * xt[(int64_t)__ldcs(idx + q + j * SLOTS_W) * TILE + col];
+#pragma unroll
+            for (int h = NA / 2; h >= 1; h >>= 1)
+#pragma unroll
+                for (int j = 0; j < h; j++) a[j] += a[j + h];
+            T acc = a[0];
+#pragma unroll
+            for (int o = 16; o >= W; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
             if (lane < W && on) chunk_epilogue<MODE, T>(out, aux, xt, toff, vr0, col, acc, dot, want_dot, dlast);
         }
     }
@@ -919,20 +942,73 @@ struct Precond {
     }
 };
 
-// Column layouts of the triangular-solve launches.  Big levels: a warp's lanes cover a tile's TILE columns of
-// one row (256-byte gathers).  Runs and levels of at most SPLIT_LEVEL_ROWS rows are latency-bound -- a lane
-// walks its rows one after another -- so there each tile is split into TILE / 8 sub-tiles of 8 columns, one
-// block each: four rows per warp step and four times the warps.  With no more than 8 real columns (the
-// autotuner's probe) every launch uses 8 columns and one sub-tile; the padding columns of y must then be zero.
+// Column layouts of the triangular-solve launches.  A level launch gives each warp row a width of W columns
+// (8, 16 or 32; TILE / W blocks per column tile): with W = 32 a warp's lanes cover a tile's columns of one row
+// (256-byte gathers); with W = 8 a warp works on four rows at once, with four times the blocks, which suits
+// latency-bound levels of few rows.  Every width gives the same values bit for bit (each (row, column) sum is
+// formed the same way, see k_chunked), so the width is a pure launch-shape choice: the fixed rule below, or
+// widths measured level by level (tune_trsv_shapes).  Runs of thin levels always use 8 columns.  With no more
+// than 8 real columns (the factor autotuner's probe) every launch uses 8 columns and one sub-tile; the padding
+// columns of y must then be zero.
 constexpr int NARROW_W = 8;
 constexpr int SPLIT_LEVEL_ROWS = 1024;
+constexpr int TRSV_NWIDTH = TILE >= 32 ? 3 : TILE >= 16 ? 2 : 1;  // widths 8, 16, 32 that fit a tile
+static inline int trsv_width(int code) { return 8 << code; }
 
+// CUDA events around each level launch of a preconditioner application (measurement only)
+struct LevelEvents {
+    std::vector<cudaEvent_t> ev;        // pairs: before, after
+    std::vector<std::pair<bool, int32_t>> tag;  // (forward, level) of each pair
+    size_t used = 0;
+    ~LevelEvents() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+    void begin(cudaStream_t s, bool fwd, int32_t l) {
+        if (2 * used == ev.size()) {
+            for (int i = 0; i < 2; i++) {
+                cudaEvent_t e;
+                SSP_CUDA(cudaEventCreate(&e));
+                ev.push_back(e);
+            }
+            tag.push_back({fwd, l});
+        }
+        tag[used] = {fwd, l};
+        SSP_CUDA(cudaEventRecord(ev[2 * used], s));
+    }
+    void end(cudaStream_t s) {
+        SSP_CUDA(cudaEventRecord(ev[2 * used + 1], s));
+        used++;
+    }
+};
+
+template <int MODE, class T, int MINB>
+static void launch_level_w(int code, dim3 grid, cudaStream_t s, int64_t n, const int32_t* ch, int32_t nc,
+                           const int64_t* ptr, const int32_t* idx, const T* val, const int32_t* rowmap, T* y,
+                           const T* aux, int64_t ld, int32_t kcols, int nsub, const T* dlast, const RowAct& ra) {
+    switch (code) {
+    case 0:
+        k_chunked<MODE, T, 8, MINB><<<grid, CH_THREADS, 0, s>>>(n, ch, nc, ptr, idx, val, rowmap, y, y, aux, ld,
+                                                                nullptr, kcols, nsub, dlast, ra);
+        break;
+    case 1:
+        k_chunked<MODE, T, (TILE >= 16 ? 16 : 8), MINB><<<grid, CH_THREADS, 0, s>>>(
+            n, ch, nc, ptr, idx, val, rowmap, y, y, aux, ld, nullptr, kcols, nsub, dlast, ra);
+        break;
+    default:
+        k_chunked<MODE, T, TILE, MINB><<<grid, CH_THREADS, 0, s>>>(n, ch, nc, ptr, idx, val, rowmap, y, y, aux, ld,
+                                                                   nullptr, kcols, nsub, dlast, ra);
+        break;
+    }
+}
+
+// sh: per-level widths (nullptr: the fixed rule); lev: events around each level launch (nullptr: none)
 template <class T>
 static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
-                              int64_t ld, int32_t kcols, const RowAct& ra = RowAct()) {
+                              int64_t ld, int32_t kcols, const RowAct& ra = RowAct(),
+                              const TrsvShapes* sh = nullptr, LevelEvents* lev = nullptr) {
     const int ntiles = (int)(ld / TILE);
     const bool narrow = TILE > NARROW_W && kcols <= NARROW_W;
-    const int nsub = narrow ? 1 : TILE / NARROW_W;  // sub-tiles of the 8-column layout
+    const int nsub = narrow ? 1 : TILE / NARROW_W;  // sub-tiles of the 8-column layout (runs)
     int64_t launches = 0;
     // segments in level order: the thin-level runs (by index into F.runs) and single wide levels (-1)
     std::vector<std::pair<int32_t, int32_t>> seg;  // (level, run or -1)
@@ -950,37 +1026,35 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
     const char* fuse_env = getenv("SSP_PRECOND_FUSE_LAST");
     const bool fuse_last = !(fuse_env && fuse_env[0] == '0') && !seg.empty() && seg.back().second < 0 &&
                            F.last_bwd_nnz == 0 && L_last >= 0;
+    auto width_code = [&](bool fwd, int32_t l) -> int {
+        if (narrow) return 0;
+        int c = F.level_ptr[l + 1] - F.level_ptr[l] <= SPLIT_LEVEL_ROWS ? 0 : 2;
+        if (sh) {
+            const auto& v = fwd ? sh->fw : sh->bw;
+            if ((size_t)l < v.size()) c = v[l];
+        }
+        return std::min(c, TRSV_NWIDTH - 1);
+    };
     auto level = [&](bool fwd, int32_t l) {
         const auto& lvl = fwd ? F.fchunk_lvl : F.bchunk_lvl;
         const int32_t c0 = lvl[l], nc = lvl[l + 1] - c0;
         if (nc == 0) return;
-        const bool split = narrow || F.level_ptr[l + 1] - F.level_ptr[l] <= SPLIT_LEVEL_ROWS;
-        const dim3 grid((unsigned)chunk_blocks(nc), (unsigned)(split ? ntiles * nsub : ntiles));
+        const int code = width_code(fwd, l);
+        const int ns = narrow ? 1 : TILE / trsv_width(code);
+        const dim3 grid((unsigned)chunk_blocks(nc), (unsigned)(ntiles * ns));
         const int32_t* ch = (fwd ? F.fchunk : F.bchunk) + c0;
         const bool last = fwd && fuse_last && l == L_last;
-        if (last && split)
-            k_chunked<M_FWD_LAST, T, NARROW_W, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, nsub, V.D,
-                ra);
-        else if (last)
-            k_chunked<M_FWD_LAST, T, TILE, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, 1, V.D, ra);
-        else if (fwd && split)
-            k_chunked<M_FWD, T, NARROW_W, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, nsub,
-                nullptr, ra);
+        if (lev) lev->begin(C.stream, fwd, l);
+        if (last)
+            launch_level_w<M_FWD_LAST, T, MINB_FWD>(code, grid, C.stream, n, ch, nc, F.prow_ptr, F.prow_idx,
+                                                    V.prow_val, F.level_rows, y, r, ld, kcols, ns, V.D, ra);
         else if (fwd)
-            k_chunked<M_FWD, T, TILE, MINB_FWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val, F.level_rows, y, y, r, ld, nullptr, kcols, 1, nullptr,
-                ra);
-        else if (split)
-            k_chunked<M_BWD, T, NARROW_W, MINB_BWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr, kcols, nsub,
-                nullptr, ra);
+            launch_level_w<M_FWD, T, MINB_FWD>(code, grid, C.stream, n, ch, nc, F.prow_ptr, F.prow_idx, V.prow_val,
+                                               F.level_rows, y, r, ld, kcols, ns, nullptr, ra);
         else
-            k_chunked<M_BWD, T, TILE, MINB_BWD><<<grid, CH_THREADS, 0, C.stream>>>(
-                n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val, F.level_rows, y, y, V.D, ld, nullptr, kcols, 1,
-                nullptr, ra);
+            launch_level_w<M_BWD, T, MINB_BWD>(code, grid, C.stream, n, ch, nc, F.pcol_ptr, F.pcol_idx, V.pcol_val,
+                                               F.level_rows, y, V.D, ld, kcols, ns, nullptr, ra);
+        if (lev) lev->end(C.stream);
         launches++;
     };
     const unsigned rgrid = (unsigned)(ntiles * nsub);
@@ -1009,6 +1083,167 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
     }
     SSP_CHECK_LAUNCH();
     return launches;
+}
+
+// Level-launch shapes by measurement.  Each width is timed on every level launch of a full preconditioner
+// application (CUDA events around each launch, on the solve's own right-hand sides), twice in interleaved
+// order, and each level keeps the width of its smaller best time.  The values are the same whatever the
+// widths, so only the time depends on the choice.  Kept per context under a signature of the factor's
+// level structure and the solve's shape, so repeated solves on the same graph measure once.  Small solves
+// (n * ld below SSP_TRSV_TUNE_MIN elements, 2^26 unless the environment variable of that name says otherwise)
+// keep the rule: there the measurement would cost more than it could save.  SSP_TRSV_TUNE=0 keeps the rule
+// everywhere; SSP_TRSV_WIDTH=8|16|32 forces one width.
+#ifndef SSP_TRSV_TUNE_MIN
+#define SSP_TRSV_TUNE_MIN (int64_t(1) << 26)
+#endif
+constexpr int TRSV_CACHE_MAX = 8;
+static int64_t trsv_tune_min() {
+    const char* e = getenv("SSP_TRSV_TUNE_MIN");  // elements n * ld from which to measure
+    return e && e[0] ? atoll(e) : (int64_t)SSP_TRSV_TUNE_MIN;
+}
+
+static uint64_t trsv_signature(const DevFactor& F, int64_t n, int64_t ld, int32_t kcols, size_t elem,
+                               bool segmented) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) {
+        for (int i = 0; i < 8; i++) {
+            h ^= (v >> (8 * i)) & 0xff;
+            h *= 1099511628211ull;
+        }
+    };
+    mix((uint64_t)n);
+    mix((uint64_t)ld);
+    mix((uint64_t)kcols);
+    mix((uint64_t)elem);
+    mix((uint64_t)segmented);
+    // the level sizes, entry counts and runs: fixed by the factor (the order of the rows inside a level, and so
+    // the chunk boundaries, may differ from one factorization to the next; the widths are chosen per level)
+    mix((uint64_t)F.nnz);
+    mix((uint64_t)F.num_levels);
+    mix((uint64_t)F.last_fwd_nnz);
+    mix((uint64_t)F.last_bwd_nnz);
+    for (int32_t v : F.level_ptr) mix((uint64_t)(uint32_t)v);
+    for (const auto& r : F.runs) mix(((uint64_t)(uint32_t)r.l0 << 32) | (uint32_t)r.l1);
+    return h;
+}
+
+static void count_trsv_widths(const DevFactor& F, const TrsvShapes& sh, PcgReport& rep) {
+    for (int i = 0; i < 3; i++) rep.trsv_levels[i] = 0;
+    std::vector<bool> in_run(F.num_levels, false);
+    for (const auto& r : F.runs)
+        for (int32_t l = r.l0; l < r.l1; l++) in_run[l] = true;
+    for (int32_t l = 0; l < F.num_levels; l++) {
+        if (in_run[l]) continue;
+        if (F.fchunk_lvl[l + 1] > F.fchunk_lvl[l]) rep.trsv_levels[sh.fw[l]]++;
+        if (F.bchunk_lvl[l + 1] > F.bchunk_lvl[l]) rep.trsv_levels[sh.bw[l]]++;
+    }
+}
+
+template <class T>
+static void tune_trsv_shapes(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
+                             int64_t ld, int32_t kcols, const RowAct& ra, TrsvShapes& out, double& ms) {
+    constexpr int ROUNDS = 2;
+    const int nw = TRSV_NWIDTH;
+    std::vector<LevelEvents> ev(nw * ROUNDS);
+    std::vector<TrsvShapes> forced(nw);
+    for (int c = 0; c < nw; c++) {
+        forced[c].fw.assign(F.num_levels, (uint8_t)c);
+        forced[c].bw.assign(F.num_levels, (uint8_t)c);
+    }
+    cudaEvent_t e0, e1;
+    SSP_CUDA(cudaEventCreate(&e0));
+    SSP_CUDA(cudaEventCreate(&e1));
+    SSP_CUDA(cudaEventRecord(e0, C.stream));
+    for (int round = 0; round < ROUNDS; round++)
+        for (int c = 0; c < nw; c++) {
+            const int cc = round % 2 ? nw - 1 - c : c;  // alternate the order between rounds
+            C.kernels_launched += launch_precond<T>(C, F, V, n, r, y, ld, kcols, ra, &forced[cc], &ev[round * nw + cc]);
+        }
+    SSP_CUDA(cudaEventRecord(e1, C.stream));
+    SSP_CUDA(cudaEventSynchronize(e1));
+    float tt = 0;
+    SSP_CUDA(cudaEventElapsedTime(&tt, e0, e1));
+    ms = tt;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // best[dir][level][width]
+    const float INF = 3.0e38f;
+    std::vector<float> best(2 * (size_t)F.num_levels * nw, INF);
+    for (int round = 0; round < ROUNDS; round++)
+        for (int c = 0; c < nw; c++) {
+            const LevelEvents& L = ev[round * nw + c];
+            for (size_t i = 0; i < L.used; i++) {
+                float t = 0;
+                SSP_CUDA(cudaEventElapsedTime(&t, L.ev[2 * i], L.ev[2 * i + 1]));
+                const size_t o = ((size_t)(L.tag[i].first ? 0 : 1) * F.num_levels + L.tag[i].second) * nw + c;
+                best[o] = std::min(best[o], t);
+            }
+        }
+    out.fw.assign(F.num_levels, 0);
+    out.bw.assign(F.num_levels, 0);
+    for (int dir = 0; dir < 2; dir++)
+        for (int32_t l = 0; l < F.num_levels; l++) {
+            const float* b = &best[((size_t)dir * F.num_levels + l) * nw];
+            // the rule's width unless another is faster
+            int pick = std::min(F.level_ptr[l + 1] - F.level_ptr[l] <= SPLIT_LEVEL_ROWS ? 0 : 2, nw - 1);
+            for (int c = 0; c < nw; c++)
+                if (b[c] < b[pick]) pick = c;
+            (dir == 0 ? out.fw : out.bw)[l] = (uint8_t)pick;
+        }
+}
+
+// The shapes a solve's preconditioner uses: forced, cached, measured now, or (nullptr) the rule.
+template <class T>
+static const TrsvShapes* trsv_shapes_for(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n,
+                                         const T* r, T* y, int64_t ld, int32_t kcols, const RowAct& ra,
+                                         TrsvShapes& store, PcgReport& rep) {
+    const bool narrow = TILE > NARROW_W && kcols <= NARROW_W;
+    rep.trsv_shapes = SSP_TRSV_RULE;
+    const TrsvShapes* out = nullptr;
+    const char* fw = getenv("SSP_TRSV_WIDTH");
+    const char* tn = getenv("SSP_TRSV_TUNE");
+    if (narrow || F.num_levels == 0) {
+        // one width for all (8 columns), nothing to choose
+    } else if (fw && fw[0]) {
+        const int w = atoi(fw);
+        const int code = w >= 32 ? 2 : w >= 16 ? 1 : 0;
+        store.fw.assign(F.num_levels, (uint8_t)std::min(code, TRSV_NWIDTH - 1));
+        store.bw = store.fw;
+        rep.trsv_shapes = SSP_TRSV_FORCED;
+        out = &store;
+    } else if (!(tn && tn[0] == '0') && n * ld >= trsv_tune_min()) {
+        const uint64_t key = trsv_signature(F, n, ld, kcols, sizeof(T), ra.act != nullptr);
+        auto& E = C.trsv_cache.entries;
+        for (auto& e : E)
+            if (e.first == key) {
+                store = e.second;
+                rep.trsv_shapes = SSP_TRSV_CACHED;
+                out = &store;
+                break;
+            }
+        if (!out) {
+            double ms = 0;
+            tune_trsv_shapes<T>(C, F, V, n, r, y, ld, kcols, ra, store, ms);
+            rep.ms_trsv_tune += ms;
+            rep.trsv_shapes = SSP_TRSV_TUNED;
+            if ((int)E.size() >= TRSV_CACHE_MAX) E.erase(E.begin());
+            E.push_back({key, store});
+            out = &store;
+        }
+    }
+    if (out) {
+        count_trsv_widths(F, *out, rep);
+    } else {
+        TrsvShapes rule;
+        rule.fw.resize(F.num_levels);
+        for (int32_t l = 0; l < F.num_levels; l++)
+            rule.fw[l] = narrow ? 0
+                                : (uint8_t)std::min(F.level_ptr[l + 1] - F.level_ptr[l] <= SPLIT_LEVEL_ROWS ? 0 : 2,
+                                                    TRSV_NWIDTH - 1);
+        rule.bw = rule.fw;
+        count_trsv_widths(F, rule, rep);
+    }
+    return out;
 }
 
 // ---------------------------------------------------------------- SpMM plan
@@ -1193,13 +1428,17 @@ static void launch_spmm(Context& C, int64_t n, const SpmmPlan& A, const T* aval,
     }
 }
 
+// The preconditioner application as a CUDA graph, with its level-launch shapes chosen first (the measurement,
+// when one runs, uses r and overwrites y; both are the solve's own buffers and y is written before it is read)
 template <class T>
 static void build_precond_graph(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
-                                int64_t ld, int32_t kcols, Precond& P, int64_t& launches,
+                                int64_t ld, int32_t kcols, Precond& P, int64_t& launches, PcgReport& rep,
                                 const RowAct& ra = RowAct()) {
+    TrsvShapes store;
+    const TrsvShapes* sh = trsv_shapes_for<T>(C, F, V, n, r, y, ld, kcols, ra, store, rep);
     SSP_CUDA(cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeThreadLocal));
     try {
-        launches = launch_precond<T>(C, F, V, n, r, y, ld, kcols, ra);
+        launches = launch_precond<T>(C, F, V, n, r, y, ld, kcols, ra, sh);
     } catch (...) {
         cudaGraph_t g;
         cudaStreamEndCapture(C.stream, &g);
@@ -1214,7 +1453,10 @@ static FactorVals<double> fp64_vals(const DevFactor& F) { return FactorVals<doub
 
 // apply M^{-1} to R into Z once (tile-major n x ld blocks; stage entry point)
 void precond_apply_device(Context& C, const DevFactor& F, const double* R, double* Z, int64_t ld) {
-    int64_t l = launch_precond<double>(C, F, fp64_vals(F), F.n, R, Z, ld, (int32_t)ld);
+    TrsvShapes store;
+    PcgReport rep;
+    const TrsvShapes* sh = trsv_shapes_for<double>(C, F, fp64_vals(F), F.n, R, Z, ld, (int32_t)ld, RowAct(), store, rep);
+    int64_t l = launch_precond<double>(C, F, fp64_vals(F), F.n, R, Z, ld, (int32_t)ld, RowAct(), sh);
     C.kernels_launched += l;
 }
 
@@ -1528,7 +1770,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         Precond P;
         int64_t pc_launches = 0;
         if (read_i64(C, S.nactive) > 0) {
-            build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P, pc_launches, ra);
+            build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P, pc_launches, rep, ra);
             it = pcg_solve<double>(C, n, k, ld, A, A.val, F, fp64_vals(F), P, pc_launches,
                                    PcgBufs<double>{x, r, z, p, q}, S, R, opt.max_iters, opt, tm, ra);
         }
@@ -1571,7 +1813,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, MIXED_INNER_REDUCTION, S.thr, Si, R.G);
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
-                if (!P32.exec) build_precond_graph<float>(C, F, V32, n, r32, z32, ld, k, P32, pc32, ra);
+                if (!P32.exec) build_precond_graph<float>(C, F, V32, n, r32, z32, ld, k, P32, pc32, rep, ra);
                 int32_t cap = opt.max_iters - it;
                 if (first_its >= 0)
                     cap = std::min(cap, std::max(MIXED_MIN_ROUND_ITERS, MIXED_ROUND_ITER_FACTOR * first_its));
@@ -1592,7 +1834,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, 0.0, S.thr, Si, R.G);
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
-                if (!P64.exec) build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P64, pc64, ra);
+                if (!P64.exec) build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P64, pc64, rep, ra);
                 its = pcg_solve<double>(C, n, k, ld, A, A.val, F, fp64_vals(F), P64, pc64,
                                         PcgBufs<double>{e64, r, z, p, q}, Si, R, opt.max_iters - it, opt, tm, ra);
                 k_add_into<double><<<grid_for(total, 256, 148 * 16), 256, 0, C.stream>>>(total, e64, x);
