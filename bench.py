@@ -708,6 +708,8 @@ def main():
     ap.add_argument("--mode", default="auto", choices=["auto", "sharded", "replicas"],
                     help="N > 1: split one graph's JL columns over the ranks (auto, sharded) or run N independent "
                          "replicas, one graph each (replicas)")
+    ap.add_argument("--no-complete", dest="complete", action="store_false",
+                    help="leave out the one-step complete-elimination measurement of the default line")
     ap.add_argument("--no-serving", dest="serving", action="store_false",
                     help="leave out the bounded serving-mix measurement of the default line")
     ap.add_argument("--no-mesh", dest="mesh", action="store_false",
@@ -898,6 +900,37 @@ def main():
                                    "pcg_refinements": stm["pcg_refinements"], "spmm_slabs": stm["spmm_slabs"],
                                    "spmm_avg_ms": stm["ms_spmm"] / max(1, stm["n_spmm"])}
         prm.precision = S.SSP_PRECISION_FP64
+    if args.complete and world == 1:
+        # the reference's own preconditioner, complete elimination (example.cc:91-323), beside the autotuner's
+        # choice: one timed step (23 s at ER 1M), with the fixed rule's level shapes so that no shape
+        # measurement falls inside it
+        deg = prm.factor_max_degree
+        prm.factor_max_degree = 0
+        old_tune = os.environ.get("SSP_TRSV_TUNE")
+        os.environ["SSP_TRSV_TUNE"] = "0"
+        torch.cuda.synchronize()
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        _, stc = step()
+        c1.record(stream)
+        torch.cuda.synchronize()
+        cms = c0.elapsed_time(c1)
+        if old_tune is None:
+            del os.environ["SSP_TRSV_TUNE"]
+        else:
+            os.environ["SSP_TRSV_TUNE"] = old_tune
+        line["complete_elimination"] = {
+            "value": m / (cms / 1000.0), "unit": "edges/s", "ms_per_step": cms, "dtype": "f64", "steps": 1,
+            "trsv_shapes": "rule",
+            "pcg_iters_max": stc["pcg_max_iters_used"], "ms_factor": stc["ms_factor"],
+            "factor_nnz": stc["nnz_factor"], "factor_levels": stc["factor_levels"],
+            "precond_avg_ms": stc["ms_precond"] / max(1, stc["n_precond"]),
+            "spmm_avg_ms": stc["ms_spmm"] / max(1, stc["n_spmm"]),
+            "autotuned_choice": {"factor_max_degree": st["factor_max_degree_used"], "factor_nnz": st["nnz_factor"],
+                                 "factor_levels": st["factor_levels"], "pcg_iters_max": st["pcg_max_iters_used"],
+                                 "ms_factor": st["ms_factor"]}}
+        prm.factor_max_degree = deg
     if args.mesh and world == 1 and args.workload == "er_n1M_deg20":
         # the mesh configuration beside the headline, on a released workspace (its n x k blocks are 141 GB)
         ctx.release_workspace()

@@ -398,9 +398,19 @@ int ssp_write_mtx_device(ssp_context* ctx, const char* path, const ssp_csc* m);
  * subnormals, inf, nan). */
 int ssp_parse_decimal(const char* s, size_t len, double* out);
 int ssp_format_g17(double v, char* buf, size_t cap);
+/* ssp_format_shortest: the device formatter of the edge-list converter, on the host: v as Rust's Display writes
+ * an f64 (shortest digits that read back as v, no exponent) into buf (NUL-terminated); returns the length, or -1
+ * for values it leaves to the host (not finite, subnormal, outside about [1e-22, 3e38], longer than cap - 1). */
+int ssp_format_shortest(double v, char* buf, size_t cap);
 /* edge list ("<n> <m>" then "u v [w]" lines) -> symmetric .mtx, first weight of a repeated pair wins
  * (edge_list_to_matrix_market, src/utils.rs:413-526) */
 int ssp_edgelist_to_mtx(const char* input_path, const char* output_path, double default_weight);
+/* the same conversion on the GPU (edge_list_to_matrix_market, src/utils.rs:413-526): lines indexed and parsed on
+ * the device, pairs sorted stably, lines formatted with Rust's f64 text; byte for byte the file
+ * ssp_edgelist_to_mtx writes.  A file the device parser does not mirror (signed or 2^32+ endpoints, unusual
+ * separators, malformed lines) is converted by ssp_edgelist_to_mtx instead, with its result or error. */
+int ssp_edgelist_to_mtx_device(ssp_context* ctx, const char* input_path, const char* output_path,
+                               double default_weight);
 
 /* ---- synthetic graphs (seeded, identical on every host) as symmetric host CSC ---- */
 int ssp_gen_grid2d(int64_t nx, int64_t ny, double w, ssp_csc_out* out);

@@ -13,7 +13,7 @@ first call that needs one raises SspError if no device is visible.
 from ._lib import (  # noqa: F401
     SspError, lib, Context, CSC, DeviceCSC, SparsifierParameters, Sparsifier, InputStream, SparsificationStats,
     sparsify_dataset, run_solve_lap, solve_lap, read_mtx, write_mtx, laplacian_to_graph, parse_decimal, format_g17, gen_grid2d, gen_grid3d, gen_er, gen_rgg, gen_rmat,
-    Server, request_footprint, edge_list_to_matrix_market,
+    Server, request_footprint, edge_list_to_matrix_market, format_shortest,
     stage_graph, stage_sketch, stage_factor, stage_precond, stage_diff_norms, stage_probs, stage_coins, stage_scan,
     stage_sample_apply, SSP_JL_DIM_REF, SSP_JL_DIM_24, SSP_JL_SCALE_FIXED, SSP_JL_SCALE_INV_SQRT_K,
     SSP_REWEIGHT_INV_SQRT_P, SSP_REWEIGHT_INV_P, SSP_PRECISION_FP64, SSP_PRECISION_MIXED, LIB_PATH, HEADER_SYMBOLS,

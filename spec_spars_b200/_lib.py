@@ -181,6 +181,8 @@ def lib():
             "ssp_gen_grid3d": ([I64, I64, I64, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_er": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_edgelist_to_mtx": ([ctypes.c_char_p, ctypes.c_char_p, DBL], ctypes.c_int),
+            "ssp_edgelist_to_mtx_device": ([P, ctypes.c_char_p, ctypes.c_char_p, DBL], ctypes.c_int),
+            "ssp_format_shortest": ([DBL, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
             "ssp_gen_rmat": ([I32, I32, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_rgg": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_check_laplacian": ([P, ctypes.POINTER(_Csc), DBL, ctypes.POINTER(I64), ctypes.POINTER(DBL),
@@ -387,9 +389,22 @@ def gen_er(n, avg_degree, wlo=0.5, whi=2.0, seed=1):
     return _take_out(out)
 
 
-def edge_list_to_matrix_market(input_path, output_path, default_weight=1.0):
-    """edge_list_to_matrix_market (utils.rs:413-526)."""
+def edge_list_to_matrix_market(input_path, output_path, default_weight=1.0, ctx=None):
+    """edge_list_to_matrix_market (utils.rs:413-526).  With a Context the conversion runs on its GPU
+    (ssp_edgelist_to_mtx_device); the file is the same either way."""
+    if ctx is not None:
+        _check(lib().ssp_edgelist_to_mtx_device(ctx._h, str(input_path).encode(), str(output_path).encode(),
+                                                default_weight))
+        return
     _check(lib().ssp_edgelist_to_mtx(str(input_path).encode(), str(output_path).encode(), default_weight))
+
+
+def format_shortest(v):
+    """The edge-list converter's device formatter, run on the host: v as Rust displays an f64 (shortest
+    round-trip digits, no exponent), or None for values it leaves to the host."""
+    buf = ctypes.create_string_buffer(64)
+    n = lib().ssp_format_shortest(float(v), buf, 64)
+    return buf.value.decode() if n >= 0 else None
 
 
 def gen_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=3):

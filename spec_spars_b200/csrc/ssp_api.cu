@@ -57,13 +57,16 @@ static void init_context(Context& C, int device) {
     SSP_CUDA(cudaSetDevice(device));
     SSP_CUDA(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
     C.own_stream = true;
+    C.ws.set_stream(C.stream);
     SSP_CUDA(cudaMallocHost(&C.h_pinned, 64 * sizeof(int64_t)));
 }
 
 static void destroy_context(Context& C) {
     cudaSetDevice(C.device);
     if (C.stream) cudaStreamSynchronize(C.stream);
-    C.ws.release();
+    C.ws.release();  // stream-ordered frees: wait for them before the stream goes
+    if (C.stream) cudaStreamSynchronize(C.stream);
+    C.ws.set_stream(nullptr);
     release_staging(C);
     if (C.h_pinned) cudaFreeHost(C.h_pinned);
     if (C.own_stream && C.stream) cudaStreamDestroy(C.stream);
@@ -235,6 +238,14 @@ static double free_for_solve(Context& C) {
         cudaGetLastError();
         return 1e300;
     }
+    // memory the device's default pool holds but does not use (stream-ordered frees) is free to this context
+    cudaMemPool_t pool;
+    uint64_t reserved = 0, used = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, C.device) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+        fr += (size_t)(reserved - used);
+    cudaGetLastError();
     // the solve's own buffers from an earlier call are reused
     return (double)fr + (double)(C.ws.bytes_with_prefix("sp_Y") + C.ws.bytes_with_prefix("pcg"));
 }
@@ -963,6 +974,8 @@ int ssp_context_set_stream(ssp_context* c, void* stream) {
             SSP_CUDA(cudaStreamCreateWithFlags(&c->ctx.stream, cudaStreamNonBlocking));
             c->ctx.own_stream = true;
         }
+        // the old stream is idle (synchronized above), so its frees are done
+        c->ctx.ws.set_stream(c->ctx.stream);
     });
 }
 
@@ -1090,31 +1103,6 @@ static void laplacian_to_graph_host(int64_t n, int64_t nnz, const int64_t* cp, c
     }
 }
 
-static void laplacian_to_host_graph(Context& C, const ssp_csc* lap, HostCsc& g) {
-    SSP_REQUIRE(lap && lap->n > 0 && lap->nnz >= 0 && lap->colptr && (lap->nnz == 0 || (lap->rowidx && lap->values)),
-                SSP_ERR_INVALID, "invalid CSC descriptor");
-    if (lap->mem == SSP_MEM_DEVICE) {
-        std::vector<int64_t> cp(lap->n + 1);
-        std::vector<int32_t> ri(lap->nnz + 1);
-        std::vector<double> va(lap->nnz + 1);
-        SSP_CUDA(cudaMemcpyAsync(cp.data(), lap->colptr, sizeof(int64_t) * (lap->n + 1), cudaMemcpyDeviceToHost,
-                                 C.stream));
-        if (lap->nnz) {
-            SSP_CUDA(cudaMemcpyAsync(ri.data(), lap->rowidx, sizeof(int32_t) * lap->nnz, cudaMemcpyDeviceToHost,
-                                     C.stream));
-            SSP_CUDA(cudaMemcpyAsync(va.data(), lap->values, sizeof(double) * lap->nnz, cudaMemcpyDeviceToHost,
-                                     C.stream));
-        }
-        SSP_CUDA(cudaStreamSynchronize(C.stream));
-        SSP_REQUIRE(cp[0] == 0 && cp[lap->n] == lap->nnz, SSP_ERR_INVALID, "CSC colptr must start at 0 and end at nnz");
-        laplacian_to_graph_host(lap->n, lap->nnz, cp.data(), ri.data(), va.data(), g);
-        return;
-    }
-    SSP_REQUIRE(lap->colptr[0] == 0 && lap->colptr[lap->n] == lap->nnz, SSP_ERR_INVALID,
-                "CSC colptr must start at 0 and end at nnz");
-    laplacian_to_graph_host(lap->n, lap->nnz, lap->colptr, lap->rowidx, lap->values, g);
-}
-
 int ssp_laplacian_to_graph(const ssp_csc* lap, ssp_csc_out* graph) {
     return guarded([&] {
         SSP_REQUIRE(lap && graph && lap->mem == SSP_MEM_HOST, SSP_ERR_INVALID, "laplacian_to_graph needs a host CSC");
@@ -1132,11 +1120,16 @@ int ssp_sparsify_laplacian(ssp_context* c, const ssp_csc* lap, const ssp_params*
                            ssp_csc_out* out, ssp_stats* stats) {
     return guarded([&] {
         SSP_REQUIRE(c, SSP_ERR_INVALID, "ctx is NULL");
-        SSP_CUDA(cudaSetDevice(c->ctx.device));
-        HostCsc g;
-        laplacian_to_host_graph(c->ctx, lap, g);
-        const ssp_csc gc{g.n, g.colptr[g.n], g.colptr.data(), g.rowidx.data(), g.val.data(), SSP_MEM_HOST};
-        sparsify_impl(c->ctx, &gc, params, out_mem, out, stats);
+        Context& C = c->ctx;
+        SSP_CUDA(cudaSetDevice(C.device));
+        // on the device: the Laplacian (copied in when it is on the host), then its graph
+        const DevCsc L = to_device(C, lap, "lapin");
+        int64_t* gp = nullptr;
+        int32_t* gi = nullptr;
+        double* gv = nullptr;
+        const int64_t gnnz = laplacian_to_graph_device(C, L.n, L.nnz, L.colptr, L.rowidx, L.val, &gp, &gi, &gv);
+        const ssp_csc gc{L.n, gnnz, gp, gi, gv, SSP_MEM_DEVICE};
+        sparsify_impl(C, &gc, params, out_mem, out, stats);
     });
 }
 
@@ -1488,6 +1481,24 @@ int ssp_edgelist_to_mtx(const char* input_path, const char* output_path, double 
     });
 }
 
+int ssp_edgelist_to_mtx_device(ssp_context* c, const char* input_path, const char* output_path,
+                               double default_weight) {
+    return guarded([&] {
+        SSP_REQUIRE(c && input_path && output_path, SSP_ERR_INVALID, "bad arguments");
+        SSP_CUDA(cudaSetDevice(c->ctx.device));
+        if (edgelist_to_mtx_device(c->ctx, input_path, output_path, default_weight)) return;
+        std::string err;
+        if (edgelist_to_mtx(input_path, output_path, default_weight, err) != 0) throw Error(SSP_ERR_IO, err);
+    });
+}
+
+int ssp_format_shortest(double v, char* buf, size_t cap) {
+    if (!buf || cap < 2) return -1;
+    const int len = dec::format_shortest_fixed(v, buf, (int)(cap - 1));
+    if (len >= 0) buf[len] = 0;
+    return len;
+}
+
 int ssp_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed, ssp_csc_out* out) {
     return guarded([&] {
         SSP_REQUIRE(scale >= 1 && scale <= 30 && edge_factor > 0 && a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0 &&
@@ -1514,6 +1525,8 @@ int ssp_context_release_workspace(ssp_context* c) {
         SSP_CUDA(cudaSetDevice(c->ctx.device));
         SSP_CUDA(cudaStreamSynchronize(c->ctx.stream));
         c->ctx.ws.release();
+        // the frees are stream-ordered: once they have run, the pool returns the memory to the device
+        SSP_CUDA(cudaStreamSynchronize(c->ctx.stream));
     });
 }
 

@@ -359,5 +359,152 @@ SSP_HD int format_g17(double v, char* buf) {
     return n;
 }
 
+// ---------------------------------------------------------------- shortest round-trip, fixed notation
+// a / P and a % P (bit by bit; P < 2^127)
+SSP_HD u128 u192_divmod(const U192& a, u128 P, u128* rem) {
+    u128 r = 0, q = 0;
+    for (int i = u192_bitlen(a) - 1; i >= 0; i--) {
+        r = (r << 1) | (u128)u192_bit(a, i);
+        q <<= 1;
+        if (r >= P) {
+            r -= P;
+            q |= 1;
+        }
+    }
+    *rem = r;
+    return q;
+}
+
+// q = floor(mant * 2^e2 * 10^k), with the remainder compared at half (cmp -1 / 0 / +1 below / at / above) and
+// whether it is zero; false outside the supported range (|k| <= 38, q < 2^64, operands within 192 bits)
+SSP_HD bool scaled_floor(uint64_t mant, int e2, int k, uint64_t* q, int* cmp, bool* exact) {
+    if (k > 38 || k < -38) return false;
+    if (k >= 0) {
+        U192 N = {{mant, 0, 0}};
+        for (int i = 0; i < k; i++) u192_mul_small(N, 10);
+        if (e2 >= 0) {
+            if (u192_bitlen(N) + e2 > 63) return false;
+            *q = N.w[0] << e2;
+            *cmp = -1;
+            *exact = true;
+            return true;
+        }
+        const int t = -e2;
+        if (t >= 192 || u192_bitlen(N) - t > 63) return false;
+        *q = (uint64_t)u192_shr(N, t);
+        const bool guard = u192_bit(N, t - 1);
+        bool sticky = false;
+        for (int i = 0; i < t - 1 && !sticky; i++) sticky = u192_bit(N, i);
+        *cmp = guard ? (sticky ? 1 : 0) : -1;
+        *exact = !guard && !sticky;
+        return true;
+    }
+    u128 P = pow10_128(-k);
+    U192 N = {{mant, 0, 0}};
+    if (e2 >= 0) {
+        if (e2 > 127) return false;
+        for (int i = 0; i < e2; i++) u192_mul_small(N, 2);
+    } else {
+        if (bitlen128(P) + (-e2) > 126) return false;
+        P <<= -e2;
+    }
+    u128 rem = 0;
+    const u128 qq = u192_divmod(N, P, &rem);
+    if (qq >> 64) return false;
+    *q = (uint64_t)qq;
+    const u128 twice = rem << 1;
+    *cmp = twice < P ? -1 : (twice == P ? 0 : 1);
+    *exact = rem == 0;
+    return true;
+}
+
+// The shortest decimal that reads back as v (the closest such one; an exact tie keeps the even last digit), in
+// fixed notation without an exponent: the text Rust's Display writes for an f64 and C++'s
+// to_chars(..., chars_format::fixed) writes.  Returns the length written to buf (at most cap), or -1 when v is
+// not finite, subnormal, outside about [1e-22, 1e54], or its text is longer than cap (format on the host).
+SSP_HD int format_shortest_fixed(double v, char* buf, int cap) {
+    union { double d; uint64_t u; } c;
+    c.d = v;
+    const bool neg = c.u >> 63;
+    const int be = (int)((c.u >> 52) & 0x7ff);
+    const uint64_t frac = c.u & ((1ull << 52) - 1);
+    if (be == 0x7ff || (be == 0 && frac != 0)) return -1;  // inf / nan / subnormal
+    int n = 0;
+    if (neg) {
+        if (cap < 1) return -1;
+        buf[n++] = '-';
+    }
+    if (be == 0) {
+        if (n + 1 > cap) return -1;
+        buf[n++] = '0';
+        return n;
+    }
+    const uint64_t mant = frac | (1ull << 52);
+    const int e2 = be - 1075;
+    // X = floor(log10 |v|) exactly: 17 digits of the floor fall in [1e16, 1e17)
+    int X = (int)floor(log10(neg ? -v : v));
+    const uint64_t LO = 10000000000000000ull, HI = 100000000000000000ull;
+    uint64_t q = 0;
+    int cmp = 0;
+    bool exact = false;
+    for (int tries = 0;; tries++) {
+        if (tries > 3 || !scaled_floor(mant, e2, 16 - X, &q, &cmp, &exact)) return -1;
+        if (q >= HI) X++;
+        else if (q < LO) X--;
+        else break;
+    }
+    // the fewest significant digits P whose floor or ceiling reads back as v
+    uint64_t digits = 0;
+    int dexp = 0;  // v's text = digits * 10^dexp
+    for (int P = 1; P <= 17; P++) {
+        const int k = P - 1 - X;
+        if (!scaled_floor(mant, e2, k, &q, &cmp, &exact)) return -1;
+        if (exact) {
+            digits = q;
+            dexp = -k;
+            break;
+        }
+        double d1 = 0, d2 = 0;
+        const int E = -k;
+        const bool in1 = m10e_to_double(q, E, &d1), in2 = m10e_to_double(q + 1, E, &d2);
+        if (!in1 || !in2) return -1;
+        const bool ok1 = d1 == (neg ? -v : v), ok2 = d2 == (neg ? -v : v);
+        if (!ok1 && !ok2) continue;
+        bool up = ok2 && (!ok1 || cmp > 0 || (cmp == 0 && (q & 1)));
+        digits = up ? q + 1 : q;
+        dexp = E;
+        break;
+    }
+    if (digits == 0) return -1;
+    while (digits % 10 == 0) {
+        digits /= 10;
+        dexp++;
+    }
+    char dig[20];
+    int L = 0;
+    for (uint64_t t = digits; t; t /= 10) dig[L++] = (char)('0' + t % 10);
+    // dig holds the digits lowest first
+    if (dexp >= 0) {
+        if (n + L + dexp > cap) return -1;
+        for (int i = L - 1; i >= 0; i--) buf[n++] = dig[i];
+        for (int i = 0; i < dexp; i++) buf[n++] = '0';
+    } else if (L + dexp > 0) {
+        if (n + L + 1 > cap) return -1;
+        const int ip = L + dexp;  // digits before the point
+        for (int i = 0; i < L; i++) {
+            if (i == ip) buf[n++] = '.';
+            buf[n++] = dig[L - 1 - i];
+        }
+    } else {
+        const int z = -dexp - L;  // zeros after the point
+        if (n + 2 + z + L > cap) return -1;
+        buf[n++] = '0';
+        buf[n++] = '.';
+        for (int i = 0; i < z; i++) buf[n++] = '0';
+        for (int i = L - 1; i >= 0; i--) buf[n++] = dig[i];
+    }
+    return n;
+}
+
 }  // namespace dec
 }  // namespace ssp

@@ -268,6 +268,69 @@ void build_graph_from_csc(Context& C, int64_t n, const int64_t* colptr, const in
     build_graph_from_edges(C, G, tag);
 }
 
+// ---------------------------------------------------------------- Laplacian input
+// A Laplacian given as the input (Sparsifier::from_matrix, sparsifier.rs:299-300): the graph is its off-diagonal
+// entries negated, in their stored order, zeros kept (edge extraction drops them later, as for any graph).  The
+// counts pass checks that the column pointers do not decrease and stay within nnz.
+namespace {
+__global__ void k_lap_offdiag_count(int64_t n, int64_t nnz, const int64_t* __restrict__ ptr,
+                                    const int32_t* __restrict__ idx, int32_t* __restrict__ cnt, int32_t* err) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = ptr[j], e = ptr[j + 1];
+        if (s > e || e > nnz || s < 0) {
+            atomicOr(err, ERR_ORDER);
+            cnt[j] = 0;
+            continue;
+        }
+        int32_t c = 0;
+        for (int64_t t = s; t < e; t++) c += idx[t] != (int32_t)j;
+        cnt[j] = c;
+    }
+}
+__global__ void k_lap_offdiag_fill(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                   const double* __restrict__ val, const int64_t* __restrict__ optr,
+                                   int32_t* __restrict__ oidx, double* __restrict__ oval) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        int64_t o = optr[j];
+        for (int64_t t = ptr[j]; t < ptr[j + 1]; t++)
+            if (idx[t] != (int32_t)j) {
+                oidx[o] = idx[t];
+                oval[o] = -val[t];
+                o++;
+            }
+    }
+}
+}  // namespace
+
+int64_t laplacian_to_graph_device(Context& C, int64_t n, int64_t nnz, const int64_t* ptr, const int32_t* idx,
+                                  const double* val, int64_t** gptr, int32_t** gidx, double** gval,
+                                  const std::string& tag) {
+    Workspace& W = C.ws;
+    int64_t ends[2] = {0, 0};
+    SSP_CUDA(cudaMemcpyAsync(&ends[0], ptr, sizeof(int64_t), cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaMemcpyAsync(&ends[1], ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    SSP_REQUIRE(ends[0] == 0 && ends[1] == nnz, SSP_ERR_INVALID, "CSC colptr must start at 0 and end at nnz");
+    int32_t* cnt = W.get_t<int32_t>(tag + "_cnt", n + 1);
+    int32_t* err = W.get_t<int32_t>(tag + "_err", 1);
+    SSP_CUDA(cudaMemsetAsync(err, 0, sizeof(int32_t), C.stream));
+    const int blocks = grid_for(n, 256, 148 * 16);
+    k_lap_offdiag_count<<<blocks, 256, 0, C.stream>>>(n, nnz, ptr, idx, cnt, err);
+    SSP_CHECK_LAUNCH();
+    int32_t herr = 0;
+    SSP_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    SSP_REQUIRE(herr == 0, SSP_ERR_INVALID, "CSC colptr must be non-decreasing");
+    *gptr = W.get_t<int64_t>(tag + "_ptr", n + 1);
+    exclusive_scan_i32_to_i64(C, cnt, *gptr, n, *gptr + n);
+    const int64_t gnnz = read_i64(C, *gptr + n);
+    *gidx = W.get_t<int32_t>(tag + "_idx", gnnz + 1);
+    *gval = W.get_t<double>(tag + "_val", gnnz + 1);
+    k_lap_offdiag_fill<<<blocks, 256, 0, C.stream>>>(n, ptr, idx, val, *gptr, *gidx, *gval);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched += 2;
+    return gnnz;
+}
 
 // ---------------------------------------------------------------- streaming update
 // Sparsifier::form_laplacian (sparsifier.rs:693-709) adds the Laplacian of the edges inserted since the last

@@ -299,11 +299,50 @@ void gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, 
     out.from_upper_edges(n, va, vb, w);
 }
 
+// An f64 as Rust's Display writes it (the weights of edge_list_to_matrix_market, utils.rs:519): the shortest
+// digits that read back as v (the closest such digits), placed without an exponent and padded with zeros
+// (2^70 -> "1180591620717411300000", 5e-324 -> "0.000...005"); "NaN", "inf", "-inf"; -0.0 -> "-0".  The digits
+// come from to_chars' shortest scientific form, which picks the same digits.
+std::string rust_display_f64(double v) {
+    if (std::isnan(v)) return "NaN";
+    if (std::isinf(v)) return v < 0 ? "-inf" : "inf";
+    char sci[64];
+    auto r = std::to_chars(sci, sci + sizeof sci - 1, v, std::chars_format::scientific);
+    *r.ptr = 0;
+    std::string out;
+    const char* p = sci;
+    if (*p == '-') {
+        out += '-';
+        p++;
+    }
+    std::string dig;
+    for (; *p && *p != 'e'; p++)
+        if (*p != '.') dig += *p;
+    const int ex = *p == 'e' ? atoi(p + 1) : 0;  // value = d.ddd * 10^ex
+    while (dig.size() > 1 && dig.back() == '0') dig.pop_back();
+    if (dig == "0") return out + "0";
+    const int L = (int)dig.size();
+    const int ip = ex + 1;  // digits before the point
+    if (ip >= L) {
+        out += dig;
+        out.append((size_t)(ip - L), '0');
+    } else if (ip > 0) {
+        out += dig.substr(0, (size_t)ip);
+        out += '.';
+        out += dig.substr((size_t)ip);
+    } else {
+        out += "0.";
+        out.append((size_t)(-ip), '0');
+        out += dig;
+    }
+    return out;
+}
+
 // Edge list -> Matrix Market (edge_list_to_matrix_market, utils.rs:413-526).  The first line holds
 // "<num_nodes> <num_edges>" (the edge count is not used); each further non-blank line "u v [w]", w defaulting
 // to default_weight.  Pairs are stored as (min, max); for repeated pairs the first weight wins.  The output is
 // a symmetric real coordinate file with the pairs sorted, indices written as read, and weights in the
-// shortest round-trip decimal without an exponent (how Rust displays an f64).
+// shortest round-trip digits without an exponent (how Rust displays an f64, rust_display_f64).
 int edgelist_to_mtx(const char* in_path, const char* out_path, double default_weight, std::string& err) {
     FILE* f = fopen(in_path, "r");
     if (!f) {
@@ -382,14 +421,11 @@ int edgelist_to_mtx(const char* in_path, const char* out_path, double default_we
         if (t == 0 || keys[t].first != keys[t - 1].first) unique++;
     fprintf(o, "%%%%MatrixMarket matrix coordinate real symmetric\n%% Converted from %s\n%llu %llu %zu\n", in_path,
             n_nodes, n_nodes, unique);
-    char num[512];
     for (size_t t = 0; t < keys.size(); t++) {
         if (t > 0 && keys[t].first == keys[t - 1].first) continue;
         const double w = edges[keys[t].second].second;
-        auto r = std::to_chars(num, num + sizeof num - 1, w, std::chars_format::fixed);
-        *r.ptr = 0;
         fprintf(o, "%llu %llu %s\n", (unsigned long long)keys[t].first.first,
-                (unsigned long long)keys[t].first.second, num);
+                (unsigned long long)keys[t].first.second, rust_display_f64(w).c_str());
     }
     const bool ok = fclose(o) == 0;
     if (!ok) err = std::string("error writing ") + out_path;

@@ -24,6 +24,8 @@ void gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, 
 
 int read_mtx(const char* path, HostCsc& out, std::string& err);
 int edgelist_to_mtx(const char* in_path, const char* out_path, double default_weight, std::string& err);
+// an f64 as Rust's Display writes it (shortest round-trip digits, no exponent)
+std::string rust_display_f64(double v);
 int write_mtx(const char* path, int64_t n, const int64_t* colptr, const int32_t* rowidx, const double* val,
               std::string& err);
 

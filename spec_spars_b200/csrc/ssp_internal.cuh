@@ -82,21 +82,26 @@ __host__ __device__ __forceinline__ double edge_coin(uint64_t seed, int64_t e) {
 }
 
 // ---------------------------------------------------------------- device memory
-// Grow-only named buffers owned by a context, so repeated calls on one
-// context do not pay cudaMalloc/cudaFree inside the hot loop.
+// Grow-only named buffers owned by a context, so repeated calls on one context do not allocate inside the hot
+// loop.  Allocations and frees are stream-ordered (cudaMallocAsync / cudaFreeAsync on the context's stream,
+// from the device's default memory pool): a buffer that grows, or a workspace that is released, never waits
+// for the whole device the way cudaFree does, so contexts working side by side (the server's slots) do not
+// stall each other.  The context's stream is the only stream that touches these buffers.
 class Workspace {
 public:
     ~Workspace() { release(); }
+    // the stream allocations and frees are ordered on (the caller synchronizes the previous one first)
+    void set_stream(cudaStream_t s) { stream_ = s; }
     void* get(const std::string& name, size_t bytes) {
         bytes = bytes ? bytes : 16;
         auto it = bufs_.find(name);
         if (it != bufs_.end() && it->second.bytes >= bytes) return it->second.ptr;
         if (it != bufs_.end()) {
-            cudaFree(it->second.ptr);
+            cudaFreeAsync(it->second.ptr, stream_);
             bufs_.erase(it);
         }
         void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, bytes);
+        cudaError_t e = cudaMallocAsync(&p, bytes, stream_);
         if (e != cudaSuccess) {
             cudaGetLastError();
             throw Error(SSP_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes for '" + name +
@@ -112,7 +117,7 @@ public:
         auto it = bufs_.find(name);
         if (it != bufs_.end() && it->second.bytes >= bytes) return it->second.ptr;
         void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, bytes);
+        cudaError_t e = cudaMallocAsync(&p, bytes, stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
             throw Error(SSP_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes for '" + name +
@@ -121,20 +126,20 @@ public:
         if (it != bufs_.end()) {
             if (keep) {
                 e = cudaMemcpyAsync(p, it->second.ptr, keep, cudaMemcpyDeviceToDevice, stream);
-                if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
                 if (e != cudaSuccess) {
-                    cudaFree(p);
+                    cudaFreeAsync(p, stream);
                     throw Error(SSP_ERR_CUDA, std::string("workspace grow copy: ") + cudaGetErrorString(e));
                 }
             }
-            cudaFree(it->second.ptr);
+            // ordered after the copy on the same stream
+            cudaFreeAsync(it->second.ptr, stream);
             bufs_.erase(it);
         }
         bufs_[name] = {p, bytes};
         return p;
     }
     void release() {
-        for (auto& kv : bufs_) cudaFree(kv.second.ptr);
+        for (auto& kv : bufs_) cudaFreeAsync(kv.second.ptr, stream_);
         bufs_.clear();
     }
     size_t total_bytes() const {
@@ -151,6 +156,7 @@ public:
 private:
     struct Buf { void* ptr; size_t bytes; };
     std::map<std::string, Buf> bufs_;
+    cudaStream_t stream_ = nullptr;
 };
 
 // Launch shapes of the preconditioner's level launches (ssp_pcg.cu): per level and direction, the column width
@@ -274,6 +280,8 @@ bool read_mtx_device(Context& C, const char* path, int64_t* n, int64_t* nnz, int
                      double** val, const std::string& tag);
 void write_mtx_device(Context& C, const char* path, int64_t n, const int64_t* colptr, const int32_t* rowidx,
                       const double* val, const std::string& tag);
+// edge list -> .mtx on the device; false when the host converter must run (it then gives the same result)
+bool edgelist_to_mtx_device(Context& C, const char* in_path, const char* out_path, double default_weight);
 // stable ascending sort of (key, value) pairs by the low key_bits bits of the keys (LSD radix, 8-bit digits);
 // tmp_* are scratch arrays of n items; a scatter outside [0, n) is skipped and recorded in *err (if given)
 void radix_sort_u64(Context& C, uint64_t* keys, int32_t* vals, int64_t n, int key_bits, uint64_t* tmp_keys,
@@ -309,6 +317,11 @@ struct DevGraph {
 // tag prefixes the workspace buffers, so that two graphs can be held at once
 void build_graph_from_csc(Context& C, int64_t n, const int64_t* colptr, const int32_t* rowidx,
                           const double* val, int64_t nnz, DevGraph& G, const std::string& tag = "g");
+// the graph of a device Laplacian: its off-diagonal entries negated, in stored order (workspace buffers
+// tag_ptr/_idx/_val); returns the graph's nnz
+int64_t laplacian_to_graph_device(Context& C, int64_t n, int64_t nnz, const int64_t* ptr, const int32_t* idx,
+                                  const double* val, int64_t** gptr, int32_t** gidx, double** gval,
+                                  const std::string& tag = "lapg");
 // adjacency + Laplacian for a given device edge list (v1<v2, CSC order)
 void build_graph_from_edges(Context& C, DevGraph& G, const std::string& tag = "g");
 

@@ -346,6 +346,62 @@ struct File {
 };
 }  // namespace
 
+// the rest of an open file (size bytes) into dbuf: fread into one pinned buffer while the other copies
+static void upload_body(Context& C, FILE* f, int64_t size, char* dbuf, const char* path) {
+    if (size <= 0) return;
+    Pinned stage(2 * STAGE_BYTES);
+    cudaEvent_t done[2];
+    SSP_CUDA(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
+    SSP_CUDA(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
+    int64_t at = 0;
+    int slot = 0;
+    bool pending[2] = {false, false};
+    try {
+        while (at < size) {
+            char* hb = (char*)stage.p + (size_t)slot * STAGE_BYTES;
+            if (pending[slot]) SSP_CUDA(cudaEventSynchronize(done[slot]));
+            const size_t want = (size_t)std::min<int64_t>(STAGE_BYTES, size - at);
+            const size_t got = fread(hb, 1, want, f);
+            if (got != want) throw Error(SSP_ERR_IO, std::string("short read of ") + path);
+            SSP_CUDA(cudaMemcpyAsync(dbuf + at, hb, got, cudaMemcpyHostToDevice, C.stream));
+            SSP_CUDA(cudaEventRecord(done[slot], C.stream));
+            pending[slot] = true;
+            at += (int64_t)got;
+            slot ^= 1;
+        }
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    } catch (...) {
+        cudaStreamSynchronize(C.stream);
+        cudaEventDestroy(done[0]);
+        cudaEventDestroy(done[1]);
+        throw;
+    }
+    cudaEventDestroy(done[0]);
+    cudaEventDestroy(done[1]);
+}
+
+// line starts of a device text buffer (workspace tag_lstart); returns the line count (the last may be empty)
+static int64_t line_index(Context& C, const char* dbuf, int64_t size, const std::string& tag,
+                          unsigned long long* derr, int64_t** starts_out) {
+    Workspace& W = C.ws;
+    auto nm = [&](const char* s) { return tag + "_" + s; };
+    const int64_t tiles = std::max<int64_t>(1, ceil_div<int64_t>(size, NL_TILE));
+    int32_t* tcnt = W.get_t<int32_t>(nm("nlcnt"), tiles);
+    int64_t* toff = W.get_t<int64_t>(nm("nloff"), tiles + 1);
+    k_nl_count<<<(unsigned)tiles, NL_THREADS, 0, C.stream>>>(dbuf, size, tcnt);
+    SSP_CHECK_LAUNCH();
+    exclusive_scan_i32_to_i64(C, tcnt, toff, tiles, toff + tiles);
+    const int64_t newlines = read_i64(C, toff + tiles);
+    const int64_t nlines = newlines + 1;
+    int64_t* starts = W.get_t<int64_t>(nm("lstart"), nlines);
+    k_nl_starts<<<(unsigned)tiles, NL_THREADS, 0, C.stream>>>(dbuf, size, toff, starts, nlines, derr);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched += 2;
+    stage_check(C, derr, "line index");
+    *starts_out = starts;
+    return nlines;
+}
+
 // result: device CSC in workspace buffers tag_{colptr,rowidx,val}; returns false when the file needs the host
 // reader (the caller then runs it)
 bool read_mtx_device(Context& C, const char* path, int64_t* n_out, int64_t* nnz_out, int64_t** colptr,
@@ -365,52 +421,9 @@ bool read_mtx_device(Context& C, const char* path, int64_t* n_out, int64_t* nnz_
     unsigned long long* derr = W.get_t<unsigned long long>(nm("err"), 1);
     SSP_CUDA(cudaMemsetAsync(derr, 0xff, sizeof(unsigned long long), C.stream));
     char* dbuf = W.get_t<char>(nm("text"), (size_t)std::max<int64_t>(size, 1));
-    // stream the body: fread into one pinned buffer while the other copies
-    if (size > 0) {
-        Pinned stage(2 * STAGE_BYTES);
-        cudaEvent_t done[2];
-        SSP_CUDA(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
-        SSP_CUDA(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
-        int64_t at = 0;
-        int slot = 0;
-        bool pending[2] = {false, false};
-        try {
-            while (at < size) {
-                char* hb = (char*)stage.p + (size_t)slot * STAGE_BYTES;
-                if (pending[slot]) SSP_CUDA(cudaEventSynchronize(done[slot]));
-                const size_t want = (size_t)std::min<int64_t>(STAGE_BYTES, size - at);
-                const size_t got = fread(hb, 1, want, F.f);
-                if (got != want) throw Error(SSP_ERR_IO, std::string("short read of ") + path);
-                SSP_CUDA(cudaMemcpyAsync(dbuf + at, hb, got, cudaMemcpyHostToDevice, C.stream));
-                SSP_CUDA(cudaEventRecord(done[slot], C.stream));
-                pending[slot] = true;
-                at += (int64_t)got;
-                slot ^= 1;
-            }
-            SSP_CUDA(cudaStreamSynchronize(C.stream));
-        } catch (...) {
-            cudaStreamSynchronize(C.stream);
-            cudaEventDestroy(done[0]);
-            cudaEventDestroy(done[1]);
-            throw;
-        }
-        cudaEventDestroy(done[0]);
-        cudaEventDestroy(done[1]);
-    }
-    // line index
-    const int64_t tiles = std::max<int64_t>(1, ceil_div<int64_t>(size, NL_TILE));
-    int32_t* tcnt = W.get_t<int32_t>(nm("nlcnt"), tiles);
-    int64_t* toff = W.get_t<int64_t>(nm("nloff"), tiles + 1);
-    k_nl_count<<<(unsigned)tiles, NL_THREADS, 0, C.stream>>>(dbuf, size, tcnt);
-    SSP_CHECK_LAUNCH();
-    exclusive_scan_i32_to_i64(C, tcnt, toff, tiles, toff + tiles);
-    const int64_t newlines = read_i64(C, toff + tiles);
-    const int64_t nlines = newlines + 1;  // the last line may be empty
-    int64_t* starts = W.get_t<int64_t>(nm("lstart"), nlines);
-    k_nl_starts<<<(unsigned)tiles, NL_THREADS, 0, C.stream>>>(dbuf, size, toff, starts, nlines, derr);
-    SSP_CHECK_LAUNCH();
-    C.kernels_launched += 2;
-    stage_check(C, derr, "line index");
+    upload_body(C, F.f, size, dbuf, path);
+    int64_t* starts = nullptr;
+    const int64_t nlines = line_index(C, dbuf, size, tag, derr, &starts);
     // parse
     int32_t* kind = W.get_t<int32_t>(nm("kind"), nlines);
     int64_t* I = W.get_t<int64_t>(nm("li"), nlines);
@@ -746,6 +759,280 @@ void write_mtx_device(Context& C, const char* path, int64_t n, const int64_t* co
         throw Error(SSP_ERR_IO, "write failed");
     }
     F.f = nullptr;
+}
+
+// ---------------------------------------------------------------- edge lists
+// edge_list_to_matrix_market (utils.rs:413-526) on the device: the body's lines are indexed and parsed in
+// parallel, the (min, max) pairs sorted stably (so the first weight of a repeated pair wins), and the lines
+// "i j w" formatted with w as Rust displays an f64.  Anything the per-line parser does not mirror exactly
+// (signs, endpoints of 2^32 or more, separators other than spaces and tabs, a malformed line, a weight whose
+// shortest text needs the host) sends the whole file to the host converter, which then writes the same bytes
+// or reports the same error.  Weights the exact converter cannot read (more than 19 digits, inf, hex, trailing
+// text) are read by strtod on the host from the line's own bytes, as the host converter reads them.
+namespace {
+enum : int32_t { EL_BLANK = 0, EL_ENTRY = 1, EL_HOST = 2 };
+constexpr int EL_WSLOT = 48;  // bytes per formatted weight
+
+__device__ __forceinline__ bool el_digit(char c) { return c >= '0' && c <= '9'; }
+
+// kind[l]; for entries key = min << 32 | max, the weight (or wfix[l] = 1 and wpos[l] = its first byte)
+__global__ void k_parse_edge_lines(const char* __restrict__ buf, int64_t size, const int64_t* __restrict__ starts,
+                                   int64_t nlines, double defw, int32_t* __restrict__ kind,
+                                   uint64_t* __restrict__ key, double* __restrict__ wt, int32_t* __restrict__ wfix,
+                                   int64_t* __restrict__ wpos) {
+    const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nlines) return;
+    const char* p = buf + starts[l];
+    const char* e = buf + (l + 1 < nlines ? starts[l + 1] - 1 : size);  // excludes the newline
+    wfix[l] = 0;
+    // blank: nothing but spaces, tabs and carriage returns (the host converter's test)
+    const char* q = p;
+    while (q < e && (*q == ' ' || *q == '\t' || *q == '\r')) q++;
+    if (q >= e) {
+        kind[l] = EL_BLANK;
+        return;
+    }
+    kind[l] = EL_HOST;
+    uint64_t ep[2];
+    for (int k = 0; k < 2; k++) {
+        if (k == 1) {
+            if (q >= e || (*q != ' ' && *q != '\t')) return;
+            while (q < e && (*q == ' ' || *q == '\t')) q++;
+        }
+        if (q >= e || !el_digit(*q)) return;
+        uint64_t v = 0;
+        int nd = 0;
+        for (; q < e && el_digit(*q); q++, nd++) {
+            if (nd == 19) return;  // might not fit: the host reads it
+            v = v * 10 + (uint64_t)(*q - '0');
+        }
+        ep[k] = v;
+    }
+    const uint64_t i = ep[0] < ep[1] ? ep[0] : ep[1], j = ep[0] < ep[1] ? ep[1] : ep[0];
+    if (j >> 32) return;
+    double w = defw;
+    if (q < e && *q != '\r') {
+        if (*q != ' ' && *q != '\t') return;  // text glued to the second endpoint
+        while (q < e && (*q == ' ' || *q == '\t')) q++;
+        if (q < e && *q != '\r') {
+            const char* t = q;
+            while (q < e && !is_space(*q)) q++;
+            if (q == t) return;  // a vertical tab or form feed: the host converter's strtod rules
+            if (dec::parse_decimal(t, q, &w) != dec::PARSE_OK) {
+                wfix[l] = 1;
+                wpos[l] = t - buf;
+                w = 0.0;
+            }
+        }
+    }
+    key[l] = i << 32 | j;
+    wt[l] = w;
+    kind[l] = EL_ENTRY;
+}
+
+__global__ void k_el_flags(int64_t nlines, const int32_t* __restrict__ kind, int32_t* __restrict__ isent,
+                           int32_t* __restrict__ nhost) {
+    const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nlines) return;
+    isent[l] = kind[l] == EL_ENTRY;
+    if (kind[l] == EL_HOST) atomicAdd(nhost, 1);
+}
+
+// entries in line order (their sort payload: the entry index), and the lines whose weight strtod reads
+__global__ void k_el_gather(int64_t nlines, const int32_t* __restrict__ kind, const int64_t* __restrict__ rank,
+                            const uint64_t* __restrict__ lkey, const double* __restrict__ lw,
+                            const int32_t* __restrict__ wfix, int64_t nent, uint64_t* __restrict__ ekey,
+                            int32_t* __restrict__ eidx, double* __restrict__ ew, int32_t* __restrict__ nfix,
+                            int64_t* __restrict__ fixline, int32_t fixcap, unsigned long long* __restrict__ err) {
+    const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nlines || kind[l] != EL_ENTRY) return;
+    const int64_t r = rank[l];
+    if (r < 0 || r >= nent) {
+        check_fail(err, 7, l);
+        return;
+    }
+    ekey[r] = lkey[l];
+    eidx[r] = (int32_t)r;
+    ew[r] = lw[l];
+    if (wfix[l]) {
+        const int32_t t = atomicAdd(nfix, 1);
+        if (t < fixcap) fixline[t] = l;
+    }
+}
+
+// after the sort: the first entry of each pair, its weight formatted, its line's length
+__global__ void k_el_format(int64_t nent, const uint64_t* __restrict__ skey, const int32_t* __restrict__ sidx,
+                            const double* __restrict__ ew, int32_t* __restrict__ head, char* __restrict__ wtxt,
+                            int32_t* __restrict__ llen, int32_t* __restrict__ nmiss) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nent) return;
+    const bool h = t == 0 || skey[t] != skey[t - 1];
+    head[t] = h;
+    llen[t] = 0;
+    if (!h) return;
+    char* o = wtxt + t * EL_WSLOT;
+    const int len = dec::format_shortest_fixed(ew[sidx[t]], o, EL_WSLOT);
+    if (len < 0) {
+        atomicAdd(nmiss, 1);
+        return;
+    }
+    const uint64_t k = skey[t];
+    llen[t] = dec_len((int64_t)(k >> 32)) + 1 + dec_len((int64_t)(k & 0xffffffffu)) + 1 + len + 1;
+}
+
+__global__ void k_el_write(int64_t nent, const uint64_t* __restrict__ skey, const int32_t* __restrict__ head,
+                           const char* __restrict__ wtxt, const int32_t* __restrict__ llen,
+                           const int64_t* __restrict__ loff, char* __restrict__ out, int64_t out_bytes,
+                           unsigned long long* __restrict__ err) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nent || !head[t]) return;
+    const uint64_t k = skey[t];
+    const int64_t at = loff[t];
+    if (at < 0 || at + llen[t] > out_bytes) {
+        check_fail(err, 8, t);
+        return;
+    }
+    char* o = out + at;
+    o = put_int(o, (int64_t)(k >> 32));
+    *o++ = ' ';
+    o = put_int(o, (int64_t)(k & 0xffffffffu));
+    *o++ = ' ';
+    const int wl = llen[t] - (int)(o - (out + at)) - 1;
+    for (int i = 0; i < wl; i++) o[i] = wtxt[t * EL_WSLOT + i];
+    o[wl] = '\n';
+}
+}  // namespace
+
+// false: the host converter must run (it then writes the same file or reports the same error)
+bool edgelist_to_mtx_device(Context& C, const char* in_path, const char* out_path, double default_weight) {
+    File F;
+    F.f = fopen(in_path, "rb");
+    if (!F.f) return false;
+    // the first line "<num_nodes> <num_edges>", read as the host converter reads it
+    std::string first;
+    {
+        char b[4096];
+        for (;;) {
+            if (!fgets(b, sizeof b, F.f)) break;
+            first += b;
+            if (!first.empty() && first.back() == '\n') break;
+        }
+    }
+    unsigned long long n_nodes = 0, n_decl = 0;
+    if (first.empty() || sscanf(first.c_str(), "%llu %llu", &n_nodes, &n_decl) != 2) return false;
+    const long body = ftell(F.f);
+    struct stat st;
+    if (body < 0 || fstat(fileno(F.f), &st) != 0) return false;
+    const int64_t size = (int64_t)st.st_size - body;
+    Workspace& W = C.ws;
+    const std::string tag = "edl";
+    auto nm = [&](const char* s) { return tag + "_" + s; };
+    unsigned long long* derr = W.get_t<unsigned long long>(nm("err"), 1);
+    SSP_CUDA(cudaMemsetAsync(derr, 0xff, sizeof(unsigned long long), C.stream));
+    char* dbuf = W.get_t<char>(nm("text"), (size_t)std::max<int64_t>(size, 1));
+    upload_body(C, F.f, size, dbuf, in_path);
+    int64_t* starts = nullptr;
+    const int64_t nlines = line_index(C, dbuf, size, tag, derr, &starts);
+    int32_t* kind = W.get_t<int32_t>(nm("kind"), nlines);
+    uint64_t* lkey = W.get_t<uint64_t>(nm("lkey"), nlines);
+    double* lw = W.get_t<double>(nm("lw"), nlines);
+    int32_t* wfix = W.get_t<int32_t>(nm("wfix"), nlines);
+    int64_t* wpos = W.get_t<int64_t>(nm("wpos"), nlines);
+    const unsigned lb = (unsigned)ceil_div<int64_t>(nlines, 256);
+    k_parse_edge_lines<<<lb, 256, 0, C.stream>>>(dbuf, size, starts, nlines, default_weight, kind, lkey, lw, wfix,
+                                                 wpos);
+    SSP_CHECK_LAUNCH();
+    int32_t* isent = W.get_t<int32_t>(nm("isent"), nlines);
+    int64_t* rank = W.get_t<int64_t>(nm("rank"), nlines + 1);
+    int32_t* cnts = W.get_t<int32_t>(nm("cnts"), 4);  // host lines, weights for strtod, weights to format
+    SSP_CUDA(cudaMemsetAsync(cnts, 0, sizeof(int32_t) * 4, C.stream));
+    k_el_flags<<<lb, 256, 0, C.stream>>>(nlines, kind, isent, cnts);
+    SSP_CHECK_LAUNCH();
+    exclusive_scan_i32_to_i64(C, isent, rank, nlines, rank + nlines);
+    C.kernels_launched += 2;
+    const int64_t nent = read_i64(C, rank + nlines);
+    int32_t hc[4];
+    SSP_CUDA(cudaMemcpyAsync(hc, cnts, sizeof hc, cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    if (hc[0] != 0 || nent >= (int64_t)INT32_MAX) return false;
+    const int64_t ne = std::max<int64_t>(nent, 1);
+    uint64_t* ekey = W.get_t<uint64_t>(nm("ekey"), ne);
+    int32_t* eidx = W.get_t<int32_t>(nm("eidx"), ne);
+    double* ew = W.get_t<double>(nm("ew"), ne);
+    int64_t* fixline = W.get_t<int64_t>(nm("fix"), HOST_FIX_CAP);
+    k_el_gather<<<lb, 256, 0, C.stream>>>(nlines, kind, rank, lkey, lw, wfix, nent, ekey, eidx, ew, cnts + 1, fixline,
+                                          HOST_FIX_CAP, derr);
+    SSP_CHECK_LAUNCH();
+    C.kernels_launched++;
+    stage_check(C, derr, "edge gather");
+    SSP_CUDA(cudaMemcpyAsync(hc, cnts, sizeof hc, cudaMemcpyDeviceToHost, C.stream));
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    const int32_t nfix = hc[1];
+    if (nfix > HOST_FIX_CAP) return false;
+    if (nfix > 0) {
+        // strtod on the host, from each line's weight to the line's end (the host converter's reading)
+        std::vector<int64_t> lines(nfix);
+        SSP_CUDA(cudaMemcpyAsync(lines.data(), fixline, sizeof(int64_t) * nfix, cudaMemcpyDeviceToHost, C.stream));
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+        for (int64_t l : lines) {
+            int64_t hp[3] = {0, 0, 0};
+            SSP_CUDA(cudaMemcpyAsync(&hp[0], wpos + l, sizeof(int64_t), cudaMemcpyDeviceToHost, C.stream));
+            if (l + 1 < nlines)
+                SSP_CUDA(cudaMemcpyAsync(&hp[1], starts + l + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaMemcpyAsync(&hp[2], rank + l, sizeof(int64_t), cudaMemcpyDeviceToHost, C.stream));
+            SSP_CUDA(cudaStreamSynchronize(C.stream));
+            const int64_t end = l + 1 < nlines ? hp[1] - 1 : size;
+            std::string text((size_t)std::max<int64_t>(end - hp[0], 0), '\0');
+            if (!text.empty()) {
+                SSP_CUDA(cudaMemcpyAsync(&text[0], dbuf + hp[0], text.size(), cudaMemcpyDeviceToHost, C.stream));
+                SSP_CUDA(cudaStreamSynchronize(C.stream));
+            }
+            char* stop = nullptr;
+            const double x = strtod(text.c_str(), &stop);
+            if (stop == text.c_str()) return false;  // "bad weight": the host converter reports it
+            SSP_CUDA(cudaMemcpyAsync(ew + hp[2], &x, sizeof(double), cudaMemcpyHostToDevice, C.stream));
+        }
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    }
+    // stable sort by (min, max): the first occurrence of a pair leads its run
+    int64_t U = 0;
+    std::string body_text;
+    if (nent > 0) {
+        uint64_t* tk = W.get_t<uint64_t>(nm("tkey"), ne);
+        int32_t* ti = W.get_t<int32_t>(nm("tidx"), ne);
+        radix_sort_u64(C, ekey, eidx, nent, 64, tk, ti, derr);
+        stage_check(C, derr, "edge sort");
+        int32_t* head = W.get_t<int32_t>(nm("head"), ne);
+        char* wtxt = W.get_t<char>(nm("wtxt"), (size_t)ne * EL_WSLOT);
+        int32_t* llen = W.get_t<int32_t>(nm("llen"), ne);
+        int64_t* loff = W.get_t<int64_t>(nm("loff"), ne + 1);
+        const unsigned eb = (unsigned)ceil_div<int64_t>(nent, 256);
+        k_el_format<<<eb, 256, 0, C.stream>>>(nent, ekey, eidx, ew, head, wtxt, llen, cnts + 2);
+        SSP_CHECK_LAUNCH();
+        exclusive_scan_i32_to_i64(C, llen, loff, nent, loff + nent);
+        C.kernels_launched++;
+        SSP_CUDA(cudaMemcpyAsync(hc, cnts, sizeof hc, cudaMemcpyDeviceToHost, C.stream));
+        const int64_t bytes = read_i64(C, loff + nent);
+        if (hc[2] != 0) return false;  // a weight whose text the device does not produce
+        int64_t* hoff = W.get_t<int64_t>(nm("hoff"), ne + 1);
+        exclusive_scan_i32_to_i64(C, head, hoff, nent, hoff + nent);
+        U = read_i64(C, hoff + nent);
+        char* dout = W.get_t<char>(nm("out"), (size_t)std::max<int64_t>(bytes, 1));
+        k_el_write<<<eb, 256, 0, C.stream>>>(nent, ekey, head, wtxt, llen, loff, dout, bytes, derr);
+        SSP_CHECK_LAUNCH();
+        C.kernels_launched++;
+        stage_check(C, derr, "edge write");
+        body_text.resize((size_t)bytes);
+        if (bytes) copy_d2h(C, &body_text[0], dout, (size_t)bytes);
+        SSP_CUDA(cudaStreamSynchronize(C.stream));
+    }
+    FILE* o = fopen(out_path, "w");
+    if (!o) return false;
+    fprintf(o, "%%%%MatrixMarket matrix coordinate real symmetric\n%% Converted from %s\n%llu %llu %lld\n", in_path,
+            n_nodes, n_nodes, (long long)U);
+    const bool ok = fwrite(body_text.data(), 1, body_text.size(), o) == body_text.size();
+    if (fclose(o) != 0 || !ok) throw Error(SSP_ERR_IO, std::string("error writing ") + out_path);
+    return true;
 }
 
 }  // namespace ssp

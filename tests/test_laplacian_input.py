@@ -129,3 +129,27 @@ def test_sparsifier_from_matrix_probabilities(ssp, ora, ctx, tmp_path):
     p = sp.compute_probs(d)
     assert np.array_equal(p, ora.probs(w, d, prm.beta(G.n), float(prm.jl_dim(G.n))))
     assert np.all((p >= 0) & (p <= 1))
+
+
+@pytest.mark.gpu
+def test_sparsify_laplacian_rejects_bad_colptr_on_the_device(ssp, ctx):
+    """The Laplacian's graph is formed on the device; column pointers that decrease, or that do not start at
+    0 and end at nnz, are rejected there with the host conversion's messages."""
+    import spec_spars_b200._lib as Lb
+    prm = ssp.SparsifierParameters.cli(0.5)
+    ri = np.array([0, 1, 0, 1, 2, 1, 2], np.int32)
+    va = np.array([1.0, -1.0, -1.0, 2.0, -1.0, -1.0, 1.0])
+    for colptr, msg in (([0, 2, 1, 7], b"non-decreasing"), ([0, 2, 5, 6], b"start at 0 and end at nnz")):
+        cp = np.array(colptr, np.int64)
+        s = Lb._Csc(3, 7, cp.ctypes.data, ri.ctypes.data, va.ctypes.data, Lb.SSP_MEM_HOST)
+        out, st = Lb._CscOut(), Lb._Stats()
+        rc = Lb.lib().ssp_sparsify_laplacian(ctx._h, ctypes.byref(s), ctypes.byref(prm._s), Lb.SSP_MEM_HOST,
+                                             ctypes.byref(out), ctypes.byref(st))
+        assert rc != 0 and msg in Lb.lib().ssp_last_error(), colptr
+    # a valid path graph 0 - 1 - 2 goes through
+    cp = np.array([0, 2, 5, 7], np.int64)
+    s = Lb._Csc(3, 7, cp.ctypes.data, ri.ctypes.data, va.ctypes.data, Lb.SSP_MEM_HOST)
+    out, st = Lb._CscOut(), Lb._Stats()
+    Lb._check(Lb.lib().ssp_sparsify_laplacian(ctx._h, ctypes.byref(s), ctypes.byref(prm._s), Lb.SSP_MEM_HOST,
+                                              ctypes.byref(out), ctypes.byref(st)))
+    assert st.m_in == 2
