@@ -408,9 +408,10 @@ int ssp_edgelist_to_mtx(const char* input_path, const char* output_path, double 
 /* the same conversion on the GPU (edge_list_to_matrix_market, src/utils.rs:413-526): lines indexed and parsed on
  * the device, pairs sorted stably, lines formatted with Rust's f64 text; byte for byte the file
  * ssp_edgelist_to_mtx writes.  A file the device parser does not mirror (signed or 2^32+ endpoints, unusual
- * separators, malformed lines) is converted by ssp_edgelist_to_mtx instead, with its result or error. */
+ * separators, malformed lines) is converted by ssp_edgelist_to_mtx instead, with its result or error;
+ * *on_device (if not NULL) says which of the two wrote the file (1: the GPU). */
 int ssp_edgelist_to_mtx_device(ssp_context* ctx, const char* input_path, const char* output_path,
-                               double default_weight);
+                               double default_weight, int32_t* on_device);
 
 /* ---- synthetic graphs (seeded, identical on every host) as symmetric host CSC ---- */
 int ssp_gen_grid2d(int64_t nx, int64_t ny, double w, ssp_csc_out* out);

@@ -181,7 +181,8 @@ def lib():
             "ssp_gen_grid3d": ([I64, I64, I64, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_er": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_edgelist_to_mtx": ([ctypes.c_char_p, ctypes.c_char_p, DBL], ctypes.c_int),
-            "ssp_edgelist_to_mtx_device": ([P, ctypes.c_char_p, ctypes.c_char_p, DBL], ctypes.c_int),
+            "ssp_edgelist_to_mtx_device": ([P, ctypes.c_char_p, ctypes.c_char_p, DBL, ctypes.POINTER(I32)],
+                                           ctypes.c_int),
             "ssp_format_shortest": ([DBL, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
             "ssp_gen_rmat": ([I32, I32, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
             "ssp_gen_rgg": ([I64, DBL, DBL, DBL, U64, ctypes.POINTER(_CscOut)], ctypes.c_int),
@@ -391,11 +392,13 @@ def gen_er(n, avg_degree, wlo=0.5, whi=2.0, seed=1):
 
 def edge_list_to_matrix_market(input_path, output_path, default_weight=1.0, ctx=None):
     """edge_list_to_matrix_market (utils.rs:413-526).  With a Context the conversion runs on its GPU
-    (ssp_edgelist_to_mtx_device); the file is the same either way."""
+    (ssp_edgelist_to_mtx_device) and returns True when the GPU wrote the file, False when the file went to the
+    host converter; the file is the same either way."""
     if ctx is not None:
+        dev = I32(0)
         _check(lib().ssp_edgelist_to_mtx_device(ctx._h, str(input_path).encode(), str(output_path).encode(),
-                                                default_weight))
-        return
+                                                default_weight, ctypes.byref(dev)))
+        return bool(dev.value)
     _check(lib().ssp_edgelist_to_mtx(str(input_path).encode(), str(output_path).encode(), default_weight))
 
 

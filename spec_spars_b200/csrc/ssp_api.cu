@@ -1482,11 +1482,15 @@ int ssp_edgelist_to_mtx(const char* input_path, const char* output_path, double 
 }
 
 int ssp_edgelist_to_mtx_device(ssp_context* c, const char* input_path, const char* output_path,
-                               double default_weight) {
+                               double default_weight, int32_t* on_device) {
     return guarded([&] {
         SSP_REQUIRE(c && input_path && output_path, SSP_ERR_INVALID, "bad arguments");
         SSP_CUDA(cudaSetDevice(c->ctx.device));
-        if (edgelist_to_mtx_device(c->ctx, input_path, output_path, default_weight)) return;
+        if (on_device) *on_device = 0;
+        if (edgelist_to_mtx_device(c->ctx, input_path, output_path, default_weight)) {
+            if (on_device) *on_device = 1;
+            return;
+        }
         std::string err;
         if (edgelist_to_mtx(input_path, output_path, default_weight, err) != 0) throw Error(SSP_ERR_IO, err);
     });

@@ -12,19 +12,20 @@ def _convert_both(ssp, ctx, tmp_path, text, default_weight=1.5):
     src.write_bytes(text.encode() if isinstance(text, str) else text)
     dh, dd = tmp_path / "host.mtx", tmp_path / "dev.mtx"
     eh = ed = None
+    on_device = None
     try:
         ssp.edge_list_to_matrix_market(src, dh, default_weight)
     except ssp.SspError as e:
         eh = (e.code, str(e))
     try:
-        ssp.edge_list_to_matrix_market(src, dd, default_weight, ctx=ctx)
+        on_device = ssp.edge_list_to_matrix_market(src, dd, default_weight, ctx=ctx)
     except ssp.SspError as e:
         ed = (e.code, str(e))
     assert eh == ed
     if eh is None:
         assert dd.read_bytes() == dh.read_bytes()
-        return dd.read_text()
-    return None
+        return dd.read_text(), on_device
+    return None, on_device
 
 
 def _random_list(rng, n, m, weights):
@@ -35,11 +36,13 @@ def _random_list(rng, n, m, weights):
         sep = rng.choice([" ", "\t", "  ", " \t "])
         ln = f"{u[k]}{sep}{v[k]}"
         r = rng.random()
-        if weights and r < 0.8:
+        weighted = weights is not None and r < 0.8
+        if weighted:
             w = weights(rng)
             ln += f"{rng.choice([' ', chr(9)])}{w}"
         if rng.random() < 0.05:
-            ln += rng.choice([" ", "\r", " trailing text"])
+            # text after the weight is ignored; after the endpoints it would be read as the weight
+            ln += rng.choice([" ", "\r", " trailing text"] if weighted else [" ", "\r"])
         lines.append(ln)
         if rng.random() < 0.02:
             lines.append(rng.choice(["", "   ", "\t"]))
@@ -65,8 +68,8 @@ def _weight(rng):
 def test_random_lists_equal_host_bytes(ssp, ctx, tmp_path, seed):
     rng = np.random.default_rng(seed)
     text = _random_list(rng, 500, 20000, _weight)
-    out = _convert_both(ssp, ctx, tmp_path, text)
-    assert out is not None and out.count("\n") > 1000
+    out, on_device = _convert_both(ssp, ctx, tmp_path, text)
+    assert out is not None and out.count("\n") > 1000 and on_device
 
 
 def test_large_list_with_duplicates(ssp, ctx, tmp_path):
@@ -75,28 +78,33 @@ def test_large_list_with_duplicates(ssp, ctx, tmp_path):
     u = rng.integers(0, n, size=m)
     v = rng.integers(0, n, size=m)
     w = rng.uniform(0.5, 2.0, size=m)
-    body = "\n".join(f"{a} {b} {c!r}" for a, b, c in zip(u, v, w))
-    out = _convert_both(ssp, ctx, tmp_path, f"{n} {m}\n" + body + "\n")
-    assert out is not None
+    body = "\n".join(f"{a} {b} {float(c)!r}" for a, b, c in zip(u, v, w))
+    out, on_device = _convert_both(ssp, ctx, tmp_path, f"{n} {m}\n" + body + "\n")
+    assert out is not None and on_device
 
 
-@pytest.mark.parametrize("text", [
-    "3 2\n0 1 2.5\n1 2\n",                      # default weight
-    "3 2\r\n0 1 2.5\r\n1 2\r\n",                # CRLF
-    "3 1\n0 1 2.5",                             # no final newline
-    "3 0\n",                                    # no edges
-    "3 0",                                      # header only, no newline
-    "4 3\n0 1 inf\n1 2 nan\n2 3 -0.0\n",        # strtod forms (host text for inf / NaN)
-    "4 2\n0 1 0x1p3\n2 3 1e400\n",              # hex and overflow: strtod on the host
-    "4 2\n+0 1 2.0\n2 3 1.0\n",                 # a sign: the host converter reads the file
-    "4 2\n0 1 2.5\n2 3x 1.0\n",                 # text glued to an endpoint: the host's error
-    "4 2\n0 1 2.5\n2\n",                        # missing endpoint: the host's error
-    "4 1\n0 1 abc\n",                           # bad weight: the host's error
-    "4 1\n0 1 2.5abc\n",                        # strtod reads the prefix
-    "",                                         # empty file: the host's error
-    "x y\n0 1\n",                               # bad header: the host's error
-    "5 1\n4294967296 1 2.0\n",                  # endpoint >= 2^32: the host converter reads the file
-    "3 2\n0 1 1e-30\n1 2 1e300\n",              # weights whose text the device leaves to the host
+# (text, written by the GPU)
+@pytest.mark.parametrize("text,dev", [
+    ("3 2\n0 1 2.5\n1 2\n", True),                       # default weight
+    ("3 2\r\n0 1 2.5\r\n1 2\r\n", True),                 # CRLF
+    ("3 1\n0 1 2.5", True),                              # no final newline
+    ("3 0\n", True),                                     # no edges
+    ("3 0", True),                                       # header only, no newline
+    ("4 2\n0 1 0x1p3\n2 3 1e-5\n", True),                 # hex: strtod on the host for that weight
+    ("4 1\n0 1 2.5abc\n", True),                         # strtod reads the prefix
+    ("4 3\n0 1 inf\n1 2 nan\n2 3 -0.0\n", False),         # host text for inf / NaN
+    ("4 2\n+0 1 2.0\n2 3 1.0\n", False),                  # a sign
+    ("4 2\n0 1 2.5\n2 3x 1.0\n", None),                   # text glued to an endpoint: the host's error
+    ("4 2\n0 1 2.5\n2\n", None),                          # missing endpoint: the host's error
+    ("4 1\n0 1 abc\n", None),                            # bad weight: the host's error
+    ("", None),                                          # empty file: the host's error
+    ("x y\n0 1\n", None),                                # bad header: the host's error
+    ("5 1\n4294967296 1 2.0\n", False),                   # endpoint >= 2^32
+    ("3 2\n0 1 1e-30\n1 2 1e300\n", False),               # weights whose text the device leaves to the host
 ])
-def test_edge_cases_match_host(ssp, ctx, tmp_path, text):
-    _convert_both(ssp, ctx, tmp_path, text)
+def test_edge_cases_match_host(ssp, ctx, tmp_path, text, dev):
+    out, on_device = _convert_both(ssp, ctx, tmp_path, text)
+    if dev is None:
+        assert out is None
+    else:
+        assert out is not None and on_device == dev
