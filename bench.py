@@ -302,9 +302,10 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def serving_mix(S, count, max_n, seed=4, precision="fp64"):
+def serving_mix(S, count, max_n, seed=4, precision="fp64", min_n=1000, eps_choices=(0.3, 0.5)):
     """The serving mix of seeded requests: random-geometric or ER graphs (equiprobable), n log-uniform in
-    [1e3, max_n], average degree uniform in 8..32, weights uniform [0.1, 10] rounded to FP32, eps 0.3 or 0.5.
+    [min_n, max_n], average degree uniform in 8..32, weights uniform [0.1, 10] rounded to FP32, eps drawn from
+    eps_choices (0.3 or 0.5).
     Every request asks for the autotuned factor without the dense tail (factor_max_degree = -1,
     dense_threshold = 0), so the server may batch it; the plain path runs the same parameters one request at a
     time."""
@@ -312,9 +313,9 @@ def serving_mix(S, count, max_n, seed=4, precision="fp64"):
     rng = np.random.default_rng(seed)
     reqs = []
     for i in range(count):
-        n = int(10 ** rng.uniform(3.0, math.log10(max_n)))
+        n = int(10 ** rng.uniform(math.log10(min_n), math.log10(max_n)))
         d = float(rng.integers(8, 33))
-        eps = float(rng.choice([0.3, 0.5]))
+        eps = float(rng.choice(list(eps_choices)))
         G = S.gen_rgg(n, d, 0.1, 10.0, 1000 + i) if rng.random() < 0.5 else S.gen_er(n, d, 0.1, 10.0, 1000 + i)
         prm = S.SparsifierParameters.baseline(eps, pcg_tol=PCG_TOL, sampling_seed=i)
         prm.dense_threshold = 0
@@ -383,10 +384,10 @@ def plain_measure(S, reqs):
     return sum(G.nnz // 2 for G, _ in reqs) / wall
 
 
-def serving_section(S, count, max_n, slots=2, max_batch=64):
+def serving_section(S, count, max_n, slots=2, max_batch=64, min_n=1000, eps_choices=(0.3, 0.5)):
     """The serving mix on the plain path, through the server without batching (slots only) and with
     continuous batching, in FP64 and in mixed precision."""
-    reqs = serving_mix(S, count, max_n)
+    reqs = serving_mix(S, count, max_n, min_n=min_n, eps_choices=eps_choices)
     m_total = sum(G.nnz // 2 for G, _ in reqs)
     plain = plain_measure(S, reqs)
     # the library's default single-graph parameters (autotuned factor with the dense tail)
@@ -395,9 +396,10 @@ def serving_section(S, count, max_n, slots=2, max_batch=64):
                                       for G, p in reqs])
     slots_only = serve_measure(S, reqs, 4, 1)
     batched = serve_measure(S, reqs, slots, max_batch)
-    batched_mixed = serve_measure(S, serving_mix(S, count, max_n, precision="mixed"), slots, max_batch)
-    return {"workload": "serving mix", "requests": count, "n_range": [1000, max_n], "degree_range": [8, 32],
-            "eps": [0.3, 0.5], "edges": m_total,
+    batched_mixed = serve_measure(S, serving_mix(S, count, max_n, precision="mixed", min_n=min_n,
+                                                 eps_choices=eps_choices), slots, max_batch)
+    return {"workload": "serving mix", "requests": count, "n_range": [min_n, max_n], "degree_range": [8, 32],
+            "eps": list(eps_choices), "edges": m_total,
             "plain_fp64_edges_per_s": plain, "plain_fp64_default_params_edges_per_s": plain_default,
             "served_slots_only_fp64": slots_only,
             "served_batched_fp64": batched, "served_batched_mixed": batched_mixed,
@@ -424,7 +426,8 @@ def serving_lite(S, count=48, max_n=20_000, slots=2, max_batch=64):
 def run_serve(args):
     """--serve: the serving mix through the persistent request loop (ssp_server_*), beside the plain path."""
     import spec_spars_b200 as S
-    sec = serving_section(S, args.serve_requests, args.serve_max_n, args.serve_slots, args.serve_batch)
+    sec = serving_section(S, args.serve_requests, args.serve_max_n, args.serve_slots, args.serve_batch,
+                          args.serve_min_n, tuple(float(x) for x in args.serve_eps.split(",")))
     best = sec["served_batched_mixed"] if args.precision == "mixed" else sec["served_batched_fp64"]
     line = {"metric": "serving mix: input edges sparsified/sec", "value": best["value"], "unit": "edges/s",
             "n_gpus": 1, "higher_is_better": True, "dtype": "f64" if args.precision == "fp64" else "mixed",
@@ -700,6 +703,8 @@ def main():
     ap.add_argument("--serve", action="store_true", help="run the serving mix through the request loop")
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--serve-max-n", type=int, default=100_000)
+    ap.add_argument("--serve-min-n", type=int, default=1000)
+    ap.add_argument("--serve-eps", default="0.3,0.5", help="comma-separated eps values the requests draw from")
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--mtx", action="store_true", help="time the GPU Matrix Market reader/writer and sparsify_dataset")
