@@ -36,6 +36,9 @@ WORKLOADS = {
     "rmat_s18": ("rmat", dict(scale=18, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=3), 0.3),
 }
 PCG_TOL = 1e-8
+# the arithmetic of each --precision: plain FP64; FP32 inner PCG inside FP64 refinement; FP64 PCG whose
+# preconditioner (the triangular solves) runs in FP32
+PREC_DTYPE = {"fp64": "f64", "mixed": "f32 inner PCG, f64 dots + refinement", "pc32": "f64 PCG, f32 preconditioner"}
 
 
 def make_graph(S, name, rank=0):
@@ -575,6 +578,23 @@ def mesh_step(S, ctx, stream, name="grid3d_128"):
                         "frac": pb / (pc_ms / 1000.0) / 1e9 / peak if pc_ms > 0 else None,
                         "spmm_avg_ms": sp_ms},
            "spectral": spec}
+    # the same step with the preconditioner in FP32 (FP64 PCG, product and dots), one timed step; its first
+    # three preconditioner applications also measure this factor's level shapes for FP32
+    prm.precision = S.SSP_PRECISION_PC32
+    e0.record(stream)
+    H32, s32 = ctx.sparsify_device(G.n, G.nnz, cp.data_ptr(), ri.data_ptr(), va.data_ptr(), prm)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms32 = e0.elapsed_time(e1)
+    spec32 = spectral_check(S, ctx, LG, S.DeviceCSC(G.n, *H32), eps, s32)
+    out["pc32"] = {"dtype": PREC_DTYPE["pc32"], "ms_per_step": ms32,
+                   "value": s32["m_in"] / (ms32 / 1000.0), "unit": "edges/s", "steps": 1,
+                   "pcg_iters_max": s32["pcg_max_iters_used"], "pcg_max_relres": s32["pcg_max_relres"],
+                   "kept_fraction": s32["m_out"] / s32["m_in"],
+                   "precond_avg_ms": s32["ms_precond"] / max(1, s32["n_precond"]),
+                   "note": "precond_avg_ms averages the first three applications, which measure the level "
+                           "shapes (one width each)",
+                   "spectral": spec32}
     del cp, ri, va
     return out
 
@@ -592,6 +612,8 @@ def run_sharded(args, S, torch, dist, world, rank, local):
         prm.jl_dim_override = args.jl_cols
     if args.precision == "mixed":
         prm.precision = S.SSP_PRECISION_MIXED
+    elif args.precision == "pc32":
+        prm.precision = S.SSP_PRECISION_PC32
     ctx = S.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
@@ -667,7 +689,7 @@ def run_sharded(args, S, torch, dist, world, rank, local):
         line = {"metric": "input edges sparsified/sec", "value": m / (ms / 1000.0), "unit": "edges/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-                "dtype": "f64" if args.precision == "fp64" else "f32 inner PCG, f64 dots + refinement",
+                "dtype": PREC_DTYPE[args.precision],
                 "data": "synthetic",
                 "config": {"workload": args.workload, "n": G.n, "m": m, "eps": eps, "k": k, "pcg_tol": PCG_TOL,
                            "precision": args.precision,
@@ -694,8 +716,9 @@ def main():
     ap.add_argument("--workload", default="er_n1M_deg20", choices=list(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
-                    help="PCG arithmetic: fp64, or FP32 inner solves inside FP64 refinement to the same tolerance")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "pc32"],
+                    help="PCG arithmetic: fp64; mixed (FP32 inner solves inside FP64 refinement to the same tolerance); "
+                         "pc32 (FP64 PCG with the preconditioner in FP32)")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the secondary mixed-precision measurement reported beside the FP64 headline")
     ap.add_argument("--jl-cols", type=int, default=0,
@@ -763,6 +786,8 @@ def main():
         prm.jl_dim_override = args.jl_cols
     if args.precision == "mixed":
         prm.precision = S.SSP_PRECISION_MIXED
+    elif args.precision == "pc32":
+        prm.precision = S.SSP_PRECISION_PC32
     ctx = S.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
@@ -866,7 +891,7 @@ def main():
     line = {"metric": "input edges sparsified/sec", "value": value, "unit": "edges/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32 inner PCG, f64 dots + refinement",
+            "dtype": PREC_DTYPE[args.precision],
             "data": "synthetic",
             "config": {"workload": args.workload, "n": n, "m": m, "eps": eps, "k": k, "pcg_tol": PCG_TOL,
                        "precision": args.precision,

@@ -59,9 +59,12 @@ extern "C" {
 #define SSP_PRECISION_FP64 0  /* every vector and matrix in FP64                                     */
 #define SSP_PRECISION_MIXED 1 /* SpMM, triangular solves and vectors in FP32 with FP64 dot products,
                                  inside FP64 iterative refinement to the same tolerance                */
+#define SSP_PRECISION_PC32 2  /* FP64 PCG (vectors, SpMM, dot products) whose preconditioner runs in FP32:
+                                 the triangular solves read FP32 factor values and gather FP32 rows    */
 /* where the preconditioner's level-launch shapes came from (ssp_stats.trsv_shapes) */
 #define SSP_TRSV_RULE 0     /* fixed rule: levels of at most 1024 rows 8 columns per warp row, wider ones 32 */
-#define SSP_TRSV_TUNED 1    /* measured in this call: every width timed per level, the fastest kept        */
+#define SSP_TRSV_TUNED 1    /* measured in this call: the solve's first applications, one per width, timed
+                               level by level; the fastest width per level kept                          */
 #define SSP_TRSV_CACHED 2   /* measured by an earlier call on the same factor shape (context cache)        */
 #define SSP_TRSV_FORCED 3   /* one width for every level, from the environment (SSP_TRSV_WIDTH)            */
 /* reweighting of kept edges */
@@ -152,7 +155,8 @@ typedef struct {
     int32_t trsv_levels_w8;         /* level launches (forward + backward) at 8 columns per warp row, */
     int32_t trsv_levels_w16;        /* ... at 16, */
     int32_t trsv_levels_w32;        /* ... at 32 (runs of thin levels are not counted: always 8) */
-    double ms_trsv_tune;            /* device time spent measuring them (0 when taken from the cache) */
+    double ms_trsv_tune;            /* device time of the applications that measured them (real
+                                       applications of the solve; 0 when taken from the cache) */
 } ssp_stats;
 
 typedef struct {

@@ -25,6 +25,7 @@ pub const SSP_JL_SCALE_FIXED: i32 = 0;
 pub const SSP_JL_SCALE_INV_SQRT_K: i32 = 1;
 pub const SSP_PRECISION_FP64: i32 = 0;
 pub const SSP_PRECISION_MIXED: i32 = 1;
+pub const SSP_PRECISION_PC32: i32 = 2;
 pub const SSP_REWEIGHT_INV_SQRT_P: i32 = 0;
 pub const SSP_REWEIGHT_INV_P: i32 = 1;
 pub const SSP_TRSV_RULE: i32 = 0;

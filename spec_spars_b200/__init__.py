@@ -16,6 +16,6 @@ from ._lib import (  # noqa: F401
     Server, request_footprint, edge_list_to_matrix_market, format_shortest,
     stage_graph, stage_sketch, stage_factor, stage_precond, stage_diff_norms, stage_probs, stage_coins, stage_scan,
     stage_sample_apply, SSP_JL_DIM_REF, SSP_JL_DIM_24, SSP_JL_SCALE_FIXED, SSP_JL_SCALE_INV_SQRT_K,
-    SSP_REWEIGHT_INV_SQRT_P, SSP_REWEIGHT_INV_P, SSP_PRECISION_FP64, SSP_PRECISION_MIXED, LIB_PATH, HEADER_SYMBOLS,
+    SSP_REWEIGHT_INV_SQRT_P, SSP_REWEIGHT_INV_P, SSP_PRECISION_FP64, SSP_PRECISION_MIXED, SSP_PRECISION_PC32, LIB_PATH, HEADER_SYMBOLS,
     SSP_TRSV_RULE, SSP_TRSV_TUNED, SSP_TRSV_CACHED, SSP_TRSV_FORCED,
 )

@@ -16,7 +16,7 @@ SSP_JL_DIM_REF, SSP_JL_DIM_24 = 0, 1
 SSP_JL_SCALE_FIXED, SSP_JL_SCALE_INV_SQRT_K = 0, 1
 SSP_REWEIGHT_INV_SQRT_P, SSP_REWEIGHT_INV_P = 0, 1
 SSP_TRSV_RULE, SSP_TRSV_TUNED, SSP_TRSV_CACHED, SSP_TRSV_FORCED = 0, 1, 2, 3
-SSP_PRECISION_FP64, SSP_PRECISION_MIXED = 0, 1
+SSP_PRECISION_FP64, SSP_PRECISION_MIXED, SSP_PRECISION_PC32 = 0, 1, 2
 
 ERROR_NAMES = {-1: "SSP_ERR_INVALID", -2: "SSP_ERR_CUDA", -3: "SSP_ERR_NOMEM", -4: "SSP_ERR_NOT_CONVERGED",
                -5: "SSP_ERR_CAPACITY", -6: "SSP_ERR_IO", -7: "SSP_ERR_NO_DEVICE", -8: "SSP_ERR_PENDING"}

@@ -23,6 +23,8 @@
 #include <cmath>
 #include <cstdlib>
 
+#include <functional>
+
 #include "ssp_internal.cuh"
 
 namespace ssp {
@@ -362,6 +364,10 @@ __global__ void k_axpy_x(int64_t n, int64_t ld, const double* __restrict__ alpha
 __global__ void k_d2f(int64_t count, const double* __restrict__ src, float* __restrict__ dst) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
         dst[i] = (float)src[i];
+}
+__global__ void k_f2d(int64_t count, const float* __restrict__ src, double* __restrict__ dst) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
 }
 
 // inner right-hand side: the FP64 residual of the columns still active, rounded to T; zero elsewhere
@@ -933,15 +939,6 @@ struct FactorVals {
     const T* D;
 };
 
-struct Precond {
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    ~Precond() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-    }
-};
-
 // Column layouts of the triangular-solve launches.  A level launch gives each warp row a width of W columns
 // (8, 16 or 32; TILE / W blocks per column tile): with W = 32 a warp's lanes cover a tile's columns of one row
 // (256-byte gathers); with W = 8 a warp works on four rows at once, with four times the blocks, which suits
@@ -1085,14 +1082,14 @@ static int64_t launch_precond(Context& C, const DevFactor& F, const FactorVals<T
     return launches;
 }
 
-// Level-launch shapes by measurement.  Each width is timed on every level launch of a full preconditioner
-// application (CUDA events around each launch, on the solve's own right-hand sides), twice in interleaved
-// order, and each level keeps the width of its smaller best time.  The values are the same whatever the
-// widths, so only the time depends on the choice.  Kept per context under a signature of the factor's
-// level structure and the solve's shape, so repeated solves on the same graph measure once.  Small solves
-// (n * ld below SSP_TRSV_TUNE_MIN elements, 2^26 unless the environment variable of that name says otherwise)
-// keep the rule: there the measurement would cost more than it could save.  SSP_TRSV_TUNE=0 keeps the rule
-// everywhere; SSP_TRSV_WIDTH=8|16|32 forces one width.
+// Level-launch shapes by measurement.  Each width is timed on every level launch of one preconditioner
+// application (CUDA events around each launch), and each level and direction keeps its fastest width.  In a PCG
+// solve the measured applications are the solve's own first three (one per width): the values are the same
+// whatever the widths, so they are real iterations and nothing is applied twice; the preconditioner's graph is
+// then rebuilt with the result.  The shapes are kept per context under a signature of the factor's level
+// structure and the solve's shape, so repeated solves on the same graph measure once.  Small solves (n * ld
+// below SSP_TRSV_TUNE_MIN elements, 2^26 unless the environment variable of that name says otherwise) keep the
+// rule.  SSP_TRSV_TUNE=0 keeps the rule everywhere; SSP_TRSV_WIDTH=8|16|32 forces one width.
 #ifndef SSP_TRSV_TUNE_MIN
 #define SSP_TRSV_TUNE_MIN (int64_t(1) << 26)
 #endif
@@ -1139,112 +1136,121 @@ static void count_trsv_widths(const DevFactor& F, const TrsvShapes& sh, PcgRepor
     }
 }
 
-template <class T>
-static void tune_trsv_shapes(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
-                             int64_t ld, int32_t kcols, const RowAct& ra, TrsvShapes& out, double& ms) {
-    constexpr int ROUNDS = 2;
-    const int nw = TRSV_NWIDTH;
-    std::vector<LevelEvents> ev(nw * ROUNDS);
-    std::vector<TrsvShapes> forced(nw);
-    for (int c = 0; c < nw; c++) {
-        forced[c].fw.assign(F.num_levels, (uint8_t)c);
-        forced[c].bw.assign(F.num_levels, (uint8_t)c);
-    }
-    cudaEvent_t e0, e1;
-    SSP_CUDA(cudaEventCreate(&e0));
-    SSP_CUDA(cudaEventCreate(&e1));
-    SSP_CUDA(cudaEventRecord(e0, C.stream));
-    for (int round = 0; round < ROUNDS; round++)
-        for (int c = 0; c < nw; c++) {
-            const int cc = round % 2 ? nw - 1 - c : c;  // alternate the order between rounds
-            C.kernels_launched += launch_precond<T>(C, F, V, n, r, y, ld, kcols, ra, &forced[cc], &ev[round * nw + cc]);
-        }
-    SSP_CUDA(cudaEventRecord(e1, C.stream));
-    SSP_CUDA(cudaEventSynchronize(e1));
-    float tt = 0;
-    SSP_CUDA(cudaEventElapsedTime(&tt, e0, e1));
-    ms = tt;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    // best[dir][level][width]
+static int rule_code(const DevFactor& F, int32_t l, bool narrow) {
+    if (narrow) return 0;
+    return std::min(F.level_ptr[l + 1] - F.level_ptr[l] <= SPLIT_LEVEL_ROWS ? 0 : 2, TRSV_NWIDTH - 1);
+}
+static TrsvShapes rule_shapes(const DevFactor& F, bool narrow) {
+    TrsvShapes s;
+    s.fw.resize(F.num_levels);
+    for (int32_t l = 0; l < F.num_levels; l++) s.fw[l] = (uint8_t)rule_code(F, l, narrow);
+    s.bw = s.fw;
+    return s;
+}
+static TrsvShapes forced_shapes(const DevFactor& F, int code) {
+    TrsvShapes s;
+    s.fw.assign(F.num_levels, (uint8_t)std::min(code, TRSV_NWIDTH - 1));
+    s.bw = s.fw;
+    return s;
+}
+
+// per level and direction, the width with the smallest time in ev[c] (one measured application per width
+// code c); the rule's width unless another is faster
+static void shapes_from_events(const DevFactor& F, const LevelEvents* ev, int nw, TrsvShapes& out) {
     const float INF = 3.0e38f;
     std::vector<float> best(2 * (size_t)F.num_levels * nw, INF);
-    for (int round = 0; round < ROUNDS; round++)
-        for (int c = 0; c < nw; c++) {
-            const LevelEvents& L = ev[round * nw + c];
-            for (size_t i = 0; i < L.used; i++) {
-                float t = 0;
-                SSP_CUDA(cudaEventElapsedTime(&t, L.ev[2 * i], L.ev[2 * i + 1]));
-                const size_t o = ((size_t)(L.tag[i].first ? 0 : 1) * F.num_levels + L.tag[i].second) * nw + c;
-                best[o] = std::min(best[o], t);
-            }
+    for (int c = 0; c < nw; c++) {
+        const LevelEvents& L = ev[c];
+        for (size_t i = 0; i < L.used; i++) {
+            float t = 0;
+            SSP_CUDA(cudaEventElapsedTime(&t, L.ev[2 * i], L.ev[2 * i + 1]));
+            const size_t o = ((size_t)(L.tag[i].first ? 0 : 1) * F.num_levels + L.tag[i].second) * nw + c;
+            best[o] = std::min(best[o], t);
         }
+    }
     out.fw.assign(F.num_levels, 0);
     out.bw.assign(F.num_levels, 0);
     for (int dir = 0; dir < 2; dir++)
         for (int32_t l = 0; l < F.num_levels; l++) {
             const float* b = &best[((size_t)dir * F.num_levels + l) * nw];
-            // the rule's width unless another is faster
-            int pick = std::min(F.level_ptr[l + 1] - F.level_ptr[l] <= SPLIT_LEVEL_ROWS ? 0 : 2, nw - 1);
+            int pick = rule_code(F, l, false);
             for (int c = 0; c < nw; c++)
                 if (b[c] < b[pick]) pick = c;
             (dir == 0 ? out.fw : out.bw)[l] = (uint8_t)pick;
         }
 }
 
-// The shapes a solve's preconditioner uses: forced, cached, measured now, or (nullptr) the rule.
-template <class T>
-static const TrsvShapes* trsv_shapes_for(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n,
-                                         const T* r, T* y, int64_t ld, int32_t kcols, const RowAct& ra,
-                                         TrsvShapes& store, PcgReport& rep) {
+// how a solve's level shapes are chosen: Forced and Cached fill store; Measure returns the cache key
+enum class ShapeSource { Rule, Forced, Cached, Measure };
+static ShapeSource trsv_shape_source(Context& C, const DevFactor& F, int64_t n, int64_t ld, int32_t kcols,
+                                     size_t elem, bool segmented, TrsvShapes& store, uint64_t& key) {
     const bool narrow = TILE > NARROW_W && kcols <= NARROW_W;
-    rep.trsv_shapes = SSP_TRSV_RULE;
-    const TrsvShapes* out = nullptr;
+    if (narrow || F.num_levels == 0) return ShapeSource::Rule;  // one width for all (8 columns)
     const char* fw = getenv("SSP_TRSV_WIDTH");
-    const char* tn = getenv("SSP_TRSV_TUNE");
-    if (narrow || F.num_levels == 0) {
-        // one width for all (8 columns), nothing to choose
-    } else if (fw && fw[0]) {
+    if (fw && fw[0]) {
         const int w = atoi(fw);
-        const int code = w >= 32 ? 2 : w >= 16 ? 1 : 0;
-        store.fw.assign(F.num_levels, (uint8_t)std::min(code, TRSV_NWIDTH - 1));
-        store.bw = store.fw;
-        rep.trsv_shapes = SSP_TRSV_FORCED;
-        out = &store;
-    } else if (!(tn && tn[0] == '0') && n * ld >= trsv_tune_min()) {
-        const uint64_t key = trsv_signature(F, n, ld, kcols, sizeof(T), ra.act != nullptr);
-        auto& E = C.trsv_cache.entries;
-        for (auto& e : E)
-            if (e.first == key) {
-                store = e.second;
-                rep.trsv_shapes = SSP_TRSV_CACHED;
-                out = &store;
-                break;
-            }
-        if (!out) {
-            double ms = 0;
-            tune_trsv_shapes<T>(C, F, V, n, r, y, ld, kcols, ra, store, ms);
-            rep.ms_trsv_tune += ms;
-            rep.trsv_shapes = SSP_TRSV_TUNED;
-            if ((int)E.size() >= TRSV_CACHE_MAX) E.erase(E.begin());
-            E.push_back({key, store});
-            out = &store;
+        store = forced_shapes(F, w >= 32 ? 2 : w >= 16 ? 1 : 0);
+        return ShapeSource::Forced;
+    }
+    const char* tn = getenv("SSP_TRSV_TUNE");
+    if ((tn && tn[0] == '0') || n * ld < trsv_tune_min()) return ShapeSource::Rule;
+    key = trsv_signature(F, n, ld, kcols, elem, segmented);
+    for (auto& e : C.trsv_cache.entries)
+        if (e.first == key) {
+            store = e.second;
+            return ShapeSource::Cached;
         }
-    }
-    if (out) {
-        count_trsv_widths(F, *out, rep);
-    } else {
-        TrsvShapes rule;
-        rule.fw.resize(F.num_levels);
-        for (int32_t l = 0; l < F.num_levels; l++)
-            rule.fw[l] = narrow ? 0
-                                : (uint8_t)std::min(F.level_ptr[l + 1] - F.level_ptr[l] <= SPLIT_LEVEL_ROWS ? 0 : 2,
-                                                    TRSV_NWIDTH - 1);
-        rule.bw = rule.fw;
-        count_trsv_widths(F, rule, rep);
-    }
-    return out;
+    return ShapeSource::Measure;
 }
+
+static void cache_shapes(Context& C, uint64_t key, const TrsvShapes& s) {
+    auto& E = C.trsv_cache.entries;
+    if ((int)E.size() >= TRSV_CACHE_MAX) E.erase(E.begin());
+    E.push_back({key, s});
+}
+
+static void report_shapes(PcgReport& rep, int32_t source, const DevFactor& F, const TrsvShapes& s) {
+    rep.trsv_shapes = source;
+    count_trsv_widths(F, s, rep);
+}
+
+// Three applications, one per width, then the per-level choice (the stage entry point's measurement).
+template <class T>
+static void tune_trsv_shapes(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
+                             int64_t ld, int32_t kcols, const RowAct& ra, TrsvShapes& out) {
+    LevelEvents ev[3];
+    for (int c = 0; c < TRSV_NWIDTH; c++) {
+        const TrsvShapes f = forced_shapes(F, c);
+        C.kernels_launched += launch_precond<T>(C, F, V, n, r, y, ld, kcols, ra, &f, &ev[c]);
+    }
+    SSP_CUDA(cudaStreamSynchronize(C.stream));
+    shapes_from_events(F, ev, TRSV_NWIDTH, out);
+}
+
+// The preconditioner application as a CUDA graph, with its level shapes.  measure: the shapes are still to be
+// measured by the solve's next applications (pcg_solve), which then rebuild the graph.
+struct Precond {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    TrsvShapes shapes;
+    bool has_shapes = false;
+    bool measure = false;
+    uint64_t key = 0;
+    int mstep = 0;                 // widths measured so far
+    LevelEvents mev[3];            // their level launches
+    cudaEvent_t m0 = nullptr, m1 = nullptr;  // around the measured applications
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+    ~Precond() {
+        drop_graph();
+        if (m0) cudaEventDestroy(m0);
+        if (m1) cudaEventDestroy(m1);
+    }
+};
 
 // ---------------------------------------------------------------- SpMM plan
 // The Laplacian as the SpMM reads it.  When one tile of the gathered operand (n rows of TILE values) is
@@ -1428,17 +1434,16 @@ static void launch_spmm(Context& C, int64_t n, const SpmmPlan& A, const T* aval,
     }
 }
 
-// The preconditioner application as a CUDA graph, with its level-launch shapes chosen first (the measurement,
-// when one runs, uses r and overwrites y; both are the solve's own buffers and y is written before it is read)
-template <class T>
-static void build_precond_graph(Context& C, const DevFactor& F, const FactorVals<T>& V, int64_t n, const T* r, T* y,
-                                int64_t ld, int32_t kcols, Precond& P, int64_t& launches, PcgReport& rep,
-                                const RowAct& ra = RowAct()) {
-    TrsvShapes store;
-    const TrsvShapes* sh = trsv_shapes_for<T>(C, F, V, n, r, y, ld, kcols, ra, store, rep);
+// One preconditioner application from the solve's r into its z with the given level shapes (nullptr: the rule)
+// and optional events around each level launch; returns the kernels it launched.
+using PcApply = std::function<int64_t(const TrsvShapes*, LevelEvents*)>;
+
+// P's graph: one application with P's shapes (the rule when it has none)
+static void capture_precond(Context& C, Precond& P, int64_t& launches, const PcApply& pc) {
+    P.drop_graph();
     SSP_CUDA(cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeThreadLocal));
     try {
-        launches = launch_precond<T>(C, F, V, n, r, y, ld, kcols, ra, sh);
+        launches = pc(P.has_shapes ? &P.shapes : nullptr, nullptr);
     } catch (...) {
         cudaGraph_t g;
         cudaStreamEndCapture(C.stream, &g);
@@ -1449,13 +1454,47 @@ static void build_precond_graph(Context& C, const DevFactor& F, const FactorVals
     SSP_CUDA(cudaGraphInstantiate(&P.exec, P.graph, 0));
 }
 
+// The solve's preconditioner: its level shapes (forced, cached, the rule, or the rule until the solve's first
+// applications have measured them) and its graph.  elem: bytes per value of the triangular solves.
+static void build_precond_graph(Context& C, const DevFactor& F, int64_t n, int64_t ld, int32_t kcols, size_t elem,
+                                Precond& P, int64_t& launches, PcgReport& rep, const RowAct& ra,
+                                const PcApply& pc) {
+    TrsvShapes store;
+    uint64_t key = 0;
+    const bool narrow = TILE > NARROW_W && kcols <= NARROW_W;
+    const ShapeSource src = trsv_shape_source(C, F, n, ld, kcols, elem, ra.act != nullptr, store, key);
+    P.measure = false;
+    P.has_shapes = src == ShapeSource::Forced || src == ShapeSource::Cached;
+    if (P.has_shapes) {
+        P.shapes = store;
+        report_shapes(rep, src == ShapeSource::Forced ? SSP_TRSV_FORCED : SSP_TRSV_CACHED, F, store);
+    } else {
+        report_shapes(rep, SSP_TRSV_RULE, F, rule_shapes(F, narrow));
+        if (src == ShapeSource::Measure) {
+            P.measure = true;
+            P.key = key;
+            P.mstep = 0;
+        }
+    }
+    capture_precond(C, P, launches, pc);
+}
+
 static FactorVals<double> fp64_vals(const DevFactor& F) { return FactorVals<double>{F.prow_val, F.pcol_val, F.D}; }
 
-// apply M^{-1} to R into Z once (tile-major n x ld blocks; stage entry point)
+// apply M^{-1} to R into Z once (tile-major n x ld blocks; stage entry point).  When the shapes are to be
+// measured, one application per width measures them first (each writes the same Z).
 void precond_apply_device(Context& C, const DevFactor& F, const double* R, double* Z, int64_t ld) {
     TrsvShapes store;
-    PcgReport rep;
-    const TrsvShapes* sh = trsv_shapes_for<double>(C, F, fp64_vals(F), F.n, R, Z, ld, (int32_t)ld, RowAct(), store, rep);
+    uint64_t key = 0;
+    const ShapeSource src = trsv_shape_source(C, F, F.n, ld, (int32_t)ld, sizeof(double), false, store, key);
+    const TrsvShapes* sh = nullptr;
+    if (src == ShapeSource::Forced || src == ShapeSource::Cached) {
+        sh = &store;
+    } else if (src == ShapeSource::Measure) {
+        tune_trsv_shapes<double>(C, F, fp64_vals(F), F.n, R, Z, ld, (int32_t)ld, RowAct(), store);
+        cache_shapes(C, key, store);
+        sh = &store;
+    }
     int64_t l = launch_precond<double>(C, F, fp64_vals(F), F.n, R, Z, ld, (int32_t)ld, RowAct(), sh);
     C.kernels_launched += l;
 }
@@ -1508,9 +1547,10 @@ struct PcgTimers {
 // caller; e zero).  Returns the iterations of the loop.
 template <class T>
 static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const SpmmPlan& A, const T* aval,
-                         const DevFactor& F, const FactorVals<T>& V,
-                         const Precond& P, int64_t pc_launches, PcgBufs<T> B, ColState& S, Reducer& R,
-                         int32_t max_iters, const PcgOptions& opt, PcgTimers& tm, const RowAct& ra = RowAct()) {
+                         const DevFactor& F, const PcApply& pc,
+                         Precond& P, int64_t& pc_launches, PcgBufs<T> B, ColState& S, Reducer& R,
+                         int32_t max_iters, const PcgOptions& opt, PcgTimers& tm, PcgReport& rep,
+                         const RowAct& ra = RowAct()) {
     // without a residual history or progress output the iterations after the first run on the device
     // SSP_PCG_HOST_LOOP=1 keeps every iteration on the host loop (the same kernels, launched one by one), for
     // profilers that do not look inside conditional graph nodes
@@ -1540,14 +1580,44 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
                                                                                         S.active, (int32_t*)ra.act);
         C.kernels_launched++;
     };
+    // one preconditioner application: the graph, or while the level shapes are being measured, one width's
+    // launches with events around each level (a real application: every width gives the same values)
+    auto apply_precond = [&]() {
+        tm.pc.begin(C.stream);
+        if (P.measure && P.mstep < TRSV_NWIDTH) {
+            if (P.mstep == 0) {
+                if (!P.m0) SSP_CUDA(cudaEventCreate(&P.m0));
+                if (!P.m1) SSP_CUDA(cudaEventCreate(&P.m1));
+                SSP_CUDA(cudaEventRecord(P.m0, C.stream));
+            }
+            const TrsvShapes f = forced_shapes(F, P.mstep);
+            C.kernels_launched += pc(&f, &P.mev[P.mstep]);
+            if (++P.mstep == TRSV_NWIDTH) SSP_CUDA(cudaEventRecord(P.m1, C.stream));
+        } else {
+            SSP_CUDA(cudaGraphLaunch(P.exec, C.stream));
+            C.kernels_launched += pc_launches;
+        }
+        tm.pc.end(C.stream);
+    };
+    // after a synchronization that follows the last measured application: keep the fastest width per level,
+    // cache it, and rebuild the graph with it
+    auto finish_measure = [&]() {
+        if (!P.measure || P.mstep < TRSV_NWIDTH) return;
+        shapes_from_events(F, P.mev, TRSV_NWIDTH, P.shapes);
+        float ms = 0;
+        SSP_CUDA(cudaEventElapsedTime(&ms, P.m0, P.m1));
+        rep.ms_trsv_tune += ms;
+        P.has_shapes = true;
+        P.measure = false;
+        cache_shapes(C, P.key, P.shapes);
+        report_shapes(rep, SSP_TRSV_TUNED, F, P.shapes);
+        capture_precond(C, P, pc_launches, pc);
+    };
     int64_t active = read_i64(C, S.nactive);
     int32_t it = 0;
     if (active == 0) return 0;
     update_act();
-    tm.pc.begin(C.stream);
-    SSP_CUDA(cudaGraphLaunch(P.exec, C.stream));
-    tm.pc.end(C.stream);
-    C.kernels_launched += pc_launches;
+    apply_precond();
     R.run<OP_DOT, T>(B.r, B.z, S.rz);
     SSP_CUDA(cudaMemcpyAsync(B.p, B.z, sizeof(T) * total, cudaMemcpyDeviceToDevice, C.stream));
     tm.loop.begin(C.stream);
@@ -1569,6 +1639,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         C.kernels_launched++;
         update_act();
         active = read_i64(C, S.nactive);
+        finish_measure();
         if (opt.history || seg_history) {
             std::vector<double> hrr(ns), hbb(ns);
             SSP_CUDA(cudaMemcpyAsync(hrr.data(), S.rr, sizeof(double) * ns, cudaMemcpyDeviceToHost, C.stream));
@@ -1595,11 +1666,8 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
             fprintf(stderr, "[ssp] pcg%s iter %d: %lld columns active\n", sizeof(T) == 4 ? " (fp32 inner)" : "", it,
                     (long long)active);
         if (active == 0) break;
-        if (device_loop) break;
-        tm.pc.begin(C.stream);
-        SSP_CUDA(cudaGraphLaunch(P.exec, C.stream));
-        tm.pc.end(C.stream);
-        C.kernels_launched += pc_launches;
+        if (device_loop && !P.measure) break;
+        apply_precond();
         R.run<OP_DOT, T>(B.r, B.z, S.rz_new);
         k_cols_beta<<<cg, 256, 0, C.stream>>>(ns, S);
         k_update_xp<T><<<egrid, 256, 0, C.stream>>>(n, ld, S.alpha, S.beta, B.z, B.p, B.e, G);
@@ -1644,7 +1712,7 @@ static int32_t pcg_solve(Context& C, int64_t n, int32_t k, int64_t ld, const Spm
         cudaGraphNode_t wnode;
         SSP_CUDA(cudaGraphAddNode(&wnode, L.graph, roots.data(), nn, &cp));
         capture(cp.conditional.phGraph_out[0], [&] {
-            body_kernels += launch_precond<T>(C, F, V, n, B.r, B.z, ld, k, ra);
+            body_kernels += pc(P.has_shapes ? &P.shapes : nullptr, nullptr);
             R.run<OP_DOT, T>(B.r, B.z, S.rz_new);
             k_cols_beta<<<cg, 256, 0, C.stream>>>(ns, S);
             k_update_xp<T><<<egrid, 256, 0, C.stream>>>(n, ld, S.alpha, S.beta, B.z, B.p, B.e, G);
@@ -1689,7 +1757,8 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 bool d2_accumulate) {
     SSP_REQUIRE(k > 0, SSP_ERR_INVALID, "pcg: k must be positive");
     const bool mixed = opt.precision == SSP_PRECISION_MIXED;
-    SSP_REQUIRE(mixed || opt.precision == SSP_PRECISION_FP64, SSP_ERR_INVALID, "pcg: unknown precision");
+    SSP_REQUIRE(mixed || opt.precision == SSP_PRECISION_FP64 || opt.precision == SSP_PRECISION_PC32, SSP_ERR_INVALID,
+                "pcg: unknown precision");
     const int64_t ld = ((int64_t)k + TILE - 1) / TILE * TILE;
     const int64_t ntiles = ld / TILE;
     const int64_t total = n * ld;
@@ -1770,9 +1839,42 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         Precond P;
         int64_t pc_launches = 0;
         if (read_i64(C, S.nactive) > 0) {
-            build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P, pc_launches, rep, ra);
-            it = pcg_solve<double>(C, n, k, ld, A, A.val, F, fp64_vals(F), P, pc_launches,
-                                   PcgBufs<double>{x, r, z, p, q}, S, R, opt.max_iters, opt, tm, ra);
+            PcApply pc;
+            size_t elem = sizeof(double);
+            if (opt.precision == SSP_PRECISION_PC32) {
+                // FP64 PCG with the triangular solves in FP32: r rounded on the way in, z widened on the way out
+                float* fv = W.get_t<float>("pcgp_fval", 2 * F.nnz + n + 1);
+                const int64_t fcount[3] = {F.nnz, F.nnz, n};
+                const double* fsrc[3] = {F.prow_val, F.pcol_val, F.D};
+                int64_t at = 0;
+                for (int i = 0; i < 3; i++) {
+                    if (fcount[i] > 0)
+                        k_d2f<<<grid_for(fcount[i], 256, 148 * 16), 256, 0, C.stream>>>(fcount[i], fsrc[i], fv + at);
+                    at += fcount[i];
+                }
+                SSP_CHECK_LAUNCH();
+                C.kernels_launched += 3;
+                const FactorVals<float> V32{fv, fv + F.nnz, fv + 2 * F.nnz};
+                float* r32 = W.get_t<float>("pcgp_r", total);
+                float* z32 = W.get_t<float>("pcgp_z", total);
+                if (TILE > NARROW_W && k <= NARROW_W) SSP_CUDA(cudaMemsetAsync(z32, 0, sizeof(float) * total, C.stream));
+                const int cgrid = grid_for(total, 256, 148 * 16);
+                pc = [&C, &F, V32, n, r32, z32, r, z, ld, k, ra, total, cgrid](const TrsvShapes* sh, LevelEvents* lev) {
+                    k_d2f<<<cgrid, 256, 0, C.stream>>>(total, r, r32);
+                    const int64_t l = launch_precond<float>(C, F, V32, n, r32, z32, ld, k, ra, sh, lev);
+                    k_f2d<<<cgrid, 256, 0, C.stream>>>(total, z32, z);
+                    SSP_CHECK_LAUNCH();
+                    return l + 2;
+                };
+                elem = sizeof(float);
+            } else {
+                pc = [&C, &F, n, r, z, ld, k, ra](const TrsvShapes* sh, LevelEvents* lev) {
+                    return launch_precond<double>(C, F, fp64_vals(F), n, r, z, ld, k, ra, sh, lev);
+                };
+            }
+            build_precond_graph(C, F, n, ld, k, elem, P, pc_launches, rep, ra, pc);
+            it = pcg_solve<double>(C, n, k, ld, A, A.val, F, pc, P, pc_launches,
+                                   PcgBufs<double>{x, r, z, p, q}, S, R, opt.max_iters, opt, tm, rep, ra);
         }
     } else {
         // FP32 copies of the Laplacian and factor values, and the FP32 inner vectors
@@ -1813,14 +1915,17 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, MIXED_INNER_REDUCTION, S.thr, Si, R.G);
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
-                if (!P32.exec) build_precond_graph<float>(C, F, V32, n, r32, z32, ld, k, P32, pc32, rep, ra);
+                const PcApply pc32f = [&C, &F, V32, n, r32, z32, ld, k, ra](const TrsvShapes* sh, LevelEvents* lev) {
+                    return launch_precond<float>(C, F, V32, n, r32, z32, ld, k, ra, sh, lev);
+                };
+                if (!P32.exec) build_precond_graph(C, F, n, ld, k, sizeof(float), P32, pc32, rep, ra, pc32f);
                 int32_t cap = opt.max_iters - it;
                 if (first_its >= 0)
                     cap = std::min(cap, std::max(MIXED_MIN_ROUND_ITERS, MIXED_ROUND_ITER_FACTOR * first_its));
                 else
                     cap = std::min(cap, std::max(MIXED_MIN_ROUND_ITERS, opt.max_iters / MIXED_FIRST_ROUND_DIV));
-                its = pcg_solve<float>(C, n, k, ld, A, aval32, F, V32, P32, pc32,
-                                       PcgBufs<float>{e32, r32, z32, p32, q32}, Si, R, cap, opt, tm, ra);
+                its = pcg_solve<float>(C, n, k, ld, A, aval32, F, pc32f, P32, pc32,
+                                       PcgBufs<float>{e32, r32, z32, p32, q32}, Si, R, cap, opt, tm, rep, ra);
                 if (first_its < 0) first_its = its;
                 hit_cap = its >= cap;
                 k_add_into<float><<<grid_for(total, 256, 148 * 16), 256, 0, C.stream>>>(total, e32, x);
@@ -1834,9 +1939,13 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 k_cols_init_inner<<<cg, 256, 0, C.stream>>>(ld, k, 0.0, S.thr, Si, R.G);
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 2;
-                if (!P64.exec) build_precond_graph<double>(C, F, fp64_vals(F), n, r, z, ld, k, P64, pc64, rep, ra);
-                its = pcg_solve<double>(C, n, k, ld, A, A.val, F, fp64_vals(F), P64, pc64,
-                                        PcgBufs<double>{e64, r, z, p, q}, Si, R, opt.max_iters - it, opt, tm, ra);
+                const PcApply pc64f = [&C, &F, n, r, z, ld, k, ra](const TrsvShapes* sh, LevelEvents* lev) {
+                    return launch_precond<double>(C, F, fp64_vals(F), n, r, z, ld, k, ra, sh, lev);
+                };
+                if (!P64.exec) build_precond_graph(C, F, n, ld, k, sizeof(double), P64, pc64, rep, ra, pc64f);
+                its = pcg_solve<double>(C, n, k, ld, A, A.val, F, pc64f, P64, pc64,
+                                        PcgBufs<double>{e64, r, z, p, q}, Si, R, opt.max_iters - it, opt, tm, rep,
+                                        ra);
                 k_add_into<double><<<grid_for(total, 256, 148 * 16), 256, 0, C.stream>>>(total, e64, x);
                 rep.fp64_rounds++;
             }
