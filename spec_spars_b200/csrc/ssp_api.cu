@@ -223,8 +223,7 @@ constexpr int64_t HOST_OUT_PREFAULT_MIN = 1 << 20;  // entries; smaller outputs 
 // the free memory, less 40 B per Laplacian entry and 48 B per edge); the batch size after it, from the memory
 // then free (80 %, less the per-edge arrays).  SSP_COLUMN_BATCH=<columns> sets the batch.
 static double column_bytes(int64_t n, int32_t precision) {
-    return (double)n * (8.0 * 6 + (precision == SSP_PRECISION_MIXED ? 4.0 * 5 + 8.0
-                                   : precision == SSP_PRECISION_PC32 ? 4.0 * 2 : 0.0));
+    return (double)n * (8.0 * 6 + (precision == SSP_PRECISION_MIXED ? 4.0 * 5 + 8.0 : 0.0));
 }
 static int32_t forced_batch(int32_t k) {
     if (const char* e = getenv("SSP_COLUMN_BATCH")) {

@@ -1841,7 +1841,7 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
         if (read_i64(C, S.nactive) > 0) {
             PcApply pc;
             size_t elem = sizeof(double);
-            if (opt.precision == SSP_PRECISION_PC32) {
+            if (opt.precision == SSP_PRECISION_PC32 && !(TILE > NARROW_W && k <= NARROW_W)) {
                 // FP64 PCG with the triangular solves in FP32: r rounded on the way in, z widened on the way out
                 float* fv = W.get_t<float>("pcgp_fval", 2 * F.nnz + n + 1);
                 const int64_t fcount[3] = {F.nnz, F.nnz, n};
@@ -1855,9 +1855,10 @@ void pcg_device(Context& C, int64_t n, const int64_t* lap_ptr, const int32_t* la
                 SSP_CHECK_LAUNCH();
                 C.kernels_launched += 3;
                 const FactorVals<float> V32{fv, fv + F.nnz, fv + 2 * F.nnz};
-                float* r32 = W.get_t<float>("pcgp_r", total);
-                float* z32 = W.get_t<float>("pcgp_z", total);
-                if (TILE > NARROW_W && k <= NARROW_W) SSP_CUDA(cudaMemsetAsync(z32, 0, sizeof(float) * total, C.stream));
+                // r32 and z32 live in q's memory: q (= A p) is dead from the r update to the next Laplacian
+                // product, and the preconditioner runs in between, so this mode needs no more memory than FP64
+                float* r32 = reinterpret_cast<float*>(q);
+                float* z32 = r32 + total;
                 const int cgrid = grid_for(total, 256, 148 * 16);
                 pc = [&C, &F, V32, n, r32, z32, r, z, ld, k, ra, total, cgrid](const TrsvShapes* sh, LevelEvents* lev) {
                     k_d2f<<<cgrid, 256, 0, C.stream>>>(total, r, r32);

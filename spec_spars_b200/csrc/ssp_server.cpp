@@ -121,9 +121,7 @@ int64_t batch_footprint(const std::vector<Job*>& js) {
         n += j->n;
         nnz += (int64_t)j->values.size();
     }
-    const double blocks = js[0]->params.precision == SSP_PRECISION_MIXED  ? 6.0 + 2.5 + 1.0
-                          : js[0]->params.precision == SSP_PRECISION_PC32 ? 6.0 + 1.0
-                                                                           : 6.0;
+    const double blocks = js[0]->params.precision == SSP_PRECISION_MIXED ? 6.0 + 2.5 + 1.0 : 6.0;
     return (int64_t)(blocks * 8.0 * (double)n * (double)ld) + 200 * nnz + 96 * n + (16ll << 20);
 }
 
@@ -326,9 +324,7 @@ int64_t ssp_request_footprint(const ssp_csc* graph, const ssp_params* params) {
     // graph, Laplacian, factor pools and sampling arrays per stored entry; the SpMM's column-slab copy of
     // the Laplacian when slabs are on and the graph has more rows than one slab holds (256-byte rows, at
     // most 16 slabs); a fixed allowance
-    const double blocks = params->precision == SSP_PRECISION_MIXED  ? 6.0 + 2.5 + 1.0
-                          : params->precision == SSP_PRECISION_PC32 ? 6.0 + 1.0
-                                                                    : 6.0;
+    const double blocks = params->precision == SSP_PRECISION_MIXED ? 6.0 + 2.5 + 1.0 : 6.0;
     const int64_t slab_rows = std::max<int64_t>(1, (int64_t)(ssp::spmm_slab_mb() * 1048576.0 / 256));
     const int64_t slabs = ssp::spmm_slab_mb() > 0 && n > slab_rows
                               ? std::min<int64_t>(16, (n + slab_rows - 1) / slab_rows) : 0;
