@@ -578,23 +578,6 @@ def mesh_step(S, ctx, stream, name="grid3d_128"):
                         "frac": pb / (pc_ms / 1000.0) / 1e9 / peak if pc_ms > 0 else None,
                         "spmm_avg_ms": sp_ms},
            "spectral": spec}
-    # the same step with the preconditioner in FP32 (FP64 PCG, product and dots), one timed step; its first
-    # three preconditioner applications also measure this factor's level shapes for FP32
-    prm.precision = S.SSP_PRECISION_PC32
-    e0.record(stream)
-    H32, s32 = ctx.sparsify_device(G.n, G.nnz, cp.data_ptr(), ri.data_ptr(), va.data_ptr(), prm)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms32 = e0.elapsed_time(e1)
-    spec32 = spectral_check(S, ctx, LG, S.DeviceCSC(G.n, *H32), eps, s32)
-    out["pc32"] = {"dtype": PREC_DTYPE["pc32"], "ms_per_step": ms32,
-                   "value": s32["m_in"] / (ms32 / 1000.0), "unit": "edges/s", "steps": 1,
-                   "pcg_iters_max": s32["pcg_max_iters_used"], "pcg_max_relres": s32["pcg_max_relres"],
-                   "kept_fraction": s32["m_out"] / s32["m_in"],
-                   "precond_avg_ms": s32["ms_precond"] / max(1, s32["n_precond"]),
-                   "note": "precond_avg_ms averages the first three applications, which measure the level "
-                           "shapes (one width each)",
-                   "spectral": spec32}
     del cp, ri, va
     return out
 
