@@ -193,9 +193,12 @@ typedef struct {
 const char* ssp_last_error(void);
 
 /* ---- context: one device, one stream, grow-only workspace ---- */
+/* The workspace is allocated and freed stream-ordered (cudaMallocAsync / cudaFreeAsync) on the context's
+ * stream, so growing or releasing it never waits for the whole device. */
 int ssp_context_create(int32_t device, ssp_context** ctx);
 int ssp_context_destroy(ssp_context* ctx);
-/* stream: a cudaStream_t (NULL = the context's own stream) */
+/* stream: a cudaStream_t (NULL = the context's own stream).  The context's frees are ordered on that stream,
+ * including those of ssp_context_destroy: destroy the context before the stream it was given. */
 int ssp_context_set_stream(ssp_context* ctx, void* stream);
 int64_t ssp_context_kernels_launched(const ssp_context* ctx);
 int64_t ssp_context_workspace_bytes(const ssp_context* ctx);
