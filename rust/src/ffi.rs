@@ -314,4 +314,6 @@ extern "C" {
     pub fn ssp_read_mtx_device(ctx: *mut SspContext, path: *const c_char, out_mem: i32, out: *mut SspCscOut) -> c_int;
     pub fn ssp_write_mtx_device(ctx: *mut SspContext, path: *const c_char, m: *const SspCsc) -> c_int;
     pub fn ssp_edgelist_to_mtx(input_path: *const c_char, output_path: *const c_char, default_weight: f64) -> c_int;
+    pub fn ssp_edgelist_to_mtx_device(ctx: *mut SspContext, input_path: *const c_char, output_path: *const c_char,
+                                      default_weight: f64, on_device: *mut i32) -> c_int;
 }

@@ -286,6 +286,27 @@ pub fn write_mtx(path: &str, m: &Csc) -> Result<(), Error> {
     check(unsafe { ffi::ssp_write_mtx(p.as_ptr(), &r) })
 }
 
+/// edge_list_to_matrix_market (utils.rs:413-526), same arguments: the edge list as a symmetric .mtx, first
+/// weight of a repeated pair kept, weights written as Display writes an f64.
+pub fn edge_list_to_matrix_market(input_path: &str, output_path: &str, default_weight: f64) -> Result<(), Error> {
+    let (i, o) = (cstring(input_path)?, cstring(output_path)?);
+    check(unsafe { ffi::ssp_edgelist_to_mtx(i.as_ptr(), o.as_ptr(), default_weight) })
+}
+
+impl Context {
+    /// edge_list_to_matrix_market on this context's GPU: the same file byte for byte.  Returns whether the GPU
+    /// wrote it (a file its line parser does not mirror is converted on the host instead).
+    pub fn edge_list_to_matrix_market(&mut self, input_path: &str, output_path: &str, default_weight: f64)
+                                      -> Result<bool, Error> {
+        let (i, o) = (cstring(input_path)?, cstring(output_path)?);
+        let mut on_device = 0i32;
+        check(unsafe {
+            ffi::ssp_edgelist_to_mtx_device(self.raw, i.as_ptr(), o.as_ptr(), default_weight, &mut on_device)
+        })?;
+        Ok(on_device != 0)
+    }
+}
+
 /// sparsify_dataset (lib.rs:158-168), same arguments: read the .mtx graph, sparsify it with the knobs the
 /// reference fixes for this call, and write L_H to output_filename (nothing written when it is empty).
 #[allow(clippy::too_many_arguments)]
